@@ -1,0 +1,318 @@
+#!/usr/bin/env python
+"""bench.py -- grid signed-distance queries/s on B200, against the reference's CPU cell list.
+
+Workload (one "step"): the signed distance of a 256^3 node grid (16,777,216 queries) over the
+bounding box padded by 0.25 of a closed tube swept along a (2,3) torus knot (131,072 triangles,
+coordinates jittered by N(0, 1e-4)), with the closest triangle's pseudo-normal sign, in double,
+computed with the FP32 traversal + FP64 fix-up kernel. Synthetic, seeded inputs (no dataset).
+
+* ``value``: queries/s with the mesh and its BVH resident in HBM (device time of each step, CUDA
+  events on the launching stream, L2 flushed between steps);
+* ``fp64_plain``: the same with the plain FP64 kernel (the reference point of the 3x target);
+* ``e2e``: queries/s through the drop-in C ABI (``ssdf_b200_sample_sdf_bvh_dd``) from host
+  arrays, i.e. mesh upload, BVH + pseudo-normal build, query and the download of the distances
+  into pinned host memory, per call, as the reference's sample_sdf_bvh does per call;
+* ``roofline``: the query kernel against the measured FP32 FMA peak of this GPU (the path is
+  FP32-pipe bound; its HBM traffic is the output stream), flops counted by an instrumented launch;
+* ``cpu_baseline``: the reference's own OpenMP ``edf_celllist<double>`` (compiled from its sources
+  into oracle/_ref) on a seeded sample of the same grid nodes, all host threads.
+
+``--impl reference`` times that reference CPU code alone. With torchrun (N > 1) every rank runs
+an independent replica (the path does not shard across GPUs here: "replicas only"), the step time
+is the max over ranks and ``value`` the total over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "grid SDF queries/s (FP32+FP64 fixup vs plain FP64 GPU); served p50/p99 latency"
+WORKLOAD = "torus-knot tube (2,3), 131072 triangles, 256^3 node grid over bbox+0.25, signed, double"
+REF_SAMPLE = 262144       # reference arm: grid nodes per step
+CPU_SAMPLE = 1048576      # cpu_baseline leg of our arm
+
+
+def parse_args():
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--grid", type=int, default=256)
+    p.add_argument("--cpu-sample", type=int, default=CPU_SAMPLE)
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def workload(n=256):
+    from ssdf_b200 import workloads as W
+
+    mesh = W.torus_knot_tube()
+    grid = W.Grid.padded_nodes(mesh, n, 0.25)
+    return mesh, grid
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(device_index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"error": "nvidia-smi unavailable"}
+        time.sleep(0.3)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [s.strip() for s in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"error": "no samples"}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def cpu_reference_rate(mesh, grid, nsample, seed=17, steps=1):
+    """The reference's edf_celllist<double> (oracle/_ref) on a seeded sample of the grid nodes."""
+    import oracle
+
+    if not oracle.ref_available():
+        raise RuntimeError("reference CPU library (oracle/_ref) is not built")
+    rng = np.random.default_rng(seed)
+    ids = np.sort(rng.choice(grid.size, size=min(nsample, grid.size), replace=False))
+    q = oracle.grid_points(grid)[:, ids].copy()
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        oracle.ref_edf(q, mesh, which="celllist")
+        times.append(time.perf_counter() - t0)
+    return len(ids), times
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    mesh, grid = workload(args.grid)
+    cores = os.cpu_count()
+    n, times = cpu_reference_rate(mesh, grid, REF_SAMPLE, steps=args.warmup + args.steps)
+    timed = times[args.warmup:]
+    t = sum(timed)
+    value = n * len(timed) / t
+    sample = (f"{n} seeded nodes of the 256^3 grid per step, ssdf::edf_celllist<double,double,int> "
+              f"(unsigned; the reference has no CPU signed grid sampler without cuBQL)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / len(timed),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "queries_per_step": n, "parallelism": "host threads"},
+            "cpu_baseline": {"value": value, "unit": "queries/s", "cores": cores, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
+    import ssdf_b200 as S
+
+    mesh, grid = workload(args.grid)
+    nq = grid.size
+    dm = S.DeviceMesh(mesh)
+    stream = torch.cuda.current_stream()
+    out = torch.empty(nq, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def step(prec):
+        dm.query_grid(grid, out, None, precision=prec, output=S.OUT_SDF, stream=stream)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def timed(prec, k, w):
+        for _ in range(w):
+            step(prec)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
+        for e0, e1 in ev:
+            flush.zero_()  # L2 flush between steps, outside the timed events
+            e0.record(stream)
+            step(prec)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = [e0.elapsed_time(e1) for e0, e1 in ev]
+        total = torch.tensor([sum(ms)], dtype=torch.float64, device="cuda")
+        if dist is not None:
+            dist.all_reduce(total, op=dist.ReduceOp.MAX)
+        return float(total.item()), ms
+
+    clocks = Clocks(local)
+    t_x, ms_x = timed(S.PREC_F32_FIXUP, args.steps, args.warmup)
+    clk = clocks.stop()
+    value = world * nq * args.steps / (t_x * 1e-3)
+    t_64, ms_64 = timed(S.PREC_F64, max(2, args.steps // 2), 1)
+    fp64_value = world * nq * max(2, args.steps // 2) / (t_64 * 1e-3)
+
+    # instrumented (untimed) launch: triangle / box / fix-up counts for the flop count
+    os.environ["SSDF_B200_COUNT"] = "1"
+    step(S.PREC_F32_FIXUP)
+    torch.cuda.synchronize()
+    counts = S.last_query_counts()
+    del os.environ["SSDF_B200_COUNT"]
+    flops = 79.0 * counts["triangle_tests"] + 8.0 * counts["box_tests"] + 79.0 * counts["fixup_evaluations"] \
+        + 25.0 * nq
+    step_s = statistics.median(ms_x) * 1e-3
+    achieved = flops / step_s / 1e12
+    peak = S.fma_peak_tflops(False)
+    stats = dm.stats()
+    alg_bytes = nq * 8 + stats["bytes"]
+    line = {
+        "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_x / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "queries_per_step": nq, "triangles": mesh.nt, "parallelism":
+                   f"replicas x{world}" if world > 1 else "1 GPU", "l2": "flushed between steps (256 MiB write)",
+                   "precision": "FP32 traversal + FP64 fix-up (bitwise the FP64 result)"},
+        "fp64_plain": {"value": fp64_value, "unit": "queries/s", "ms_per_step": t_64 / max(2, args.steps // 2),
+                       "speedup_fixup_vs_fp64": value / fp64_value},
+        "gpu_launches": 2 * args.steps,
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "peak_source": "measured FP32 FMA microbenchmark on this GPU (ssdf_b200_fma_peak)",
+                     "traffic": None, "flops_per_launch": flops, "counts": counts,
+                     "hbm": {"algorithmic_bytes": alg_bytes, "achieved_gbs": alg_bytes / step_s / 1e9,
+                             "peak_gbs": _hbm_peak()}},
+        "clocks": clk,
+        "mesh": stats,
+    }
+    _attach_traffic(line)
+
+    if not args.no_e2e:
+        try:
+            line["e2e"] = e2e(S, mesh, grid, args)
+        except Exception as ex:  # pragma: no cover - reported, not fatal
+            line["e2e"] = {"error": repr(ex)}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            n, times = cpu_reference_rate(mesh, grid, args.cpu_sample)
+            line["cpu_baseline"] = {"value": n / times[0], "unit": "queries/s", "cores": os.cpu_count(),
+                                    "kind": "reference",
+                                    "sample": f"{n} seeded grid nodes, ssdf::edf_celllist<double> (unsigned), "
+                                              f"oracle/_ref built from the reference's sources"}
+        except Exception as ex:
+            line["cpu_baseline"] = {"error": repr(ex)}
+    dm.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def e2e(S, mesh, grid, args):
+    """Through the drop-in C ABI from host arrays: upload, build, query, download (pinned)."""
+    import torch
+
+    nq = grid.size
+    host_out = torch.empty(nq, dtype=torch.float64, pin_memory=True).numpy()
+    hm = S.capi._HostMesh(mesh, np.float64)
+    nx, ny, nz = grid.n
+    import ctypes as C
+
+    def call():
+        st = S.lib.ssdf_b200_sample_sdf_bvh_dd(*hm.args(), nx, ny, nz, *[C.c_double(v) for v in grid.lo],
+                                               *[C.c_double(v) for v in grid.hi], C.c_void_p(host_out.ctypes.data))
+        if st != 0:
+            raise RuntimeError(S.last_error())
+
+    for _ in range(max(1, args.warmup)):
+        call()
+    torch.cuda.synchronize()
+    k = max(2, args.steps)
+    t0 = time.perf_counter()
+    for _ in range(k):
+        call()
+    dt = (time.perf_counter() - t0) / k
+    h2d = sum(a.nbytes for a in (hm.sx, hm.sy, hm.sz, hm.s0, hm.s1, hm.s2))
+    return {"value": nq / dt, "unit": "queries/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": nq * 8,
+            "ms_per_call": dt * 1e3, "api": "ssdf_b200_sample_sdf_bvh_dd (host arrays, blocking; wall clock)"}
+
+
+def _hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)["hbm_gbs"]
+    except Exception:
+        return 6650.0
+
+
+def _attach_traffic(line):
+    """DRAM bytes per launch of the query kernel from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            t = json.load(f)
+        line["roofline"]["traffic"] = t["dram_bytes_per_launch"]
+        line["roofline"]["traffic_source"] = t.get("source")
+    except Exception:
+        pass
+
+
+if __name__ == "__main__":
+    main()

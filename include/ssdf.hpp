@@ -1,0 +1,148 @@
+// ssdf.hpp -- the reference's C++ template API (namespace ssdf), served by the B200 library.
+//
+// A drop-in for zulianp/ssdf's serial/ssdf.hpp (edf, edf_celllist, edf_select) and
+// serial/bvh/bvh.hpp (edf_bvh, closest_point_bvh, sample_sqedf_bvh, sample_sdf_bvh): same names,
+// template parameters <G coordinates, T outputs, I indices>, argument order, in/out semantics and
+// int return (0 on success). Each instantiation the reference provides maps onto one C symbol of
+// libssdf_b200.so (include/ssdf_b200.h); other type combinations do not compile.
+// Link with -lssdf_b200. Unlike the reference, a failure returns a non-zero status
+// (SSDF_ERR_*) instead of aborting; ssdf_last_error() describes it.
+#ifndef SSDF_B200_SSDF_HPP
+#define SSDF_B200_SSDF_HPP
+
+#include <stddef.h>
+
+#include <type_traits>
+
+#include "ssdf_b200.h"
+
+#ifndef SSDF_RESTRICT
+#define SSDF_RESTRICT __restrict__
+#endif
+
+namespace ssdf {
+
+namespace detail {
+template <typename...>
+struct always_false : std::false_type {};
+}  // namespace detail
+
+#define SSDF_B200_EDF_SIG(G, T)                                                                                   \
+    const ptrdiff_t npoints, const G *const SSDF_RESTRICT x, const G *const SSDF_RESTRICT y,                      \
+        const G *const SSDF_RESTRICT z, const ptrdiff_t nselements, const I *const SSDF_RESTRICT s0,               \
+        const I *const SSDF_RESTRICT s1, const I *const SSDF_RESTRICT s2, const ptrdiff_t nspoints,               \
+        const G *const SSDF_RESTRICT sx, const G *const SSDF_RESTRICT sy, const G *const SSDF_RESTRICT sz,         \
+        T *const SSDF_RESTRICT out
+#define SSDF_B200_EDF_PASS npoints, x, y, z, nselements, s0, s1, s2, nspoints, sx, sy, sz, out
+
+// serial/ssdf.hpp:447-619
+template <typename G, typename T, typename I>
+int edf(SSDF_B200_EDF_SIG(G, T)) {
+    static_assert(std::is_same<I, int>::value, "ssdf_b200 indices are int");
+    if constexpr (std::is_same<G, float>::value && std::is_same<T, float>::value)
+        return ssdf_b200_edf_ff(SSDF_B200_EDF_PASS);
+    else if constexpr (std::is_same<G, double>::value && std::is_same<T, double>::value)
+        return ssdf_b200_edf_dd(SSDF_B200_EDF_PASS);
+    else
+        static_assert(detail::always_false<G, T>::value, "edf is instantiated for <float,float> and <double,double>");
+}
+
+// serial/ssdf.hpp:642-963
+template <typename G, typename T, typename I>
+int edf_celllist(SSDF_B200_EDF_SIG(G, T)) {
+    static_assert(std::is_same<I, int>::value, "ssdf_b200 indices are int");
+    if constexpr (std::is_same<G, float>::value && std::is_same<T, float>::value)
+        return ssdf_b200_edf_celllist_ff(SSDF_B200_EDF_PASS);
+    else if constexpr (std::is_same<G, double>::value && std::is_same<T, double>::value)
+        return ssdf_b200_edf_celllist_dd(SSDF_B200_EDF_PASS);
+    else
+        static_assert(detail::always_false<G, T>::value,
+                      "edf_celllist is instantiated for <float,float> and <double,double>");
+}
+
+// serial/ssdf.hpp:965-1016 (SSDF_USE_BVH / SSDF_CELL_VALIDATE / SSDF_USE_CELL_LIST)
+template <typename G, typename T, typename I>
+int edf_select(SSDF_B200_EDF_SIG(G, T)) {
+    static_assert(std::is_same<I, int>::value, "ssdf_b200 indices are int");
+    if constexpr (std::is_same<G, float>::value && std::is_same<T, float>::value)
+        return ssdf_edf_f(SSDF_B200_EDF_PASS);
+    else if constexpr (std::is_same<G, double>::value && std::is_same<T, double>::value)
+        return ssdf_edf_d(SSDF_B200_EDF_PASS);
+    else
+        static_assert(detail::always_false<G, T>::value,
+                      "edf_select is instantiated for <float,float> and <double,double>");
+}
+
+// serial/bvh/bvh.hpp:19-32 (instantiations serial/bvh/bvh.cpp:1216-1256)
+template <typename G, typename T, typename I>
+int edf_bvh(SSDF_B200_EDF_SIG(G, T)) {
+    static_assert(std::is_same<I, int>::value, "ssdf_b200 indices are int");
+    if constexpr (std::is_same<G, float>::value && std::is_same<T, float>::value)
+        return ssdf_b200_edf_bvh_ff(SSDF_B200_EDF_PASS);
+    else if constexpr (std::is_same<G, float>::value && std::is_same<T, double>::value)
+        return ssdf_b200_edf_bvh_fd(SSDF_B200_EDF_PASS);
+    else if constexpr (std::is_same<G, double>::value && std::is_same<T, double>::value)
+        return ssdf_b200_edf_bvh_dd(SSDF_B200_EDF_PASS);
+    else
+        static_assert(detail::always_false<G, T>::value, "edf_bvh: <float,float>, <float,double>, <double,double>");
+}
+
+// serial/bvh/bvh.hpp:34-51
+template <typename G, typename T, typename I>
+int closest_point_bvh(const ptrdiff_t npoints, const G *const SSDF_RESTRICT x, const G *const SSDF_RESTRICT y,
+                      const G *const SSDF_RESTRICT z, const ptrdiff_t nselements, const I *const SSDF_RESTRICT s0,
+                      const I *const SSDF_RESTRICT s1, const I *const SSDF_RESTRICT s2, const ptrdiff_t nspoints,
+                      const G *const SSDF_RESTRICT sx, const G *const SSDF_RESTRICT sy,
+                      const G *const SSDF_RESTRICT sz, T *const SSDF_RESTRICT outd, G *const SSDF_RESTRICT outx,
+                      G *const SSDF_RESTRICT outy, G *const SSDF_RESTRICT outz, I *const SSDF_RESTRICT outtri) {
+    static_assert(std::is_same<I, int>::value, "ssdf_b200 indices are int");
+    if constexpr (std::is_same<G, float>::value && std::is_same<T, float>::value)
+        return ssdf_b200_closest_point_bvh_ff(npoints, x, y, z, nselements, s0, s1, s2, nspoints, sx, sy, sz, outd,
+                                              outx, outy, outz, outtri);
+    else if constexpr (std::is_same<G, double>::value && std::is_same<T, double>::value)
+        return ssdf_b200_closest_point_bvh_dd(npoints, x, y, z, nselements, s0, s1, s2, nspoints, sx, sy, sz, outd,
+                                              outx, outy, outz, outtri);
+    else
+        static_assert(detail::always_false<G, T>::value, "closest_point_bvh: <float,float>, <double,double>");
+}
+
+#define SSDF_B200_GRID_SIG(G, T)                                                                                  \
+    const ptrdiff_t nselements, const I *const SSDF_RESTRICT s0, const I *const SSDF_RESTRICT s1,                 \
+        const I *const SSDF_RESTRICT s2, const ptrdiff_t nspoints, const G *const SSDF_RESTRICT sx,                \
+        const G *const SSDF_RESTRICT sy, const G *const SSDF_RESTRICT sz, const ptrdiff_t nx, const ptrdiff_t ny,  \
+        const ptrdiff_t nz, const G xmin, const G ymin, const G zmin, const G xmax, const G ymax, const G zmax,    \
+        T *const SSDF_RESTRICT out
+#define SSDF_B200_GRID_PASS nselements, s0, s1, s2, nspoints, sx, sy, sz, nx, ny, nz, xmin, ymin, zmin, xmax, ymax, zmax, out
+
+// serial/bvh/bvh.hpp:183-201
+template <typename G, typename T, typename I>
+int sample_sqedf_bvh(SSDF_B200_GRID_SIG(G, T)) {
+    static_assert(std::is_same<I, int>::value, "ssdf_b200 indices are int");
+    if constexpr (std::is_same<G, float>::value && std::is_same<T, float>::value)
+        return ssdf_b200_sample_sqedf_bvh_ff(SSDF_B200_GRID_PASS);
+    else if constexpr (std::is_same<G, double>::value && std::is_same<T, double>::value)
+        return ssdf_b200_sample_sqedf_bvh_dd(SSDF_B200_GRID_PASS);
+    else
+        static_assert(detail::always_false<G, T>::value, "sample_sqedf_bvh: <float,float>, <double,double>");
+}
+
+// serial/bvh/bvh.hpp:203-227: positive on the side the right-handed normals point to
+template <typename G, typename T, typename I>
+int sample_sdf_bvh(SSDF_B200_GRID_SIG(G, T)) {
+    static_assert(std::is_same<I, int>::value, "ssdf_b200 indices are int");
+    if constexpr (std::is_same<G, float>::value && std::is_same<T, float>::value)
+        return ssdf_b200_sample_sdf_bvh_ff(SSDF_B200_GRID_PASS);
+    else if constexpr (std::is_same<G, double>::value && std::is_same<T, double>::value)
+        return ssdf_b200_sample_sdf_bvh_dd(SSDF_B200_GRID_PASS);
+    else
+        static_assert(detail::always_false<G, T>::value, "sample_sdf_bvh: <float,float>, <double,double>");
+}
+
+#undef SSDF_B200_EDF_SIG
+#undef SSDF_B200_EDF_PASS
+#undef SSDF_B200_GRID_SIG
+#undef SSDF_B200_GRID_PASS
+
+}  // namespace ssdf
+
+#endif  // SSDF_B200_SSDF_HPP

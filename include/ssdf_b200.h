@@ -1,0 +1,216 @@
+/*
+ * ssdf_b200.h -- C ABI of the B200 (sm_100a) closest-point distance-field library.
+ *
+ * Everything here is plain C: pointers, sizes and integer status codes. Paths in the comments are
+ * zulianp/ssdf source files, the interface each entry point stands in for.
+ *
+ * Conventions shared by every entry point:
+ *   - SoA layout exactly as ssdf's: query points x, y, z [npoints]; triangles s0, s1, s2
+ *     [nselements] (0-based int32 vertex ids); vertices sx, sy, sz [nspoints].
+ *   - The drop-in entry points take HOST pointers and are blocking, like the reference
+ *     (serial/ssdf.hpp:447-460, serial/bvh/bvh.hpp:19-227). The handle API (ssdf_mesh_*,
+ *     ssdf_query_*) takes DEVICE pointers and a cudaStream_t (as void*), and is asynchronous.
+ *   - `out` of the edf family is in/out: on entry the current best distance (squared for the
+ *     sqedf family), on exit min(incoming, surface distance) (serial/ssdf.hpp:439-440).
+ *   - Closest triangle: the lowest triangle index among those at the minimum squared distance.
+ *   - Sign: positive on the side the right-handed (s0, s1, s2) normals point to, negative inside a
+ *     closed outward-oriented surface, + where the pseudo-normal dot product is 0
+ *     (serial/bvh/bvh.hpp:203-208, serial/bvh/bvh.cpp:1790-1792).
+ *   - An empty mesh leaves the outputs untouched and returns SSDF_OK (serial/ssdf.hpp:462).
+ *   - Every entry point returns a status code and never aborts the process; the CUDA path is the
+ *     only path (no CPU fallback): without a usable GPU they return SSDF_ERR_CUDA.
+ */
+#ifndef SSDF_B200_H
+#define SSDF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------------------------- */
+#define SSDF_OK 0
+#define SSDF_ERR_INVALID_ARGUMENT 1 /* null pointer, negative size, out-of-range index        */
+#define SSDF_ERR_OUT_OF_MEMORY 2    /* a device or pinned host allocation failed              */
+#define SSDF_ERR_CUDA 3             /* a CUDA runtime call or kernel launch failed            */
+#define SSDF_ERR_NOT_SUPPORTED 4    /* a size or option beyond what this build handles        */
+#define SSDF_ERR_INTERNAL 5         /* a device-side check fired (bounded wait, stack depth)  */
+
+/* Human-readable name of a status code. */
+const char *ssdf_status_string(int status);
+/* The calling thread's last error message ("" when none). */
+const char *ssdf_last_error(void);
+/* Library version string. */
+const char *ssdf_b200_version(void);
+
+/* ---- drop-in: the reference's exported C ABI ------------------------------------------------ */
+
+/* ssdf_edf_f / ssdf_edf_d (serial/ssdf.cpp:36-66): unsigned distance, in/out `out`, dispatched as
+ * ssdf::edf_select (serial/ssdf.hpp:965-1016) by the same environment variables:
+ * SSDF_USE_BVH (default 1: the device BVH), SSDF_CELL_VALIDATE (run edf and edf_celllist and
+ * report their relative difference on stderr), SSDF_USE_CELL_LIST (default 1) else edf. */
+int ssdf_edf_f(ptrdiff_t npoints, const float *x, const float *y, const float *z, ptrdiff_t nselements,
+               const int *s0, const int *s1, const int *s2, ptrdiff_t nspoints, const float *sx, const float *sy,
+               const float *sz, float *out);
+int ssdf_edf_d(ptrdiff_t npoints, const double *x, const double *y, const double *z, ptrdiff_t nselements,
+               const int *s0, const int *s1, const int *s2, ptrdiff_t nspoints, const double *sx, const double *sy,
+               const double *sz, double *out);
+
+/* ---- drop-in: one symbol per template instantiation of the C++ API ---------------------------
+ * include/ssdf.hpp maps ssdf::<name><G, T, int> onto these. Suffix: G then T, f = float,
+ * d = double (edf and edf_celllist are instantiated for G == T only, serial/ssdf.cpp:4-30). */
+
+/* ssdf::edf (serial/ssdf.hpp:447-619): brute force on the GPU, triangle tiles staged in shared
+ * memory. Result bitwise equal to the reference's in T's precision. */
+int ssdf_b200_edf_ff(ptrdiff_t npoints, const float *x, const float *y, const float *z, ptrdiff_t nselements,
+                     const int *s0, const int *s1, const int *s2, ptrdiff_t nspoints, const float *sx,
+                     const float *sy, const float *sz, float *out);
+int ssdf_b200_edf_dd(ptrdiff_t npoints, const double *x, const double *y, const double *z, ptrdiff_t nselements,
+                     const int *s0, const int *s1, const int *s2, ptrdiff_t nspoints, const double *sx,
+                     const double *sy, const double *sz, double *out);
+
+/* ssdf::edf_celllist (serial/ssdf.hpp:642-963): 2-D cell list over the two widest axes on the
+ * GPU. Result bitwise equal to the reference's in T's precision. */
+int ssdf_b200_edf_celllist_ff(ptrdiff_t npoints, const float *x, const float *y, const float *z,
+                              ptrdiff_t nselements, const int *s0, const int *s1, const int *s2, ptrdiff_t nspoints,
+                              const float *sx, const float *sy, const float *sz, float *out);
+int ssdf_b200_edf_celllist_dd(ptrdiff_t npoints, const double *x, const double *y, const double *z,
+                              ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                              ptrdiff_t nspoints, const double *sx, const double *sy, const double *sz,
+                              double *out);
+
+/* ssdf::edf_bvh (serial/bvh/bvh.hpp:19-32, bvh.cpp:298-316; instantiations bvh.cpp:1216-1256):
+ * device BVH. <float,float> computes in the reference's float arithmetic; <float,double> and
+ * <double,double> return the double result (FP32 traversal with FP64 fix-up by default,
+ * SSDF_B200_PRECISION=f64 for the plain double kernel). */
+int ssdf_b200_edf_bvh_ff(ptrdiff_t npoints, const float *x, const float *y, const float *z, ptrdiff_t nselements,
+                         const int *s0, const int *s1, const int *s2, ptrdiff_t nspoints, const float *sx,
+                         const float *sy, const float *sz, float *out);
+int ssdf_b200_edf_bvh_fd(ptrdiff_t npoints, const float *x, const float *y, const float *z, ptrdiff_t nselements,
+                         const int *s0, const int *s1, const int *s2, ptrdiff_t nspoints, const float *sx,
+                         const float *sy, const float *sz, double *out);
+int ssdf_b200_edf_bvh_dd(ptrdiff_t npoints, const double *x, const double *y, const double *z,
+                         ptrdiff_t nselements, const int *s0, const int *s1, const int *s2, ptrdiff_t nspoints,
+                         const double *sx, const double *sy, const double *sz, double *out);
+
+/* ssdf::closest_point_bvh (serial/bvh/bvh.hpp:34-51, bvh.cpp:125-219): distance, closest point
+ * and triangle, all four written only where the distance is below the incoming outd. */
+int ssdf_b200_closest_point_bvh_ff(ptrdiff_t npoints, const float *x, const float *y, const float *z,
+                                   ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                   ptrdiff_t nspoints, const float *sx, const float *sy, const float *sz, float *outd,
+                                   float *outx, float *outy, float *outz, int *outtri);
+int ssdf_b200_closest_point_bvh_dd(ptrdiff_t npoints, const double *x, const double *y, const double *z,
+                                   ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                   ptrdiff_t nspoints, const double *sx, const double *sy, const double *sz,
+                                   double *outd, double *outx, double *outy, double *outz, int *outtri);
+
+/* ssdf::sample_sqedf_bvh (serial/bvh/bvh.hpp:183-201, bvh.cpp:1574-1639): squared distance on
+ * the node grid nx*ny*nz over [min, max] (x fastest), out = min(out, d^2). */
+int ssdf_b200_sample_sqedf_bvh_ff(ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                  ptrdiff_t nspoints, const float *sx, const float *sy, const float *sz, ptrdiff_t nx,
+                                  ptrdiff_t ny, ptrdiff_t nz, float xmin, float ymin, float zmin, float xmax,
+                                  float ymax, float zmax, float *out);
+int ssdf_b200_sample_sqedf_bvh_dd(ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                  ptrdiff_t nspoints, const double *sx, const double *sy, const double *sz,
+                                  ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, double xmin, double ymin, double zmin,
+                                  double xmax, double ymax, double zmax, double *out);
+
+/* ssdf::sample_sdf_bvh (serial/bvh/bvh.hpp:203-227, bvh.cpp:1641-1798): signed distance on the
+ * node grid; sign from the angle-weighted pseudo-normal at the closest point (barycentric
+ * tolerance 1e-4, bvh.cpp:1738). */
+int ssdf_b200_sample_sdf_bvh_ff(ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                ptrdiff_t nspoints, const float *sx, const float *sy, const float *sz, ptrdiff_t nx,
+                                ptrdiff_t ny, ptrdiff_t nz, float xmin, float ymin, float zmin, float xmax,
+                                float ymax, float zmax, float *out);
+int ssdf_b200_sample_sdf_bvh_dd(ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                ptrdiff_t nspoints, const double *sx, const double *sy, const double *sz,
+                                ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, double xmin, double ymin, double zmin,
+                                double xmax, double ymax, double zmax, double *out);
+
+/* ---- additive entry points (no reference counterpart; patterned on closest_point_bvh) -------- */
+
+/* Unsigned distance (in/out, as edf_bvh) plus the closest triangle, written where it improves. */
+int ssdf_b200_edf_index_dd(ptrdiff_t npoints, const double *x, const double *y, const double *z,
+                           ptrdiff_t nselements, const int *s0, const int *s1, const int *s2, ptrdiff_t nspoints,
+                           const double *sx, const double *sy, const double *sz, double *out, int *outtri);
+int ssdf_b200_edf_index_ff(ptrdiff_t npoints, const float *x, const float *y, const float *z,
+                           ptrdiff_t nselements, const int *s0, const int *s1, const int *s2, ptrdiff_t nspoints,
+                           const float *sx, const float *sy, const float *sz, float *out, int *outtri);
+/* Signed distance and closest triangle at a point list (sample_sdf_bvh's sign rule). */
+int ssdf_b200_sdf_points_dd(ptrdiff_t npoints, const double *x, const double *y, const double *z,
+                            ptrdiff_t nselements, const int *s0, const int *s1, const int *s2, ptrdiff_t nspoints,
+                            const double *sx, const double *sy, const double *sz, double *out, int *outtri);
+/* sample_sdf_bvh plus the closest triangle per grid node. */
+int ssdf_b200_sample_sdf_index_bvh_dd(ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                      ptrdiff_t nspoints, const double *sx, const double *sy, const double *sz,
+                                      ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, double xmin, double ymin,
+                                      double zmin, double xmax, double ymax, double zmax, double *out, int *outtri);
+
+/* ---- device-resident meshes (no reference counterpart: the reference rebuilds per call,
+ *      serial/bvh/bvh.cu:80-158) ------------------------------------------------------------ */
+
+typedef struct ssdf_mesh ssdf_mesh;
+
+#define SSDF_F32 0
+#define SSDF_F64 1
+
+/* Arithmetic of the closest-triangle search. */
+#define SSDF_PREC_F32 0       /* float throughout, the reference's float expressions           */
+#define SSDF_PREC_F64 1       /* double throughout: the plain FP64 kernel                      */
+#define SSDF_PREC_F32_FIXUP 2 /* float traversal, double re-evaluation of the near-tied set:
+                                 bitwise the double result                                    */
+
+/* What a query writes. */
+#define SSDF_OUT_EDF 0     /* out = sqrt(min(out^2, d^2)) (in/out), outtri where it improves   */
+#define SSDF_OUT_SQEDF 1   /* out = min(out, d^2) (in/out)                                     */
+#define SSDF_OUT_SDF 2     /* out = +-d (overwrite), outtri                                    */
+#define SSDF_OUT_CLOSEST 3 /* closest_point_bvh: outd/outxyz/outtri where d < outd (in/out)   */
+
+typedef struct {
+    int leaf_size;    /* triangles per BVH leaf, 1..16 (0: 4)                                 */
+    int keep_fp64;    /* 1: also keep double triangles and nodes (F64 and fix-up queries)      */
+    int normals;      /* 1: build pseudo-normals (signed queries)                             */
+    int treelet_opt;  /* 1: SAH treelet refinement of the LBVH (0: plain LBVH)                 */
+} ssdf_build_opts;
+
+typedef struct {
+    int precision;    /* SSDF_PREC_*                                                          */
+    int output;       /* SSDF_OUT_*                                                           */
+    int coord_type;   /* SSDF_F32 / SSDF_F64: type of x, y, z or of the grid bounds (G)       */
+    int out_type;     /* SSDF_F32 / SSDF_F64: type of out / outd (T)                          */
+    int reserved[4];
+} ssdf_query_opts;
+
+/* Creates a device-resident mesh (triangles, BVH, optional normals) from HOST (device_ptrs=0)
+ * or DEVICE (device_ptrs=1) arrays of coord_type. Blocks until built. */
+int ssdf_mesh_create(ssdf_mesh **mesh, ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                     ptrdiff_t nspoints, const void *sx, const void *sy, const void *sz, int coord_type,
+                     int device_ptrs, const ssdf_build_opts *opts, void *stream);
+int ssdf_mesh_destroy(ssdf_mesh *mesh);
+/* BVH statistics: nodes, leaves, depth, bytes resident on the device. */
+int ssdf_mesh_stats(const ssdf_mesh *mesh, int64_t *nodes, int64_t *leaves, int64_t *depth, int64_t *bytes);
+
+/* Query at device points (x, y, z of coord_type). outx/outy/outz (coord_type) and outtri may be NULL
+ * except for SSDF_OUT_CLOSEST. Asynchronous on `stream`. */
+int ssdf_query_points(ssdf_mesh *mesh, ptrdiff_t npoints, const void *x, const void *y, const void *z, void *out,
+                      int *outtri, void *outx, void *outy, void *outz, const ssdf_query_opts *opts, void *stream);
+/* Query at the node grid nx*ny*nz over [lo, hi] (ssdf's convention, G = coord_type precision). */
+int ssdf_query_grid(ssdf_mesh *mesh, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, const double lo[3],
+                    const double hi[3], void *out, int *outtri, const ssdf_query_opts *opts, void *stream);
+
+/* Diagnostics for measurement: per-query triangle and box test counts of the last query on this
+ * thread when SSDF_B200_COUNT=1 was set at its launch (an untimed, instrumented launch). */
+int ssdf_last_query_counts(int64_t *triangle_tests, int64_t *box_tests, int64_t *fixup_queries,
+                           int64_t *fallback_queries);
+
+/* Measured fused multiply-add throughput of the current GPU in TFLOP/s (f64 = 0: float, 1: double),
+ * the denominator of the traversal kernels' roofline. */
+int ssdf_b200_fma_peak(int f64, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SSDF_B200_H */

@@ -1,0 +1,229 @@
+"""CPU oracle for ssdf's closest-point distance path -- TEST INFRASTRUCTURE ONLY.
+
+This package is the checker: only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU
+baseline leg import it. The product (``ssdf_b200``) never imports, links or falls back to it.
+
+Two CPU libraries sit behind it, both built by ``oracle/Makefile``:
+
+* ``liboracle.so`` -- the C restatement in ``ssdf_oracle.c`` (see its header for the reference
+  lines each function follows), always present once built;
+* ``_ref/libssdf_ref.so`` -- zulianp/ssdf's own CPU code (``serial/ssdf.cpp`` + ``ssdf.hpp``)
+  compiled from its sources, with ``ref_harness.cpp`` exporting ``edf`` and ``edf_celllist``.
+  It exists only where the reference sources were present at build time (it then travels with
+  the repository snapshot as a built file).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libssdf_ref.so")
+REF_SRC = "/root/reference"
+
+_pd = C.c_ssize_t
+_dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int)
+
+
+def build(ref_src: str | None = None) -> None:
+    """Compile liboracle.so, and the reference's CPU library when its sources are present."""
+    src = ref_src or REF_SRC
+    targets = ["oracle"]
+    if os.path.isdir(os.path.join(src, "serial")):
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={src}", *targets], check=True)
+
+
+def _load(path: str) -> C.CDLL:
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is not built (run `make -C oracle`)")
+    return C.CDLL(path)
+
+
+_lib = None
+_ref = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        _lib = _load(ORACLE_SO)
+        for suf, fptr, ft in (("_d", _dp, C.c_double), ("_f", _fp, C.c_float)):
+            f = getattr(_lib, "oracle_point_triangle_dist_sq" + suf)
+            f.restype = ft
+            f.argtypes = [ft] * 12
+            f = getattr(_lib, "oracle_point_triangle_closest_point" + suf)
+            f.restype = None
+            f.argtypes = [ft] * 12 + [fptr] * 3
+            for n in ("oracle_point_aabb_distance_squared", "oracle_point_aabb_signed_distance"):
+                f = getattr(_lib, n + suf)
+                f.restype = ft
+                f.argtypes = [ft] * 9
+            f = getattr(_lib, "oracle_edf" + suf)
+            f.restype = C.c_int
+            f.argtypes = [_pd, fptr, fptr, fptr, _pd, _ip, _ip, _ip, _pd, fptr, fptr, fptr, fptr, _ip]
+            f = getattr(_lib, "oracle_grid_points" + suf)
+            f.restype = None
+            f.argtypes = [_pd, _pd, _pd] + [ft] * 6 + [_dp, _dp, _dp]
+        _lib.oracle_pseudonormals_d.restype = C.c_int
+        _lib.oracle_pseudonormals_d.argtypes = [_pd, _ip, _ip, _ip, _pd, _dp, _dp, _dp, _dp, _dp, _dp]
+        _lib.oracle_sdf_points_d.restype = C.c_int
+        _lib.oracle_sdf_points_d.argtypes = [_pd, _dp, _dp, _dp, _pd, _ip, _ip, _ip, _pd, _dp, _dp, _dp,
+                                             _dp, _dp, _dp, _dp, _ip]
+        _lib.oracle_closest_point_d.restype = C.c_int
+        _lib.oracle_closest_point_d.argtypes = [_pd, _dp, _dp, _dp, _pd, _ip, _ip, _ip, _pd, _dp, _dp, _dp,
+                                                _dp, _dp, _dp, _dp, _ip]
+        _lib.oracle_sqedf_points_d.restype = C.c_int
+        _lib.oracle_sqedf_points_d.argtypes = [_pd, _dp, _dp, _dp, _pd, _ip, _ip, _ip, _pd, _dp, _dp, _dp, _dp]
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref() -> C.CDLL:
+    """The reference's own CPU library (raises if it was not built)."""
+    global _ref
+    if _ref is None:
+        _ref = _load(REF_SO)
+        for suf, fptr in (("_d", _dp), ("_f", _fp)):
+            for n in ("ref_edf", "ref_edf_celllist", "ssdf_edf"):
+                f = getattr(_ref, n + suf)
+                f.restype = C.c_int
+                f.argtypes = [_pd, fptr, fptr, fptr, _pd, _ip, _ip, _ip, _pd, fptr, fptr, fptr, fptr]
+        _ref.ref_point_triangle_dist_sq_d.restype = C.c_double
+        _ref.ref_point_triangle_dist_sq_d.argtypes = [C.c_double] * 12
+        _ref.ref_point_triangle_dist_sq_f.restype = C.c_float
+        _ref.ref_point_triangle_dist_sq_f.argtypes = [C.c_float] * 12
+        _ref.ref_point_triangle_closest_point_d.restype = None
+        _ref.ref_point_triangle_closest_point_d.argtypes = [C.c_double] * 12 + [_dp] * 3
+        for n in ("ref_point_aabb_distance_squared_d", "ref_point_aabb_signed_distance_d"):
+            getattr(_ref, n).restype = C.c_double
+            getattr(_ref, n).argtypes = [C.c_double] * 9
+        _ref.ref_set_quiet.restype = None
+        _ref.ref_set_quiet.argtypes = [C.c_int]
+        _ref.ref_set_quiet(1)
+    return _ref
+
+
+# ----------------------------------------------------------------------------------------------
+# numpy conveniences
+# ----------------------------------------------------------------------------------------------
+
+def _ptr(a: np.ndarray, ct):
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+def _real(dtype):
+    return (C.c_double, "_d") if np.dtype(dtype) == np.float64 else (C.c_float, "_f")
+
+
+def _mesh_args(mesh, dtype):
+    ct, _ = _real(dtype)
+    sx, sy, sz = (np.ascontiguousarray(a, dtype=dtype) for a in mesh.coords())
+    s0, s1, s2 = (np.ascontiguousarray(a, dtype=np.int32) for a in mesh.indices())
+    keep = (sx, sy, sz, s0, s1, s2)
+    return keep, [len(s0), _ptr(s0, C.c_int), _ptr(s1, C.c_int), _ptr(s2, C.c_int), len(sx),
+                  _ptr(sx, ct), _ptr(sy, ct), _ptr(sz, ct)]
+
+
+def edf(points, mesh, out=None, dtype=np.float64, with_index=False):
+    """Brute-force edf value (and closest triangle) at points (3, n) -- the oracle's restatement."""
+    ct, suf = _real(dtype)
+    x, y, z = (np.ascontiguousarray(a, dtype=dtype) for a in points)
+    n = len(x)
+    o = np.full(n, np.finfo(dtype).max, dtype=dtype) if out is None else np.array(out, dtype=dtype, copy=True)
+    tri = np.full(n, -1, dtype=np.int32)
+    keep, margs = _mesh_args(mesh, dtype)
+    rc = getattr(lib(), "oracle_edf" + suf)(n, _ptr(x, ct), _ptr(y, ct), _ptr(z, ct), *margs, _ptr(o, ct),
+                                            _ptr(tri, C.c_int))
+    assert rc == 0
+    return (o, tri) if with_index else o
+
+
+def ref_edf(points, mesh, out=None, dtype=np.float64, which="edf"):
+    """The reference's own edf / edf_celllist / ssdf_edf (edf_select) on the CPU."""
+    ct, suf = _real(dtype)
+    x, y, z = (np.ascontiguousarray(a, dtype=dtype) for a in points)
+    n = len(x)
+    o = np.full(n, np.finfo(dtype).max, dtype=dtype) if out is None else np.array(out, dtype=dtype, copy=True)
+    keep, margs = _mesh_args(mesh, dtype)
+    fn = {"edf": "ref_edf", "celllist": "ref_edf_celllist", "select": "ssdf_edf"}[which]
+    rc = getattr(ref(), fn + suf)(n, _ptr(x, ct), _ptr(y, ct), _ptr(z, ct), *margs, _ptr(o, ct))
+    assert rc == 0
+    return o
+
+
+def pseudonormals(mesh):
+    sx, sy, sz = (np.ascontiguousarray(a, dtype=np.float64) for a in mesh.coords())
+    s0, s1, s2 = (np.ascontiguousarray(a, dtype=np.int32) for a in mesh.indices())
+    nt, nv = len(s0), len(sx)
+    fn = np.zeros(3 * nt)
+    en = np.zeros(9 * nt)
+    vn = np.zeros(3 * nv)
+    rc = lib().oracle_pseudonormals_d(nt, _ptr(s0, C.c_int), _ptr(s1, C.c_int), _ptr(s2, C.c_int), nv,
+                                      _ptr(sx, C.c_double), _ptr(sy, C.c_double), _ptr(sz, C.c_double),
+                                      _ptr(fn, C.c_double), _ptr(en, C.c_double), _ptr(vn, C.c_double))
+    assert rc == 0
+    return fn, en, vn
+
+
+def sdf_points(points, mesh, normals=None):
+    """Signed double distance and closest triangle at double points (3, n)."""
+    x, y, z = (np.ascontiguousarray(a, dtype=np.float64) for a in points)
+    n = len(x)
+    fn, en, vn = normals if normals is not None else pseudonormals(mesh)
+    out = np.zeros(n)
+    tri = np.zeros(n, dtype=np.int32)
+    keep, margs = _mesh_args(mesh, np.float64)
+    rc = lib().oracle_sdf_points_d(n, _ptr(x, C.c_double), _ptr(y, C.c_double), _ptr(z, C.c_double), *margs,
+                                   _ptr(fn, C.c_double), _ptr(en, C.c_double), _ptr(vn, C.c_double),
+                                   _ptr(out, C.c_double), _ptr(tri, C.c_int))
+    assert rc == 0
+    return out, tri
+
+
+def closest_point(points, mesh, outd=None):
+    x, y, z = (np.ascontiguousarray(a, dtype=np.float64) for a in points)
+    n = len(x)
+    d = np.full(n, np.finfo(np.float64).max) if outd is None else np.array(outd, dtype=np.float64, copy=True)
+    ox, oy, oz = np.zeros(n), np.zeros(n), np.zeros(n)
+    tri = np.full(n, -1, dtype=np.int32)
+    keep, margs = _mesh_args(mesh, np.float64)
+    rc = lib().oracle_closest_point_d(n, _ptr(x, C.c_double), _ptr(y, C.c_double), _ptr(z, C.c_double), *margs,
+                                      _ptr(d, C.c_double), _ptr(ox, C.c_double), _ptr(oy, C.c_double),
+                                      _ptr(oz, C.c_double), _ptr(tri, C.c_int))
+    assert rc == 0
+    return d, ox, oy, oz, tri
+
+
+def sqedf_points(points, mesh, out=None):
+    x, y, z = (np.ascontiguousarray(a, dtype=np.float64) for a in points)
+    n = len(x)
+    o = np.full(n, np.finfo(np.float64).max) if out is None else np.array(out, dtype=np.float64, copy=True)
+    keep, margs = _mesh_args(mesh, np.float64)
+    rc = lib().oracle_sqedf_points_d(n, _ptr(x, C.c_double), _ptr(y, C.c_double), _ptr(z, C.c_double), *margs,
+                                     _ptr(o, C.c_double))
+    assert rc == 0
+    return o
+
+
+def grid_points(grid, dtype=np.float64):
+    """Node-grid coordinates (3, nx*ny*nz) in the reference's G precision, widened to double."""
+    ct, suf = _real(dtype)
+    nx, ny, nz = grid.n
+    n = nx * ny * nz
+    q = np.zeros((3, n))
+    lo = [ct(v) for v in grid.lo]
+    hi = [ct(v) for v in grid.hi]
+    getattr(lib(), "oracle_grid_points" + suf)(nx, ny, nz, *lo, *hi, _ptr(q[0], C.c_double),
+                                               _ptr(q[1], C.c_double), _ptr(q[2], C.c_double))
+    return q

@@ -1,0 +1,65 @@
+// ref_harness.cpp -- C entry points over the reference's own templates (serial/ssdf.hpp,
+// serial/edf/edf.hpp), compiled from the sources where they lie by oracle/Makefile into
+// oracle/_ref/libssdf_ref.so.
+//
+// TEST INFRASTRUCTURE ONLY: used to pin the oracle and as the timed CPU baseline
+// (bench.py --impl reference); the product never loads it. The reference's own exports
+// ssdf_edf_f / ssdf_edf_d (serial/ssdf.cpp:36-66) come from serial/ssdf.cpp in the same link.
+#include <iostream>
+#include <streambuf>
+
+#include "ssdf.hpp"
+
+namespace {
+    // The reference prints "<name> took X ms" from inside edf / edf_celllist (SSDF_TIMER,
+    // serial/ssdf.hpp:25-46); a timed caller can route std::cout to this sink.
+    struct NullBuf : std::streambuf {
+        int overflow(int c) override { return c; }
+    };
+    NullBuf null_buf;
+    std::streambuf *saved_buf = nullptr;
+}  // namespace
+
+#define REF_ARGS(G)                                                                                       \
+    const ptrdiff_t npoints, const G *x, const G *y, const G *z, const ptrdiff_t nselements, const int *s0, \
+        const int *s1, const int *s2, const ptrdiff_t nspoints, const G *sx, const G *sy, const G *sz, G *out
+#define REF_PASS npoints, x, y, z, nselements, s0, s1, s2, nspoints, sx, sy, sz, out
+
+extern "C" {
+
+void ref_set_quiet(const int quiet) {
+    if (quiet && !saved_buf) {
+        saved_buf = std::cout.rdbuf(&null_buf);
+    } else if (!quiet && saved_buf) {
+        std::cout.rdbuf(saved_buf);
+        saved_buf = nullptr;
+    }
+}
+
+int ref_edf_d(REF_ARGS(double)) { return ssdf::edf<double, double, int>(REF_PASS); }
+int ref_edf_f(REF_ARGS(float)) { return ssdf::edf<float, float, int>(REF_PASS); }
+int ref_edf_celllist_d(REF_ARGS(double)) { return ssdf::edf_celllist<double, double, int>(REF_PASS); }
+int ref_edf_celllist_f(REF_ARGS(float)) { return ssdf::edf_celllist<float, float, int>(REF_PASS); }
+
+double ref_point_triangle_dist_sq_d(double px, double py, double pz, double ax, double ay, double az, double bx,
+                                    double by, double bz, double cx, double cy, double cz) {
+    return ssdf::point_triangle_dist_sq<double>(px, py, pz, ax, ay, az, bx, by, bz, cx, cy, cz);
+}
+float ref_point_triangle_dist_sq_f(float px, float py, float pz, float ax, float ay, float az, float bx, float by,
+                                   float bz, float cx, float cy, float cz) {
+    return ssdf::point_triangle_dist_sq<float>(px, py, pz, ax, ay, az, bx, by, bz, cx, cy, cz);
+}
+void ref_point_triangle_closest_point_d(double px, double py, double pz, double ax, double ay, double az, double bx,
+                                        double by, double bz, double cx, double cy, double cz, double *ox, double *oy,
+                                        double *oz) {
+    ssdf::point_triangle_closest_point<double>(px, py, pz, ax, ay, az, bx, by, bz, cx, cy, cz, ox, oy, oz);
+}
+double ref_point_aabb_distance_squared_d(double px, double py, double pz, double minx, double maxx, double miny,
+                                         double maxy, double minz, double maxz) {
+    return ssdf::point_aabb_distance_squared<double>(px, py, pz, minx, maxx, miny, maxy, minz, maxz);
+}
+double ref_point_aabb_signed_distance_d(double px, double py, double pz, double minx, double maxx, double miny,
+                                        double maxy, double minz, double maxz) {
+    return ssdf::point_aabb_signed_distance<double>(px, py, pz, minx, maxx, miny, maxy, minz, maxz);
+}
+}

@@ -1,0 +1,337 @@
+"""ssdf_b200.capi -- ctypes binding of the CUDA library's C ABI.
+
+A ctypes binding over the C ABI of ``ssdf_b200/_lib/libssdf_b200.so`` (declared in
+``include/ssdf_b200.h``). Every call runs the CUDA library: there is no CPU path, and importing
+this package raises if the library is not built (``python -m ssdf_b200.build``).
+
+Two layers:
+
+* drop-in functions over host (numpy) arrays, one per reference entry point --
+  :func:`edf_select` (``ssdf_edf_f/_d``), :func:`edf`, :func:`edf_celllist`, :func:`edf_bvh`,
+  :func:`closest_point_bvh`, :func:`sample_sqedf_bvh`, :func:`sample_sdf_bvh` -- plus the additive
+  :func:`edf_index`, :func:`sdf_points`;
+* :class:`DeviceMesh`: a mesh and its BVH resident on the GPU, queried with device buffers
+  (torch tensors or raw pointers) on a caller-chosen stream.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libssdf_b200.so")
+
+SSDF_OK = 0
+F32, F64 = 0, 1
+PREC_F32, PREC_F64, PREC_F32_FIXUP = 0, 1, 2
+OUT_EDF, OUT_SQEDF, OUT_SDF, OUT_CLOSEST = 0, 1, 2, 3
+
+_pd = C.c_ssize_t
+_vp = C.c_void_p
+_ip = C.POINTER(C.c_int)
+
+
+class SsdfError(RuntimeError):
+    def __init__(self, status: int, fn: str, message: str):
+        super().__init__(f"{fn} -> {_status_name(status)}: {message}")
+        self.status = status
+
+
+class BuildOpts(C.Structure):
+    _fields_ = [("leaf_size", C.c_int), ("keep_fp64", C.c_int), ("normals", C.c_int), ("treelet_opt", C.c_int)]
+
+
+class QueryOpts(C.Structure):
+    _fields_ = [("precision", C.c_int), ("output", C.c_int), ("coord_type", C.c_int), ("out_type", C.c_int),
+                ("reserved", C.c_int * 4)]
+
+
+def _load() -> C.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build the CUDA library first (python -m ssdf_b200.build)")
+    return C.CDLL(LIB_PATH)
+
+
+lib = _load()
+
+
+def _sig(name, args, res=C.c_int):
+    f = getattr(lib, name)
+    f.argtypes = args
+    f.restype = res
+    return f
+
+
+_sig("ssdf_status_string", [C.c_int], C.c_char_p)
+_sig("ssdf_last_error", [], C.c_char_p)
+_sig("ssdf_b200_version", [], C.c_char_p)
+
+_EDF = [_pd, _vp, _vp, _vp, _pd, _ip, _ip, _ip, _pd, _vp, _vp, _vp, _vp]
+_GRID = [_pd, _ip, _ip, _ip, _pd, _vp, _vp, _vp, _pd, _pd, _pd]
+for _n in ("ssdf_edf_f", "ssdf_edf_d", "ssdf_b200_edf_ff", "ssdf_b200_edf_dd", "ssdf_b200_edf_celllist_ff",
+           "ssdf_b200_edf_celllist_dd", "ssdf_b200_edf_bvh_ff", "ssdf_b200_edf_bvh_fd", "ssdf_b200_edf_bvh_dd"):
+    _sig(_n, _EDF)
+for _n in ("ssdf_b200_edf_index_dd", "ssdf_b200_edf_index_ff", "ssdf_b200_sdf_points_dd"):
+    _sig(_n, _EDF + [_ip])
+for _n in ("ssdf_b200_closest_point_bvh_ff", "ssdf_b200_closest_point_bvh_dd"):
+    _sig(_n, _EDF + [_vp, _vp, _vp, _ip])
+_sig("ssdf_b200_sample_sqedf_bvh_ff", _GRID + [C.c_float] * 6 + [_vp])
+_sig("ssdf_b200_sample_sdf_bvh_ff", _GRID + [C.c_float] * 6 + [_vp])
+_sig("ssdf_b200_sample_sqedf_bvh_dd", _GRID + [C.c_double] * 6 + [_vp])
+_sig("ssdf_b200_sample_sdf_bvh_dd", _GRID + [C.c_double] * 6 + [_vp])
+_sig("ssdf_b200_sample_sdf_index_bvh_dd", _GRID + [C.c_double] * 6 + [_vp, _ip])
+_sig("ssdf_mesh_create", [C.POINTER(_vp), _pd, _ip, _ip, _ip, _pd, _vp, _vp, _vp, C.c_int, C.c_int,
+                          C.POINTER(BuildOpts), _vp])
+_sig("ssdf_mesh_destroy", [_vp])
+_sig("ssdf_mesh_stats", [_vp] + [C.POINTER(C.c_int64)] * 4)
+_sig("ssdf_query_points", [_vp, _pd, _vp, _vp, _vp, _vp, _ip, _vp, _vp, _vp, C.POINTER(QueryOpts), _vp])
+_sig("ssdf_query_grid", [_vp, _pd, _pd, _pd, C.POINTER(C.c_double * 3), C.POINTER(C.c_double * 3), _vp, _ip,
+                         C.POINTER(QueryOpts), _vp])
+_sig("ssdf_last_query_counts", [C.POINTER(C.c_int64)] * 4)
+_sig("ssdf_b200_fma_peak", [C.c_int, C.POINTER(C.c_double)])
+
+EXPORTED = ["ssdf_status_string", "ssdf_last_error", "ssdf_b200_version", "ssdf_edf_f", "ssdf_edf_d",
+            "ssdf_b200_edf_ff", "ssdf_b200_edf_dd", "ssdf_b200_edf_celllist_ff", "ssdf_b200_edf_celllist_dd",
+            "ssdf_b200_edf_bvh_ff", "ssdf_b200_edf_bvh_fd", "ssdf_b200_edf_bvh_dd", "ssdf_b200_closest_point_bvh_ff",
+            "ssdf_b200_closest_point_bvh_dd", "ssdf_b200_sample_sqedf_bvh_ff", "ssdf_b200_sample_sqedf_bvh_dd",
+            "ssdf_b200_sample_sdf_bvh_ff", "ssdf_b200_sample_sdf_bvh_dd", "ssdf_b200_edf_index_dd",
+            "ssdf_b200_edf_index_ff", "ssdf_b200_sdf_points_dd", "ssdf_b200_sample_sdf_index_bvh_dd",
+            "ssdf_mesh_create", "ssdf_mesh_destroy", "ssdf_mesh_stats", "ssdf_query_points", "ssdf_query_grid",
+            "ssdf_last_query_counts", "ssdf_b200_fma_peak"]
+
+
+def _status_name(status: int) -> str:
+    return lib.ssdf_status_string(status).decode()
+
+
+def last_error() -> str:
+    return lib.ssdf_last_error().decode()
+
+
+def _check(status: int, fn: str) -> None:
+    if status != SSDF_OK:
+        raise SsdfError(status, fn, last_error())
+
+
+def version() -> str:
+    return lib.ssdf_b200_version().decode()
+
+
+# ----------------------------------------------------------------------------------------------
+# host (numpy) drop-in layer
+# ----------------------------------------------------------------------------------------------
+
+def _arr(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def _p(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+def _ipp(a):
+    return a.ctypes.data_as(_ip)
+
+
+def _suffix(dtype) -> str:
+    return "d" if np.dtype(dtype) == np.float64 else "f"
+
+
+class _HostMesh:
+    def __init__(self, mesh, dtype):
+        self.sx, self.sy, self.sz = (_arr(a, dtype) for a in mesh.coords())
+        self.s0, self.s1, self.s2 = (_arr(a, np.int32) for a in mesh.indices())
+
+    def args(self):
+        return [len(self.s0), _ipp(self.s0), _ipp(self.s1), _ipp(self.s2), len(self.sx), _p(self.sx), _p(self.sy),
+                _p(self.sz)]
+
+
+def _points(points, dtype):
+    x, y, z = (_arr(a, dtype) for a in points)
+    return x, y, z
+
+
+def _init_out(n, dtype, out):
+    if out is None:
+        return np.full(n, np.finfo(dtype).max, dtype=dtype)
+    return np.array(out, dtype=dtype, copy=True)
+
+
+def _edf_call(fn, points, mesh, out, gdtype, tdtype, extra=()):
+    x, y, z = _points(points, gdtype)
+    o = _init_out(len(x), tdtype, out)
+    hm = _HostMesh(mesh, gdtype)
+    _check(getattr(lib, fn)(len(x), _p(x), _p(y), _p(z), *hm.args(), _p(o), *extra), fn)
+    return o
+
+
+def edf_select(points, mesh, out=None, dtype=np.float64):
+    """ssdf_edf_f / ssdf_edf_d: the reference's C ABI (environment-dispatched edf_select)."""
+    return _edf_call("ssdf_edf_" + _suffix(dtype), points, mesh, out, dtype, dtype)
+
+
+def edf(points, mesh, out=None, dtype=np.float64):
+    """ssdf::edf<G, G, int>: GPU brute force, bitwise the reference's value."""
+    s = _suffix(dtype)
+    return _edf_call(f"ssdf_b200_edf_{s}{s}", points, mesh, out, dtype, dtype)
+
+
+def edf_celllist(points, mesh, out=None, dtype=np.float64):
+    """ssdf::edf_celllist<G, G, int>: GPU cell list, bitwise the reference's value."""
+    s = _suffix(dtype)
+    return _edf_call(f"ssdf_b200_edf_celllist_{s}{s}", points, mesh, out, dtype, dtype)
+
+
+def edf_bvh(points, mesh, out=None, gdtype=np.float64, tdtype=None):
+    """ssdf::edf_bvh<G, T, int> over the device BVH."""
+    tdtype = tdtype or gdtype
+    return _edf_call(f"ssdf_b200_edf_bvh_{_suffix(gdtype)}{_suffix(tdtype)}", points, mesh, out, gdtype, tdtype)
+
+
+def edf_index(points, mesh, out=None, dtype=np.float64):
+    """Unsigned distance (in/out) and the closest triangle (-1 where nothing improved)."""
+    x, y, z = _points(points, dtype)
+    tri = np.full(len(x), -1, dtype=np.int32)
+    s = _suffix(dtype)
+    o = _edf_call(f"ssdf_b200_edf_index_{s}{s}", (x, y, z), mesh, out, dtype, dtype, extra=(_ipp(tri),))
+    return o, tri
+
+
+def sdf_points(points, mesh):
+    """Signed distance (double) and closest triangle at a point list."""
+    x, y, z = _points(points, np.float64)
+    tri = np.full(len(x), -1, dtype=np.int32)
+    o = _edf_call("ssdf_b200_sdf_points_dd", (x, y, z), mesh, np.zeros(len(x)), np.float64, np.float64,
+                  extra=(_ipp(tri),))
+    return o, tri
+
+
+def closest_point_bvh(points, mesh, outd=None, dtype=np.float64):
+    """ssdf::closest_point_bvh: (outd, outx, outy, outz, outtri), updated where closer than outd."""
+    x, y, z = _points(points, dtype)
+    n = len(x)
+    d = _init_out(n, dtype, outd)
+    ox, oy, oz = np.zeros(n, dtype), np.zeros(n, dtype), np.zeros(n, dtype)
+    tri = np.full(n, -1, dtype=np.int32)
+    s = _suffix(dtype)
+    hm = _HostMesh(mesh, dtype)
+    fn = f"ssdf_b200_closest_point_bvh_{s}{s}"
+    _check(getattr(lib, fn)(n, _p(x), _p(y), _p(z), *hm.args(), _p(d), _p(ox), _p(oy), _p(oz), _ipp(tri)), fn)
+    return d, ox, oy, oz, tri
+
+
+def _grid_call(fn, mesh, grid, out, dtype, extra=()):
+    nx, ny, nz = (int(v) for v in grid.n)
+    hm = _HostMesh(mesh, dtype)
+    ct = C.c_double if np.dtype(dtype) == np.float64 else C.c_float
+    bounds = [ct(v) for v in grid.lo] + [ct(v) for v in grid.hi]
+    _check(getattr(lib, fn)(*hm.args(), nx, ny, nz, *bounds, _p(out), *extra), fn)
+    return out
+
+
+def sample_sqedf_bvh(mesh, grid, out=None, dtype=np.float64):
+    """ssdf::sample_sqedf_bvh: squared distance on the node grid, min with the incoming out."""
+    o = _init_out(grid.size, dtype, out)
+    s = _suffix(dtype)
+    return _grid_call(f"ssdf_b200_sample_sqedf_bvh_{s}{s}", mesh, grid, o, dtype)
+
+
+def sample_sdf_bvh(mesh, grid, dtype=np.float64, with_index=False):
+    """ssdf::sample_sdf_bvh: signed distance on the node grid (x fastest)."""
+    o = np.zeros(grid.size, dtype=dtype)
+    s = _suffix(dtype)
+    if with_index:
+        if s != "d":
+            raise ValueError("the indexed grid sampler is double only")
+        tri = np.full(grid.size, -1, dtype=np.int32)
+        _grid_call("ssdf_b200_sample_sdf_index_bvh_dd", mesh, grid, o, dtype, extra=(_ipp(tri),))
+        return o, tri
+    return _grid_call(f"ssdf_b200_sample_sdf_bvh_{s}{s}", mesh, grid, o, dtype)
+
+
+def fma_peak_tflops(f64: bool = False) -> float:
+    """Measured FMA throughput of the current GPU (TFLOP/s)."""
+    v = C.c_double()
+    _check(lib.ssdf_b200_fma_peak(int(f64), C.byref(v)), "ssdf_b200_fma_peak")
+    return v.value
+
+
+def last_query_counts():
+    v = [C.c_int64() for _ in range(4)]
+    _check(lib.ssdf_last_query_counts(*[C.byref(a) for a in v]), "ssdf_last_query_counts")
+    return dict(triangle_tests=v[0].value, box_tests=v[1].value, fixup_evaluations=v[2].value,
+                fallback_queries=v[3].value)
+
+
+# ----------------------------------------------------------------------------------------------
+# device-resident meshes
+# ----------------------------------------------------------------------------------------------
+
+def _dptr(t) -> int:
+    """Device pointer of a torch tensor (or an int pointer)."""
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    return t.data_ptr()
+
+
+def _stream_handle(stream) -> int:
+    if stream is None:
+        return 0
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+class DeviceMesh:
+    """A mesh, its BVH and (optionally) pseudo-normals, resident on the current GPU."""
+
+    def __init__(self, mesh, coord_dtype=np.float64, leaf_size=0, keep_fp64=True, normals=True, treelet=False,
+                 stream=None):
+        hm = _HostMesh(mesh, coord_dtype)
+        self._h = C.c_void_p()
+        opts = BuildOpts(int(leaf_size), int(keep_fp64), int(normals), int(treelet))
+        ct = F64 if np.dtype(coord_dtype) == np.float64 else F32
+        _check(lib.ssdf_mesh_create(C.byref(self._h), *hm.args(), ct, 0, C.byref(opts), _stream_handle(stream)),
+               "ssdf_mesh_create")
+        self.nt = mesh.nt
+        self.nv = mesh.nv
+
+    def close(self):
+        if self._h:
+            lib.ssdf_mesh_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def stats(self):
+        v = [C.c_int64() for _ in range(4)]
+        _check(lib.ssdf_mesh_stats(self._h, *[C.byref(a) for a in v]), "ssdf_mesh_stats")
+        return dict(nodes=v[0].value, leaves=v[1].value, depth=v[2].value, bytes=v[3].value)
+
+    def query_points(self, x, y, z, out, outtri=None, outx=None, outy=None, outz=None, precision=PREC_F32_FIXUP,
+                     output=OUT_EDF, coord_type=F64, out_type=F64, stream=None):
+        o = QueryOpts(precision, output, coord_type, out_type)
+        tri = C.cast(C.c_void_p(_dptr(outtri)), _ip) if outtri is not None else None
+        _check(lib.ssdf_query_points(self._h, int(x.numel() if hasattr(x, "numel") else len(x)), _dptr(x), _dptr(y),
+                                     _dptr(z), _dptr(out), tri, _dptr(outx), _dptr(outy), _dptr(outz), C.byref(o),
+                                     _stream_handle(stream)), "ssdf_query_points")
+
+    def query_grid(self, grid, out, outtri=None, precision=PREC_F32_FIXUP, output=OUT_SDF, coord_type=F64,
+                   out_type=F64, stream=None):
+        o = QueryOpts(precision, output, coord_type, out_type)
+        lo = (C.c_double * 3)(*grid.lo)
+        hi = (C.c_double * 3)(*grid.hi)
+        tri = C.cast(C.c_void_p(_dptr(outtri)), _ip) if outtri is not None else None
+        nx, ny, nz = (int(v) for v in grid.n)
+        _check(lib.ssdf_query_grid(self._h, nx, ny, nz, C.byref(lo), C.byref(hi), _dptr(out), tri, C.byref(o),
+                                   _stream_handle(stream)), "ssdf_query_grid")

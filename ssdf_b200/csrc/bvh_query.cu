@@ -1,0 +1,690 @@
+// bvh_query.cu -- closest-triangle queries over the device BVH, one thread per query.
+//
+// Stands in for the reference's device query (serial/bvh/bvh.cu:60-76 + cuBQL CPAT) and its CPU
+// grid samplers (serial/bvh/bvh.cpp:1574-1798). Three arithmetics (SSDF_PREC_*):
+//   F64   double nodes and triangles, the reference's exact double expression; lexicographic
+//         (d^2, triangle index) minimum: bitwise the reference's double value;
+//   F32   the same over float nodes/triangles with the reference's float expression (its
+//         edf<float> value);
+//   F32X  float traversal with fused multiply-adds keeps the K smallest float d^2 inside a
+//         window (sqrt(best) + tau)^2; the window's members are re-evaluated in double and the
+//         lexicographic minimum taken. tau bounds twice the float error of one distance, so the
+//         double winner is always in the window; a query whose window overflowed the K slots is
+//         handed to the F64 kernel (k_fallback). Result: bitwise the F64 result.
+// Traversal: nearest child first, the farther one pushed with its box distance on a per-thread
+// stack and culled on pop against the current threshold. Grid queries map a warp to a 4x4x2 brick
+// of nodes and a block to 8x4x4, so a warp's traversals stay coherent.
+// Outputs (SSDF_OUT_*): in/out distance (edf), in/out squared distance (sqedf), signed distance
+// with the pseudo-normal rule of serial/bvh/bvh.cpp:1751-1792, closest point + triangle
+// (closest_point_bvh, serial/bvh/bvh.cpp:178-194).
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cstring>
+
+#include "device_geom.cuh"
+#include "internal.h"
+
+namespace ssdf_b200 {
+
+namespace {
+
+constexpr int kThreads = 128;
+constexpr int kCand = 8;  // F32X window slots
+
+struct Counters {
+    unsigned long long tri = 0, box = 0, fix = 0;
+};
+
+__device__ __forceinline__ double dinf() { return __longlong_as_double(0x7ff0000000000000ll); }
+__device__ __forceinline__ float finf() { return __int_as_float(0x7f800000); }
+
+// ---- query mapping ------------------------------------------------------------------------------
+
+// Grid brick: block = 8 (x) * 4 (y) * 4 (z) nodes, warp = 4 * 4 * 2.
+__device__ __forceinline__ bool map_thread(const QueryArgs &a, long long &q, long long &i, long long &j,
+                                           long long &k) {
+    if (!a.is_grid) {
+        q = (long long)blockIdx.x * kThreads + threadIdx.x;
+        return q < a.npoints;
+    }
+    const long long bxn = (a.nx + 7) >> 3, byn = (a.ny + 3) >> 2;
+    const long long b = blockIdx.x;
+    const long long bx = b % bxn, r = b / bxn;
+    const long long by = r % byn, bz = r / byn;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    i = bx * 8 + (warp & 1) * 4 + (lane & 3);
+    j = by * 4 + ((lane >> 2) & 3);
+    k = bz * 4 + (warp >> 1) * 2 + (lane >> 4);
+    q = i + a.nx * (j + a.ny * k);
+    return i < a.nx && j < a.ny && k < a.nz;
+}
+
+__device__ __forceinline__ void grid_ijk(const QueryArgs &a, long long q, long long &i, long long &j, long long &k) {
+    i = q % a.nx;
+    const long long r = q / a.nx;
+    j = r % a.ny;
+    k = r / a.ny;
+}
+
+__device__ __forceinline__ void query_point(const QueryArgs &a, long long q, long long i, long long j, long long k,
+                                            double &x, double &y, double &z) {
+    if (a.is_grid) {
+        if (a.coord_f64) {
+            x = grid_coord<double>(a.lo64[0], a.h64[0], i);
+            y = grid_coord<double>(a.lo64[1], a.h64[1], j);
+            z = grid_coord<double>(a.lo64[2], a.h64[2], k);
+        } else {
+            x = grid_coord<float>(a.lo32[0], a.h32[0], i);
+            y = grid_coord<float>(a.lo32[1], a.h32[1], j);
+            z = grid_coord<float>(a.lo32[2], a.h32[2], k);
+        }
+    } else if (a.coord_f64) {
+        x = __ldg((const double *)a.x + q);
+        y = __ldg((const double *)a.y + q);
+        z = __ldg((const double *)a.z + q);
+    } else {
+        x = double(__ldg((const float *)a.x + q));
+        y = double(__ldg((const float *)a.y + q));
+        z = double(__ldg((const float *)a.z + q));
+    }
+}
+
+__device__ __forceinline__ double load_out(const QueryArgs &a, long long q) {
+    return a.out_f64 ? ((const double *)a.out)[q] : double(((const float *)a.out)[q]);
+}
+__device__ __forceinline__ void store_out(const QueryArgs &a, long long q, double v) {
+    if (a.out_f64)
+        ((double *)a.out)[q] = v;
+    else
+        ((float *)a.out)[q] = float(v);
+}
+
+// ---- node and triangle loads ----------------------------------------------------------------------
+
+struct Node32 {
+    float4 a, b, c;
+    int r0, r1;
+};
+__device__ __forceinline__ Node32 load_node32(const float4 *__restrict__ nodes, int n) {
+    Node32 o;
+    o.a = __ldg(nodes + 4 * n);
+    o.b = __ldg(nodes + 4 * n + 1);
+    o.c = __ldg(nodes + 4 * n + 2);
+    const float4 d = __ldg(nodes + 4 * n + 3);
+    o.r0 = __float_as_int(d.x);
+    o.r1 = __float_as_int(d.y);
+    return o;
+}
+
+struct Node64 {
+    double2 x0, y0, z0, x1, y1, z1;
+    int r0, r1;
+};
+__device__ __forceinline__ Node64 load_node64(const double2 *__restrict__ nodes, int n) {
+    Node64 o;
+    const double2 *p = nodes + 8 * n;
+    o.x0 = __ldg(p);
+    o.y0 = __ldg(p + 1);
+    o.z0 = __ldg(p + 2);
+    o.x1 = __ldg(p + 3);
+    o.y1 = __ldg(p + 4);
+    o.z1 = __ldg(p + 5);
+    const double2 r = __ldg(p + 6);
+    o.r0 = int((unsigned)__double_as_longlong(r.x));
+    o.r1 = int((unsigned)__double_as_longlong(r.y));
+    return o;
+}
+
+struct Tri32 {
+    float ax, ay, az, bx, by, bz, cx, cy, cz;
+    int id;
+};
+__device__ __forceinline__ Tri32 load_tri32(const float4 *__restrict__ t, int p) {
+    const float4 u = __ldg(t + 3 * p), v = __ldg(t + 3 * p + 1), w = __ldg(t + 3 * p + 2);
+    return Tri32{u.x, u.y, u.z, u.w, v.x, v.y, v.z, v.w, w.x, __float_as_int(w.y)};
+}
+
+struct Tri64 {
+    double ax, ay, az, bx, by, bz, cx, cy, cz;
+    int id;
+};
+__device__ __forceinline__ Tri64 load_tri64(const double2 *__restrict__ t, int p) {
+    const double2 *r = t + 5 * p;
+    const double2 u = __ldg(r), v = __ldg(r + 1), w = __ldg(r + 2), x = __ldg(r + 3), y = __ldg(r + 4);
+    return Tri64{u.x, u.y, v.x, v.y, w.x, w.y, x.x, x.y, y.x, int(y.y)};
+}
+
+// ---- exact traversal (F64 over double data, F32 over float data) ------------------------------------
+
+template <typename T>
+struct ExactData;
+template <>
+struct ExactData<double> {
+    static constexpr double rel = 1.0 + 1.0 / 65536.0;
+    static __device__ __forceinline__ double abs_margin(float scale) {
+        const double s = double(scale) * 0x1p-40;
+        return s * s;
+    }
+    static __device__ __forceinline__ void boxes(const DeviceMesh &m, int node, double px, double py, double pz,
+                                                 double &d0, double &d1, int &r0, int &r1) {
+        const Node64 n = load_node64(m.nodes64, node);
+        d0 = box_dist_sq<double>(px, py, pz, n.x0.x, n.x0.y, n.y0.x, n.y0.y, n.z0.x, n.z0.y);
+        d1 = box_dist_sq<double>(px, py, pz, n.x1.x, n.x1.y, n.y1.x, n.y1.y, n.z1.x, n.z1.y);
+        r0 = n.r0;
+        r1 = n.r1;
+    }
+    static __device__ __forceinline__ double tri(const DeviceMesh &m, int pos, double px, double py, double pz,
+                                                 int &id) {
+        const Tri64 t = load_tri64(m.tris64, pos);
+        id = t.id;
+        return tri_dist_sq_exact<double>(px, py, pz, t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
+    }
+};
+template <>
+struct ExactData<float> {
+    static constexpr float rel = 1.0f + 1.0f / 65536.0f;
+    static __device__ __forceinline__ float abs_margin(float scale) {
+        const float s = scale * 0x1p-16f;
+        return s * s;
+    }
+    static __device__ __forceinline__ void boxes(const DeviceMesh &m, int node, float px, float py, float pz,
+                                                 float &d0, float &d1, int &r0, int &r1) {
+        const Node32 n = load_node32(m.nodes32, node);
+        d0 = box_dist_sq<float>(px, py, pz, n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y);
+        d1 = box_dist_sq<float>(px, py, pz, n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w);
+        r0 = n.r0;
+        r1 = n.r1;
+    }
+    static __device__ __forceinline__ float tri(const DeviceMesh &m, int pos, float px, float py, float pz, int &id) {
+        const Tri32 t = load_tri32(m.tris32, pos);
+        id = t.id;
+        return tri_dist_sq_exact<float>(px, py, pz, t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
+    }
+};
+
+// Lexicographic (d^2, id) minimum over all triangles, starting from (best, -1): a triangle
+// replaces the incumbent if strictly closer, or equally close with a lower index (never the
+// initial bound on a tie). Pruning keeps every box whose distance is below
+// best * (1 + 2^-16) + margin, so rounding in box distances never drops a tie.
+template <typename T, bool COUNT>
+__device__ void traverse_exact(const DeviceMesh &m, const T px, const T py, const T pz, T &best, int &bid,
+                               int &bpos, Counters &cnt) {
+    using D = ExactData<T>;
+    const T margin = D::abs_margin(m.coord_scale);
+    T thr = best * D::rel + margin;
+    int snode[kStackSize];
+    T sdist[kStackSize];
+    int sp = 0;
+    int node = 0;
+    while (true) {
+        T d0, d1;
+        int r0, r1;
+        D::boxes(m, node, px, py, pz, d0, d1, r0, r1);
+        if (COUNT) cnt.box += 2;
+        // near child first
+        if (d1 < d0) {
+            const T td = d0;
+            d0 = d1;
+            d1 = td;
+            const int tr = r0;
+            r0 = r1;
+            r1 = tr;
+        }
+        int next = -1;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const T dc = h ? d1 : d0;
+            const int rc = h ? r1 : r0;
+            if (!(dc < thr) || rc == kEmptyRef) continue;
+            if (rc < 0) {
+                const int first = leaf_first(rc), n = leaf_count(rc);
+                for (int k = 0; k < n; k++) {
+                    int id;
+                    const T d2 = D::tri(m, first + k, px, py, pz, id);
+                    if (COUNT) cnt.tri++;
+                    if (d2 < best || (d2 == best && bid >= 0 && id < bid)) {
+                        best = d2;
+                        bid = id;
+                        bpos = first + k;
+                        thr = best * D::rel + margin;
+                    }
+                }
+            } else if (next < 0) {
+                next = rc;
+            } else if (sp < kStackSize) {
+                snode[sp] = rc;
+                sdist[sp] = dc;
+                sp++;
+            }
+        }
+        if (next < 0) {
+            while (sp > 0) {
+                sp--;
+                if (sdist[sp] < thr) {
+                    next = snode[sp];
+                    break;
+                }
+            }
+            if (next < 0) break;
+        }
+        node = next;
+    }
+}
+
+// ---- F32X: float filter + window ------------------------------------------------------------------
+
+struct Window {
+    float d[kCand];
+    int p[kCand];
+    float evicted;  // smallest d^2 pushed out of the slots
+};
+
+__device__ __forceinline__ float window_thr(float best, float tau_rel, float scale) {
+    if (!(best < finf())) return finf();
+    const float d = sqrtf(best);
+    const float w = d + tau_rel * (scale + d);
+    return w * w * (1.0f + 1.0f / 65536.0f);
+}
+
+template <bool COUNT>
+__device__ void traverse_fast(const DeviceMesh &m, const float px, const float py, const float pz, float &best,
+                              const float tau_rel, Window &win, float &thr, Counters &cnt) {
+    thr = window_thr(best, tau_rel, m.coord_scale);
+    int snode[kStackSize];
+    float sdist[kStackSize];
+    int sp = 0;
+    int node = 0;
+    while (true) {
+        const Node32 n = load_node32(m.nodes32, node);
+        float d0 = box_dist_sq_fast(px, py, pz, n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y);
+        float d1 = box_dist_sq_fast(px, py, pz, n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w);
+        int r0 = n.r0, r1 = n.r1;
+        if (COUNT) cnt.box += 2;
+        if (d1 < d0) {
+            const float td = d0;
+            d0 = d1;
+            d1 = td;
+            const int tr = r0;
+            r0 = r1;
+            r1 = tr;
+        }
+        int next = -1;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const float dc = h ? d1 : d0;
+            const int rc = h ? r1 : r0;
+            if (!(dc < thr) || rc == kEmptyRef) continue;
+            if (rc < 0) {
+                const int first = leaf_first(rc), cntl = leaf_count(rc);
+                for (int k = 0; k < cntl; k++) {
+                    const Tri32 t = load_tri32(m.tris32, first + k);
+                    const float d2 =
+                        tri_dist_sq_fast(px, py, pz, t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
+                    if (COUNT) cnt.tri++;
+                    if (d2 < thr) {
+                        float d = d2;
+                        int p = first + k;
+#pragma unroll
+                        for (int s = 0; s < kCand; s++) {
+                            if (d < win.d[s]) {
+                                const float td = win.d[s];
+                                const int tp = win.p[s];
+                                win.d[s] = d;
+                                win.p[s] = p;
+                                d = td;
+                                p = tp;
+                            }
+                        }
+                        win.evicted = fminf(win.evicted, d);
+                        if (d2 < best) {
+                            best = d2;
+                            thr = window_thr(best, tau_rel, m.coord_scale);
+                        }
+                    }
+                }
+            } else if (next < 0) {
+                next = rc;
+            } else if (sp < kStackSize) {
+                snode[sp] = rc;
+                sdist[sp] = dc;
+                sp++;
+            }
+        }
+        if (next < 0) {
+            while (sp > 0) {
+                sp--;
+                if (sdist[sp] < thr) {
+                    next = snode[sp];
+                    break;
+                }
+            }
+            if (next < 0) break;
+        }
+        node = next;
+    }
+}
+
+// ---- outputs ----------------------------------------------------------------------------------------
+
+// Signed distance from the closest triangle (caller's index t, leaf position pos) and d^2, in
+// double: the closest point, its barycentric coordinates, the pseudo-normal they select and the
+// sign of (q - c) . n (serial/bvh/bvh.cpp:1751-1792, tolerance 1e-4 from bvh.cpp:1738).
+__device__ double signed_distance(const DeviceMesh &m, int pos, int t, double qx, double qy, double qz, double d2,
+                                  double &cx, double &cy, double &cz) {
+    const Tri64 tr = load_tri64(m.tris64, pos);
+    tri_closest_point_exact<double>(qx, qy, qz, tr.ax, tr.ay, tr.az, tr.bx, tr.by, tr.bz, tr.cx, tr.cy, tr.cz, cx, cy,
+                                    cz);
+    const double e1[3] = {tr.bx - tr.ax, tr.by - tr.ay, tr.bz - tr.az};
+    const double e2[3] = {tr.cx - tr.ax, tr.cy - tr.ay, tr.cz - tr.az};
+    const double r[3] = {cx - tr.ax, cy - tr.ay, cz - tr.az};
+    const double d11 = e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2];
+    const double d12 = e1[0] * e2[0] + e1[1] * e2[1] + e1[2] * e2[2];
+    const double d22 = e2[0] * e2[0] + e2[1] * e2[1] + e2[2] * e2[2];
+    const double r1 = r[0] * e1[0] + r[1] * e1[1] + r[2] * e1[2];
+    const double r2 = r[0] * e2[0] + r[1] * e2[1] + r[2] * e2[2];
+    const double det = d11 * d22 - d12 * d12;
+    const double l1 = det > 0 ? (d22 * r1 - d12 * r2) / det : 0;
+    const double l2 = det > 0 ? (d11 * r2 - d12 * r1) / det : 0;
+    const double l[3] = {1 - l1 - l2, l1, l2};
+    const double tol = 1e-4;
+    int small = 0, last_small = -1, last_large = -1;
+#pragma unroll
+    for (int v = 0; v < 3; v++) {
+        if (l[v] < tol) {
+            small++;
+            last_small = v;
+        } else {
+            last_large = v;
+        }
+    }
+    const double *n;
+    if (small == 0) {
+        n = m.face_n + 3 * (size_t)t;
+    } else if (small == 1) {
+        n = m.edge_n + 9 * (size_t)t + 3 * ((last_small + 1) % 3);
+    } else {
+        const int *s = last_large == 0 ? m.s0 : (last_large == 1 ? m.s1 : m.s2);
+        n = m.vertex_n + 3 * (size_t)__ldg(s + t);
+    }
+    const double dot = (qx - cx) * __ldg(n) + (qy - cy) * __ldg(n + 1) + (qz - cz) * __ldg(n + 2);
+    const double dist = sqrt(d2);
+    return dot < 0 ? -dist : dist;
+}
+
+// Writes one query's outputs from its double result (best, bid, bpos); `init` is the bound the
+// search started from (incoming value for the in/out outputs).
+__device__ void write_result(const QueryArgs &a, long long q, double qx, double qy, double qz, double best, int bid,
+                             int bpos) {
+    switch (a.output) {
+        case SSDF_OUT_EDF:
+            store_out(a, q, sqrt(best));
+            if (a.outtri && bid >= 0) a.outtri[q] = bid;
+            break;
+        case SSDF_OUT_SQEDF:
+            store_out(a, q, best);
+            break;
+        case SSDF_OUT_SDF: {
+            double cx, cy, cz;
+            const double v = bid >= 0 ? signed_distance(a.m, bpos, bid, qx, qy, qz, best, cx, cy, cz) : sqrt(best);
+            store_out(a, q, v);
+            if (a.outtri) a.outtri[q] = bid;
+            break;
+        }
+        case SSDF_OUT_CLOSEST: {
+            if (bid < 0) break;
+            const double dist = sqrt(best);
+            const double din = load_out(a, q);
+            const double dist_t = a.out_f64 ? dist : double(float(dist));
+            if (din > dist_t) {
+                const Tri64 tr = load_tri64(a.m.tris64, bpos);
+                double cx, cy, cz;
+                tri_closest_point_exact<double>(qx, qy, qz, tr.ax, tr.ay, tr.az, tr.bx, tr.by, tr.bz, tr.cx, tr.cy,
+                                                tr.cz, cx, cy, cz);
+                store_out(a, q, dist);
+                if (a.coord_f64) {
+                    ((double *)a.outx)[q] = cx, ((double *)a.outy)[q] = cy, ((double *)a.outz)[q] = cz;
+                } else {
+                    ((float *)a.outx)[q] = float(cx), ((float *)a.outy)[q] = float(cy), ((float *)a.outz)[q] = float(cz);
+                }
+                a.outtri[q] = bid;
+            }
+            break;
+        }
+        default:
+            break;
+    }
+}
+
+// Incoming bound of the search, as a squared distance in double.
+__device__ __forceinline__ double initial_bound(const QueryArgs &a, long long q) {
+    switch (a.output) {
+        case SSDF_OUT_EDF:
+        case SSDF_OUT_CLOSEST: {
+            const double o = load_out(a, q);
+            return o * o;
+        }
+        case SSDF_OUT_SQEDF:
+            return load_out(a, q);
+        default:
+            return dinf();
+    }
+}
+
+__device__ __forceinline__ void flush_counters(const QueryArgs &a, const Counters &c) {
+    unsigned long long t = c.tri, b = c.box, f = c.fix;
+    for (int o = 16; o > 0; o >>= 1) {
+        t += __shfl_xor_sync(0xffffffffu, t, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+        f += __shfl_xor_sync(0xffffffffu, f, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(a.counters + 0, t);
+        atomicAdd(a.counters + 1, b);
+        atomicAdd(a.counters + 2, f);
+    }
+}
+
+// ---- kernels ----------------------------------------------------------------------------------------
+
+template <bool COUNT>
+__global__ void __launch_bounds__(kThreads) k_query_f64(const QueryArgs a) {
+    long long q, i = 0, j = 0, k = 0;
+    const bool valid = map_thread(a, q, i, j, k);
+    Counters cnt;
+    if (valid) {
+        double qx, qy, qz;
+        query_point(a, q, i, j, k, qx, qy, qz);
+        double best = initial_bound(a, q);
+        int bid = -1, bpos = -1;
+        traverse_exact<double, COUNT>(a.m, qx, qy, qz, best, bid, bpos, cnt);
+        write_result(a, q, qx, qy, qz, best, bid, bpos);
+    }
+    if (COUNT) flush_counters(a, cnt);
+}
+
+// The reference's float arithmetic end to end (edf<float> value); in/out outputs only.
+template <bool COUNT>
+__global__ void __launch_bounds__(kThreads) k_query_f32(const QueryArgs a) {
+    long long q, i = 0, j = 0, k = 0;
+    const bool valid = map_thread(a, q, i, j, k);
+    Counters cnt;
+    if (valid) {
+        double qx, qy, qz;
+        query_point(a, q, i, j, k, qx, qy, qz);
+        const float o = a.out_f64 ? float(((const double *)a.out)[q]) : ((const float *)a.out)[q];
+        float best = a.output == SSDF_OUT_SQEDF ? o : o * o;
+        int bid = -1, bpos = -1;
+        traverse_exact<float, COUNT>(a.m, float(qx), float(qy), float(qz), best, bid, bpos, cnt);
+        if (a.output == SSDF_OUT_SQEDF) {
+            store_out(a, q, double(best));
+        } else {
+            store_out(a, q, double(sqrtf(best)));
+            if (a.outtri && bid >= 0) a.outtri[q] = bid;
+        }
+    }
+    if (COUNT) flush_counters(a, cnt);
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(kThreads) k_query_f32x(const QueryArgs a) {
+    long long q, i = 0, j = 0, k = 0;
+    const bool valid = map_thread(a, q, i, j, k);
+    Counters cnt;
+    if (valid) {
+        double qx, qy, qz;
+        query_point(a, q, i, j, k, qx, qy, qz);
+        const double init = initial_bound(a, q);
+        // float start bound rounded up, so no triangle closer in double is cut off
+        float best = init < dinf() ? __double2float_ru(init) : finf();
+        Window win;
+#pragma unroll
+        for (int s = 0; s < kCand; s++) win.d[s] = finf(), win.p[s] = -1;
+        win.evicted = finf();
+        float thr;
+        traverse_fast<COUNT>(a.m, float(qx), float(qy), float(qz), best, a.tau_rel, win, thr, cnt);
+        if (win.evicted < thr) {
+            const int slot = atomicAdd(a.fallback_count, 1);
+            a.fallback_ids[slot] = int(q);  // q < 2^31 is checked on the host
+        } else {
+            double b = init;
+            int bid = -1, bpos = -1;
+#pragma unroll
+            for (int s = 0; s < kCand; s++) {
+                if (win.d[s] < thr) {
+                    const Tri64 t = load_tri64(a.m.tris64, win.p[s]);
+                    const double d2 =
+                        tri_dist_sq_exact<double>(qx, qy, qz, t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
+                    if (COUNT) cnt.fix++;
+                    if (d2 < b || (d2 == b && bid >= 0 && t.id < bid)) {
+                        b = d2;
+                        bid = t.id;
+                        bpos = win.p[s];
+                    }
+                }
+            }
+            write_result(a, q, qx, qy, qz, b, bid, bpos);
+        }
+    }
+    if (COUNT) flush_counters(a, cnt);
+}
+
+// Queries whose F32X window overflowed, finished with the F64 traversal (grid-stride over the list).
+template <bool COUNT>
+__global__ void __launch_bounds__(kThreads) k_fallback(const QueryArgs a) {
+    const int n = *a.fallback_count;
+    Counters cnt;
+    for (int idx = blockIdx.x * kThreads + threadIdx.x; idx < n; idx += gridDim.x * kThreads) {
+        const long long q = a.fallback_ids[idx];
+        long long i = 0, j = 0, k = 0;
+        if (a.is_grid) grid_ijk(a, q, i, j, k);
+        double qx, qy, qz;
+        query_point(a, q, i, j, k, qx, qy, qz);
+        double best = initial_bound(a, q);
+        int bid = -1, bpos = -1;
+        traverse_exact<double, COUNT>(a.m, qx, qy, qz, best, bid, bpos, cnt);
+        write_result(a, q, qx, qy, qz, best, bid, bpos);
+    }
+    if (COUNT) flush_counters(a, cnt);
+}
+
+thread_local unsigned long long t_last_counts[4] = {0, 0, 0, 0};
+
+}  // namespace
+
+int query_counts(int64_t *tri, int64_t *box, int64_t *fix, int64_t *fallback) {
+    if (tri) *tri = (int64_t)t_last_counts[0];
+    if (box) *box = (int64_t)t_last_counts[1];
+    if (fix) *fix = (int64_t)t_last_counts[2];
+    if (fallback) *fallback = (int64_t)t_last_counts[3];
+    return SSDF_OK;
+}
+
+int launch_query(const QueryArgs &args_in, int precision, cudaStream_t stream) {
+    QueryArgs a = args_in;
+    const long long n = a.is_grid ? a.nx * a.ny * a.nz : a.npoints;
+    if (n <= 0) return SSDF_OK;
+    if (precision == SSDF_PREC_F64 && !a.m.nodes64)
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "mesh built without double data (keep_fp64=0)");
+    if (precision == SSDF_PREC_F32_FIXUP && !a.m.tris64)
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "fix-up queries need the double triangles (keep_fp64=1)");
+    if (a.output == SSDF_OUT_SDF && !a.m.face_n)
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "signed queries need a mesh built with normals=1");
+    if (a.output == SSDF_OUT_SDF && !a.m.tris64)
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "signed queries need the double triangles (keep_fp64=1)");
+    if (a.output == SSDF_OUT_CLOSEST && (!a.m.tris64 || !a.outx || !a.outy || !a.outz || !a.outtri))
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "closest-point queries need outx/outy/outz/outtri and double data");
+    if (precision == SSDF_PREC_F32 && (a.output == SSDF_OUT_SDF || a.output == SSDF_OUT_CLOSEST))
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "SSDF_PREC_F32 serves the edf and sqedf outputs");
+    const bool count = env_int("SSDF_B200_COUNT", 0) != 0;
+    long long nblocks;
+    if (a.is_grid)
+        nblocks = ((a.nx + 7) / 8) * ((a.ny + 3) / 4) * ((a.nz + 3) / 4);
+    else
+        nblocks = (n + kThreads - 1) / kThreads;
+    if (nblocks > 0x7fffffffll) return fail(SSDF_ERR_NOT_SUPPORTED, "too many queries in one launch");
+    unsigned long long *counters = nullptr;
+    int *fb = nullptr;
+    int st = SSDF_OK;
+    if (count) {
+        SSDF_CUDA(cudaMallocAsync(&counters, 4 * sizeof(unsigned long long), stream));
+        SSDF_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(unsigned long long), stream));
+    }
+    a.counters = counters;
+    if (precision == SSDF_PREC_F32_FIXUP) {
+        if (n >= 0x7fffffffll) {
+            st = fail(SSDF_ERR_NOT_SUPPORTED, "more than 2^31 - 1 queries in one fix-up launch");
+        } else if (cudaMallocAsync(&fb, sizeof(int) * size_t(n + 1), stream) != cudaSuccess) {
+            st = fail(SSDF_ERR_OUT_OF_MEMORY, "fix-up overflow list");
+        } else {
+            a.fallback_count = fb;
+            a.fallback_ids = fb + 1;
+            cudaMemsetAsync(fb, 0, sizeof(int), stream);
+            if (count)
+                k_query_f32x<true><<<unsigned(nblocks), kThreads, 0, stream>>>(a);
+            else
+                k_query_f32x<false><<<unsigned(nblocks), kThreads, 0, stream>>>(a);
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) st = cuda_fail(e, "k_query_f32x", __FILE__, __LINE__);
+            if (st == SSDF_OK && a.m.nodes64) {
+                if (count)
+                    k_fallback<true><<<296, kThreads, 0, stream>>>(a);
+                else
+                    k_fallback<false><<<296, kThreads, 0, stream>>>(a);
+                e = cudaGetLastError();
+                if (e != cudaSuccess) st = cuda_fail(e, "k_fallback", __FILE__, __LINE__);
+            } else if (st == SSDF_OK) {
+                st = fail(SSDF_ERR_INVALID_ARGUMENT, "fix-up queries need the double BVH (keep_fp64=1)");
+            }
+        }
+    } else if (precision == SSDF_PREC_F64) {
+        if (count)
+            k_query_f64<true><<<unsigned(nblocks), kThreads, 0, stream>>>(a);
+        else
+            k_query_f64<false><<<unsigned(nblocks), kThreads, 0, stream>>>(a);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) st = cuda_fail(e, "k_query_f64", __FILE__, __LINE__);
+    } else {
+        if (count)
+            k_query_f32<true><<<unsigned(nblocks), kThreads, 0, stream>>>(a);
+        else
+            k_query_f32<false><<<unsigned(nblocks), kThreads, 0, stream>>>(a);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) st = cuda_fail(e, "k_query_f32", __FILE__, __LINE__);
+    }
+    if (count && st == SSDF_OK) {
+        unsigned long long h[4] = {0, 0, 0, 0};
+        int nfb = 0;
+        cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, stream);
+        if (fb) cudaMemcpyAsync(&nfb, fb, sizeof(int), cudaMemcpyDeviceToHost, stream);
+        cudaError_t e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) st = cuda_fail(e, "query counters", __FILE__, __LINE__);
+        h[3] = (unsigned long long)nfb;
+        memcpy(t_last_counts, h, sizeof(h));
+    }
+    if (fb) cudaFreeAsync(fb, stream);
+    if (counters) cudaFreeAsync(counters, stream);
+    return st;
+}
+
+}  // namespace ssdf_b200

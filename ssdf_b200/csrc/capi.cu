@@ -1,0 +1,509 @@
+// capi.cu -- the exported C ABI (include/ssdf_b200.h): drop-in entry points over host arrays,
+// the device-resident mesh handle API, status codes and error messages.
+//
+// Host-array entry points follow the reference's contract (serial/ssdf.hpp:447-460,
+// serial/bvh/bvh.hpp:19-227): blocking, caller owns every buffer, scratch freed before return,
+// `out` in/out where the reference's is. They stage through device memory on a per-thread
+// non-blocking stream. No entry point aborts: failures return a status and set a message.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+struct ssdf_mesh {
+    ssdf_b200::DeviceMesh m;
+    ssdf_b200::MeshStorage *storage = nullptr;
+    int device = 0;
+};
+
+namespace ssdf_b200 {
+
+int query_counts(int64_t *tri, int64_t *box, int64_t *fix, int64_t *fallback);
+
+namespace {
+thread_local std::string t_error;
+thread_local cudaStream_t t_stream = nullptr;
+thread_local int t_stream_device = -1;
+}  // namespace
+
+void set_error(const std::string &msg) { t_error = msg; }
+
+int fail(int status, const std::string &msg) {
+    t_error = msg;
+    return status;
+}
+
+int cuda_fail(cudaError_t err, const char *what, const char *file, int line) {
+    const char *base = strrchr(file, '/');
+    t_error = std::string(what) + ": " + cudaGetErrorString(err) + " (" + (base ? base + 1 : file) + ":" +
+              std::to_string(line) + ")";
+    return err == cudaErrorMemoryAllocation ? SSDF_ERR_OUT_OF_MEMORY : SSDF_ERR_CUDA;
+}
+
+int env_int(const char *name, int dflt) {
+    const char *v = getenv(name);
+    return v ? atoi(v) : dflt;
+}
+
+const char *env_str(const char *name) { return getenv(name); }
+
+cudaStream_t library_stream() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    if (!t_stream || t_stream_device != dev) {
+        cudaStream_t s = nullptr;
+        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+        t_stream = s;
+        t_stream_device = dev;
+    }
+    return t_stream;
+}
+
+namespace {
+
+// Device buffer list freed (stream-ordered) when it goes out of scope.
+struct Scratch {
+    cudaStream_t stream;
+    std::vector<void *> ptrs;
+    explicit Scratch(cudaStream_t s) : stream(s) {}
+    ~Scratch() {
+        for (void *p : ptrs) cudaFreeAsync(p, stream);
+        cudaStreamSynchronize(stream);
+    }
+    int alloc(void **p, size_t bytes) {
+        cudaError_t e = cudaMallocAsync(p, bytes ? bytes : 16, stream);
+        if (e != cudaSuccess) return fail(SSDF_ERR_OUT_OF_MEMORY, "device allocation of " + std::to_string(bytes) + " bytes");
+        ptrs.push_back(*p);
+        return SSDF_OK;
+    }
+    int upload(void **dst, const void *src, size_t bytes) {
+        SSDF_CHECK(alloc(dst, bytes));
+        SSDF_CUDA(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, stream));
+        return SSDF_OK;
+    }
+};
+
+int ready_stream(cudaStream_t *s) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0)
+        return fail(SSDF_ERR_CUDA, std::string("no usable CUDA device: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "none"));
+    *s = library_stream();
+    if (!*s) return fail(SSDF_ERR_CUDA, "could not create the library stream");
+    return SSDF_OK;
+}
+
+int check_mesh_host(ptrdiff_t nt, const int *s0, const int *s1, const int *s2, ptrdiff_t nv, const void *sx,
+                    const void *sy, const void *sz) {
+    if (nt < 0 || nv < 0) return fail(SSDF_ERR_INVALID_ARGUMENT, "negative mesh size");
+    if (nt > 0 && (!s0 || !s1 || !s2)) return fail(SSDF_ERR_INVALID_ARGUMENT, "null triangle index array");
+    if (nv > 0 && (!sx || !sy || !sz)) return fail(SSDF_ERR_INVALID_ARGUMENT, "null vertex coordinate array");
+    for (ptrdiff_t t = 0; t < nt; t++) {
+        if (s0[t] < 0 || s0[t] >= nv || s1[t] < 0 || s1[t] >= nv || s2[t] < 0 || s2[t] >= nv)
+            return fail(SSDF_ERR_INVALID_ARGUMENT,
+                        "triangle " + std::to_string(t) + " has a vertex index outside [0, " + std::to_string(nv) + ")");
+    }
+    return SSDF_OK;
+}
+
+int precision_from_env(int dflt) {
+    const char *v = env_str("SSDF_B200_PRECISION");
+    if (!v) return dflt;
+    if (!strcmp(v, "f64")) return SSDF_PREC_F64;
+    if (!strcmp(v, "f32")) return SSDF_PREC_F32;
+    if (!strcmp(v, "f32x") || !strcmp(v, "fixup")) return SSDF_PREC_F32_FIXUP;
+    return dflt;
+}
+
+float tau_rel_from_env() {
+    const char *v = env_str("SSDF_B200_TAU");
+    const float t = v ? float(atof(v)) : 0.f;
+    return t > 0.f ? t : 1.0f / 65536.0f;
+}
+
+ssdf_build_opts build_opts_for(int precision, int output) {
+    ssdf_build_opts o;
+    o.leaf_size = env_int("SSDF_B200_LEAF", 0);
+    o.keep_fp64 = (precision != SSDF_PREC_F32 || output == SSDF_OUT_SDF || output == SSDF_OUT_CLOSEST) ? 1 : 0;
+    o.normals = output == SSDF_OUT_SDF ? 1 : 0;
+    o.treelet_opt = env_int("SSDF_B200_TREELET", 0);
+    return o;
+}
+
+struct MeshGuard {
+    ssdf_mesh *mesh = nullptr;
+    ~MeshGuard() {
+        if (mesh) ssdf_mesh_destroy(mesh);
+    }
+};
+
+// The BVH entry points over host arrays: build, upload, query, download.
+template <typename G, typename T>
+int bvh_points_host(ptrdiff_t npoints, const G *x, const G *y, const G *z, ptrdiff_t nt, const int *s0, const int *s1,
+                    const int *s2, ptrdiff_t nv, const G *sx, const G *sy, const G *sz, T *out, int *outtri, G *outx,
+                    G *outy, G *outz, int output, int precision) {
+    if (npoints < 0) return fail(SSDF_ERR_INVALID_ARGUMENT, "negative npoints");
+    SSDF_CHECK(check_mesh_host(nt, s0, s1, s2, nv, sx, sy, sz));
+    if (nt == 0 || nv == 0 || npoints == 0) return SSDF_OK;
+    if (!x || !y || !z || !out) return fail(SSDF_ERR_INVALID_ARGUMENT, "null point or output array");
+    cudaStream_t stream;
+    SSDF_CHECK(ready_stream(&stream));
+    const int cf = sizeof(G) == 8 ? SSDF_F64 : SSDF_F32;
+    MeshGuard mg;
+    const ssdf_build_opts bo = build_opts_for(precision, output);
+    SSDF_CHECK(ssdf_mesh_create(&mg.mesh, nt, s0, s1, s2, nv, sx, sy, sz, cf, 0, &bo, stream));
+    Scratch sc(stream);
+    void *dx, *dy, *dz, *dout, *dtri = nullptr, *dox = nullptr, *doy = nullptr, *doz = nullptr;
+    const size_t gb = sizeof(G) * size_t(npoints), tb = sizeof(T) * size_t(npoints), ib = sizeof(int) * size_t(npoints);
+    SSDF_CHECK(sc.upload(&dx, x, gb));
+    SSDF_CHECK(sc.upload(&dy, y, gb));
+    SSDF_CHECK(sc.upload(&dz, z, gb));
+    if (output == SSDF_OUT_SDF) SSDF_CHECK(sc.alloc(&dout, tb));
+    else SSDF_CHECK(sc.upload(&dout, out, tb));
+    if (outtri) {
+        if (output == SSDF_OUT_SDF) SSDF_CHECK(sc.alloc(&dtri, ib));
+        else SSDF_CHECK(sc.upload(&dtri, outtri, ib));
+    }
+    if (output == SSDF_OUT_CLOSEST) {
+        SSDF_CHECK(sc.upload(&dox, outx, gb));
+        SSDF_CHECK(sc.upload(&doy, outy, gb));
+        SSDF_CHECK(sc.upload(&doz, outz, gb));
+    }
+    ssdf_query_opts qo;
+    memset(&qo, 0, sizeof(qo));
+    qo.precision = precision;
+    qo.output = output;
+    qo.coord_type = cf;
+    qo.out_type = sizeof(T) == 8 ? SSDF_F64 : SSDF_F32;
+    SSDF_CHECK(ssdf_query_points(mg.mesh, npoints, dx, dy, dz, dout, (int *)dtri, dox, doy, doz, &qo, stream));
+    SSDF_CUDA(cudaMemcpyAsync(out, dout, tb, cudaMemcpyDeviceToHost, stream));
+    if (outtri) SSDF_CUDA(cudaMemcpyAsync(outtri, dtri, ib, cudaMemcpyDeviceToHost, stream));
+    if (output == SSDF_OUT_CLOSEST) {
+        SSDF_CUDA(cudaMemcpyAsync(outx, dox, gb, cudaMemcpyDeviceToHost, stream));
+        SSDF_CUDA(cudaMemcpyAsync(outy, doy, gb, cudaMemcpyDeviceToHost, stream));
+        SSDF_CUDA(cudaMemcpyAsync(outz, doz, gb, cudaMemcpyDeviceToHost, stream));
+    }
+    SSDF_CUDA(cudaStreamSynchronize(stream));
+    return SSDF_OK;
+}
+
+template <typename G, typename T>
+int bvh_grid_host(ptrdiff_t nt, const int *s0, const int *s1, const int *s2, ptrdiff_t nv, const G *sx, const G *sy,
+                  const G *sz, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, G xmin, G ymin, G zmin, G xmax, G ymax,
+                  G zmax, T *out, int *outtri, int output, int precision) {
+    if (nx < 0 || ny < 0 || nz < 0) return fail(SSDF_ERR_INVALID_ARGUMENT, "negative grid size");
+    SSDF_CHECK(check_mesh_host(nt, s0, s1, s2, nv, sx, sy, sz));
+    const long long n = (long long)nx * ny * nz;
+    if (nt == 0 || nv == 0 || n == 0) return SSDF_OK;
+    if (!out) return fail(SSDF_ERR_INVALID_ARGUMENT, "null output array");
+    cudaStream_t stream;
+    SSDF_CHECK(ready_stream(&stream));
+    const int cf = sizeof(G) == 8 ? SSDF_F64 : SSDF_F32;
+    MeshGuard mg;
+    const ssdf_build_opts bo = build_opts_for(precision, output);
+    SSDF_CHECK(ssdf_mesh_create(&mg.mesh, nt, s0, s1, s2, nv, sx, sy, sz, cf, 0, &bo, stream));
+    Scratch sc(stream);
+    void *dout, *dtri = nullptr;
+    const size_t tb = sizeof(T) * size_t(n);
+    if (output == SSDF_OUT_SDF) SSDF_CHECK(sc.alloc(&dout, tb));
+    else SSDF_CHECK(sc.upload(&dout, out, tb));
+    if (outtri) SSDF_CHECK(sc.alloc(&dtri, sizeof(int) * size_t(n)));
+    ssdf_query_opts qo;
+    memset(&qo, 0, sizeof(qo));
+    qo.precision = precision;
+    qo.output = output;
+    qo.coord_type = cf;
+    qo.out_type = sizeof(T) == 8 ? SSDF_F64 : SSDF_F32;
+    const double lo[3] = {double(xmin), double(ymin), double(zmin)}, hi[3] = {double(xmax), double(ymax), double(zmax)};
+    SSDF_CHECK(ssdf_query_grid(mg.mesh, nx, ny, nz, lo, hi, dout, (int *)dtri, &qo, stream));
+    SSDF_CUDA(cudaMemcpyAsync(out, dout, tb, cudaMemcpyDeviceToHost, stream));
+    if (outtri) SSDF_CUDA(cudaMemcpyAsync(outtri, dtri, sizeof(int) * size_t(n), cudaMemcpyDeviceToHost, stream));
+    SSDF_CUDA(cudaStreamSynchronize(stream));
+    return SSDF_OK;
+}
+
+// edf / edf_celllist over host arrays (G == T).
+template <typename T>
+int dense_host(int celllist, ptrdiff_t npoints, const T *x, const T *y, const T *z, ptrdiff_t nt, const int *s0,
+               const int *s1, const int *s2, ptrdiff_t nv, const T *sx, const T *sy, const T *sz, T *out,
+               int *outtri) {
+    if (npoints < 0) return fail(SSDF_ERR_INVALID_ARGUMENT, "negative npoints");
+    SSDF_CHECK(check_mesh_host(nt, s0, s1, s2, nv, sx, sy, sz));
+    if (nt == 0 || nv == 0 || npoints == 0) return SSDF_OK;
+    if (!x || !y || !z || !out) return fail(SSDF_ERR_INVALID_ARGUMENT, "null point or output array");
+    cudaStream_t stream;
+    SSDF_CHECK(ready_stream(&stream));
+    Scratch sc(stream);
+    void *dx, *dy, *dz, *dout, *ds0, *ds1, *ds2, *dsx, *dsy, *dsz, *dtri = nullptr;
+    const size_t pb = sizeof(T) * size_t(npoints), vb = sizeof(T) * size_t(nv), ib = sizeof(int) * size_t(nt);
+    SSDF_CHECK(sc.upload(&dx, x, pb));
+    SSDF_CHECK(sc.upload(&dy, y, pb));
+    SSDF_CHECK(sc.upload(&dz, z, pb));
+    SSDF_CHECK(sc.upload(&dout, out, pb));
+    SSDF_CHECK(sc.upload(&ds0, s0, ib));
+    SSDF_CHECK(sc.upload(&ds1, s1, ib));
+    SSDF_CHECK(sc.upload(&ds2, s2, ib));
+    SSDF_CHECK(sc.upload(&dsx, sx, vb));
+    SSDF_CHECK(sc.upload(&dsy, sy, vb));
+    SSDF_CHECK(sc.upload(&dsz, sz, vb));
+    if (outtri) SSDF_CHECK(sc.upload(&dtri, outtri, sizeof(int) * size_t(npoints)));
+    const int f64 = sizeof(T) == 8;
+    if (celllist)
+        SSDF_CHECK(celllist_edf(f64, npoints, dx, dy, dz, nt, (int *)ds0, (int *)ds1, (int *)ds2, nv, dsx, dsy, dsz, dout,
+                                (int *)dtri, stream));
+    else
+        SSDF_CHECK(brute_force_edf(f64, npoints, dx, dy, dz, nt, (int *)ds0, (int *)ds1, (int *)ds2, nv, dsx, dsy, dsz,
+                                   dout, (int *)dtri, stream));
+    SSDF_CUDA(cudaMemcpyAsync(out, dout, pb, cudaMemcpyDeviceToHost, stream));
+    if (outtri) SSDF_CUDA(cudaMemcpyAsync(outtri, dtri, sizeof(int) * size_t(npoints), cudaMemcpyDeviceToHost, stream));
+    SSDF_CUDA(cudaStreamSynchronize(stream));
+    return SSDF_OK;
+}
+
+// ssdf::edf_select (serial/ssdf.hpp:965-1016), same environment variables; the BVH is this
+// build's default, as it is the reference's in its cuBQL build.
+template <typename T>
+int edf_select_host(ptrdiff_t npoints, const T *x, const T *y, const T *z, ptrdiff_t nt, const int *s0, const int *s1,
+                    const int *s2, ptrdiff_t nv, const T *sx, const T *sy, const T *sz, T *out) {
+    if (env_int("SSDF_USE_BVH", 1)) {
+        const int prec = precision_from_env(sizeof(T) == 8 ? SSDF_PREC_F32_FIXUP : SSDF_PREC_F32);
+        return bvh_points_host<T, T>(npoints, x, y, z, nt, s0, s1, s2, nv, sx, sy, sz, out, nullptr, nullptr, nullptr,
+                                     nullptr, SSDF_OUT_EDF, prec);
+    }
+    if (env_int("SSDF_CELL_VALIDATE", 0)) {
+        if (npoints < 0 || (npoints > 0 && !out)) return fail(SSDF_ERR_INVALID_ARGUMENT, "null output array");
+        std::vector<T> ref(out, out + npoints), test(out, out + npoints);
+        SSDF_CHECK(dense_host<T>(0, npoints, x, y, z, nt, s0, s1, s2, nv, sx, sy, sz, ref.data(), nullptr));
+        SSDF_CHECK(dense_host<T>(1, npoints, x, y, z, nt, s0, s1, s2, nv, sx, sy, sz, test.data(), nullptr));
+        T max_diff = 0, diff_norm = 0;
+        for (ptrdiff_t i = 0; i < npoints; ++i) {
+            const T rel = std::abs(ref[i] - test[i]) / (std::abs(ref[i]) + T(1e-16));
+            max_diff = std::max<T>(max_diff, rel);
+            diff_norm += rel * rel;
+        }
+        if (max_diff > T(1e-5)) {
+            fprintf(stderr, "EDF cell-list validation max rel diff: %g\n", double(max_diff));
+            fprintf(stderr, "EDF cell-list validation rel diff norm: %g\n", double(std::sqrt(diff_norm)));
+        }
+        std::copy(test.begin(), test.end(), out);
+        return SSDF_OK;
+    }
+    return dense_host<T>(env_int("SSDF_USE_CELL_LIST", 1) ? 1 : 0, npoints, x, y, z, nt, s0, s1, s2, nv, sx, sy, sz,
+                         out, nullptr);
+}
+
+}  // namespace
+}  // namespace ssdf_b200
+
+using namespace ssdf_b200;
+
+extern "C" {
+
+const char *ssdf_status_string(int status) {
+    switch (status) {
+        case SSDF_OK: return "SSDF_OK";
+        case SSDF_ERR_INVALID_ARGUMENT: return "SSDF_ERR_INVALID_ARGUMENT";
+        case SSDF_ERR_OUT_OF_MEMORY: return "SSDF_ERR_OUT_OF_MEMORY";
+        case SSDF_ERR_CUDA: return "SSDF_ERR_CUDA";
+        case SSDF_ERR_NOT_SUPPORTED: return "SSDF_ERR_NOT_SUPPORTED";
+        case SSDF_ERR_INTERNAL: return "SSDF_ERR_INTERNAL";
+        default: return "SSDF_ERR_UNKNOWN";
+    }
+}
+
+const char *ssdf_last_error(void) { return t_error.c_str(); }
+
+const char *ssdf_b200_version(void) { return "ssdf_b200 0.1 (sm_100a)"; }
+
+#define EDF_ARGS(G, T)                                                                                            \
+    ptrdiff_t npoints, const G *x, const G *y, const G *z, ptrdiff_t nselements, const int *s0, const int *s1,    \
+        const int *s2, ptrdiff_t nspoints, const G *sx, const G *sy, const G *sz, T *out
+#define EDF_PASS npoints, x, y, z, nselements, s0, s1, s2, nspoints, sx, sy, sz, out
+
+int ssdf_edf_f(EDF_ARGS(float, float)) { return edf_select_host<float>(EDF_PASS); }
+int ssdf_edf_d(EDF_ARGS(double, double)) { return edf_select_host<double>(EDF_PASS); }
+
+int ssdf_b200_edf_ff(EDF_ARGS(float, float)) { return dense_host<float>(0, EDF_PASS, nullptr); }
+int ssdf_b200_edf_dd(EDF_ARGS(double, double)) { return dense_host<double>(0, EDF_PASS, nullptr); }
+int ssdf_b200_edf_celllist_ff(EDF_ARGS(float, float)) { return dense_host<float>(1, EDF_PASS, nullptr); }
+int ssdf_b200_edf_celllist_dd(EDF_ARGS(double, double)) { return dense_host<double>(1, EDF_PASS, nullptr); }
+
+int ssdf_b200_edf_bvh_ff(EDF_ARGS(float, float)) {
+    return bvh_points_host<float, float>(EDF_PASS, nullptr, nullptr, nullptr, nullptr, SSDF_OUT_EDF,
+                                         precision_from_env(SSDF_PREC_F32));
+}
+int ssdf_b200_edf_bvh_fd(EDF_ARGS(float, double)) {
+    return bvh_points_host<float, double>(EDF_PASS, nullptr, nullptr, nullptr, nullptr, SSDF_OUT_EDF,
+                                          precision_from_env(SSDF_PREC_F32_FIXUP));
+}
+int ssdf_b200_edf_bvh_dd(EDF_ARGS(double, double)) {
+    return bvh_points_host<double, double>(EDF_PASS, nullptr, nullptr, nullptr, nullptr, SSDF_OUT_EDF,
+                                           precision_from_env(SSDF_PREC_F32_FIXUP));
+}
+
+int ssdf_b200_edf_index_dd(EDF_ARGS(double, double), int *outtri) {
+    return bvh_points_host<double, double>(EDF_PASS, outtri, nullptr, nullptr, nullptr, SSDF_OUT_EDF,
+                                           precision_from_env(SSDF_PREC_F32_FIXUP));
+}
+int ssdf_b200_edf_index_ff(EDF_ARGS(float, float), int *outtri) {
+    return bvh_points_host<float, float>(EDF_PASS, outtri, nullptr, nullptr, nullptr, SSDF_OUT_EDF,
+                                         precision_from_env(SSDF_PREC_F32));
+}
+int ssdf_b200_sdf_points_dd(EDF_ARGS(double, double), int *outtri) {
+    return bvh_points_host<double, double>(EDF_PASS, outtri, nullptr, nullptr, nullptr, SSDF_OUT_SDF,
+                                           precision_from_env(SSDF_PREC_F32_FIXUP));
+}
+
+int ssdf_b200_closest_point_bvh_ff(ptrdiff_t npoints, const float *x, const float *y, const float *z,
+                                   ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                   ptrdiff_t nspoints, const float *sx, const float *sy, const float *sz, float *outd,
+                                   float *outx, float *outy, float *outz, int *outtri) {
+    if (npoints > 0 && nselements > 0 && (!outx || !outy || !outz || !outtri))
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "null closest-point output array");
+    return bvh_points_host<float, float>(npoints, x, y, z, nselements, s0, s1, s2, nspoints, sx, sy, sz, outd, outtri,
+                                         outx, outy, outz, SSDF_OUT_CLOSEST, precision_from_env(SSDF_PREC_F32_FIXUP));
+}
+int ssdf_b200_closest_point_bvh_dd(ptrdiff_t npoints, const double *x, const double *y, const double *z,
+                                   ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                   ptrdiff_t nspoints, const double *sx, const double *sy, const double *sz,
+                                   double *outd, double *outx, double *outy, double *outz, int *outtri) {
+    if (npoints > 0 && nselements > 0 && (!outx || !outy || !outz || !outtri))
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "null closest-point output array");
+    return bvh_points_host<double, double>(npoints, x, y, z, nselements, s0, s1, s2, nspoints, sx, sy, sz, outd,
+                                           outtri, outx, outy, outz, SSDF_OUT_CLOSEST,
+                                           precision_from_env(SSDF_PREC_F32_FIXUP));
+}
+
+#define GRID_ARGS(G, T)                                                                                           \
+    ptrdiff_t nselements, const int *s0, const int *s1, const int *s2, ptrdiff_t nspoints, const G *sx,           \
+        const G *sy, const G *sz, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, G xmin, G ymin, G zmin, G xmax, G ymax, \
+        G zmax, T *out
+#define GRID_PASS nselements, s0, s1, s2, nspoints, sx, sy, sz, nx, ny, nz, xmin, ymin, zmin, xmax, ymax, zmax, out
+
+int ssdf_b200_sample_sqedf_bvh_ff(GRID_ARGS(float, float)) {
+    return bvh_grid_host<float, float>(GRID_PASS, nullptr, SSDF_OUT_SQEDF, precision_from_env(SSDF_PREC_F32));
+}
+int ssdf_b200_sample_sqedf_bvh_dd(GRID_ARGS(double, double)) {
+    return bvh_grid_host<double, double>(GRID_PASS, nullptr, SSDF_OUT_SQEDF, precision_from_env(SSDF_PREC_F32_FIXUP));
+}
+int ssdf_b200_sample_sdf_bvh_ff(GRID_ARGS(float, float)) {
+    return bvh_grid_host<float, float>(GRID_PASS, nullptr, SSDF_OUT_SDF, precision_from_env(SSDF_PREC_F32_FIXUP));
+}
+int ssdf_b200_sample_sdf_bvh_dd(GRID_ARGS(double, double)) {
+    return bvh_grid_host<double, double>(GRID_PASS, nullptr, SSDF_OUT_SDF, precision_from_env(SSDF_PREC_F32_FIXUP));
+}
+int ssdf_b200_sample_sdf_index_bvh_dd(GRID_ARGS(double, double), int *outtri) {
+    return bvh_grid_host<double, double>(GRID_PASS, outtri, SSDF_OUT_SDF, precision_from_env(SSDF_PREC_F32_FIXUP));
+}
+
+// ---- handle API ---------------------------------------------------------------------------------------
+
+int ssdf_mesh_create(ssdf_mesh **mesh, ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                     ptrdiff_t nspoints, const void *sx, const void *sy, const void *sz, int coord_type,
+                     int device_ptrs, const ssdf_build_opts *opts, void *stream) {
+    if (!mesh) return fail(SSDF_ERR_INVALID_ARGUMENT, "null mesh handle pointer");
+    *mesh = nullptr;
+    if (coord_type != SSDF_F32 && coord_type != SSDF_F64) return fail(SSDF_ERR_INVALID_ARGUMENT, "bad coord_type");
+    ssdf_build_opts o;
+    if (opts) {
+        o = *opts;
+    } else {
+        o.leaf_size = 0, o.keep_fp64 = 1, o.normals = 1, o.treelet_opt = 0;
+    }
+    if (!device_ptrs) SSDF_CHECK(check_mesh_host(nselements, s0, s1, s2, nspoints, sx, sy, sz));
+    cudaStream_t s = (cudaStream_t)stream;
+    ssdf_mesh *h = new ssdf_mesh();
+    cudaGetDevice(&h->device);
+    const int st = mesh_build(&h->storage, &h->m, nselements, s0, s1, s2, nspoints, sx, sy, sz,
+                              coord_type == SSDF_F64, device_ptrs, o, s);
+    if (st != SSDF_OK) {
+        delete h;
+        return st;
+    }
+    *mesh = h;
+    return SSDF_OK;
+}
+
+int ssdf_mesh_destroy(ssdf_mesh *mesh) {
+    if (!mesh) return SSDF_OK;
+    mesh_free(mesh->storage);
+    delete mesh;
+    return SSDF_OK;
+}
+
+int ssdf_mesh_stats(const ssdf_mesh *mesh, int64_t *nodes, int64_t *leaves, int64_t *depth, int64_t *bytes) {
+    if (!mesh) return fail(SSDF_ERR_INVALID_ARGUMENT, "null mesh");
+    if (nodes) *nodes = mesh->m.nnodes;
+    if (leaves) *leaves = mesh->m.nleaves;
+    if (depth) *depth = mesh->m.depth;
+    if (bytes) *bytes = (int64_t)mesh_bytes(mesh->storage);
+    return SSDF_OK;
+}
+
+static int fill_query(const ssdf_mesh *mesh, const ssdf_query_opts *opts, QueryArgs *a) {
+    if (!mesh) return fail(SSDF_ERR_INVALID_ARGUMENT, "null mesh");
+    if (!opts) return fail(SSDF_ERR_INVALID_ARGUMENT, "null query options");
+    if (opts->output < SSDF_OUT_EDF || opts->output > SSDF_OUT_CLOSEST) return fail(SSDF_ERR_INVALID_ARGUMENT, "bad output");
+    if (opts->precision < SSDF_PREC_F32 || opts->precision > SSDF_PREC_F32_FIXUP)
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "bad precision");
+    memset(a, 0, sizeof(*a));
+    a->m = mesh->m;
+    a->output = opts->output;
+    a->coord_f64 = opts->coord_type == SSDF_F64;
+    a->out_f64 = opts->out_type == SSDF_F64;
+    a->tau_rel = tau_rel_from_env();
+    return SSDF_OK;
+}
+
+int ssdf_query_points(ssdf_mesh *mesh, ptrdiff_t npoints, const void *x, const void *y, const void *z, void *out,
+                      int *outtri, void *outx, void *outy, void *outz, const ssdf_query_opts *opts, void *stream) {
+    QueryArgs a;
+    SSDF_CHECK(fill_query(mesh, opts, &a));
+    if (npoints < 0) return fail(SSDF_ERR_INVALID_ARGUMENT, "negative npoints");
+    if (npoints == 0) return SSDF_OK;
+    if (!x || !y || !z || !out) return fail(SSDF_ERR_INVALID_ARGUMENT, "null point or output array");
+    a.is_grid = 0;
+    a.npoints = npoints;
+    a.x = x, a.y = y, a.z = z;
+    a.out = out;
+    a.outtri = outtri;
+    a.outx = outx, a.outy = outy, a.outz = outz;
+    return launch_query(a, opts->precision, (cudaStream_t)stream);
+}
+
+int ssdf_query_grid(ssdf_mesh *mesh, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, const double lo[3], const double hi[3],
+                    void *out, int *outtri, const ssdf_query_opts *opts, void *stream) {
+    QueryArgs a;
+    SSDF_CHECK(fill_query(mesh, opts, &a));
+    if (nx < 0 || ny < 0 || nz < 0) return fail(SSDF_ERR_INVALID_ARGUMENT, "negative grid size");
+    if ((long long)nx * ny * nz == 0) return SSDF_OK;
+    if (!lo || !hi || !out) return fail(SSDF_ERR_INVALID_ARGUMENT, "null grid bounds or output array");
+    if (opts->output == SSDF_OUT_CLOSEST) return fail(SSDF_ERR_INVALID_ARGUMENT, "closest-point output is for point lists");
+    a.is_grid = 1;
+    a.nx = nx, a.ny = ny, a.nz = nz;
+    const long long n[3] = {nx, ny, nz};
+    for (int d = 0; d < 3; d++) {
+        // h = (max - min) / (n - 1) in G precision (serial/bvh/bvh.cpp:1665-1667)
+        a.lo64[d] = lo[d];
+        a.h64[d] = n[d] > 1 ? (hi[d] - lo[d]) / double(n[d] - 1) : 0.0;
+        a.lo32[d] = float(lo[d]);
+        a.h32[d] = n[d] > 1 ? (float(hi[d]) - float(lo[d])) / float(n[d] - 1) : 0.f;
+    }
+    a.out = out;
+    a.outtri = outtri;
+    return launch_query(a, opts->precision, (cudaStream_t)stream);
+}
+
+int ssdf_last_query_counts(int64_t *triangle_tests, int64_t *box_tests, int64_t *fixup_queries,
+                           int64_t *fallback_queries) {
+    return query_counts(triangle_tests, box_tests, fixup_queries, fallback_queries);
+}
+
+}  // extern "C"

@@ -1,0 +1,136 @@
+// internal.h -- shared declarations of the library's host runtime and kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/ssdf_b200.h"
+
+namespace ssdf_b200 {
+
+// ---- error plumbing ------------------------------------------------------------------------------
+void set_error(const std::string &msg);
+int fail(int status, const std::string &msg);
+int cuda_fail(cudaError_t err, const char *what, const char *file, int line);
+
+#define SSDF_CUDA(call)                                                             \
+    do {                                                                            \
+        cudaError_t ssdf_err_ = (call);                                             \
+        if (ssdf_err_ != cudaSuccess)                                               \
+            return ::ssdf_b200::cuda_fail(ssdf_err_, #call, __FILE__, __LINE__);    \
+    } while (0)
+
+#define SSDF_CHECK(call)                           \
+    do {                                           \
+        int ssdf_st_ = (call);                     \
+        if (ssdf_st_ != SSDF_OK) return ssdf_st_;  \
+    } while (0)
+
+// ---- device layouts ------------------------------------------------------------------------------
+//
+// BVH: binary, child-box layout. Every internal node holds both children's boxes and references,
+// so one visit tests two boxes from one 64-byte (FP32) or 128-byte (FP64) record:
+//   FP32 node (4 x float4): (c0.lox, c0.hix, c0.loy, c0.hiy), (c1.lox, c1.hix, c1.loy, c1.hiy),
+//                           (c0.loz, c0.hiz, c1.loz, c1.hiz), (ref0, ref1, -, -) as int bits
+//   FP64 node (8 x double2): c0 x, c0 y, c0 z, c1 x, c1 y, c1 z as (lo, hi), (ref0, ref1) as
+//                            int bits, padding
+// A reference >= 0 is an internal node; < 0 is a leaf ~((first << 5) | (count - 1)) over the
+// triangle records in leaf order; kEmptyRef is an empty slot (its box is inverted).
+// Triangles in leaf order:
+//   FP32 record (3 x float4): (ax, ay, az, bx), (by, bz, cx, cy), (cz, id bits, -, -)
+//   FP64 record (5 x double2): (ax, ay), (az, bx), (by, bz), (cx, cy), (cz, id)
+// where id is the triangle's index in the caller's s0/s1/s2 and a, b, c its vertices s0, s1, s2.
+constexpr int kEmptyRef = -2147483647 - 1;  // INT_MIN
+constexpr int kLeafCountBits = 5;
+constexpr int kMaxLeafSize = 16;
+constexpr int kMaxTriangles = 1 << 26;
+constexpr int kStackSize = 64;
+
+__host__ __device__ inline int leaf_ref(int first, int count) { return ~((first << kLeafCountBits) | (count - 1)); }
+__host__ __device__ inline int leaf_first(int ref) { return (~ref) >> kLeafCountBits; }
+__host__ __device__ inline int leaf_count(int ref) { return ((~ref) & ((1 << kLeafCountBits) - 1)) + 1; }
+
+struct DeviceMesh {
+    int nt = 0;            // triangles
+    int nv = 0;            // vertices
+    int nnodes = 0;        // node records (>= 1)
+    int depth = 0;         // max internal-node depth of the BVH (root = 1)
+    int leaf_size = 4;
+    int nleaves = 0;
+    const float4 *nodes32 = nullptr;   // [4 * nnodes]
+    const double2 *nodes64 = nullptr;  // [8 * nnodes] or null
+    const float4 *tris32 = nullptr;    // [3 * nt], leaf order
+    const double2 *tris64 = nullptr;   // [5 * nt], leaf order, or null
+    // sign data, caller's triangle order
+    const int *s0 = nullptr, *s1 = nullptr, *s2 = nullptr;  // [nt]
+    const double *face_n = nullptr;    // [3 * nt]
+    const double *edge_n = nullptr;    // [9 * nt]
+    const double *vertex_n = nullptr;  // [3 * nv]
+    // scale of the coordinates (max |coordinate| over the mesh), for the fix-up window
+    float coord_scale = 0.f;
+};
+
+// Everything a query launch needs; built by the host entry points.
+struct QueryArgs {
+    DeviceMesh m;
+    int output;        // SSDF_OUT_*
+    int coord_f64;     // G == double
+    int out_f64;       // T == double
+    int is_grid;
+    long long npoints;
+    // point source
+    const void *x, *y, *z;
+    // grid source: nodes n, origin lo and spacing h in G precision (both views kept)
+    long long nx, ny, nz;
+    double lo64[3], h64[3];
+    float lo32[3], h32[3];
+    // outputs
+    void *out;
+    int *outtri;
+    void *outx, *outy, *outz;
+    // fix-up window: tau = tau_rel * (coord_scale + d)
+    float tau_rel;
+    // overflow list of the FP32 fix-up kernel, finished by the FP64 kernel
+    int *fallback_ids;
+    int *fallback_count;
+    // optional counters [4]: triangle tests, box tests, fix-up evaluations, fallbacks
+    unsigned long long *counters;
+};
+
+// ---- mesh build (mesh_build.cu) ------------------------------------------------------------------
+struct MeshStorage;  // owns the device allocations behind a DeviceMesh
+int mesh_build(MeshStorage **storage, DeviceMesh *mesh, ptrdiff_t nt, const int *s0, const int *s1, const int *s2,
+               ptrdiff_t nv, const void *sx, const void *sy, const void *sz, int coord_f64, int device_ptrs,
+               const ssdf_build_opts &opts, cudaStream_t stream);
+void mesh_free(MeshStorage *storage);
+size_t mesh_bytes(const MeshStorage *storage);
+
+// ---- radix sort (radix_sort.cu) ------------------------------------------------------------------
+// Stable LSD sort of (key, value) pairs on the device, keys of `key_bits` low bits. Scratch is
+// allocated on `stream` (stream-ordered).
+int radix_sort_pairs_u32(uint32_t *keys, int *vals, int n, int key_bits, cudaStream_t stream);
+int radix_sort_pairs_u64(uint64_t *keys, int *vals, int n, int key_bits, cudaStream_t stream);
+// Exclusive prefix sum of n ints (out may alias in).
+int exclusive_scan_i32(const int *in, int *out, int n, cudaStream_t stream);
+
+// ---- queries (bvh_query.cu) ----------------------------------------------------------------------
+int launch_query(const QueryArgs &args, int precision, cudaStream_t stream);
+
+// ---- brute force and cell list (brute_force.cu, celllist.cu) -------------------------------------
+int brute_force_edf(int f64, ptrdiff_t npoints, const void *x, const void *y, const void *z, ptrdiff_t nt,
+                    const int *s0, const int *s1, const int *s2, ptrdiff_t nv, const void *sx, const void *sy,
+                    const void *sz, void *out, int *outtri, cudaStream_t stream);
+int celllist_edf(int f64, ptrdiff_t npoints, const void *x, const void *y, const void *z, ptrdiff_t nt,
+                 const int *s0, const int *s1, const int *s2, ptrdiff_t nv, const void *sx, const void *sy,
+                 const void *sz, void *out, int *outtri, cudaStream_t stream);
+
+// ---- small helpers -------------------------------------------------------------------------------
+inline int grid_blocks(long long n, int threads) { return int((n + threads - 1) / threads); }
+int env_int(const char *name, int dflt);
+const char *env_str(const char *name);
+cudaStream_t library_stream();  // per-thread non-blocking stream for the blocking entry points
+
+}  // namespace ssdf_b200

@@ -1,0 +1,668 @@
+// mesh_build.cu -- device-resident mesh: triangle records, LBVH, refit, pseudo-normals.
+//
+// Replaces the reference's per-call host packing + cuBQL build (serial/bvh/bvh.cu:108-130,
+// serial/bvh/bvh.cpp:155-165) with a device pipeline that runs once per mesh:
+//   1. validate indices, gather vertices, triangle boxes (FP32 and FP64), scene box of centroids;
+//   2. 30-bit Morton codes of the centroids, stable radix sort (radix_sort.cu);
+//   3. Karras LBVH topology over the sorted primitives (index tie-break for equal codes);
+//   4. bottom-up refit with per-node arrival counters;
+//   5. optional SAH treelet refinement (treelet_opt.cu);
+//   6. node records in the child-box layout, subtrees of <= leaf_size triangles collapsed into
+//      leaves, triangle records in leaf order (internal.h documents both layouts);
+//   7. optional angle-weighted pseudo-normals (serial/bvh/bvh.cpp:1669-1721), summed in the
+//      reference's order so they are bitwise its values up to the last bit of acos.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <vector>
+
+#include "internal.h"
+
+namespace ssdf_b200 {
+
+// SAH treelet refinement (treelet_opt.cu): restructures the topology in place, refits the boxes and
+// re-derives the leaf order (ids, leaf references, first_of) so subtrees stay contiguous ranges.
+int treelet_optimize(int n, int *child_l, int *child_r, int *parent_int, int *parent_leaf, int *first_of,
+                     float *nbox32, double *nbox64, const float *pbox32, const double *pbox64, int *sorted_ids,
+                     cudaStream_t stream);
+
+struct MeshStorage {
+    std::vector<void *> blocks;
+    size_t bytes = 0;
+};
+
+namespace {
+
+template <typename T>
+int dalloc(MeshStorage *s, T **p, size_t count, cudaStream_t stream) {
+    void *ptr = nullptr;
+    const size_t b = sizeof(T) * (count ? count : 1);
+    cudaError_t e = cudaMallocAsync(&ptr, b, stream);
+    if (e != cudaSuccess) return fail(SSDF_ERR_OUT_OF_MEMORY, "device allocation of " + std::to_string(b) + " bytes");
+    s->blocks.push_back(ptr);
+    s->bytes += b;
+    *p = reinterpret_cast<T *>(ptr);
+    return SSDF_OK;
+}
+
+// Monotone float <-> int for atomicMin/atomicMax on floats.
+__device__ __forceinline__ int f2o(float f) {
+    const int i = __float_as_int(f);
+    return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__device__ __forceinline__ float o2f(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff); }
+
+__global__ void k_validate(int nt, int nv, const int *__restrict__ s0, const int *__restrict__ s1,
+                           const int *__restrict__ s2, int *__restrict__ bad) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nt) return;
+    const int a = s0[t], b = s1[t], c = s2[t];
+    if (a < 0 || a >= nv || b < 0 || b >= nv || c < 0 || c >= nv) atomicMin(bad, t);
+}
+
+template <typename G>
+__global__ void k_widen(int nv, const G *__restrict__ sx, const G *__restrict__ sy, const G *__restrict__ sz,
+                        double *__restrict__ vx, double *__restrict__ vy, double *__restrict__ vz) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv) return;
+    vx[i] = double(sx[i]);
+    vy[i] = double(sy[i]);
+    vz[i] = double(sz[i]);
+}
+
+// Per triangle: FP32 / FP64 boxes, FP32 centroid; scene centroid bounds and coordinate scale.
+__global__ void k_prep(int nt, const int *__restrict__ s0, const int *__restrict__ s1, const int *__restrict__ s2,
+                       const double *__restrict__ vx, const double *__restrict__ vy, const double *__restrict__ vz,
+                       float *__restrict__ box32, double *__restrict__ box64, float *__restrict__ cen,
+                       int *__restrict__ scene /* 6 ordered ints: lo xyz, hi xyz */, int *__restrict__ scale) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    float c[3] = {0.f, 0.f, 0.f};
+    float amax = 0.f;
+    const bool ok = t < nt;
+    if (ok) {
+        const int id[3] = {s0[t], s1[t], s2[t]};
+        double p[3][3];
+        for (int v = 0; v < 3; v++) p[v][0] = vx[id[v]], p[v][1] = vy[id[v]], p[v][2] = vz[id[v]];
+        for (int d = 0; d < 3; d++) {
+            const double lo = fmin(fmin(p[0][d], p[1][d]), p[2][d]);
+            const double hi = fmax(fmax(p[0][d], p[1][d]), p[2][d]);
+            box64[6 * t + 2 * d] = lo;
+            box64[6 * t + 2 * d + 1] = hi;
+            const float f0 = float(p[0][d]), f1 = float(p[1][d]), f2 = float(p[2][d]);
+            const float flo = fminf(fminf(f0, f1), f2), fhi = fmaxf(fmaxf(f0, f1), f2);
+            box32[6 * t + 2 * d] = flo;
+            box32[6 * t + 2 * d + 1] = fhi;
+            c[d] = 0.5f * (flo + fhi);
+            cen[3 * t + d] = c[d];
+            amax = fmaxf(amax, fmaxf(fabsf(flo), fabsf(fhi)));
+        }
+    }
+    // warp-level reduction then one atomic per warp
+    float lo[3], hi[3];
+    for (int d = 0; d < 3; d++) lo[d] = ok ? c[d] : FLT_MAX, hi[d] = ok ? c[d] : -FLT_MAX;
+    for (int o = 16; o > 0; o >>= 1) {
+        for (int d = 0; d < 3; d++) {
+            lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+            hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+        }
+        amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        for (int d = 0; d < 3; d++) {
+            atomicMin(&scene[d], f2o(lo[d]));
+            atomicMax(&scene[3 + d], f2o(hi[d]));
+        }
+        atomicMax(scale, __float_as_int(amax));
+    }
+}
+
+__device__ __forceinline__ uint32_t expand_bits(uint32_t v) {
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+
+__global__ void k_morton(int nt, const float *__restrict__ cen, const int *__restrict__ scene,
+                         uint32_t *__restrict__ keys, int *__restrict__ vals) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nt) return;
+    uint32_t q[3];
+    for (int d = 0; d < 3; d++) {
+        const float lo = o2f(scene[d]), hi = o2f(scene[3 + d]);
+        const float ext = hi - lo;
+        float u = ext > 0.f ? (cen[3 * t + d] - lo) / ext : 0.5f;
+        u = fminf(fmaxf(u, 0.f), 1.f);
+        q[d] = uint32_t(fminf(u * 1024.f, 1023.f));
+    }
+    keys[t] = (expand_bits(q[0]) << 2) | (expand_bits(q[1]) << 1) | expand_bits(q[2]);
+    vals[t] = t;
+}
+
+__device__ __forceinline__ int karras_delta(const uint32_t *__restrict__ k, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    const uint32_t a = k[i], b = k[j];
+    if (a == b) return 32 + __clz(i ^ j);
+    return __clz(a ^ b);
+}
+
+// Internal node i of the n-1: children (>= 0 internal, < 0 leaf -(pos + 1)), range, parents.
+__global__ void k_karras(int n, const uint32_t *__restrict__ k, int *__restrict__ child_l, int *__restrict__ child_r,
+                         int *__restrict__ first_of, int *__restrict__ last_of, int *__restrict__ parent_int,
+                         int *__restrict__ parent_leaf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    const int d = (karras_delta(k, n, i, i + 1) - karras_delta(k, n, i, i - 1)) >= 0 ? 1 : -1;
+    const int dmin = karras_delta(k, n, i, i - d);
+    int lmax = 2;
+    while (karras_delta(k, n, i, i + lmax * d) > dmin) lmax *= 2;
+    int l = 0;
+    for (int t = lmax / 2; t >= 1; t /= 2)
+        if (karras_delta(k, n, i, i + (l + t) * d) > dmin) l += t;
+    const int j = i + l * d;
+    const int dnode = karras_delta(k, n, i, j);
+    int s = 0, t = l;
+    do {
+        t = (t + 1) >> 1;
+        if (karras_delta(k, n, i, i + (s + t) * d) > dnode) s += t;
+    } while (t > 1);
+    const int gamma = i + s * d + min(d, 0);
+    const int first = min(i, j), last = max(i, j);
+    const int left = (first == gamma) ? -(gamma + 1) : gamma;
+    const int right = (last == gamma + 1) ? -(gamma + 2) : gamma + 1;
+    child_l[i] = left;
+    child_r[i] = right;
+    first_of[i] = first;
+    last_of[i] = last;
+    if (left < 0) parent_leaf[gamma] = i; else parent_int[gamma] = i;
+    if (right < 0) parent_leaf[gamma + 1] = i; else parent_int[gamma + 1] = i;
+    if (i == 0) parent_int[0] = -1;
+}
+
+// Bottom-up refit: the second thread to reach a node unions its two children's boxes.
+__global__ void k_refit(int n, const int *__restrict__ sorted_ids, const int *__restrict__ child_l,
+                        const int *__restrict__ child_r, const int *__restrict__ parent_int,
+                        const int *__restrict__ parent_leaf, const float *__restrict__ pbox32,
+                        const double *__restrict__ pbox64, float *nbox32, double *nbox64, int *arrivals) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    int node = parent_leaf[p];
+    while (node >= 0) {
+        __threadfence();
+        if (atomicAdd(&arrivals[node], 1) == 0) return;
+        __threadfence();
+        const int c[2] = {child_l[node], child_r[node]};
+        float b32[6];
+        double b64[6];
+        for (int k = 0; k < 6; k++) b32[k] = (k & 1) ? -FLT_MAX : FLT_MAX, b64[k] = (k & 1) ? -DBL_MAX : DBL_MAX;
+        for (int h = 0; h < 2; h++) {
+            const float *s32;
+            const double *s64;
+            if (c[h] < 0) {
+                const int prim = sorted_ids[-c[h] - 1];
+                s32 = pbox32 + 6 * prim;
+                s64 = pbox64 + 6 * prim;
+            } else {
+                s32 = nbox32 + 6 * c[h];
+                s64 = nbox64 + 6 * c[h];
+            }
+            for (int k = 0; k < 6; k += 2) {
+                b32[k] = fminf(b32[k], __ldcg(s32 + k));
+                b32[k + 1] = fmaxf(b32[k + 1], __ldcg(s32 + k + 1));
+                b64[k] = fmin(b64[k], __ldcg(s64 + k));
+                b64[k + 1] = fmax(b64[k + 1], __ldcg(s64 + k + 1));
+            }
+        }
+        for (int k = 0; k < 6; k++) {
+            __stcg(nbox32 + 6 * node + k, b32[k]);
+            __stcg(nbox64 + 6 * node + k, b64[k]);
+        }
+        node = parent_int[node];
+    }
+}
+
+// Subtree sizes after treelet restructuring: recomputed bottom-up the same way.
+__global__ void k_counts(int n, const int *__restrict__ child_l, const int *__restrict__ child_r,
+                         const int *__restrict__ parent_int, const int *__restrict__ parent_leaf, int *count,
+                         int *arrivals) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    int node = parent_leaf[p];
+    while (node >= 0) {
+        __threadfence();
+        if (atomicAdd(&arrivals[node], 1) == 0) return;
+        __threadfence();
+        const int l = child_l[node], r = child_r[node];
+        const int cl = l < 0 ? 1 : __ldcg(count + l);
+        const int cr = r < 0 ? 1 : __ldcg(count + r);
+        __stcg(count + node, cl + cr);
+        node = parent_int[node];
+    }
+}
+
+// Node records. A child with <= L triangles in its subtree becomes a leaf over its range.
+__global__ void k_write_nodes(int n, int L, const int *__restrict__ child_l, const int *__restrict__ child_r,
+                              const int *__restrict__ first_of, const int *__restrict__ count,
+                              const int *__restrict__ sorted_ids, const float *__restrict__ pbox32,
+                              const double *__restrict__ pbox64, const float *__restrict__ nbox32,
+                              const double *__restrict__ nbox64, float4 *__restrict__ nodes32,
+                              double2 *__restrict__ nodes64) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int ref[2];
+    const float *b32[2];
+    const double *b64[2];
+    const int c[2] = {child_l[i], child_r[i]};
+    for (int h = 0; h < 2; h++) {
+        if (c[h] < 0) {
+            const int pos = -c[h] - 1;
+            ref[h] = leaf_ref(pos, 1);
+            b32[h] = pbox32 + 6 * sorted_ids[pos];
+            b64[h] = pbox64 + 6 * sorted_ids[pos];
+        } else {
+            ref[h] = count[c[h]] <= L ? leaf_ref(first_of[c[h]], count[c[h]]) : c[h];
+            b32[h] = nbox32 + 6 * c[h];
+            b64[h] = nbox64 + 6 * c[h];
+        }
+    }
+    nodes32[4 * i + 0] = make_float4(b32[0][0], b32[0][1], b32[0][2], b32[0][3]);
+    nodes32[4 * i + 1] = make_float4(b32[1][0], b32[1][1], b32[1][2], b32[1][3]);
+    nodes32[4 * i + 2] = make_float4(b32[0][4], b32[0][5], b32[1][4], b32[1][5]);
+    nodes32[4 * i + 3] = make_float4(__int_as_float(ref[0]), __int_as_float(ref[1]), 0.f, 0.f);
+    if (nodes64) {
+        for (int h = 0; h < 2; h++)
+            for (int d = 0; d < 3; d++) nodes64[8 * i + 3 * h + d] = make_double2(b64[h][2 * d], b64[h][2 * d + 1]);
+        nodes64[8 * i + 6] = make_double2(__longlong_as_double((long long)(unsigned)ref[0]),
+                                          __longlong_as_double((long long)(unsigned)ref[1]));
+        nodes64[8 * i + 7] = make_double2(0.0, 0.0);
+    }
+}
+
+// A single root holding one leaf over all n <= L triangles (child 1 empty, inverted box).
+__global__ void k_write_small_root(int n, const float *__restrict__ box32, const double *__restrict__ box64,
+                                   float4 *__restrict__ nodes32, double2 *__restrict__ nodes64) {
+    float b[6] = {FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX};
+    double e[6] = {DBL_MAX, -DBL_MAX, DBL_MAX, -DBL_MAX, DBL_MAX, -DBL_MAX};
+    for (int t = 0; t < n; t++)
+        for (int k = 0; k < 6; k += 2) {
+            b[k] = fminf(b[k], box32[6 * t + k]), b[k + 1] = fmaxf(b[k + 1], box32[6 * t + k + 1]);
+            e[k] = fmin(e[k], box64[6 * t + k]), e[k + 1] = fmax(e[k + 1], box64[6 * t + k + 1]);
+        }
+    const float inf = __int_as_float(0x7f800000);
+    nodes32[0] = make_float4(b[0], b[1], b[2], b[3]);
+    nodes32[1] = make_float4(inf, -inf, inf, -inf);
+    nodes32[2] = make_float4(b[4], b[5], inf, -inf);
+    nodes32[3] = make_float4(__int_as_float(leaf_ref(0, n)), __int_as_float(kEmptyRef), 0.f, 0.f);
+    if (nodes64) {
+        const double dinf = __longlong_as_double(0x7ff0000000000000ll);
+        for (int d = 0; d < 3; d++) {
+            nodes64[d] = make_double2(e[2 * d], e[2 * d + 1]);
+            nodes64[3 + d] = make_double2(dinf, -dinf);
+        }
+        nodes64[6] = make_double2(__longlong_as_double((long long)(unsigned)leaf_ref(0, n)),
+                                  __longlong_as_double((long long)(unsigned)kEmptyRef));
+        nodes64[7] = make_double2(0.0, 0.0);
+    }
+}
+
+// Depth and leaf count of the collapsed tree: a node is kept iff its subtree has > L triangles
+// (its ancestors then have more), so walk parents from every kept node.
+__global__ void k_depth(int n, int L, const int *__restrict__ count, const int *__restrict__ parent_int,
+                        const int *__restrict__ child_l, const int *__restrict__ child_r, int *__restrict__ stats) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    if (i != 0 && count[i] <= L) return;
+    int depth = 1;
+    for (int p = parent_int[i]; p >= 0 && depth < 1 << 20; p = parent_int[p]) depth++;
+    atomicMax(&stats[0], depth);
+    int leaves = 0;
+    const int c[2] = {child_l[i], child_r[i]};
+    for (int h = 0; h < 2; h++) leaves += (c[h] < 0 || count[c[h]] <= L) ? 1 : 0;
+    atomicAdd(&stats[1], leaves);
+}
+
+__global__ void k_tri_records(int nt, const int *__restrict__ sorted_ids, const int *__restrict__ s0,
+                              const int *__restrict__ s1, const int *__restrict__ s2, const double *__restrict__ vx,
+                              const double *__restrict__ vy, const double *__restrict__ vz, float4 *__restrict__ t32,
+                              double2 *__restrict__ t64) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nt) return;
+    const int t = sorted_ids[p];
+    const int a = s0[t], b = s1[t], c = s2[t];
+    const double ax = vx[a], ay = vy[a], az = vz[a], bx = vx[b], by = vy[b], bz = vz[b];
+    const double cx = vx[c], cy = vy[c], cz = vz[c];
+    t32[3 * p + 0] = make_float4(float(ax), float(ay), float(az), float(bx));
+    t32[3 * p + 1] = make_float4(float(by), float(bz), float(cx), float(cy));
+    t32[3 * p + 2] = make_float4(float(cz), __int_as_float(t), 0.f, 0.f);
+    if (t64) {
+        t64[5 * p + 0] = make_double2(ax, ay);
+        t64[5 * p + 1] = make_double2(az, bx);
+        t64[5 * p + 2] = make_double2(by, bz);
+        t64[5 * p + 3] = make_double2(cx, cy);
+        t64[5 * p + 4] = make_double2(cz, double(t));
+    }
+}
+
+// ---- pseudo-normals --------------------------------------------------------------------------------
+
+// Face normals, the per-(face, corner) angle contributions in visit order 3t + v, the vertex and
+// edge sort keys; edge normals initialised to the face's own (serial/bvh/bvh.cpp:1681-1710).
+__global__ void k_face_normals(int nt, int nv, const int *__restrict__ s0, const int *__restrict__ s1,
+                               const int *__restrict__ s2, const double *__restrict__ vx,
+                               const double *__restrict__ vy, const double *__restrict__ vz,
+                               double *__restrict__ face_n, double *__restrict__ edge_n, double *__restrict__ contrib,
+                               uint32_t *__restrict__ vkey, int *__restrict__ vval, uint64_t *__restrict__ ekey,
+                               int *__restrict__ eval) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nt) return;
+    const int id[3] = {s0[t], s1[t], s2[t]};
+    double p[3][3];
+    for (int v = 0; v < 3; v++) p[v][0] = vx[id[v]], p[v][1] = vy[id[v]], p[v][2] = vz[id[v]];
+    const double u[3] = {p[1][0] - p[0][0], p[1][1] - p[0][1], p[1][2] - p[0][2]};
+    const double w[3] = {p[2][0] - p[0][0], p[2][1] - p[0][1], p[2][2] - p[0][2]};
+    double n[3] = {u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]};
+    const double len = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    if (len > 0) {
+        for (int d = 0; d < 3; d++) n[d] /= len;
+    }
+    for (int d = 0; d < 3; d++) face_n[3 * t + d] = n[d];
+    for (int v = 0; v < 3; v++) {
+        const double *a = p[v], *b = p[(v + 1) % 3], *c = p[(v + 2) % 3];
+        const double e1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+        const double e2[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+        const double l1 = sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
+        const double l2 = sqrt(e2[0] * e2[0] + e2[1] * e2[1] + e2[2] * e2[2]);
+        const double cosine = (l1 > 0 && l2 > 0) ? (e1[0] * e2[0] + e1[1] * e2[1] + e1[2] * e2[2]) / (l1 * l2) : 1.0;
+        const double mn = (cosine < 1.0) ? cosine : 1.0;
+        const double cl = (-1.0 < mn) ? mn : -1.0;
+        const double angle = acos(cl);
+        for (int d = 0; d < 3; d++) contrib[3 * (3 * t + v) + d] = angle * n[d];
+        vkey[3 * t + v] = uint32_t(id[v]);
+        vval[3 * t + v] = 3 * t + v;
+    }
+    for (int e = 0; e < 3; e++) {
+        for (int d = 0; d < 3; d++) edge_n[9 * t + 3 * e + d] = n[d];
+        const uint64_t a = uint64_t(id[e]), b = uint64_t(id[(e + 1) % 3]);
+        ekey[3 * t + e] = (a < b ? a : b) * uint64_t(nv) + (a < b ? b : a);
+        eval[3 * t + e] = 3 * t + e;
+    }
+}
+
+// One thread per run of equal vertex keys: sums the contributions in visit order.
+__global__ void k_vertex_sums(int nocc, const uint32_t *__restrict__ vkey, const int *__restrict__ vval,
+                              const double *__restrict__ contrib, double *__restrict__ vertex_n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nocc) return;
+    if (i > 0 && vkey[i - 1] == vkey[i]) return;
+    double acc[3] = {0.0, 0.0, 0.0};
+    int j = i;
+    for (; j < nocc && vkey[j] == vkey[i]; j++) {
+        const int o = vval[j];
+        for (int d = 0; d < 3; d++) acc[d] += contrib[3 * o + d];
+    }
+    for (int d = 0; d < 3; d++) vertex_n[3 * size_t(vkey[i]) + d] = acc[d];
+}
+
+// One thread per run of equal edge keys: replays the reference's first-occurrence map.
+__global__ void k_edge_sums(int nocc, const uint64_t *__restrict__ ekey, const int *__restrict__ eval,
+                            const double *__restrict__ face_n, double *__restrict__ edge_n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nocc) return;
+    if (i > 0 && ekey[i - 1] == ekey[i]) return;
+    const int first = eval[i];
+    int j = i + 1;
+    for (; j < nocc && ekey[j] == ekey[i]; j++) {
+        const int o = eval[j];
+        for (int d = 0; d < 3; d++) {
+            const double sum = face_n[3 * (first / 3) + d] + face_n[3 * (o / 3) + d];
+            edge_n[9 * (o / 3) + 3 * (o % 3) + d] = sum;
+            edge_n[9 * (first / 3) + 3 * (first % 3) + d] = sum;
+        }
+    }
+}
+
+int bits_for(uint64_t maxval) {
+    int b = 1;
+    while (b < 64 && (maxval >> b) != 0) b++;
+    return b;
+}
+
+#define LAUNCH_CHECK(what)                                                  \
+    do {                                                                    \
+        cudaError_t e_ = cudaGetLastError();                                \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what, __FILE__, __LINE__); \
+    } while (0)
+
+int build_normals(MeshStorage *s, DeviceMesh *m, const int *s0, const int *s1, const int *s2, const double *vx,
+                  const double *vy, const double *vz, cudaStream_t stream) {
+    const int nt = m->nt, nv = m->nv, nocc = 3 * nt;
+    double *face_n, *edge_n, *vertex_n;
+    SSDF_CHECK(dalloc(s, &face_n, 3 * size_t(nt), stream));
+    SSDF_CHECK(dalloc(s, &edge_n, 9 * size_t(nt), stream));
+    SSDF_CHECK(dalloc(s, &vertex_n, 3 * size_t(nv), stream));
+    MeshStorage tmp;
+    double *contrib;
+    uint32_t *vkey;
+    uint64_t *ekey;
+    int *vval, *eval;
+    int st = SSDF_OK;
+    if ((st = dalloc(&tmp, &contrib, 3 * size_t(nocc), stream)) == SSDF_OK &&
+        (st = dalloc(&tmp, &vkey, nocc, stream)) == SSDF_OK && (st = dalloc(&tmp, &vval, nocc, stream)) == SSDF_OK &&
+        (st = dalloc(&tmp, &ekey, nocc, stream)) == SSDF_OK && (st = dalloc(&tmp, &eval, nocc, stream)) == SSDF_OK) {
+        cudaMemsetAsync(vertex_n, 0, sizeof(double) * 3 * size_t(nv), stream);
+        k_face_normals<<<grid_blocks(nt, 128), 128, 0, stream>>>(nt, nv, s0, s1, s2, vx, vy, vz, face_n, edge_n,
+                                                                 contrib, vkey, vval, ekey, eval);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) st = cuda_fail(e, "k_face_normals", __FILE__, __LINE__);
+        if (st == SSDF_OK) st = radix_sort_pairs_u32(vkey, vval, nocc, bits_for(uint64_t(nv)), stream);
+        if (st == SSDF_OK)
+            st = radix_sort_pairs_u64(ekey, eval, nocc, bits_for(uint64_t(nv) * uint64_t(nv)), stream);
+        if (st == SSDF_OK) {
+            k_vertex_sums<<<grid_blocks(nocc, 256), 256, 0, stream>>>(nocc, vkey, vval, contrib, vertex_n);
+            k_edge_sums<<<grid_blocks(nocc, 256), 256, 0, stream>>>(nocc, ekey, eval, face_n, edge_n);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) st = cuda_fail(e, "normal sums", __FILE__, __LINE__);
+        }
+    }
+    for (void *p : tmp.blocks) cudaFreeAsync(p, stream);
+    m->face_n = face_n;
+    m->edge_n = edge_n;
+    m->vertex_n = vertex_n;
+    return st;
+}
+
+}  // namespace
+
+void mesh_free(MeshStorage *storage) {
+    if (!storage) return;
+    for (void *p : storage->blocks) cudaFree(p);
+    delete storage;
+}
+
+size_t mesh_bytes(const MeshStorage *storage) { return storage ? storage->bytes : 0; }
+
+static int mesh_build_impl(MeshStorage *s, MeshStorage *tmp, DeviceMesh *m, int nt, const int *s0_in,
+                           const int *s1_in, const int *s2_in, int nv, const void *sx, const void *sy, const void *sz,
+                           int coord_f64, int device_ptrs, const ssdf_build_opts &opts, cudaStream_t stream) {
+    const int L = opts.leaf_size > 0 ? opts.leaf_size : 4;
+    m->nt = nt;
+    m->nv = nv;
+    m->leaf_size = L;
+    // indices (kept: the sign step needs the caller's vertex ids)
+    int *s0, *s1, *s2;
+    SSDF_CHECK(dalloc(s, &s0, nt, stream));
+    SSDF_CHECK(dalloc(s, &s1, nt, stream));
+    SSDF_CHECK(dalloc(s, &s2, nt, stream));
+    const cudaMemcpyKind kind = device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    SSDF_CUDA(cudaMemcpyAsync(s0, s0_in, sizeof(int) * size_t(nt), kind, stream));
+    SSDF_CUDA(cudaMemcpyAsync(s1, s1_in, sizeof(int) * size_t(nt), kind, stream));
+    SSDF_CUDA(cudaMemcpyAsync(s2, s2_in, sizeof(int) * size_t(nt), kind, stream));
+    m->s0 = s0, m->s1 = s1, m->s2 = s2;
+    // vertices, widened to double
+    const size_t gsz = coord_f64 ? sizeof(double) : sizeof(float);
+    void *gx, *gy, *gz;
+    double *vx, *vy, *vz;
+    SSDF_CHECK(dalloc(tmp, &vx, nv, stream));
+    SSDF_CHECK(dalloc(tmp, &vy, nv, stream));
+    SSDF_CHECK(dalloc(tmp, &vz, nv, stream));
+    if (device_ptrs) {
+        gx = const_cast<void *>(sx), gy = const_cast<void *>(sy), gz = const_cast<void *>(sz);
+    } else {
+        char *g;
+        SSDF_CHECK(dalloc(tmp, &g, 3 * gsz * size_t(nv), stream));
+        gx = g, gy = g + gsz * nv, gz = g + 2 * gsz * nv;
+        SSDF_CUDA(cudaMemcpyAsync(gx, sx, gsz * nv, cudaMemcpyHostToDevice, stream));
+        SSDF_CUDA(cudaMemcpyAsync(gy, sy, gsz * nv, cudaMemcpyHostToDevice, stream));
+        SSDF_CUDA(cudaMemcpyAsync(gz, sz, gsz * nv, cudaMemcpyHostToDevice, stream));
+    }
+    if (coord_f64)
+        k_widen<double><<<grid_blocks(nv, 256), 256, 0, stream>>>(nv, (const double *)gx, (const double *)gy,
+                                                                  (const double *)gz, vx, vy, vz);
+    else
+        k_widen<float><<<grid_blocks(nv, 256), 256, 0, stream>>>(nv, (const float *)gx, (const float *)gy,
+                                                                 (const float *)gz, vx, vy, vz);
+    LAUNCH_CHECK("k_widen");
+    // validation + per-triangle boxes
+    int *flags;  // [0] first bad triangle, [1..6] scene, [7] scale, [8..9] depth / leaves
+    SSDF_CHECK(dalloc(tmp, &flags, 16, stream));
+    {
+        // ordered-int encodings (f2o) of +FLT_MAX and -FLT_MAX seed the scene min / max
+        int h[16] = {0};
+        h[0] = 0x7fffffff;
+        for (int d = 0; d < 3; d++) h[1 + d] = 0x7f7fffff, h[4 + d] = int(0xff7fffffu ^ 0x7fffffffu);
+        SSDF_CUDA(cudaMemcpyAsync(flags, h, sizeof(h), cudaMemcpyHostToDevice, stream));
+        SSDF_CUDA(cudaStreamSynchronize(stream));  // h lives on this stack frame
+    }
+    k_validate<<<grid_blocks(nt, 256), 256, 0, stream>>>(nt, nv, s0, s1, s2, flags);
+    LAUNCH_CHECK("k_validate");
+    int bad = 0;
+    SSDF_CUDA(cudaMemcpyAsync(&bad, flags, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    SSDF_CUDA(cudaStreamSynchronize(stream));
+    if (bad != 0x7fffffff)
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "triangle " + std::to_string(bad) + " has a vertex index outside [0, " +
+                                                   std::to_string(nv) + ")");
+    float *box32, *cen;
+    double *box64;
+    SSDF_CHECK(dalloc(tmp, &box32, 6 * size_t(nt), stream));
+    SSDF_CHECK(dalloc(tmp, &box64, 6 * size_t(nt), stream));
+    SSDF_CHECK(dalloc(tmp, &cen, 3 * size_t(nt), stream));
+    k_prep<<<grid_blocks(nt, 256), 256, 0, stream>>>(nt, s0, s1, s2, vx, vy, vz, box32, box64, cen, flags + 1,
+                                                     flags + 7);
+    LAUNCH_CHECK("k_prep");
+    // Morton order
+    uint32_t *keys;
+    int *ids;
+    SSDF_CHECK(dalloc(tmp, &keys, nt, stream));
+    SSDF_CHECK(dalloc(tmp, &ids, nt, stream));
+    k_morton<<<grid_blocks(nt, 256), 256, 0, stream>>>(nt, cen, flags + 1, keys, ids);
+    LAUNCH_CHECK("k_morton");
+    SSDF_CHECK(radix_sort_pairs_u32(keys, ids, nt, 30, stream));
+    // topology
+    const bool keep64 = opts.keep_fp64 != 0;
+    const int nint = nt > 1 ? nt - 1 : 0;
+    m->nnodes = nint > 0 ? nint : 1;
+    float4 *nodes32;
+    double2 *nodes64 = nullptr;
+    SSDF_CHECK(dalloc(s, &nodes32, 4 * size_t(m->nnodes), stream));
+    if (keep64) SSDF_CHECK(dalloc(s, &nodes64, 8 * size_t(m->nnodes), stream));
+    int depth_leaves[2] = {1, 1};
+    if (nt <= L) {
+        // one leaf over everything (its triangle order is the Morton order)
+        double *pb64 = box64;
+        float *pb32 = box32;
+        k_write_small_root<<<1, 1, 0, stream>>>(nt, pb32, pb64, nodes32, nodes64);
+        LAUNCH_CHECK("k_write_small_root");
+    } else {
+        int *child_l, *child_r, *first_of, *last_of, *parent_int, *parent_leaf, *arrivals, *count;
+        float *nbox32;
+        double *nbox64;
+        SSDF_CHECK(dalloc(tmp, &child_l, nint, stream));
+        SSDF_CHECK(dalloc(tmp, &child_r, nint, stream));
+        SSDF_CHECK(dalloc(tmp, &first_of, nint, stream));
+        SSDF_CHECK(dalloc(tmp, &last_of, nint, stream));
+        SSDF_CHECK(dalloc(tmp, &parent_int, nint, stream));
+        SSDF_CHECK(dalloc(tmp, &parent_leaf, nt, stream));
+        SSDF_CHECK(dalloc(tmp, &arrivals, nint, stream));
+        SSDF_CHECK(dalloc(tmp, &count, nint, stream));
+        SSDF_CHECK(dalloc(tmp, &nbox32, 6 * size_t(nint), stream));
+        SSDF_CHECK(dalloc(tmp, &nbox64, 6 * size_t(nint), stream));
+        k_karras<<<grid_blocks(nint, 256), 256, 0, stream>>>(nt, keys, child_l, child_r, first_of, last_of,
+                                                             parent_int, parent_leaf);
+        LAUNCH_CHECK("k_karras");
+        SSDF_CUDA(cudaMemsetAsync(arrivals, 0, sizeof(int) * nint, stream));
+        k_refit<<<grid_blocks(nt, 256), 256, 0, stream>>>(nt, ids, child_l, child_r, parent_int, parent_leaf, box32,
+                                                          box64, nbox32, nbox64, arrivals);
+        LAUNCH_CHECK("k_refit");
+        if (opts.treelet_opt) {
+            SSDF_CHECK(treelet_optimize(nt, child_l, child_r, parent_int, parent_leaf, first_of, nbox32, nbox64,
+                                        box32, box64, ids, stream));
+        }
+        SSDF_CUDA(cudaMemsetAsync(arrivals, 0, sizeof(int) * nint, stream));
+        k_counts<<<grid_blocks(nt, 256), 256, 0, stream>>>(nt, child_l, child_r, parent_int, parent_leaf, count,
+                                                           arrivals);
+        LAUNCH_CHECK("k_counts");
+        k_write_nodes<<<grid_blocks(nint, 256), 256, 0, stream>>>(nt, L, child_l, child_r, first_of, count, ids,
+                                                                  box32, box64, nbox32, nbox64, nodes32, nodes64);
+        LAUNCH_CHECK("k_write_nodes");
+        k_depth<<<grid_blocks(nint, 256), 256, 0, stream>>>(nt, L, count, parent_int, child_l, child_r, flags + 8);
+        LAUNCH_CHECK("k_depth");
+        SSDF_CUDA(cudaMemcpyAsync(depth_leaves, flags + 8, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    }
+    // triangle records in leaf order
+    float4 *t32;
+    double2 *t64 = nullptr;
+    SSDF_CHECK(dalloc(s, &t32, 3 * size_t(nt), stream));
+    if (keep64) SSDF_CHECK(dalloc(s, &t64, 5 * size_t(nt), stream));
+    k_tri_records<<<grid_blocks(nt, 256), 256, 0, stream>>>(nt, ids, s0, s1, s2, vx, vy, vz, t32, t64);
+    LAUNCH_CHECK("k_tri_records");
+    int scale_bits = 0;
+    SSDF_CUDA(cudaMemcpyAsync(&scale_bits, flags + 7, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    if (opts.normals) SSDF_CHECK(build_normals(s, m, s0, s1, s2, vx, vy, vz, stream));
+    SSDF_CUDA(cudaStreamSynchronize(stream));
+    float scale;
+    memcpy(&scale, &scale_bits, sizeof(float));
+    m->coord_scale = scale;
+    m->depth = depth_leaves[0];
+    m->nleaves = depth_leaves[1];
+    m->nodes32 = nodes32;
+    m->nodes64 = nodes64;
+    m->tris32 = t32;
+    m->tris64 = t64;
+    if (m->depth >= kStackSize)
+        return fail(SSDF_ERR_NOT_SUPPORTED,
+                    "BVH depth " + std::to_string(m->depth) + " exceeds the traversal stack (" +
+                        std::to_string(kStackSize) + ")");
+    return SSDF_OK;
+}
+
+int mesh_build(MeshStorage **storage, DeviceMesh *mesh, ptrdiff_t nt, const int *s0, const int *s1, const int *s2,
+               ptrdiff_t nv, const void *sx, const void *sy, const void *sz, int coord_f64, int device_ptrs,
+               const ssdf_build_opts &opts, cudaStream_t stream) {
+    if (nt <= 0 || nv <= 0) return fail(SSDF_ERR_INVALID_ARGUMENT, "empty mesh");
+    if (nt >= kMaxTriangles) return fail(SSDF_ERR_NOT_SUPPORTED, "more than 2^26 triangles in one mesh");
+    if (nv >= (1ll << 31)) return fail(SSDF_ERR_NOT_SUPPORTED, "more than 2^31 vertices");
+    if (opts.leaf_size < 0 || opts.leaf_size > kMaxLeafSize)
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "leaf_size must be 0 (default) or 1.." + std::to_string(kMaxLeafSize));
+    if (!s0 || !s1 || !s2 || !sx || !sy || !sz) return fail(SSDF_ERR_INVALID_ARGUMENT, "null mesh array");
+    MeshStorage *s = new MeshStorage();
+    MeshStorage tmp;
+    *mesh = DeviceMesh();
+    int st = mesh_build_impl(s, &tmp, mesh, int(nt), s0, s1, s2, int(nv), sx, sy, sz, coord_f64, device_ptrs, opts,
+                             stream);
+    for (void *p : tmp.blocks) cudaFreeAsync(p, stream);
+    if (st == SSDF_OK) {
+        cudaError_t e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) st = cuda_fail(e, "mesh build", __FILE__, __LINE__);
+    }
+    if (st != SSDF_OK) {
+        cudaStreamSynchronize(stream);
+        mesh_free(s);
+        *mesh = DeviceMesh();
+        return st;
+    }
+    *storage = s;
+    return SSDF_OK;
+}
+
+}  // namespace ssdf_b200

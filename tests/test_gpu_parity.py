@@ -1,0 +1,167 @@
+"""GPU parity against the oracle on the workloads' own meshes and queries.
+
+Integer outputs (closest triangle) and double distances are compared for equality. The oracle is
+brute force; it runs over a whole workload where that takes seconds (the icosphere's 64^3 grid)
+and over a seeded sample of query points elsewhere, while the GPU runs the full query set. At
+full size the size-independent property is checked instead: the FP32-with-FP64-fix-up result
+equals the plain FP64 result at every query, bit for bit.
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import ssdf_b200 as S
+from ssdf_b200 import workloads as W
+from test_gpu_golden import env
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ico():
+    mesh = W.icosphere()
+    grid = W.Grid.cell_centred(mesh, 64, 0.2)
+    q = oracle.grid_points(grid)
+    d, tri = oracle.edf(q, mesh, with_index=True)
+    normals = oracle.pseudonormals(mesh)
+    sd, stri = oracle.sdf_points(q, mesh, normals)
+    return dict(mesh=mesh, grid=grid, q=q, d=d, tri=tri, sd=sd, stri=stri)
+
+
+def test_icosphere_unsigned_every_method(ico):
+    mesh, q = ico["mesh"], ico["q"]
+    assert np.array_equal(S.edf(q, mesh), ico["d"])
+    assert np.array_equal(S.edf_celllist(q, mesh), ico["d"])
+    for prec in ("f32x", "f64"):
+        with env(SSDF_B200_PRECISION=prec):
+            d, tri = S.edf_index(q, mesh)
+        assert np.array_equal(d, ico["d"]), prec
+        assert np.array_equal(tri, ico["tri"]), prec
+
+
+def test_icosphere_float(ico):
+    mesh, q = ico["mesh"], ico["q"].astype(np.float32)
+    want = oracle.edf(q, mesh, dtype=np.float32)
+    assert np.array_equal(S.edf(q, mesh, dtype=np.float32), want)
+    assert np.array_equal(S.edf_celllist(q, mesh, dtype=np.float32), want)
+    assert np.array_equal(S.edf_bvh(q, mesh, gdtype=np.float32), want)
+    assert np.array_equal(S.edf_select(q, mesh, dtype=np.float32), want)
+
+
+def test_icosphere_signed_grid(ico):
+    for prec in ("f32x", "f64"):
+        with env(SSDF_B200_PRECISION=prec):
+            sd, tri = S.sample_sdf_bvh(ico["mesh"], ico["grid"], with_index=True)
+        assert np.array_equal(tri, ico["stri"]), prec
+        assert np.array_equal(sd, ico["sd"]), prec  # bitwise: same magnitude and same sign everywhere
+
+
+def test_icosphere_signed_points_and_incoming_values(ico):
+    mesh, q = ico["mesh"], ico["q"][:, ::7]
+    sd, tri = S.sdf_points(q, mesh)
+    assert np.array_equal(sd, ico["sd"][::7])
+    # in/out: where the incoming value is already smaller it stays, elsewhere the distance wins
+    init = np.where(np.arange(q.shape[1]) % 3 == 0, 0.01, np.finfo(np.float64).max)
+    want, wtri = oracle.edf(q, mesh, out=init, with_index=True)
+    got, gtri = S.edf_index(q, mesh, out=init)
+    assert np.array_equal(got, want) and np.array_equal(gtri, wtri)
+    assert np.array_equal(S.edf(q, mesh, out=init), want)
+    assert np.array_equal(S.edf_celllist(q, mesh, out=init), want)
+
+
+@pytest.fixture(scope="module")
+def knot():
+    mesh = W.torus_knot_tube()
+    grid = W.Grid.padded_nodes(mesh, 256, 0.25)
+    rng = np.random.default_rng(21)
+    ids = np.sort(rng.choice(grid.size, size=3000, replace=False))
+    q = oracle.grid_points(grid)[:, ids]
+    sd, stri = oracle.sdf_points(q, mesh)
+    return dict(mesh=mesh, grid=grid, ids=ids, q=q, sd=sd, stri=stri)
+
+
+def test_torus_knot_full_grid(knot):
+    with env(SSDF_B200_PRECISION="f32x"):
+        sdx, trix = S.sample_sdf_bvh(knot["mesh"], knot["grid"], with_index=True)
+    with env(SSDF_B200_PRECISION="f64"):
+        sd64, tri64 = S.sample_sdf_bvh(knot["mesh"], knot["grid"], with_index=True)
+    # the fix-up path is the double result, at all 16.8M nodes
+    assert np.array_equal(sdx, sd64)
+    assert np.array_equal(trix, tri64)
+    # and both are the oracle's at the sampled nodes
+    assert np.array_equal(sd64[knot["ids"]], knot["sd"])
+    assert np.array_equal(tri64[knot["ids"]], knot["stri"])
+    diag = knot["mesh"].diagonal()
+    assert np.max(np.abs(sdx[knot["ids"]] - knot["sd"])) <= 1e-6 * diag
+
+
+def test_torus_knot_sqedf_and_float_grid(knot):
+    mesh, grid = knot["mesh"], knot["grid"]
+    sq = S.sample_sqedf_bvh(mesh, grid)
+    assert np.array_equal(np.sqrt(sq[knot["ids"]]), np.abs(knot["sd"]))
+    # float grid: nodes in float arithmetic, value the double distance of the float mesh, cast
+    gf = W.Grid(grid.n, tuple(float(np.float32(v)) for v in grid.lo), tuple(float(np.float32(v)) for v in grid.hi))
+    sdf = S.sample_sdf_bvh(mesh, gf, dtype=np.float32)
+    qf = oracle.grid_points(gf, dtype=np.float32)[:, knot["ids"]]
+    meshf = W.Mesh(mesh.vertices.astype(np.float32).astype(np.float64), mesh.triangles)
+    want, _ = oracle.sdf_points(qf, meshf)
+    assert np.array_equal(sdf[knot["ids"]], want.astype(np.float32))
+
+
+def test_beam_lattice_points():
+    mesh = W.beam_lattice()
+    pts = W.uniform_points(400000, -0.1, 1.1, seed=13)
+    sub = pts[:, ::100]
+    wantf = oracle.edf(sub.astype(np.float32), mesh, dtype=np.float32)
+    gotf = S.edf_bvh(pts.astype(np.float32), mesh, gdtype=np.float32)
+    assert np.array_equal(gotf[::100], wantf)
+    want, wtri = oracle.edf(sub, mesh, with_index=True)
+    got, gtri = S.edf_index(pts, mesh)
+    assert np.array_equal(got[::100], want)
+    assert np.array_equal(gtri[::100], wtri)
+    with env(SSDF_B200_PRECISION="f64"):
+        g64, t64 = S.edf_index(pts, mesh)
+    assert np.array_equal(g64, got) and np.array_equal(t64, gtri)
+
+
+def test_closest_point_bvh():
+    mesh = W.torus(nu=80, nv=40, jitter=0.01)
+    lo, hi = mesh.bbox()
+    pts = W.uniform_points(20000, lo - 0.2, hi + 0.2, seed=5)
+    init = np.where(np.arange(20000) % 4 == 0, 0.05, np.finfo(np.float64).max)
+    want = oracle.closest_point(pts, mesh, outd=init)
+    got = S.closest_point_bvh(pts, mesh, outd=init)
+    for w, g, name in zip(want, got, ("d", "x", "y", "z", "tri")):
+        assert np.array_equal(w, g), name
+
+
+def test_sqedf_incoming_values():
+    mesh = W.icosphere(3)
+    grid = W.Grid((17, 9, 13), (-1.3, -1.2, -1.1), (1.2, 1.3, 1.1))
+    q = oracle.grid_points(grid)
+    init = np.where(np.arange(grid.size) % 2 == 0, 0.02, np.finfo(np.float64).max)
+    want = oracle.sqedf_points(q, mesh, out=init)
+    assert np.array_equal(S.sample_sqedf_bvh(mesh, grid, out=init), want)
+
+
+def test_device_mesh_handle_matches_drop_in():
+    import torch
+
+    mesh = W.torus_knot_tube(nu=256, nv=32)
+    grid = W.Grid.padded_nodes(mesh, 48, 0.25)
+    want, wtri = S.sample_sdf_bvh(mesh, grid, with_index=True)
+    dm = S.DeviceMesh(mesh)
+    out = torch.empty(grid.size, dtype=torch.float64, device="cuda")
+    tri = torch.empty(grid.size, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    for prec in (S.PREC_F32_FIXUP, S.PREC_F64):
+        dm.query_grid(grid, out, tri, precision=prec, output=S.OUT_SDF, stream=stream)
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy(), want)
+        assert np.array_equal(tri.cpu().numpy(), wtri)
+    st = dm.stats()
+    assert st["depth"] < 64 and st["leaves"] > 0
+    dm.close()

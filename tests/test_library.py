@@ -1,0 +1,58 @@
+"""CPU checks of the boundary: the library builds, loads and exports every entry point that
+include/ssdf_b200.h declares; status names; no compute call is made without a GPU."""
+
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "ssdf_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(ssdf_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    import ssdf_b200.capi as capi
+
+    names = declared_functions()
+    assert len(names) >= 25
+    for n in names:
+        assert hasattr(capi.lib, n), n
+        assert n in capi.EXPORTED, n
+
+
+def test_status_strings():
+    import ssdf_b200 as S
+
+    assert S.lib.ssdf_status_string(0) == b"SSDF_OK"
+    assert S.lib.ssdf_status_string(1) == b"SSDF_ERR_INVALID_ARGUMENT"
+    assert S.version().startswith("ssdf_b200")
+
+
+def test_cpp_header_compiles_against_c_abi(tmp_path):
+    """include/ssdf.hpp (the C++ drop-in templates) compiles and links against the library."""
+    import subprocess
+
+    src = tmp_path / "use.cpp"
+    src.write_text(
+        '#include "ssdf.hpp"\n'
+        "int main() {\n"
+        "  double x[1] = {0}, y[1] = {0}, z[1] = {2}, sx[3] = {0, 1, 0}, sy[3] = {0, 0, 1}, sz[3] = {0, 0, 0};\n"
+        "  int s0[1] = {0}, s1[1] = {1}, s2[1] = {2};\n"
+        "  double out[1] = {1e300};\n"
+        "  (void)ssdf::edf_select<double, double, int>(1, x, y, z, 1, s0, s1, s2, 3, sx, sy, sz, out);\n"
+        "  (void)ssdf::edf<double, double, int>;\n"
+        "  (void)ssdf::edf_celllist<float, float, int>;\n"
+        "  (void)ssdf::edf_bvh<float, double, int>;\n"
+        "  (void)ssdf::closest_point_bvh<double, double, int>;\n"
+        "  (void)ssdf::sample_sdf_bvh<float, float, int>;\n"
+        "  (void)ssdf::sample_sqedf_bvh<double, double, int>;\n"
+        "  return 0;\n}\n")
+    lib = os.path.join(ROOT, "ssdf_b200", "_lib")
+    res = subprocess.run(["g++", "-std=c++17", f"-I{ROOT}/include", str(src), "-o", str(tmp_path / "use"),
+                          f"-L{lib}", "-lssdf_b200", f"-Wl,-rpath,{lib}"], capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr
