@@ -22,7 +22,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_lib", "libssdf_b200.so")
+LIB_PATH = os.environ.get("SSDF_B200_LIBRARY") or os.path.join(HERE, "_lib", "libssdf_b200.so")
 
 SSDF_OK = 0
 F32, F64 = 0, 1

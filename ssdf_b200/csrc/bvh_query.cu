@@ -10,7 +10,8 @@
 //         window (sqrt(best) + tau)^2; the window's members are re-evaluated in double and the
 //         lexicographic minimum taken. tau bounds twice the float error of one distance, so the
 //         double winner is always in the window; a query whose window overflowed the K slots is
-//         handed to the F64 kernel (k_fallback). Result: bitwise the F64 result.
+//         walked again with the window fixed, re-evaluating every member in double (k_window).
+//         Result: bitwise the F64 result.
 // Traversal: nearest child first, the farther one pushed with its box distance on a per-thread
 // stack and culled on pop against the current threshold. Grid queries map a warp to a 4x4x2 brick
 // of nodes and a block to 8x4x4, so a warp's traversals stay coherent.
@@ -31,6 +32,12 @@ namespace {
 
 constexpr int kThreads = 128;
 constexpr int kCand = 8;  // F32X window slots
+// Minimum resident blocks per SM the float query kernels are compiled for: 8 blocks of 128 caps
+// them at 64 registers. The traversal is latency-bound, so the occupancy this buys outweighs the
+// few spills (measured: -22 % time on the torus-knot grid); the double kernel keeps its registers.
+#ifndef SSDF_B200_QUERY_MIN_BLOCKS
+#define SSDF_B200_QUERY_MIN_BLOCKS 8
+#endif
 
 struct Counters {
     unsigned long long tri = 0, box = 0, fix = 0;
@@ -155,7 +162,11 @@ __device__ __forceinline__ Tri64 load_tri64(const double2 *__restrict__ t, int p
     return Tri64{u.x, u.y, v.x, v.y, w.x, w.y, x.x, x.y, y.x, int(y.y)};
 }
 
-// ---- exact traversal (F64 over double data, F32 over float data) ------------------------------------
+// ---- traversal policies ---------------------------------------------------------------------------
+//
+// A policy owns one query's state (point, incumbent, prune threshold `thr`) and knows how to test a
+// node's two child boxes and a leaf's triangles in its arithmetic. `want` tells a leaf which lanes
+// asked for it (in warp mode every lane walks every leaf the warp visits).
 
 template <typename T>
 struct ExactData;
@@ -203,81 +214,46 @@ struct ExactData<float> {
     }
 };
 
-// Lexicographic (d^2, id) minimum over all triangles, starting from (best, -1): a triangle
-// replaces the incumbent if strictly closer, or equally close with a lower index (never the
-// initial bound on a tie). Pruning keeps every box whose distance is below
-// best * (1 + 2^-16) + margin, so rounding in box distances never drops a tie.
-template <typename T, bool COUNT>
-__device__ void traverse_exact(const DeviceMesh &m, const T px, const T py, const T pz, T &best, int &bid,
-                               int &bpos, Counters &cnt) {
-    using D = ExactData<T>;
-    const T margin = D::abs_margin(m.coord_scale);
-    T thr = best * D::rel + margin;
-    int snode[kStackSize];
-    T sdist[kStackSize];
-    int sp = 0;
-    int node = 0;
-    while (true) {
-        T d0, d1;
-        int r0, r1;
-        D::boxes(m, node, px, py, pz, d0, d1, r0, r1);
-        if (COUNT) cnt.box += 2;
-        // near child first
-        if (d1 < d0) {
-            const T td = d0;
-            d0 = d1;
-            d1 = td;
-            const int tr = r0;
-            r0 = r1;
-            r1 = tr;
-        }
-        int next = -1;
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const T dc = h ? d1 : d0;
-            const int rc = h ? r1 : r0;
-            if (!(dc < thr) || rc == kEmptyRef) continue;
-            if (rc < 0) {
-                const int first = leaf_first(rc), n = leaf_count(rc);
-                for (int k = 0; k < n; k++) {
-                    int id;
-                    const T d2 = D::tri(m, first + k, px, py, pz, id);
-                    if (COUNT) cnt.tri++;
-                    if (d2 < best || (d2 == best && bid >= 0 && id < bid)) {
-                        best = d2;
-                        bid = id;
-                        bpos = first + k;
-                        thr = best * D::rel + margin;
-                    }
-                }
-            } else if (next < 0) {
-                next = rc;
-            } else if (sp < kStackSize) {
-                snode[sp] = rc;
-                sdist[sp] = dc;
-                sp++;
-            }
-        }
-        if (next < 0) {
-            while (sp > 0) {
-                sp--;
-                if (sdist[sp] < thr) {
-                    next = snode[sp];
-                    break;
-                }
-            }
-            if (next < 0) break;
-        }
-        node = next;
+// Lexicographic (d^2, id) minimum over all triangles, starting from (best, -1): a triangle replaces
+// the incumbent if strictly closer, or equally close with a lower index (never the initial bound on
+// a tie). Boxes are kept while their distance is below best * (1 + 2^-16) + margin, so rounding in
+// box distances never drops a tie.
+template <typename T>
+struct ExactPolicy {
+    using R = T;
+    const DeviceMesh &m;
+    T px, py, pz, best, thr, margin;
+    int bid = -1, bpos = -1;
+    __device__ ExactPolicy(const DeviceMesh &mesh, T x, T y, T z, T init) : m(mesh), px(x), py(y), pz(z), best(init) {
+        margin = ExactData<T>::abs_margin(m.coord_scale);
+        thr = best * ExactData<T>::rel + margin;
     }
-}
+    __device__ __forceinline__ void boxes(int node, T &d0, T &d1, int &r0, int &r1) const {
+        ExactData<T>::boxes(m, node, px, py, pz, d0, d1, r0, r1);
+    }
+    template <bool COUNT>
+    __device__ __forceinline__ void leaf(int first, int n, bool want, Counters &cnt) {
+        for (int k = 0; k < n; k++) {
+            if (!want) continue;
+            int id;
+            const T d2 = ExactData<T>::tri(m, first + k, px, py, pz, id);
+            if (COUNT) cnt.tri++;
+            if (d2 < best || (d2 == best && bid >= 0 && id < bid)) {
+                best = d2;
+                bid = id;
+                bpos = first + k;
+                thr = best * ExactData<T>::rel + margin;
+            }
+        }
+    }
+};
 
-// ---- F32X: float filter + window ------------------------------------------------------------------
-
+// F32X: float filter. Keeps the kCand smallest float d^2 inside the window
+// (sqrt(best) + tau)^2 and the smallest d^2 that was pushed out of the slots.
 struct Window {
     float d[kCand];
     int p[kCand];
-    float evicted;  // smallest d^2 pushed out of the slots
+    float evicted;
 };
 
 __device__ __forceinline__ float window_thr(float best, float tau_rel, float scale) {
@@ -287,22 +263,116 @@ __device__ __forceinline__ float window_thr(float best, float tau_rel, float sca
     return w * w * (1.0f + 1.0f / 65536.0f);
 }
 
-template <bool COUNT>
-__device__ void traverse_fast(const DeviceMesh &m, const float px, const float py, const float pz, float &best,
-                              const float tau_rel, Window &win, float &thr, Counters &cnt) {
-    thr = window_thr(best, tau_rel, m.coord_scale);
+struct FastPolicy {
+    using R = float;
+    const DeviceMesh &m;
+    float px, py, pz, best, thr, tau_rel;
+    Window win;
+    __device__ FastPolicy(const DeviceMesh &mesh, float x, float y, float z, float init, float tau)
+        : m(mesh), px(x), py(y), pz(z), best(init), tau_rel(tau) {
+#pragma unroll
+        for (int s = 0; s < kCand; s++) win.d[s] = finf(), win.p[s] = -1;
+        win.evicted = finf();
+        thr = window_thr(best, tau_rel, m.coord_scale);
+    }
+    __device__ __forceinline__ void boxes(int node, float &d0, float &d1, int &r0, int &r1) const {
+        const Node32 n = load_node32(m.nodes32, node);
+        d0 = box_dist_sq_fast(px, py, pz, n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y);
+        d1 = box_dist_sq_fast(px, py, pz, n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w);
+        r0 = n.r0;
+        r1 = n.r1;
+    }
+    template <bool COUNT>
+    __device__ __forceinline__ void leaf(int first, int n, bool want, Counters &cnt) {
+        for (int k = 0; k < n; k++) {
+            if (!want) continue;
+            const Tri32 t = load_tri32(m.tris32, first + k);
+            const float d2 = tri_dist_sq_fast(px, py, pz, t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
+            if (COUNT) cnt.tri++;
+            if (d2 < thr) {
+                float d = d2;
+                int p = first + k;
+#pragma unroll
+                for (int s = 0; s < kCand; s++) {
+                    if (d < win.d[s]) {
+                        const float td = win.d[s];
+                        const int tp = win.p[s];
+                        win.d[s] = d;
+                        win.p[s] = p;
+                        d = td;
+                        p = tp;
+                    }
+                }
+                win.evicted = fminf(win.evicted, d);
+                if (d2 < best) {
+                    best = d2;
+                    thr = window_thr(best, tau_rel, m.coord_scale);
+                }
+            }
+        }
+    }
+};
+
+// Second stage of F32X for queries whose window overflowed its slots: the float walk again, now
+// with the window fixed at its final extent, and every triangle inside it re-evaluated in double on
+// the spot (the same float test decides membership, so the set is exactly the window).
+struct WindowPolicy {
+    using R = float;
+    const DeviceMesh &m;
+    float px, py, pz, thr;
+    double qx, qy, qz, best;
+    int bid = -1, bpos = -1;
+    __device__ WindowPolicy(const DeviceMesh &mesh, double x, double y, double z, float window, double init)
+        : m(mesh), px(float(x)), py(float(y)), pz(float(z)), thr(window), qx(x), qy(y), qz(z), best(init) {}
+    __device__ __forceinline__ void boxes(int node, float &d0, float &d1, int &r0, int &r1) const {
+        const Node32 n = load_node32(m.nodes32, node);
+        d0 = box_dist_sq_fast(px, py, pz, n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y);
+        d1 = box_dist_sq_fast(px, py, pz, n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w);
+        r0 = n.r0;
+        r1 = n.r1;
+    }
+    template <bool COUNT>
+    __device__ __forceinline__ void leaf(int first, int n, bool want, Counters &cnt) {
+        for (int k = 0; k < n; k++) {
+            if (!want) continue;
+            const Tri32 t = load_tri32(m.tris32, first + k);
+            const float d2 = tri_dist_sq_fast(px, py, pz, t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
+            if (COUNT) cnt.tri++;
+            if (d2 < thr) {
+                const Tri64 u = load_tri64(m.tris64, first + k);
+                const double e2 =
+                    tri_dist_sq_exact<double>(qx, qy, qz, u.ax, u.ay, u.az, u.bx, u.by, u.bz, u.cx, u.cy, u.cz);
+                if (COUNT) cnt.fix++;
+                if (e2 < best || (e2 == best && bid >= 0 && u.id < bid)) {
+                    best = e2;
+                    bid = u.id;
+                    bpos = first + k;
+                }
+            }
+        }
+    }
+};
+
+// Nearest-child-first traversal with a per-lane stack of (node, box distance), culled on pop.
+// WARP = false: every thread walks its own query. WARP = true (packet): the 32 lanes of a warp walk
+// one path together -- a child is entered if any lane wants it, the nearer child is the one most
+// lanes rank first -- so node and triangle loads are warp-uniform (broadcast) and leaf work does
+// not diverge. Every lane must call it (warp-synchronous when WARP).
+template <bool WARP, bool COUNT, class P>
+__device__ __forceinline__ void traverse(P &p, Counters &cnt) {
+    using R = typename P::R;
     int snode[kStackSize];
-    float sdist[kStackSize];
+    R sdist[kStackSize];
     int sp = 0;
     int node = 0;
     while (true) {
-        const Node32 n = load_node32(m.nodes32, node);
-        float d0 = box_dist_sq_fast(px, py, pz, n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y);
-        float d1 = box_dist_sq_fast(px, py, pz, n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w);
-        int r0 = n.r0, r1 = n.r1;
+        R d0, d1;
+        int r0, r1;
+        p.boxes(node, d0, d1, r0, r1);
         if (COUNT) cnt.box += 2;
-        if (d1 < d0) {
-            const float td = d0;
+        const bool swap = WARP ? (__popc(__ballot_sync(0xffffffffu, d1 < d0)) > 16) : (d1 < d0);
+        if (swap) {
+            const R td = d0;
             d0 = d1;
             d1 = td;
             const int tr = r0;
@@ -312,37 +382,12 @@ __device__ void traverse_fast(const DeviceMesh &m, const float px, const float p
         int next = -1;
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-            const float dc = h ? d1 : d0;
+            const R dc = h ? d1 : d0;
             const int rc = h ? r1 : r0;
-            if (!(dc < thr) || rc == kEmptyRef) continue;
+            const bool want = dc < p.thr && rc != kEmptyRef;
+            if (WARP ? !__any_sync(0xffffffffu, want) : !want) continue;
             if (rc < 0) {
-                const int first = leaf_first(rc), cntl = leaf_count(rc);
-                for (int k = 0; k < cntl; k++) {
-                    const Tri32 t = load_tri32(m.tris32, first + k);
-                    const float d2 =
-                        tri_dist_sq_fast(px, py, pz, t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
-                    if (COUNT) cnt.tri++;
-                    if (d2 < thr) {
-                        float d = d2;
-                        int p = first + k;
-#pragma unroll
-                        for (int s = 0; s < kCand; s++) {
-                            if (d < win.d[s]) {
-                                const float td = win.d[s];
-                                const int tp = win.p[s];
-                                win.d[s] = d;
-                                win.p[s] = p;
-                                d = td;
-                                p = tp;
-                            }
-                        }
-                        win.evicted = fminf(win.evicted, d);
-                        if (d2 < best) {
-                            best = d2;
-                            thr = window_thr(best, tau_rel, m.coord_scale);
-                        }
-                    }
-                }
+                p.template leaf<COUNT>(leaf_first(rc), leaf_count(rc), want, cnt);
             } else if (next < 0) {
                 next = rc;
             } else if (sp < kStackSize) {
@@ -354,7 +399,8 @@ __device__ void traverse_fast(const DeviceMesh &m, const float px, const float p
         if (next < 0) {
             while (sp > 0) {
                 sp--;
-                if (sdist[sp] < thr) {
+                const bool w = sdist[sp] < p.thr;
+                if (WARP ? __any_sync(0xffffffffu, w) : w) {
                     next = snode[sp];
                     break;
                 }
@@ -487,91 +533,81 @@ __device__ __forceinline__ void flush_counters(const QueryArgs &a, const Counter
 
 // ---- kernels ----------------------------------------------------------------------------------------
 
-template <bool COUNT>
-__global__ void __launch_bounds__(kThreads) k_query_f64(const QueryArgs a) {
-    long long q, i = 0, j = 0, k = 0;
+// One kernel per (arithmetic, traversal mode, instrumentation). Lanes without a query (the edge of
+// a grid brick, the tail of a point list) take part in warp-mode traversal with a negative
+// threshold, so they never ask for a node.
+template <int PREC, bool WARP, bool COUNT>
+__global__ void __launch_bounds__(kThreads, PREC == SSDF_PREC_F64 ? 1 : SSDF_B200_QUERY_MIN_BLOCKS)
+    k_query(const QueryArgs a) {
+    long long q = 0, i = 0, j = 0, k = 0;
     const bool valid = map_thread(a, q, i, j, k);
     Counters cnt;
-    if (valid) {
-        double qx, qy, qz;
-        query_point(a, q, i, j, k, qx, qy, qz);
-        double best = initial_bound(a, q);
-        int bid = -1, bpos = -1;
-        traverse_exact<double, COUNT>(a.m, qx, qy, qz, best, bid, bpos, cnt);
-        write_result(a, q, qx, qy, qz, best, bid, bpos);
-    }
-    if (COUNT) flush_counters(a, cnt);
-}
-
-// The reference's float arithmetic end to end (edf<float> value); in/out outputs only.
-template <bool COUNT>
-__global__ void __launch_bounds__(kThreads) k_query_f32(const QueryArgs a) {
-    long long q, i = 0, j = 0, k = 0;
-    const bool valid = map_thread(a, q, i, j, k);
-    Counters cnt;
-    if (valid) {
-        double qx, qy, qz;
-        query_point(a, q, i, j, k, qx, qy, qz);
-        const float o = a.out_f64 ? float(((const double *)a.out)[q]) : ((const float *)a.out)[q];
-        float best = a.output == SSDF_OUT_SQEDF ? o : o * o;
-        int bid = -1, bpos = -1;
-        traverse_exact<float, COUNT>(a.m, float(qx), float(qy), float(qz), best, bid, bpos, cnt);
-        if (a.output == SSDF_OUT_SQEDF) {
-            store_out(a, q, double(best));
-        } else {
-            store_out(a, q, double(sqrtf(best)));
-            if (a.outtri && bid >= 0) a.outtri[q] = bid;
+    double qx = 0.0, qy = 0.0, qz = 0.0;
+    if (valid) query_point(a, q, i, j, k, qx, qy, qz);
+    if (PREC == SSDF_PREC_F64) {
+        const double init = valid ? initial_bound(a, q) : 0.0;
+        ExactPolicy<double> p(a.m, qx, qy, qz, init);
+        if (!valid) p.thr = -1.0;
+        if (WARP || valid) traverse<WARP, COUNT>(p, cnt);
+        if (valid) write_result(a, q, qx, qy, qz, p.best, p.bid, p.bpos);
+    } else if (PREC == SSDF_PREC_F32) {
+        // the reference's float arithmetic end to end (edf<float>'s value); edf and sqedf outputs
+        float init = 0.f;
+        if (valid) {
+            const float o = a.out_f64 ? float(((const double *)a.out)[q]) : ((const float *)a.out)[q];
+            init = a.output == SSDF_OUT_SQEDF ? o : o * o;
         }
-    }
-    if (COUNT) flush_counters(a, cnt);
-}
-
-template <bool COUNT>
-__global__ void __launch_bounds__(kThreads) k_query_f32x(const QueryArgs a) {
-    long long q, i = 0, j = 0, k = 0;
-    const bool valid = map_thread(a, q, i, j, k);
-    Counters cnt;
-    if (valid) {
-        double qx, qy, qz;
-        query_point(a, q, i, j, k, qx, qy, qz);
-        const double init = initial_bound(a, q);
+        ExactPolicy<float> p(a.m, float(qx), float(qy), float(qz), init);
+        if (!valid) p.thr = -1.f;
+        if (WARP || valid) traverse<WARP, COUNT>(p, cnt);
+        if (valid) {
+            if (a.output == SSDF_OUT_SQEDF) {
+                store_out(a, q, double(p.best));
+            } else {
+                store_out(a, q, double(sqrtf(p.best)));
+                if (a.outtri && p.bid >= 0) a.outtri[q] = p.bid;
+            }
+        }
+    } else {
+        const double init = valid ? initial_bound(a, q) : 0.0;
         // float start bound rounded up, so no triangle closer in double is cut off
-        float best = init < dinf() ? __double2float_ru(init) : finf();
-        Window win;
+        const float finit = init < dinf() ? __double2float_ru(init) : finf();
+        FastPolicy p(a.m, float(qx), float(qy), float(qz), finit, a.tau_rel);
+        if (!valid) p.thr = -1.f;
+        if (WARP || valid) traverse<WARP, COUNT>(p, cnt);
+        if (valid) {
+            if (p.win.evicted < p.thr) {
+                const int slot = atomicAdd(a.fallback_count, 1);
+                a.fallback_ids[slot] = int(q);  // q < 2^31 is checked on the host
+                a.fallback_thr[slot] = p.thr;
+            } else {
+                double b = init;
+                int bid = -1, bpos = -1;
 #pragma unroll
-        for (int s = 0; s < kCand; s++) win.d[s] = finf(), win.p[s] = -1;
-        win.evicted = finf();
-        float thr;
-        traverse_fast<COUNT>(a.m, float(qx), float(qy), float(qz), best, a.tau_rel, win, thr, cnt);
-        if (win.evicted < thr) {
-            const int slot = atomicAdd(a.fallback_count, 1);
-            a.fallback_ids[slot] = int(q);  // q < 2^31 is checked on the host
-        } else {
-            double b = init;
-            int bid = -1, bpos = -1;
-#pragma unroll
-            for (int s = 0; s < kCand; s++) {
-                if (win.d[s] < thr) {
-                    const Tri64 t = load_tri64(a.m.tris64, win.p[s]);
-                    const double d2 =
-                        tri_dist_sq_exact<double>(qx, qy, qz, t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
-                    if (COUNT) cnt.fix++;
-                    if (d2 < b || (d2 == b && bid >= 0 && t.id < bid)) {
-                        b = d2;
-                        bid = t.id;
-                        bpos = win.p[s];
+                for (int s = 0; s < kCand; s++) {
+                    if (p.win.d[s] < p.thr) {
+                        const Tri64 t = load_tri64(a.m.tris64, p.win.p[s]);
+                        const double d2 = tri_dist_sq_exact<double>(qx, qy, qz, t.ax, t.ay, t.az, t.bx, t.by, t.bz,
+                                                                    t.cx, t.cy, t.cz);
+                        if (COUNT) cnt.fix++;
+                        if (d2 < b || (d2 == b && bid >= 0 && t.id < bid)) {
+                            b = d2;
+                            bid = t.id;
+                            bpos = p.win.p[s];
+                        }
                     }
                 }
+                write_result(a, q, qx, qy, qz, b, bid, bpos);
             }
-            write_result(a, q, qx, qy, qz, b, bid, bpos);
         }
     }
     if (COUNT) flush_counters(a, cnt);
 }
 
-// Queries whose F32X window overflowed, finished with the F64 traversal (grid-stride over the list).
+// Queries whose F32X window overflowed its slots, finished by the WindowPolicy walk (grid-stride
+// over the list, one thread per query: these are few and scattered).
 template <bool COUNT>
-__global__ void __launch_bounds__(kThreads) k_fallback(const QueryArgs a) {
+__global__ void __launch_bounds__(kThreads) k_window(const QueryArgs a) {
     const int n = *a.fallback_count;
     Counters cnt;
     for (int idx = blockIdx.x * kThreads + threadIdx.x; idx < n; idx += gridDim.x * kThreads) {
@@ -580,15 +616,29 @@ __global__ void __launch_bounds__(kThreads) k_fallback(const QueryArgs a) {
         if (a.is_grid) grid_ijk(a, q, i, j, k);
         double qx, qy, qz;
         query_point(a, q, i, j, k, qx, qy, qz);
-        double best = initial_bound(a, q);
-        int bid = -1, bpos = -1;
-        traverse_exact<double, COUNT>(a.m, qx, qy, qz, best, bid, bpos, cnt);
-        write_result(a, q, qx, qy, qz, best, bid, bpos);
+        WindowPolicy p(a.m, qx, qy, qz, a.fallback_thr[idx], initial_bound(a, q));
+        traverse<false, COUNT>(p, cnt);
+        write_result(a, q, qx, qy, qz, p.best, p.bid, p.bpos);
     }
     if (COUNT) flush_counters(a, cnt);
 }
 
 thread_local unsigned long long t_last_counts[4] = {0, 0, 0, 0};
+
+template <int PREC, bool WARP>
+cudaError_t launch_main(const QueryArgs &a, bool count, unsigned nblocks, cudaStream_t stream) {
+    if (count)
+        k_query<PREC, WARP, true><<<nblocks, kThreads, 0, stream>>>(a);
+    else
+        k_query<PREC, WARP, false><<<nblocks, kThreads, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+template <int PREC>
+cudaError_t launch_prec(const QueryArgs &a, bool warp, bool count, unsigned nblocks, cudaStream_t stream) {
+    return warp ? launch_main<PREC, true>(a, count, nblocks, stream)
+                : launch_main<PREC, false>(a, count, nblocks, stream);
+}
 
 }  // namespace
 
@@ -600,14 +650,23 @@ int query_counts(int64_t *tri, int64_t *box, int64_t *fix, int64_t *fallback) {
     return SSDF_OK;
 }
 
+// Traversal mode: SSDF_B200_TRAVERSAL=warp|thread overrides; by default grids (coherent bricks) walk
+// in warp packets and point lists thread by thread.
+static bool use_warp(const QueryArgs &a) {
+    const char *v = env_str("SSDF_B200_TRAVERSAL");
+    if (v && !strcmp(v, "warp")) return true;
+    if (v && !strcmp(v, "thread")) return false;
+    return a.is_grid != 0;
+}
+
 int launch_query(const QueryArgs &args_in, int precision, cudaStream_t stream) {
     QueryArgs a = args_in;
     const long long n = a.is_grid ? a.nx * a.ny * a.nz : a.npoints;
     if (n <= 0) return SSDF_OK;
     if (precision == SSDF_PREC_F64 && !a.m.nodes64)
         return fail(SSDF_ERR_INVALID_ARGUMENT, "mesh built without double data (keep_fp64=0)");
-    if (precision == SSDF_PREC_F32_FIXUP && !a.m.tris64)
-        return fail(SSDF_ERR_INVALID_ARGUMENT, "fix-up queries need the double triangles (keep_fp64=1)");
+    if (precision == SSDF_PREC_F32_FIXUP && (!a.m.tris64 || !a.m.nodes64))
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "fix-up queries need the double triangles and BVH (keep_fp64=1)");
     if (a.output == SSDF_OUT_SDF && !a.m.face_n)
         return fail(SSDF_ERR_INVALID_ARGUMENT, "signed queries need a mesh built with normals=1");
     if (a.output == SSDF_OUT_SDF && !a.m.tris64)
@@ -617,6 +676,7 @@ int launch_query(const QueryArgs &args_in, int precision, cudaStream_t stream) {
     if (precision == SSDF_PREC_F32 && (a.output == SSDF_OUT_SDF || a.output == SSDF_OUT_CLOSEST))
         return fail(SSDF_ERR_INVALID_ARGUMENT, "SSDF_PREC_F32 serves the edf and sqedf outputs");
     const bool count = env_int("SSDF_B200_COUNT", 0) != 0;
+    const bool warp = use_warp(a);
     long long nblocks;
     if (a.is_grid)
         nblocks = ((a.nx + 7) / 8) * ((a.ny + 3) / 4) * ((a.nz + 3) / 4);
@@ -631,53 +691,38 @@ int launch_query(const QueryArgs &args_in, int precision, cudaStream_t stream) {
         SSDF_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(unsigned long long), stream));
     }
     a.counters = counters;
+    cudaError_t e = cudaSuccess;
     if (precision == SSDF_PREC_F32_FIXUP) {
         if (n >= 0x7fffffffll) {
             st = fail(SSDF_ERR_NOT_SUPPORTED, "more than 2^31 - 1 queries in one fix-up launch");
-        } else if (cudaMallocAsync(&fb, sizeof(int) * size_t(n + 1), stream) != cudaSuccess) {
+        } else if (cudaMallocAsync(&fb, sizeof(int) * size_t(2 * n + 1), stream) != cudaSuccess) {
             st = fail(SSDF_ERR_OUT_OF_MEMORY, "fix-up overflow list");
         } else {
             a.fallback_count = fb;
             a.fallback_ids = fb + 1;
-            cudaMemsetAsync(fb, 0, sizeof(int), stream);
-            if (count)
-                k_query_f32x<true><<<unsigned(nblocks), kThreads, 0, stream>>>(a);
-            else
-                k_query_f32x<false><<<unsigned(nblocks), kThreads, 0, stream>>>(a);
-            cudaError_t e = cudaGetLastError();
-            if (e != cudaSuccess) st = cuda_fail(e, "k_query_f32x", __FILE__, __LINE__);
-            if (st == SSDF_OK && a.m.nodes64) {
+            a.fallback_thr = reinterpret_cast<float *>(fb + 1 + n);
+            e = cudaMemsetAsync(fb, 0, sizeof(int), stream);
+            if (e == cudaSuccess) e = launch_prec<SSDF_PREC_F32_FIXUP>(a, warp, count, unsigned(nblocks), stream);
+            if (e == cudaSuccess) {
                 if (count)
-                    k_fallback<true><<<296, kThreads, 0, stream>>>(a);
+                    k_window<true><<<296, kThreads, 0, stream>>>(a);
                 else
-                    k_fallback<false><<<296, kThreads, 0, stream>>>(a);
+                    k_window<false><<<296, kThreads, 0, stream>>>(a);
                 e = cudaGetLastError();
-                if (e != cudaSuccess) st = cuda_fail(e, "k_fallback", __FILE__, __LINE__);
-            } else if (st == SSDF_OK) {
-                st = fail(SSDF_ERR_INVALID_ARGUMENT, "fix-up queries need the double BVH (keep_fp64=1)");
             }
         }
     } else if (precision == SSDF_PREC_F64) {
-        if (count)
-            k_query_f64<true><<<unsigned(nblocks), kThreads, 0, stream>>>(a);
-        else
-            k_query_f64<false><<<unsigned(nblocks), kThreads, 0, stream>>>(a);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) st = cuda_fail(e, "k_query_f64", __FILE__, __LINE__);
+        e = launch_prec<SSDF_PREC_F64>(a, warp, count, unsigned(nblocks), stream);
     } else {
-        if (count)
-            k_query_f32<true><<<unsigned(nblocks), kThreads, 0, stream>>>(a);
-        else
-            k_query_f32<false><<<unsigned(nblocks), kThreads, 0, stream>>>(a);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) st = cuda_fail(e, "k_query_f32", __FILE__, __LINE__);
+        e = launch_prec<SSDF_PREC_F32>(a, warp, count, unsigned(nblocks), stream);
     }
+    if (e != cudaSuccess && st == SSDF_OK) st = cuda_fail(e, "query launch", __FILE__, __LINE__);
     if (count && st == SSDF_OK) {
         unsigned long long h[4] = {0, 0, 0, 0};
         int nfb = 0;
         cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, stream);
         if (fb) cudaMemcpyAsync(&nfb, fb, sizeof(int), cudaMemcpyDeviceToHost, stream);
-        cudaError_t e = cudaStreamSynchronize(stream);
+        e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) st = cuda_fail(e, "query counters", __FILE__, __LINE__);
         h[3] = (unsigned long long)nfb;
         memcpy(t_last_counts, h, sizeof(h));

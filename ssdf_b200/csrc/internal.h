@@ -93,8 +93,9 @@ struct QueryArgs {
     void *outx, *outy, *outz;
     // fix-up window: tau = tau_rel * (coord_scale + d)
     float tau_rel;
-    // overflow list of the FP32 fix-up kernel, finished by the FP64 kernel
+    // overflow list of the FP32 fix-up kernel (query, final window), finished by k_window
     int *fallback_ids;
+    float *fallback_thr;
     int *fallback_count;
     // optional counters [4]: triangle tests, box tests, fix-up evaluations, fallbacks
     unsigned long long *counters;

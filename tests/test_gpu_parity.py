@@ -165,3 +165,18 @@ def test_device_mesh_handle_matches_drop_in():
     st = dm.stats()
     assert st["depth"] < 64 and st["leaves"] > 0
     dm.close()
+
+
+@pytest.mark.parametrize("mode", ["warp", "thread"])
+def test_traversal_modes(mode, knot):
+    """Thread-per-query and warp-packet traversal give the oracle's values, grid and point list."""
+    mesh = knot["mesh"]
+    q = knot["q"]
+    with env(SSDF_B200_TRAVERSAL=mode):
+        sd, tri = S.sdf_points(q, mesh)
+        for prec in ("f32x", "f64"):
+            with env(SSDF_B200_PRECISION=prec):
+                gsd, gtri = S.sample_sdf_bvh(mesh, knot["grid"], with_index=True)
+            assert np.array_equal(gsd[knot["ids"]], knot["sd"]), prec
+            assert np.array_equal(gtri[knot["ids"]], knot["stri"]), prec
+    assert np.array_equal(sd, knot["sd"]) and np.array_equal(tri, knot["stri"])
