@@ -31,7 +31,12 @@ namespace ssdf_b200 {
 namespace {
 
 constexpr int kThreads = 128;
-constexpr int kCand = 8;  // F32X window slots
+// F32X window slots: candidates kept per query in registers. A window that overflows them sends
+// its query to the second stage (k_window); fewer slots means fewer registers, more second stage.
+#ifndef SSDF_B200_WINDOW_SLOTS
+#define SSDF_B200_WINDOW_SLOTS 8
+#endif
+constexpr int kCand = SSDF_B200_WINDOW_SLOTS;
 // Minimum resident blocks per SM the float query kernels are compiled for: 8 blocks of 128 caps
 // them at 64 registers. The traversal is latency-bound, so the occupancy this buys outweighs the
 // few spills (measured: -22 % time on the torus-knot grid); the double kernel keeps its registers.
@@ -49,14 +54,13 @@ __device__ __forceinline__ float finf() { return __int_as_float(0x7f800000); }
 // ---- query mapping ------------------------------------------------------------------------------
 
 // Grid brick: block = 8 (x) * 4 (y) * 4 (z) nodes, warp = 4 * 4 * 2.
-__device__ __forceinline__ bool map_thread(const QueryArgs &a, long long &q, long long &i, long long &j,
-                                           long long &k) {
+__device__ __forceinline__ bool map_thread(const QueryArgs &a, long long b, long long &q, long long &i,
+                                           long long &j, long long &k) {
     if (!a.is_grid) {
-        q = (long long)blockIdx.x * kThreads + threadIdx.x;
+        q = b * kThreads + threadIdx.x;
         return q < a.npoints;
     }
     const long long bxn = (a.nx + 7) >> 3, byn = (a.ny + 3) >> 2;
-    const long long b = blockIdx.x;
     const long long bx = b % bxn, r = b / bxn;
     const long long by = r % byn, bz = r / byn;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -141,6 +145,54 @@ __device__ __forceinline__ Node64 load_node64(const double2 *__restrict__ nodes,
     o.r0 = int((unsigned)__double_as_longlong(r.x));
     o.r1 = int((unsigned)__double_as_longlong(r.y));
     return o;
+}
+
+// 4-wide node: per child c, box (lox, hix, loy, hiy, loz, hiz)[c] and reference r[c].
+template <typename T>
+__device__ __forceinline__ void boxes4_exact(const DeviceMesh &m, int node, T px, T py, T pz, T (&d)[4], int (&r)[4]);
+
+template <>
+__device__ __forceinline__ void boxes4_exact<float>(const DeviceMesh &m, int node, float px, float py, float pz,
+                                                    float (&d)[4], int (&r)[4]) {
+    const float4 *p = m.nodes4_32 + 8 * node;
+    const float4 lx = __ldg(p), hx = __ldg(p + 1), ly = __ldg(p + 2), hy = __ldg(p + 3), lz = __ldg(p + 4),
+                 hz = __ldg(p + 5), rr = __ldg(p + 6);
+    d[0] = box_dist_sq<float>(px, py, pz, lx.x, hx.x, ly.x, hy.x, lz.x, hz.x);
+    d[1] = box_dist_sq<float>(px, py, pz, lx.y, hx.y, ly.y, hy.y, lz.y, hz.y);
+    d[2] = box_dist_sq<float>(px, py, pz, lx.z, hx.z, ly.z, hy.z, lz.z, hz.z);
+    d[3] = box_dist_sq<float>(px, py, pz, lx.w, hx.w, ly.w, hy.w, lz.w, hz.w);
+    r[0] = __float_as_int(rr.x), r[1] = __float_as_int(rr.y), r[2] = __float_as_int(rr.z), r[3] = __float_as_int(rr.w);
+}
+
+template <>
+__device__ __forceinline__ void boxes4_exact<double>(const DeviceMesh &m, int node, double px, double py, double pz,
+                                                     double (&d)[4], int (&r)[4]) {
+    const double2 *p = m.nodes4_64 + 14 * node;
+    double2 row[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) row[k] = __ldg(p + k);
+    const double2 rr = __ldg(p + 12);
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const int h = c >> 1;
+        auto pick = [&](int rw) { return (c & 1) ? row[2 * rw + h].y : row[2 * rw + h].x; };
+        d[c] = box_dist_sq<double>(px, py, pz, pick(0), pick(1), pick(2), pick(3), pick(4), pick(5));
+    }
+    const unsigned long long a = (unsigned long long)__double_as_longlong(rr.x);
+    const unsigned long long b = (unsigned long long)__double_as_longlong(rr.y);
+    r[0] = int(unsigned(a)), r[1] = int(unsigned(a >> 32)), r[2] = int(unsigned(b)), r[3] = int(unsigned(b >> 32));
+}
+
+__device__ __forceinline__ void boxes4_fast(const DeviceMesh &m, int node, float px, float py, float pz,
+                                            float (&d)[4], int (&r)[4]) {
+    const float4 *p = m.nodes4_32 + 8 * node;
+    const float4 lx = __ldg(p), hx = __ldg(p + 1), ly = __ldg(p + 2), hy = __ldg(p + 3), lz = __ldg(p + 4),
+                 hz = __ldg(p + 5), rr = __ldg(p + 6);
+    d[0] = box_dist_sq_fast(px, py, pz, lx.x, hx.x, ly.x, hy.x, lz.x, hz.x);
+    d[1] = box_dist_sq_fast(px, py, pz, lx.y, hx.y, ly.y, hy.y, lz.y, hz.y);
+    d[2] = box_dist_sq_fast(px, py, pz, lx.z, hx.z, ly.z, hy.z, lz.z, hz.z);
+    d[3] = box_dist_sq_fast(px, py, pz, lx.w, hx.w, ly.w, hy.w, lz.w, hz.w);
+    r[0] = __float_as_int(rr.x), r[1] = __float_as_int(rr.y), r[2] = __float_as_int(rr.z), r[3] = __float_as_int(rr.w);
 }
 
 struct Tri32 {
@@ -231,6 +283,9 @@ struct ExactPolicy {
     __device__ __forceinline__ void boxes(int node, T &d0, T &d1, int &r0, int &r1) const {
         ExactData<T>::boxes(m, node, px, py, pz, d0, d1, r0, r1);
     }
+    __device__ __forceinline__ void boxes4(int node, T (&d)[4], int (&r)[4]) const {
+        boxes4_exact<T>(m, node, px, py, pz, d, r);
+    }
     template <bool COUNT>
     __device__ __forceinline__ void leaf(int first, int n, bool want, Counters &cnt) {
         for (int k = 0; k < n; k++) {
@@ -282,6 +337,9 @@ struct FastPolicy {
         r0 = n.r0;
         r1 = n.r1;
     }
+    __device__ __forceinline__ void boxes4(int node, float (&d)[4], int (&r)[4]) const {
+        boxes4_fast(m, node, px, py, pz, d, r);
+    }
     template <bool COUNT>
     __device__ __forceinline__ void leaf(int first, int n, bool want, Counters &cnt) {
         for (int k = 0; k < n; k++) {
@@ -330,6 +388,9 @@ struct WindowPolicy {
         d1 = box_dist_sq_fast(px, py, pz, n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w);
         r0 = n.r0;
         r1 = n.r1;
+    }
+    __device__ __forceinline__ void boxes4(int node, float (&d)[4], int (&r)[4]) const {
+        boxes4_fast(m, node, px, py, pz, d, r);
     }
     template <bool COUNT>
     __device__ __forceinline__ void leaf(int first, int n, bool want, Counters &cnt) {
@@ -409,6 +470,91 @@ __device__ __forceinline__ void traverse(P &p, Counters &cnt) {
         }
         node = next;
     }
+}
+
+// The same over the 4-wide BVH. Children are visited in ascending box distance -- the lane's own in
+// thread mode, a representative lane's (the brick centre) in warp mode -- leaves first in that
+// order, then the nearest wanted internal child is entered and the others pushed farthest-first.
+constexpr int kRepLane = 21;  // (1, 1, 1) of the 4 x 4 x 2 brick
+
+template <typename R>
+__device__ __forceinline__ void cswap4(float (&k)[4], R (&d)[4], int (&r)[4], int i, int j) {
+    if (k[j] < k[i]) {
+        const float tk = k[i];
+        k[i] = k[j];
+        k[j] = tk;
+        const R td = d[i];
+        d[i] = d[j];
+        d[j] = td;
+        const int tr = r[i];
+        r[i] = r[j];
+        r[j] = tr;
+    }
+}
+
+template <bool WARP, bool COUNT, class P>
+__device__ __forceinline__ void traverse4(P &p, Counters &cnt) {
+    using R = typename P::R;
+    int snode[kStackSize];
+    R sdist[kStackSize];
+    int sp = 0;
+    int node = 0;
+    while (true) {
+        R d[4];
+        int r[4];
+        p.boxes4(node, d, r);
+        if (COUNT) cnt.box += 4;
+        float key[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++) key[c] = WARP ? __shfl_sync(0xffffffffu, float(d[c]), kRepLane) : float(d[c]);
+        cswap4(key, d, r, 0, 1);
+        cswap4(key, d, r, 2, 3);
+        cswap4(key, d, r, 0, 2);
+        cswap4(key, d, r, 1, 3);
+        cswap4(key, d, r, 1, 2);
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            if (r[c] >= 0 || r[c] == kEmptyRef) continue;
+            const bool want = d[c] < p.thr;
+            if (WARP ? !__any_sync(0xffffffffu, want) : !want) continue;
+            p.template leaf<COUNT>(leaf_first(r[c]), leaf_count(r[c]), want, cnt);
+        }
+        int next = -1;
+        R next_d = R(0);
+#pragma unroll
+        for (int c = 3; c >= 0; c--) {
+            if (r[c] < 0) continue;
+            const bool want = d[c] < p.thr;
+            if (WARP ? !__any_sync(0xffffffffu, want) : !want) continue;
+            if (next >= 0 && sp < kStackSize) {
+                snode[sp] = next;
+                sdist[sp] = next_d;
+                sp++;
+            }
+            next = r[c];
+            next_d = d[c];
+        }
+        if (next < 0) {
+            while (sp > 0) {
+                sp--;
+                const bool w = sdist[sp] < p.thr;
+                if (WARP ? __any_sync(0xffffffffu, w) : w) {
+                    next = snode[sp];
+                    break;
+                }
+            }
+            if (next < 0) break;
+        }
+        node = next;
+    }
+}
+
+template <bool WARP, bool WIDE, bool COUNT, class P>
+__device__ __forceinline__ void walk(P &p, Counters &cnt) {
+    if (WIDE)
+        traverse4<WARP, COUNT>(p, cnt);
+    else
+        traverse<WARP, COUNT>(p, cnt);
 }
 
 // ---- outputs ----------------------------------------------------------------------------------------
@@ -536,19 +682,17 @@ __device__ __forceinline__ void flush_counters(const QueryArgs &a, const Counter
 // One kernel per (arithmetic, traversal mode, instrumentation). Lanes without a query (the edge of
 // a grid brick, the tail of a point list) take part in warp-mode traversal with a negative
 // threshold, so they never ask for a node.
-template <int PREC, bool WARP, bool COUNT>
-__global__ void __launch_bounds__(kThreads, PREC == SSDF_PREC_F64 ? 1 : SSDF_B200_QUERY_MIN_BLOCKS)
-    k_query(const QueryArgs a) {
+template <int PREC, bool WARP, bool WIDE, bool COUNT>
+__device__ __forceinline__ void query_block(const QueryArgs &a, long long block, Counters &cnt) {
     long long q = 0, i = 0, j = 0, k = 0;
-    const bool valid = map_thread(a, q, i, j, k);
-    Counters cnt;
+    const bool valid = map_thread(a, block, q, i, j, k);
     double qx = 0.0, qy = 0.0, qz = 0.0;
     if (valid) query_point(a, q, i, j, k, qx, qy, qz);
     if (PREC == SSDF_PREC_F64) {
         const double init = valid ? initial_bound(a, q) : 0.0;
         ExactPolicy<double> p(a.m, qx, qy, qz, init);
         if (!valid) p.thr = -1.0;
-        if (WARP || valid) traverse<WARP, COUNT>(p, cnt);
+        if (WARP || valid) walk<WARP, WIDE, COUNT>(p, cnt);
         if (valid) write_result(a, q, qx, qy, qz, p.best, p.bid, p.bpos);
     } else if (PREC == SSDF_PREC_F32) {
         // the reference's float arithmetic end to end (edf<float>'s value); edf and sqedf outputs
@@ -559,7 +703,7 @@ __global__ void __launch_bounds__(kThreads, PREC == SSDF_PREC_F64 ? 1 : SSDF_B20
         }
         ExactPolicy<float> p(a.m, float(qx), float(qy), float(qz), init);
         if (!valid) p.thr = -1.f;
-        if (WARP || valid) traverse<WARP, COUNT>(p, cnt);
+        if (WARP || valid) walk<WARP, WIDE, COUNT>(p, cnt);
         if (valid) {
             if (a.output == SSDF_OUT_SQEDF) {
                 store_out(a, q, double(p.best));
@@ -569,25 +713,31 @@ __global__ void __launch_bounds__(kThreads, PREC == SSDF_PREC_F64 ? 1 : SSDF_B20
             }
         }
     } else {
-        const double init = valid ? initial_bound(a, q) : 0.0;
-        // float start bound rounded up, so no triangle closer in double is cut off
-        const float finit = init < dinf() ? __double2float_ru(init) : finf();
+        // the double point and bound are recomputed after the walk rather than kept live through it
+        float finit = -1.f;
+        if (valid) {
+            const double init = initial_bound(a, q);
+            // float start bound rounded up, so no triangle closer in double is cut off
+            finit = init < dinf() ? __double2float_ru(init) : finf();
+        }
         FastPolicy p(a.m, float(qx), float(qy), float(qz), finit, a.tau_rel);
         if (!valid) p.thr = -1.f;
-        if (WARP || valid) traverse<WARP, COUNT>(p, cnt);
+        if (WARP || valid) walk<WARP, WIDE, COUNT>(p, cnt);
         if (valid) {
             if (p.win.evicted < p.thr) {
                 const int slot = atomicAdd(a.fallback_count, 1);
                 a.fallback_ids[slot] = int(q);  // q < 2^31 is checked on the host
                 a.fallback_thr[slot] = p.thr;
             } else {
-                double b = init;
+                double rx, ry, rz;
+                query_point(a, q, i, j, k, rx, ry, rz);
+                double b = initial_bound(a, q);
                 int bid = -1, bpos = -1;
 #pragma unroll
                 for (int s = 0; s < kCand; s++) {
                     if (p.win.d[s] < p.thr) {
                         const Tri64 t = load_tri64(a.m.tris64, p.win.p[s]);
-                        const double d2 = tri_dist_sq_exact<double>(qx, qy, qz, t.ax, t.ay, t.az, t.bx, t.by, t.bz,
+                        const double d2 = tri_dist_sq_exact<double>(rx, ry, rz, t.ax, t.ay, t.az, t.bx, t.by, t.bz,
                                                                     t.cx, t.cy, t.cz);
                         if (COUNT) cnt.fix++;
                         if (d2 < b || (d2 == b && bid >= 0 && t.id < bid)) {
@@ -597,47 +747,138 @@ __global__ void __launch_bounds__(kThreads, PREC == SSDF_PREC_F64 ? 1 : SSDF_B20
                         }
                     }
                 }
-                write_result(a, q, qx, qy, qz, b, bid, bpos);
+                write_result(a, q, rx, ry, rz, b, bid, bpos);
             }
         }
     }
+}
+
+template <int PREC, bool WARP, bool WIDE, bool COUNT>
+__global__ void __launch_bounds__(kThreads, PREC == SSDF_PREC_F64 ? 1 : SSDF_B200_QUERY_MIN_BLOCKS)
+    k_query(const QueryArgs a) {
+    Counters cnt;
+    query_block<PREC, WARP, WIDE, COUNT>(a, blockIdx.x, cnt);
     if (COUNT) flush_counters(a, cnt);
 }
 
 // Queries whose F32X window overflowed its slots, finished by the WindowPolicy walk (grid-stride
 // over the list, one thread per query: these are few and scattered).
-template <bool COUNT>
+template <bool WIDE, bool COUNT>
+__device__ __forceinline__ void window_one(const QueryArgs &a, int idx, Counters &cnt) {
+    const long long q = a.fallback_ids[idx];
+    long long i = 0, j = 0, k = 0;
+    if (a.is_grid) grid_ijk(a, q, i, j, k);
+    double qx, qy, qz;
+    query_point(a, q, i, j, k, qx, qy, qz);
+    WindowPolicy p(a.m, qx, qy, qz, a.fallback_thr[idx], initial_bound(a, q));
+    walk<false, WIDE, COUNT>(p, cnt);
+    write_result(a, q, qx, qy, qz, p.best, p.bid, p.bpos);
+}
+
+template <bool WIDE, bool COUNT>
 __global__ void __launch_bounds__(kThreads) k_window(const QueryArgs a) {
     const int n = *a.fallback_count;
     Counters cnt;
-    for (int idx = blockIdx.x * kThreads + threadIdx.x; idx < n; idx += gridDim.x * kThreads) {
-        const long long q = a.fallback_ids[idx];
-        long long i = 0, j = 0, k = 0;
-        if (a.is_grid) grid_ijk(a, q, i, j, k);
-        double qx, qy, qz;
-        query_point(a, q, i, j, k, qx, qy, qz);
-        WindowPolicy p(a.m, qx, qy, qz, a.fallback_thr[idx], initial_bound(a, q));
-        traverse<false, COUNT>(p, cnt);
-        write_result(a, q, qx, qy, qz, p.best, p.bid, p.bpos);
-    }
+    for (int idx = blockIdx.x * kThreads + threadIdx.x; idx < n; idx += gridDim.x * kThreads)
+        window_one<WIDE, COUNT>(a, idx, cnt);
     if (COUNT) flush_counters(a, cnt);
 }
 
-thread_local unsigned long long t_last_counts[4] = {0, 0, 0, 0};
+// ---- batches: many (mesh, query set) jobs in one persistent launch -----------------------------------
+//
+// The job table lives in device memory (BatchHeader + QueryArgs[] + first block of each job), so a
+// captured CUDA graph of these two kernels replays for any batch composition without being
+// re-instantiated: only the table is rewritten before each replay. Blocks pull work items (one
+// 128-query block of one job) from an atomic counter, largest jobs first (the host orders them).
 
-template <int PREC, bool WARP>
-cudaError_t launch_main(const QueryArgs &a, bool count, unsigned nblocks, cudaStream_t stream) {
+template <int PREC, bool WARP, bool WIDE, bool COUNT>
+__global__ void __launch_bounds__(kThreads, PREC == SSDF_PREC_F64 ? 1 : SSDF_B200_QUERY_MIN_BLOCKS)
+    k_query_batch(const BatchHeader *__restrict__ hdr, const QueryArgs *__restrict__ jobs,
+                  const long long *__restrict__ first_block, unsigned long long *__restrict__ next_item) {
+    __shared__ long long s_item;
+    const int njobs = hdr->njobs;
+    const long long total = hdr->total_blocks;
+    Counters cnt;
+    while (true) {
+        if (threadIdx.x == 0) s_item = (long long)atomicAdd(next_item, 1ull);
+        __syncthreads();
+        const long long it = s_item;
+        __syncthreads();
+        if (it >= total) break;
+        int lo = 0, hi = njobs - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(first_block + mid) <= it) lo = mid; else hi = mid - 1;
+        }
+        query_block<PREC, WARP, WIDE, COUNT>(jobs[lo], it - __ldg(first_block + lo), cnt);
+    }
+    if (COUNT && njobs > 0) flush_counters(jobs[0], cnt);
+}
+
+template <bool WIDE, bool COUNT>
+__global__ void __launch_bounds__(kThreads) k_window_batch(const BatchHeader *__restrict__ hdr,
+                                                           const QueryArgs *__restrict__ jobs) {
+    const int njobs = hdr->njobs;
+    Counters cnt;
+    for (int jb = 0; jb < njobs; jb++) {
+        const QueryArgs &a = jobs[jb];
+        if (!a.fallback_count) continue;
+        const int n = *a.fallback_count;
+        for (int idx = blockIdx.x * kThreads + threadIdx.x; idx < n; idx += gridDim.x * kThreads)
+            window_one<WIDE, COUNT>(a, idx, cnt);
+    }
+    if (COUNT && njobs > 0) flush_counters(jobs[0], cnt);
+}
+
+template <int PREC, bool WARP, bool WIDE>
+cudaError_t launch_batch_main(const BatchLaunch &b, bool count, cudaStream_t stream) {
     if (count)
-        k_query<PREC, WARP, true><<<nblocks, kThreads, 0, stream>>>(a);
+        k_query_batch<PREC, WARP, WIDE, true><<<b.grid, kThreads, 0, stream>>>(b.hdr, b.jobs, b.first_block, b.next_item);
     else
-        k_query<PREC, WARP, false><<<nblocks, kThreads, 0, stream>>>(a);
+        k_query_batch<PREC, WARP, WIDE, false><<<b.grid, kThreads, 0, stream>>>(b.hdr, b.jobs, b.first_block, b.next_item);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || PREC != SSDF_PREC_F32_FIXUP) return e;
+    if (count)
+        k_window_batch<WIDE, true><<<2 * b.sms, kThreads, 0, stream>>>(b.hdr, b.jobs);
+    else
+        k_window_batch<WIDE, false><<<2 * b.sms, kThreads, 0, stream>>>(b.hdr, b.jobs);
     return cudaGetLastError();
 }
 
 template <int PREC>
-cudaError_t launch_prec(const QueryArgs &a, bool warp, bool count, unsigned nblocks, cudaStream_t stream) {
-    return warp ? launch_main<PREC, true>(a, count, nblocks, stream)
-                : launch_main<PREC, false>(a, count, nblocks, stream);
+cudaError_t launch_batch_prec(const BatchLaunch &b, bool count, cudaStream_t stream) {
+    if (b.wide)
+        return b.warp ? launch_batch_main<PREC, true, true>(b, count, stream)
+                      : launch_batch_main<PREC, false, true>(b, count, stream);
+    return b.warp ? launch_batch_main<PREC, true, false>(b, count, stream)
+                  : launch_batch_main<PREC, false, false>(b, count, stream);
+}
+
+template <int PREC, bool WARP, bool WIDE>
+int batch_occupancy() {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_query_batch<PREC, WARP, WIDE, false>, kThreads, 0);
+    return nb > 0 ? nb : 1;
+}
+
+thread_local unsigned long long t_last_counts[4] = {0, 0, 0, 0};
+
+template <int PREC, bool WARP, bool WIDE>
+cudaError_t launch_main(const QueryArgs &a, bool count, unsigned nblocks, cudaStream_t stream) {
+    if (count)
+        k_query<PREC, WARP, WIDE, true><<<nblocks, kThreads, 0, stream>>>(a);
+    else
+        k_query<PREC, WARP, WIDE, false><<<nblocks, kThreads, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+template <int PREC>
+cudaError_t launch_prec(const QueryArgs &a, bool warp, bool wide, bool count, unsigned nblocks, cudaStream_t stream) {
+    if (wide)
+        return warp ? launch_main<PREC, true, true>(a, count, nblocks, stream)
+                    : launch_main<PREC, false, true>(a, count, nblocks, stream);
+    return warp ? launch_main<PREC, true, false>(a, count, nblocks, stream)
+                : launch_main<PREC, false, false>(a, count, nblocks, stream);
 }
 
 }  // namespace
@@ -652,6 +893,9 @@ int query_counts(int64_t *tri, int64_t *box, int64_t *fix, int64_t *fallback) {
 
 // Traversal mode: SSDF_B200_TRAVERSAL=warp|thread overrides; by default grids (coherent bricks) walk
 // in warp packets and point lists thread by thread.
+// BVH arity: SSDF_B200_ARITY=2|4; binary by default (measured as fast as 4-wide on the torus knot).
+static bool use_wide() { return env_int("SSDF_B200_ARITY", 2) == 4; }
+
 static bool use_warp(const QueryArgs &a) {
     const char *v = env_str("SSDF_B200_TRAVERSAL");
     if (v && !strcmp(v, "warp")) return true;
@@ -677,6 +921,7 @@ int launch_query(const QueryArgs &args_in, int precision, cudaStream_t stream) {
         return fail(SSDF_ERR_INVALID_ARGUMENT, "SSDF_PREC_F32 serves the edf and sqedf outputs");
     const bool count = env_int("SSDF_B200_COUNT", 0) != 0;
     const bool warp = use_warp(a);
+    const bool wide = use_wide();
     long long nblocks;
     if (a.is_grid)
         nblocks = ((a.nx + 7) / 8) * ((a.ny + 3) / 4) * ((a.nz + 3) / 4);
@@ -702,19 +947,21 @@ int launch_query(const QueryArgs &args_in, int precision, cudaStream_t stream) {
             a.fallback_ids = fb + 1;
             a.fallback_thr = reinterpret_cast<float *>(fb + 1 + n);
             e = cudaMemsetAsync(fb, 0, sizeof(int), stream);
-            if (e == cudaSuccess) e = launch_prec<SSDF_PREC_F32_FIXUP>(a, warp, count, unsigned(nblocks), stream);
+            if (e == cudaSuccess) e = launch_prec<SSDF_PREC_F32_FIXUP>(a, warp, wide, count, unsigned(nblocks), stream);
             if (e == cudaSuccess) {
-                if (count)
-                    k_window<true><<<296, kThreads, 0, stream>>>(a);
+                if (wide)
+                    count ? k_window<true, true><<<296, kThreads, 0, stream>>>(a)
+                          : k_window<true, false><<<296, kThreads, 0, stream>>>(a);
                 else
-                    k_window<false><<<296, kThreads, 0, stream>>>(a);
+                    count ? k_window<false, true><<<296, kThreads, 0, stream>>>(a)
+                          : k_window<false, false><<<296, kThreads, 0, stream>>>(a);
                 e = cudaGetLastError();
             }
         }
     } else if (precision == SSDF_PREC_F64) {
-        e = launch_prec<SSDF_PREC_F64>(a, warp, count, unsigned(nblocks), stream);
+        e = launch_prec<SSDF_PREC_F64>(a, warp, wide, count, unsigned(nblocks), stream);
     } else {
-        e = launch_prec<SSDF_PREC_F32>(a, warp, count, unsigned(nblocks), stream);
+        e = launch_prec<SSDF_PREC_F32>(a, warp, wide, count, unsigned(nblocks), stream);
     }
     if (e != cudaSuccess && st == SSDF_OK) st = cuda_fail(e, "query launch", __FILE__, __LINE__);
     if (count && st == SSDF_OK) {
@@ -731,5 +978,43 @@ int launch_query(const QueryArgs &args_in, int precision, cudaStream_t stream) {
     if (counters) cudaFreeAsync(counters, stream);
     return st;
 }
+
+// Resident blocks per SM of the batch kernel for this arithmetic / traversal.
+int batch_blocks_per_sm(int precision, bool warp, bool wide) {
+    if (precision == SSDF_PREC_F64)
+        return warp ? (wide ? batch_occupancy<SSDF_PREC_F64, true, true>() : batch_occupancy<SSDF_PREC_F64, true, false>())
+                    : (wide ? batch_occupancy<SSDF_PREC_F64, false, true>() : batch_occupancy<SSDF_PREC_F64, false, false>());
+    if (precision == SSDF_PREC_F32)
+        return warp ? (wide ? batch_occupancy<SSDF_PREC_F32, true, true>() : batch_occupancy<SSDF_PREC_F32, true, false>())
+                    : (wide ? batch_occupancy<SSDF_PREC_F32, false, true>() : batch_occupancy<SSDF_PREC_F32, false, false>());
+    return warp ? (wide ? batch_occupancy<SSDF_PREC_F32_FIXUP, true, true>()
+                        : batch_occupancy<SSDF_PREC_F32_FIXUP, true, false>())
+                : (wide ? batch_occupancy<SSDF_PREC_F32_FIXUP, false, true>()
+                        : batch_occupancy<SSDF_PREC_F32_FIXUP, false, false>());
+}
+
+// Enqueues the persistent batch kernel (and the fix-up window stage) on `stream`; the job table and
+// counters in `b` must already be in device memory. Capturable in a CUDA graph.
+int launch_batch(const BatchLaunch &b, int precision, cudaStream_t stream) {
+    const bool count = env_int("SSDF_B200_COUNT", 0) != 0;
+    cudaError_t e;
+    if (precision == SSDF_PREC_F64)
+        e = launch_batch_prec<SSDF_PREC_F64>(b, count, stream);
+    else if (precision == SSDF_PREC_F32)
+        e = launch_batch_prec<SSDF_PREC_F32>(b, count, stream);
+    else
+        e = launch_batch_prec<SSDF_PREC_F32_FIXUP>(b, count, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "batch launch", __FILE__, __LINE__);
+    return SSDF_OK;
+}
+
+bool default_warp(int is_grid) {
+    const char *v = env_str("SSDF_B200_TRAVERSAL");
+    if (v && !strcmp(v, "warp")) return true;
+    if (v && !strcmp(v, "thread")) return false;
+    return is_grid != 0;
+}
+
+bool default_wide() { return env_int("SSDF_B200_ARITY", 2) == 4; }
 
 }  // namespace ssdf_b200

@@ -37,6 +37,10 @@ int cuda_fail(cudaError_t err, const char *what, const char *file, int line);
 //                           (c0.loz, c0.hiz, c1.loz, c1.hiz), (ref0, ref1, -, -) as int bits
 //   FP64 node (8 x double2): c0 x, c0 y, c0 z, c1 x, c1 y, c1 z as (lo, hi), (ref0, ref1) as
 //                            int bits, padding
+//   4-wide FP32 node (8 x float4): lo x / hi x / lo y / hi y / lo z / hi z of children 0..3, then
+//                           the 4 references as int bits, padding
+//   4-wide FP64 node (14 x double2): the same six rows as pairs of double2, the 4 references as
+//                            int bits in one double2, padding
 // A reference >= 0 is an internal node; < 0 is a leaf ~((first << 5) | (count - 1)) over the
 // triangle records in leaf order; kEmptyRef is an empty slot (its box is inverted).
 // Triangles in leaf order:
@@ -62,6 +66,11 @@ struct DeviceMesh {
     int nleaves = 0;
     const float4 *nodes32 = nullptr;   // [4 * nnodes]
     const double2 *nodes64 = nullptr;  // [8 * nnodes] or null
+    // 4-wide BVH over the same leaves (collapsed from the binary one)
+    int nnodes4 = 0;
+    int depth4 = 0;
+    const float4 *nodes4_32 = nullptr;   // [8 * nnodes4]
+    const double2 *nodes4_64 = nullptr;  // [14 * nnodes4] or null
     const float4 *tris32 = nullptr;    // [3 * nt], leaf order
     const double2 *tris64 = nullptr;   // [5 * nt], leaf order, or null
     // sign data, caller's triangle order
@@ -101,6 +110,24 @@ struct QueryArgs {
     unsigned long long *counters;
 };
 
+// Job table header of a batch (device memory).
+struct BatchHeader {
+    int njobs;
+    int pad;
+    long long total_blocks;
+};
+
+// Device pointers and launch shape of one batch launch.
+struct BatchLaunch {
+    const BatchHeader *hdr;
+    const QueryArgs *jobs;
+    const long long *first_block;
+    unsigned long long *next_item;
+    int grid;   // persistent blocks (SMs x resident blocks per SM)
+    int sms;
+    bool warp, wide;
+};
+
 // ---- mesh build (mesh_build.cu) ------------------------------------------------------------------
 struct MeshStorage;  // owns the device allocations behind a DeviceMesh
 int mesh_build(MeshStorage **storage, DeviceMesh *mesh, ptrdiff_t nt, const int *s0, const int *s1, const int *s2,
@@ -119,6 +146,15 @@ int exclusive_scan_i32(const int *in, int *out, int n, cudaStream_t stream);
 
 // ---- queries (bvh_query.cu) ----------------------------------------------------------------------
 int launch_query(const QueryArgs &args, int precision, cudaStream_t stream);
+int launch_batch(const BatchLaunch &b, int precision, cudaStream_t stream);
+int batch_blocks_per_sm(int precision, bool warp, bool wide);
+bool default_warp(int is_grid);
+bool default_wide();
+// Blocks of 128 queries one job needs (grid bricks of 8x4x4 or 128 consecutive points).
+inline long long query_blocks(const QueryArgs &a) {
+    if (a.is_grid) return ((a.nx + 7) / 8) * ((a.ny + 3) / 4) * ((a.nz + 3) / 4);
+    return (a.npoints + 127) / 128;
+}
 
 // ---- brute force and cell list (brute_force.cu, celllist.cu) -------------------------------------
 int brute_force_edf(int f64, ptrdiff_t npoints, const void *x, const void *y, const void *z, ptrdiff_t nt,

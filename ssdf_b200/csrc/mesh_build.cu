@@ -306,6 +306,118 @@ __global__ void k_write_small_root(int n, const float *__restrict__ box32, const
     }
 }
 
+// 4-wide nodes, top-down: a node starts from its binary node's two children and repeatedly opens
+// the expandable child (internal, > L triangles) of largest surface area until it has four.
+// Internal children become the next level's nodes (slots taken from an atomic counter).
+__device__ __forceinline__ float box_area(const float *b) {
+    const float dx = b[1] - b[0], dy = b[3] - b[2], dz = b[5] - b[4];
+    return dx * dy + dy * dz + dz * dx;
+}
+
+__global__ void k_collapse4(int n_in, const int2 *__restrict__ qin, int2 *__restrict__ qout, int *__restrict__ n_out,
+                            int *__restrict__ slots, int L, const int *__restrict__ child_l,
+                            const int *__restrict__ child_r, const int *__restrict__ first_of,
+                            const int *__restrict__ count, const int *__restrict__ sorted_ids,
+                            const float *__restrict__ pbox32, const double *__restrict__ pbox64,
+                            const float *__restrict__ nbox32, const double *__restrict__ nbox64,
+                            float4 *__restrict__ n32, double2 *__restrict__ n64) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_in) return;
+    const int b = qin[i].x, slot = qin[i].y;
+    int c[4] = {child_l[b], child_r[b], 0, 0};
+    int nc = 2;
+    while (nc < 4) {
+        int pick = -1;
+        float area = -1.f;
+        for (int k = 0; k < nc; k++) {
+            if (c[k] >= 0 && count[c[k]] > L) {
+                const float a = box_area(nbox32 + 6 * c[k]);
+                if (a > area) area = a, pick = k;
+            }
+        }
+        if (pick < 0) break;
+        const int x = c[pick];
+        c[pick] = child_l[x];
+        c[nc++] = child_r[x];
+    }
+    const float inf = __int_as_float(0x7f800000);
+    const double dinf = __longlong_as_double(0x7ff0000000000000ll);
+    float b32[6][4];
+    double b64[6][4];
+    int ref[4];
+    for (int k = 0; k < 4; k++) {
+        const float *f = nullptr;
+        const double *d = nullptr;
+        if (k >= nc) {
+            ref[k] = kEmptyRef;
+        } else if (c[k] < 0) {
+            const int pos = -c[k] - 1;
+            ref[k] = leaf_ref(pos, 1);
+            f = pbox32 + 6 * sorted_ids[pos];
+            d = pbox64 + 6 * sorted_ids[pos];
+        } else {
+            f = nbox32 + 6 * c[k];
+            d = nbox64 + 6 * c[k];
+            if (count[c[k]] <= L) {
+                ref[k] = leaf_ref(first_of[c[k]], count[c[k]]);
+            } else {
+                ref[k] = atomicAdd(slots, 1);
+                qout[atomicAdd(n_out, 1)] = make_int2(c[k], ref[k]);
+            }
+        }
+        for (int r = 0; r < 6; r++) {
+            b32[r][k] = f ? f[r] : ((r & 1) ? -inf : inf);
+            b64[r][k] = d ? d[r] : ((r & 1) ? -dinf : dinf);
+        }
+    }
+    // rows: lo x, hi x, lo y, hi y, lo z, hi z (box arrays are lo/hi interleaved per axis)
+    for (int r = 0; r < 6; r++) {
+        n32[8 * slot + r] = make_float4(b32[r][0], b32[r][1], b32[r][2], b32[r][3]);
+        if (n64) {
+            n64[14 * slot + 2 * r] = make_double2(b64[r][0], b64[r][1]);
+            n64[14 * slot + 2 * r + 1] = make_double2(b64[r][2], b64[r][3]);
+        }
+    }
+    n32[8 * slot + 6] =
+        make_float4(__int_as_float(ref[0]), __int_as_float(ref[1]), __int_as_float(ref[2]), __int_as_float(ref[3]));
+    n32[8 * slot + 7] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (n64) {
+        n64[14 * slot + 12] =
+            make_double2(__longlong_as_double((long long)(unsigned(ref[0])) | ((long long)(unsigned(ref[1])) << 32)),
+                         __longlong_as_double((long long)(unsigned(ref[2])) | ((long long)(unsigned(ref[3])) << 32)));
+        n64[14 * slot + 13] = make_double2(0.0, 0.0);
+    }
+}
+
+// The 4-wide root of a mesh of <= L triangles: one leaf, three empty slots.
+__global__ void k_write_small_root4(int n, const float *__restrict__ box32, const double *__restrict__ box64,
+                                    float4 *__restrict__ n32, double2 *__restrict__ n64) {
+    float b[6] = {FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX};
+    double e[6] = {DBL_MAX, -DBL_MAX, DBL_MAX, -DBL_MAX, DBL_MAX, -DBL_MAX};
+    for (int t = 0; t < n; t++)
+        for (int k = 0; k < 6; k += 2) {
+            b[k] = fminf(b[k], box32[6 * t + k]), b[k + 1] = fmaxf(b[k + 1], box32[6 * t + k + 1]);
+            e[k] = fmin(e[k], box64[6 * t + k]), e[k + 1] = fmax(e[k + 1], box64[6 * t + k + 1]);
+        }
+    const float inf = __int_as_float(0x7f800000);
+    const double dinf = __longlong_as_double(0x7ff0000000000000ll);
+    for (int r = 0; r < 6; r++) {
+        const float pad = (r & 1) ? -inf : inf;
+        const double dpad = (r & 1) ? -dinf : dinf;
+        n32[r] = make_float4(b[r], pad, pad, pad);
+        if (n64) n64[2 * r] = make_double2(e[r], dpad), n64[2 * r + 1] = make_double2(dpad, dpad);
+    }
+    const int e0 = kEmptyRef;
+    n32[6] = make_float4(__int_as_float(leaf_ref(0, n)), __int_as_float(e0), __int_as_float(e0), __int_as_float(e0));
+    n32[7] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (n64) {
+        n64[12] = make_double2(
+            __longlong_as_double((long long)(unsigned(leaf_ref(0, n))) | ((long long)(unsigned(e0)) << 32)),
+            __longlong_as_double((long long)(unsigned(e0)) | ((long long)(unsigned(e0)) << 32)));
+        n64[13] = make_double2(0.0, 0.0);
+    }
+}
+
 // Depth and leaf count of the collapsed tree: a node is kept iff its subtree has > L triangles
 // (its ancestors then have more), so walk parents from every kept node.
 __global__ void k_depth(int n, int L, const int *__restrict__ count, const int *__restrict__ parent_int,
@@ -566,13 +678,18 @@ static int mesh_build_impl(MeshStorage *s, MeshStorage *tmp, DeviceMesh *m, int 
     double2 *nodes64 = nullptr;
     SSDF_CHECK(dalloc(s, &nodes32, 4 * size_t(m->nnodes), stream));
     if (keep64) SSDF_CHECK(dalloc(s, &nodes64, 8 * size_t(m->nnodes), stream));
+    float4 *nodes4_32;
+    double2 *nodes4_64 = nullptr;
+    SSDF_CHECK(dalloc(s, &nodes4_32, 8 * size_t(m->nnodes), stream));
+    if (keep64) SSDF_CHECK(dalloc(s, &nodes4_64, 14 * size_t(m->nnodes), stream));
     int depth_leaves[2] = {1, 1};
+    int nnodes4 = 1, depth4 = 1;
     if (nt <= L) {
         // one leaf over everything (its triangle order is the Morton order)
-        double *pb64 = box64;
-        float *pb32 = box32;
-        k_write_small_root<<<1, 1, 0, stream>>>(nt, pb32, pb64, nodes32, nodes64);
+        k_write_small_root<<<1, 1, 0, stream>>>(nt, box32, box64, nodes32, nodes64);
         LAUNCH_CHECK("k_write_small_root");
+        k_write_small_root4<<<1, 1, 0, stream>>>(nt, box32, box64, nodes4_32, nodes4_64);
+        LAUNCH_CHECK("k_write_small_root4");
     } else {
         int *child_l, *child_r, *first_of, *last_of, *parent_int, *parent_leaf, *arrivals, *count;
         float *nbox32;
@@ -608,6 +725,35 @@ static int mesh_build_impl(MeshStorage *s, MeshStorage *tmp, DeviceMesh *m, int 
         k_depth<<<grid_blocks(nint, 256), 256, 0, stream>>>(nt, L, count, parent_int, child_l, child_r, flags + 8);
         LAUNCH_CHECK("k_depth");
         SSDF_CUDA(cudaMemcpyAsync(depth_leaves, flags + 8, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+        // 4-wide collapse, one level per launch
+        int2 *qa, *qb;
+        int *qcount;  // [0] next-level size, [1] slots used
+        SSDF_CHECK(dalloc(tmp, &qa, nint, stream));
+        SSDF_CHECK(dalloc(tmp, &qb, nint, stream));
+        SSDF_CHECK(dalloc(tmp, &qcount, 2, stream));
+        const int2 root = make_int2(0, 0);
+        const int hq[2] = {0, 1};
+        SSDF_CUDA(cudaMemcpyAsync(qa, &root, sizeof(root), cudaMemcpyHostToDevice, stream));
+        SSDF_CUDA(cudaMemcpyAsync(qcount, hq, sizeof(hq), cudaMemcpyHostToDevice, stream));
+        int level_n = 1;
+        depth4 = 0;
+        while (level_n > 0) {
+            depth4++;
+            SSDF_CUDA(cudaMemsetAsync(qcount, 0, sizeof(int), stream));
+            k_collapse4<<<grid_blocks(level_n, 128), 128, 0, stream>>>(level_n, qa, qb, qcount, qcount + 1, L,
+                                                                       child_l, child_r, first_of, count, ids, box32,
+                                                                       box64, nbox32, nbox64, nodes4_32, nodes4_64);
+            LAUNCH_CHECK("k_collapse4");
+            int hc[2];
+            SSDF_CUDA(cudaMemcpyAsync(hc, qcount, sizeof(hc), cudaMemcpyDeviceToHost, stream));
+            SSDF_CUDA(cudaStreamSynchronize(stream));
+            level_n = hc[0];
+            nnodes4 = hc[1];
+            int2 *t = qa;
+            qa = qb;
+            qb = t;
+            if (depth4 > 4 * kStackSize) return fail(SSDF_ERR_INTERNAL, "4-wide collapse did not terminate");
+        }
     }
     // triangle records in leaf order
     float4 *t32;
@@ -627,9 +773,13 @@ static int mesh_build_impl(MeshStorage *s, MeshStorage *tmp, DeviceMesh *m, int 
     m->nleaves = depth_leaves[1];
     m->nodes32 = nodes32;
     m->nodes64 = nodes64;
+    m->nodes4_32 = nodes4_32;
+    m->nodes4_64 = nodes4_64;
+    m->nnodes4 = nnodes4;
+    m->depth4 = depth4;
     m->tris32 = t32;
     m->tris64 = t64;
-    if (m->depth >= kStackSize)
+    if (m->depth >= kStackSize || 3 * m->depth4 >= kStackSize)
         return fail(SSDF_ERR_NOT_SUPPORTED,
                     "BVH depth " + std::to_string(m->depth) + " exceeds the traversal stack (" +
                         std::to_string(kStackSize) + ")");

@@ -167,12 +167,14 @@ def test_device_mesh_handle_matches_drop_in():
     dm.close()
 
 
+@pytest.mark.parametrize("arity", [2, 4])
 @pytest.mark.parametrize("mode", ["warp", "thread"])
-def test_traversal_modes(mode, knot):
-    """Thread-per-query and warp-packet traversal give the oracle's values, grid and point list."""
+def test_traversal_modes(mode, arity, knot):
+    """Thread-per-query and warp-packet traversal over the binary and the 4-wide BVH give the
+    oracle's values, grid and point list."""
     mesh = knot["mesh"]
     q = knot["q"]
-    with env(SSDF_B200_TRAVERSAL=mode):
+    with env(SSDF_B200_TRAVERSAL=mode, SSDF_B200_ARITY=arity):
         sd, tri = S.sdf_points(q, mesh)
         for prec in ("f32x", "f64"):
             with env(SSDF_B200_PRECISION=prec):
