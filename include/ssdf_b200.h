@@ -200,6 +200,31 @@ int ssdf_query_points(ssdf_mesh *mesh, ptrdiff_t npoints, const void *x, const v
 int ssdf_query_grid(ssdf_mesh *mesh, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, const double lo[3],
                     const double hi[3], void *out, int *outtri, const ssdf_query_opts *opts, void *stream);
 
+/* ---- batches: many resident meshes and query sets in one persistent launch (no reference
+ *      counterpart; ssdf answers one mesh per call) --------------------------------------------- */
+
+typedef struct ssdf_batch ssdf_batch;
+
+/* traversal: 0 automatic (warp packets for grids), 1 warp packets, 2 thread per query;
+ * arity: 0 automatic (binary), 2, 4. One arithmetic (precision) per batch. */
+int ssdf_batch_create(ssdf_batch **batch, int max_jobs, int precision, int traversal, int arity);
+int ssdf_batch_destroy(ssdf_batch *batch);
+/* Removes every job (the device table is rewritten on the next run). */
+int ssdf_batch_clear(ssdf_batch *batch);
+int ssdf_batch_size(const ssdf_batch *batch);
+/* Adds one job: a node grid or a device point list against a resident mesh, outputs in device
+ * memory; opts->precision must equal the batch's. */
+int ssdf_batch_add_grid(ssdf_batch *batch, ssdf_mesh *mesh, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz,
+                        const double lo[3], const double hi[3], void *out, int *outtri, const ssdf_query_opts *opts);
+int ssdf_batch_add_points(ssdf_batch *batch, ssdf_mesh *mesh, ptrdiff_t npoints, const void *x, const void *y,
+                          const void *z, void *out, int *outtri, const ssdf_query_opts *opts);
+/* Runs every job in one persistent launch (plus the fix-up window stage) on `stream`, asynchronously.
+ * use_graph = 1: the launch sequence is captured into a CUDA graph on the first run and replayed
+ * afterwards for any composition of jobs (the job table is device-resident). */
+int ssdf_batch_run(ssdf_batch *batch, int use_graph, void *stream);
+/* 128-query work items of the last run. */
+long long ssdf_batch_last_blocks(const ssdf_batch *batch);
+
 /* Diagnostics for measurement: per-query triangle and box test counts of the last query on this
  * thread when SSDF_B200_COUNT=1 was set at its launch (an untimed, instrumented launch). */
 int ssdf_last_query_counts(int64_t *triangle_tests, int64_t *box_tests, int64_t *fixup_queries,

@@ -92,6 +92,15 @@ _sig("ssdf_query_grid", [_vp, _pd, _pd, _pd, C.POINTER(C.c_double * 3), C.POINTE
                          C.POINTER(QueryOpts), _vp])
 _sig("ssdf_last_query_counts", [C.POINTER(C.c_int64)] * 4)
 _sig("ssdf_b200_fma_peak", [C.c_int, C.POINTER(C.c_double)])
+_sig("ssdf_batch_create", [C.POINTER(_vp), C.c_int, C.c_int, C.c_int, C.c_int])
+_sig("ssdf_batch_destroy", [_vp])
+_sig("ssdf_batch_clear", [_vp])
+_sig("ssdf_batch_size", [_vp])
+_sig("ssdf_batch_add_grid", [_vp, _vp, _pd, _pd, _pd, C.POINTER(C.c_double * 3), C.POINTER(C.c_double * 3), _vp, _ip,
+                             C.POINTER(QueryOpts)])
+_sig("ssdf_batch_add_points", [_vp, _vp, _pd, _vp, _vp, _vp, _vp, _ip, C.POINTER(QueryOpts)])
+_sig("ssdf_batch_run", [_vp, C.c_int, _vp])
+_sig("ssdf_batch_last_blocks", [_vp], C.c_longlong)
 
 EXPORTED = ["ssdf_status_string", "ssdf_last_error", "ssdf_b200_version", "ssdf_edf_f", "ssdf_edf_d",
             "ssdf_b200_edf_ff", "ssdf_b200_edf_dd", "ssdf_b200_edf_celllist_ff", "ssdf_b200_edf_celllist_dd",
@@ -100,7 +109,9 @@ EXPORTED = ["ssdf_status_string", "ssdf_last_error", "ssdf_b200_version", "ssdf_
             "ssdf_b200_sample_sdf_bvh_ff", "ssdf_b200_sample_sdf_bvh_dd", "ssdf_b200_edf_index_dd",
             "ssdf_b200_edf_index_ff", "ssdf_b200_sdf_points_dd", "ssdf_b200_sample_sdf_index_bvh_dd",
             "ssdf_mesh_create", "ssdf_mesh_destroy", "ssdf_mesh_stats", "ssdf_query_points", "ssdf_query_grid",
-            "ssdf_last_query_counts", "ssdf_b200_fma_peak"]
+            "ssdf_last_query_counts", "ssdf_b200_fma_peak", "ssdf_batch_create", "ssdf_batch_destroy", "ssdf_batch_clear",
+            "ssdf_batch_size", "ssdf_batch_add_grid", "ssdf_batch_add_points", "ssdf_batch_run",
+            "ssdf_batch_last_blocks"]
 
 
 def _status_name(status: int) -> str:
@@ -335,3 +346,56 @@ class DeviceMesh:
         nx, ny, nz = (int(v) for v in grid.n)
         _check(lib.ssdf_query_grid(self._h, nx, ny, nz, C.byref(lo), C.byref(hi), _dptr(out), tri, C.byref(o),
                                    _stream_handle(stream)), "ssdf_query_grid")
+
+
+class Batch:
+    """Many (resident mesh, query set) jobs run in one persistent launch, optionally as a CUDA graph."""
+
+    def __init__(self, max_jobs, precision=PREC_F32_FIXUP, traversal=0, arity=0):
+        self._h = C.c_void_p()
+        self.precision = precision
+        _check(lib.ssdf_batch_create(C.byref(self._h), int(max_jobs), int(precision), int(traversal), int(arity)),
+               "ssdf_batch_create")
+        self._keep = []
+
+    def close(self):
+        if self._h:
+            lib.ssdf_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def clear(self):
+        _check(lib.ssdf_batch_clear(self._h), "ssdf_batch_clear")
+        self._keep = []
+
+    def __len__(self):
+        return lib.ssdf_batch_size(self._h)
+
+    def add_grid(self, mesh: "DeviceMesh", grid, out, outtri=None, output=OUT_SDF, coord_type=F64, out_type=F64):
+        o = QueryOpts(self.precision, output, coord_type, out_type)
+        lo = (C.c_double * 3)(*grid.lo)
+        hi = (C.c_double * 3)(*grid.hi)
+        tri = C.cast(C.c_void_p(_dptr(outtri)), _ip) if outtri is not None else None
+        nx, ny, nz = (int(v) for v in grid.n)
+        _check(lib.ssdf_batch_add_grid(self._h, mesh._h, nx, ny, nz, C.byref(lo), C.byref(hi), _dptr(out), tri,
+                                       C.byref(o)), "ssdf_batch_add_grid")
+        self._keep.append((mesh, out, outtri))
+
+    def add_points(self, mesh: "DeviceMesh", x, y, z, out, outtri=None, output=OUT_SDF, coord_type=F64, out_type=F64):
+        o = QueryOpts(self.precision, output, coord_type, out_type)
+        tri = C.cast(C.c_void_p(_dptr(outtri)), _ip) if outtri is not None else None
+        _check(lib.ssdf_batch_add_points(self._h, mesh._h, int(x.numel()), _dptr(x), _dptr(y), _dptr(z), _dptr(out),
+                                         tri, C.byref(o)), "ssdf_batch_add_points")
+        self._keep.append((mesh, x, y, z, out, outtri))
+
+    def run(self, use_graph=True, stream=None):
+        _check(lib.ssdf_batch_run(self._h, int(bool(use_graph)), _stream_handle(stream)), "ssdf_batch_run")
+
+    def last_blocks(self) -> int:
+        return int(lib.ssdf_batch_last_blocks(self._h))
+

@@ -1,0 +1,244 @@
+// batch.cu -- many (mesh, query set) jobs in one persistent launch, replayed as a CUDA graph.
+//
+// No reference counterpart: ssdf answers one mesh per call and rebuilds its BVH each time
+// (serial/bvh/bvh.cu:80-158). Here resident meshes (ssdf_mesh) of very different sizes are queried
+// together: the host writes a job table (one QueryArgs per job, largest first, with each job's first
+// 128-query block), the persistent kernel's blocks pull (job, block) items from an atomic counter,
+// and the fix-up window stage finishes every job's overflowed queries. The table lives in device
+// memory and the kernels read it there, so the captured graph (two memsets + two kernels) replays
+// for any batch composition; only the table is rewritten (from pinned memory) before each replay.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "internal.h"
+
+using namespace ssdf_b200;
+
+struct ssdf_batch {
+    int max_jobs = 0;
+    int precision = SSDF_PREC_F32_FIXUP;
+    int traversal = 0;  // 0 auto, 1 warp, 2 thread
+    int arity = 0;      // 0 auto, 2, 4
+    std::vector<QueryArgs> jobs;
+    // device table
+    BatchHeader *d_hdr = nullptr;
+    QueryArgs *d_jobs = nullptr;
+    long long *d_first = nullptr;
+    unsigned long long *d_next = nullptr;
+    int *d_fbcount = nullptr;
+    int *d_fb = nullptr;
+    size_t fb_cap = 0;  // ints
+    // pinned staging
+    BatchHeader *h_hdr = nullptr;
+    QueryArgs *h_jobs = nullptr;
+    long long *h_first = nullptr;
+    // captured graph for (warp, wide)
+    cudaGraphExec_t exec = nullptr;
+    int exec_key = -1;
+    int sms = 0;
+    long long last_total = 0;
+};
+
+static void batch_free(ssdf_batch *b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    cudaFree(b->d_hdr);
+    cudaFree(b->d_jobs);
+    cudaFree(b->d_first);
+    cudaFree(b->d_next);
+    cudaFree(b->d_fbcount);
+    cudaFree(b->d_fb);
+    cudaFreeHost(b->h_hdr);
+    cudaFreeHost(b->h_jobs);
+    cudaFreeHost(b->h_first);
+}
+
+extern "C" {
+
+int ssdf_batch_create(ssdf_batch **out, int max_jobs, int precision, int traversal, int arity) {
+    if (!out || max_jobs <= 0) return fail(SSDF_ERR_INVALID_ARGUMENT, "ssdf_batch_create: bad arguments");
+    if (precision < SSDF_PREC_F32 || precision > SSDF_PREC_F32_FIXUP)
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "ssdf_batch_create: bad precision");
+    *out = nullptr;
+    ssdf_batch *b = new ssdf_batch();
+    b->max_jobs = max_jobs;
+    b->precision = precision;
+    b->traversal = traversal;
+    b->arity = arity;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_hdr, sizeof(BatchHeader));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_jobs, sizeof(QueryArgs) * max_jobs);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_first, sizeof(long long) * max_jobs);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_next, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_fbcount, sizeof(int) * max_jobs);
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_hdr, sizeof(BatchHeader));
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_jobs, sizeof(QueryArgs) * max_jobs);
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_first, sizeof(long long) * max_jobs);
+    if (e != cudaSuccess) {
+        batch_free(b);
+        delete b;
+        return cuda_fail(e, "ssdf_batch_create", __FILE__, __LINE__);
+    }
+    *out = b;
+    return SSDF_OK;
+}
+
+int ssdf_batch_destroy(ssdf_batch *b) {
+    if (!b) return SSDF_OK;
+    cudaDeviceSynchronize();
+    batch_free(b);
+    delete b;
+    return SSDF_OK;
+}
+
+int ssdf_batch_clear(ssdf_batch *b) {
+    if (!b) return fail(SSDF_ERR_INVALID_ARGUMENT, "null batch");
+    b->jobs.clear();
+    return SSDF_OK;
+}
+
+int ssdf_batch_size(const ssdf_batch *b) { return b ? int(b->jobs.size()) : 0; }
+
+static int batch_add(ssdf_batch *b, const QueryArgs &a, const ssdf_query_opts *opts) {
+    if (opts->precision != b->precision)
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "a batch runs one arithmetic: job precision differs from the batch's");
+    if (int(b->jobs.size()) >= b->max_jobs) return fail(SSDF_ERR_INVALID_ARGUMENT, "batch is full");
+    if (b->precision == SSDF_PREC_F64 && !a.m.nodes64)
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "mesh built without double data (keep_fp64=0)");
+    if (b->precision == SSDF_PREC_F32_FIXUP && (!a.m.tris64 || !a.m.nodes64))
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "fix-up queries need the double triangles and BVH (keep_fp64=1)");
+    if (a.output == SSDF_OUT_SDF && (!a.m.face_n || !a.m.tris64))
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "signed queries need a mesh built with normals=1 and keep_fp64=1");
+    if (b->precision == SSDF_PREC_F32 && (a.output == SSDF_OUT_SDF || a.output == SSDF_OUT_CLOSEST))
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "SSDF_PREC_F32 serves the edf and sqedf outputs");
+    const long long n = a.is_grid ? a.nx * a.ny * a.nz : a.npoints;
+    if (n >= 0x7fffffffll) return fail(SSDF_ERR_NOT_SUPPORTED, "more than 2^31 - 1 queries in one job");
+    if (n > 0) b->jobs.push_back(a);
+    return SSDF_OK;
+}
+
+int ssdf_batch_add_grid(ssdf_batch *b, ssdf_mesh *mesh, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, const double lo[3],
+                        const double hi[3], void *out, int *outtri, const ssdf_query_opts *opts) {
+    if (!b || !opts) return fail(SSDF_ERR_INVALID_ARGUMENT, "null batch or options");
+    QueryArgs a;
+    SSDF_CHECK(fill_grid_args(mesh, nx, ny, nz, lo, hi, out, outtri, opts, &a));
+    return batch_add(b, a, opts);
+}
+
+int ssdf_batch_add_points(ssdf_batch *b, ssdf_mesh *mesh, ptrdiff_t npoints, const void *x, const void *y,
+                          const void *z, void *out, int *outtri, const ssdf_query_opts *opts) {
+    if (!b || !opts) return fail(SSDF_ERR_INVALID_ARGUMENT, "null batch or options");
+    QueryArgs a;
+    SSDF_CHECK(fill_point_args(mesh, npoints, x, y, z, out, outtri, nullptr, nullptr, nullptr, opts, &a));
+    return batch_add(b, a, opts);
+}
+
+// One persistent launch over every job (+ the fix-up window stage). use_graph: capture the launch
+// sequence once (per traversal mode and arity) and replay it afterwards.
+int ssdf_batch_run(ssdf_batch *b, int use_graph, void *stream_) {
+    if (!b) return fail(SSDF_ERR_INVALID_ARGUMENT, "null batch");
+    cudaStream_t stream = (cudaStream_t)stream_;
+    const int njobs = int(b->jobs.size());
+    if (njobs == 0) return SSDF_OK;
+    bool any_grid = false;
+    for (const auto &j : b->jobs) any_grid |= j.is_grid != 0;
+    const bool warp = b->traversal == 1 ? true : b->traversal == 2 ? false : default_warp(any_grid);
+    const bool wide = b->arity == 4 ? true : b->arity == 2 ? false : default_wide();
+    // largest jobs first: the tail of the launch is then made of small items
+    std::vector<int> order(njobs);
+    for (int i = 0; i < njobs; i++) order[i] = i;
+    auto cost = [&](const QueryArgs &a) { return double(query_blocks(a)) * std::log2(2.0 + a.m.nt); };
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost(b->jobs[x]) > cost(b->jobs[y]); });
+    // fix-up overflow lists: one slice of (ids, thresholds) per job
+    size_t need = 0;
+    if (b->precision == SSDF_PREC_F32_FIXUP)
+        for (const auto &j : b->jobs) need += 2 * size_t(j.is_grid ? j.nx * j.ny * j.nz : j.npoints);
+    if (need > b->fb_cap) {
+        SSDF_CUDA(cudaStreamSynchronize(stream));
+        cudaFree(b->d_fb);
+        b->d_fb = nullptr;
+        b->fb_cap = 0;
+        SSDF_CUDA(cudaMalloc(&b->d_fb, sizeof(int) * need));
+        b->fb_cap = need;
+    }
+    // the staging buffers may still feed the previous run's copies
+    SSDF_CUDA(cudaStreamSynchronize(stream));
+    long long total = 0;
+    size_t off = 0;
+    for (int k = 0; k < njobs; k++) {
+        QueryArgs a = b->jobs[order[k]];
+        if (b->precision == SSDF_PREC_F32_FIXUP) {
+            const size_t n = size_t(a.is_grid ? a.nx * a.ny * a.nz : a.npoints);
+            a.fallback_count = b->d_fbcount + k;
+            a.fallback_ids = b->d_fb + off;
+            a.fallback_thr = reinterpret_cast<float *>(b->d_fb + off + n);
+            off += 2 * n;
+        } else {
+            a.fallback_count = nullptr;
+            a.fallback_ids = nullptr;
+            a.fallback_thr = nullptr;
+        }
+        a.counters = nullptr;
+        b->h_jobs[k] = a;
+        b->h_first[k] = total;
+        total += query_blocks(a);
+    }
+    b->h_hdr->njobs = njobs;
+    b->h_hdr->pad = 0;
+    b->h_hdr->total_blocks = total;
+    b->last_total = total;
+    SSDF_CUDA(cudaMemcpyAsync(b->d_hdr, b->h_hdr, sizeof(BatchHeader), cudaMemcpyHostToDevice, stream));
+    SSDF_CUDA(cudaMemcpyAsync(b->d_jobs, b->h_jobs, sizeof(QueryArgs) * njobs, cudaMemcpyHostToDevice, stream));
+    SSDF_CUDA(cudaMemcpyAsync(b->d_first, b->h_first, sizeof(long long) * njobs, cudaMemcpyHostToDevice, stream));
+    BatchLaunch L;
+    L.hdr = b->d_hdr;
+    L.jobs = b->d_jobs;
+    L.first_block = b->d_first;
+    L.next_item = b->d_next;
+    L.sms = b->sms;
+    L.warp = warp;
+    L.wide = wide;
+    L.grid = b->sms * batch_blocks_per_sm(b->precision, warp, wide);
+    const bool count = env_int("SSDF_B200_COUNT", 0) != 0;
+    auto enqueue = [&](cudaStream_t s) -> int {
+        cudaError_t e = cudaMemsetAsync(b->d_next, 0, sizeof(unsigned long long), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(b->d_fbcount, 0, sizeof(int) * b->max_jobs, s);
+        if (e != cudaSuccess) return cuda_fail(e, "batch reset", __FILE__, __LINE__);
+        return launch_batch(L, b->precision, s);
+    };
+    if (!use_graph || count) return enqueue(stream);
+    const int key = (warp ? 1 : 0) | (wide ? 2 : 0);
+    if (!b->exec || b->exec_key != key) {
+        if (b->exec) {
+            cudaGraphExecDestroy(b->exec);
+            b->exec = nullptr;
+        }
+        cudaStream_t cap;
+        SSDF_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+        int st = SSDF_OK;
+        if (e == cudaSuccess) {
+            st = enqueue(cap);
+            e = cudaStreamEndCapture(cap, &g);
+        }
+        if (e == cudaSuccess && st == SSDF_OK) e = cudaGraphInstantiate(&b->exec, g, 0);
+        if (g) cudaGraphDestroy(g);
+        cudaStreamDestroy(cap);
+        if (st != SSDF_OK) return st;
+        if (e != cudaSuccess) return cuda_fail(e, "batch graph capture", __FILE__, __LINE__);
+        b->exec_key = key;
+    }
+    SSDF_CUDA(cudaGraphLaunch(b->exec, stream));
+    return SSDF_OK;
+}
+
+// Work items (128-query blocks) of the last run.
+long long ssdf_batch_last_blocks(const ssdf_batch *b) { return b ? b->last_total : 0; }
+
+}  // extern "C"

@@ -17,12 +17,6 @@
 
 #include "internal.h"
 
-struct ssdf_mesh {
-    ssdf_b200::DeviceMesh m;
-    ssdf_b200::MeshStorage *storage = nullptr;
-    int device = 0;
-};
-
 namespace ssdf_b200 {
 
 int query_counts(int64_t *tri, int64_t *box, int64_t *fix, int64_t *fallback);
@@ -447,6 +441,10 @@ int ssdf_mesh_stats(const ssdf_mesh *mesh, int64_t *nodes, int64_t *leaves, int6
     return SSDF_OK;
 }
 
+}  // extern "C"
+
+namespace ssdf_b200 {
+
 static int fill_query(const ssdf_mesh *mesh, const ssdf_query_opts *opts, QueryArgs *a) {
     if (!mesh) return fail(SSDF_ERR_INVALID_ARGUMENT, "null mesh");
     if (!opts) return fail(SSDF_ERR_INVALID_ARGUMENT, "null query options");
@@ -462,42 +460,59 @@ static int fill_query(const ssdf_mesh *mesh, const ssdf_query_opts *opts, QueryA
     return SSDF_OK;
 }
 
+int fill_point_args(ssdf_mesh *mesh, ptrdiff_t npoints, const void *x, const void *y, const void *z, void *out,
+                    int *outtri, void *outx, void *outy, void *outz, const ssdf_query_opts *opts, QueryArgs *a) {
+    SSDF_CHECK(fill_query(mesh, opts, a));
+    if (npoints < 0) return fail(SSDF_ERR_INVALID_ARGUMENT, "negative npoints");
+    if (npoints > 0 && (!x || !y || !z || !out)) return fail(SSDF_ERR_INVALID_ARGUMENT, "null point or output array");
+    a->is_grid = 0;
+    a->npoints = npoints;
+    a->x = x, a->y = y, a->z = z;
+    a->out = out;
+    a->outtri = outtri;
+    a->outx = outx, a->outy = outy, a->outz = outz;
+    return SSDF_OK;
+}
+
+int fill_grid_args(ssdf_mesh *mesh, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, const double lo[3], const double hi[3],
+                   void *out, int *outtri, const ssdf_query_opts *opts, QueryArgs *a) {
+    SSDF_CHECK(fill_query(mesh, opts, a));
+    if (nx < 0 || ny < 0 || nz < 0) return fail(SSDF_ERR_INVALID_ARGUMENT, "negative grid size");
+    if ((long long)nx * ny * nz > 0 && (!lo || !hi || !out))
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "null grid bounds or output array");
+    if (opts->output == SSDF_OUT_CLOSEST) return fail(SSDF_ERR_INVALID_ARGUMENT, "closest-point output is for point lists");
+    a->is_grid = 1;
+    a->nx = nx, a->ny = ny, a->nz = nz;
+    const long long n[3] = {nx, ny, nz};
+    for (int d = 0; d < 3 && lo && hi; d++) {
+        // h = (max - min) / (n - 1) in G precision (serial/bvh/bvh.cpp:1665-1667)
+        a->lo64[d] = lo[d];
+        a->h64[d] = n[d] > 1 ? (hi[d] - lo[d]) / double(n[d] - 1) : 0.0;
+        a->lo32[d] = float(lo[d]);
+        a->h32[d] = n[d] > 1 ? (float(hi[d]) - float(lo[d])) / float(n[d] - 1) : 0.f;
+    }
+    a->out = out;
+    a->outtri = outtri;
+    return SSDF_OK;
+}
+
+}  // namespace ssdf_b200
+
+extern "C" {
+
 int ssdf_query_points(ssdf_mesh *mesh, ptrdiff_t npoints, const void *x, const void *y, const void *z, void *out,
                       int *outtri, void *outx, void *outy, void *outz, const ssdf_query_opts *opts, void *stream) {
     QueryArgs a;
-    SSDF_CHECK(fill_query(mesh, opts, &a));
-    if (npoints < 0) return fail(SSDF_ERR_INVALID_ARGUMENT, "negative npoints");
+    SSDF_CHECK(fill_point_args(mesh, npoints, x, y, z, out, outtri, outx, outy, outz, opts, &a));
     if (npoints == 0) return SSDF_OK;
-    if (!x || !y || !z || !out) return fail(SSDF_ERR_INVALID_ARGUMENT, "null point or output array");
-    a.is_grid = 0;
-    a.npoints = npoints;
-    a.x = x, a.y = y, a.z = z;
-    a.out = out;
-    a.outtri = outtri;
-    a.outx = outx, a.outy = outy, a.outz = outz;
     return launch_query(a, opts->precision, (cudaStream_t)stream);
 }
 
 int ssdf_query_grid(ssdf_mesh *mesh, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, const double lo[3], const double hi[3],
                     void *out, int *outtri, const ssdf_query_opts *opts, void *stream) {
     QueryArgs a;
-    SSDF_CHECK(fill_query(mesh, opts, &a));
-    if (nx < 0 || ny < 0 || nz < 0) return fail(SSDF_ERR_INVALID_ARGUMENT, "negative grid size");
+    SSDF_CHECK(fill_grid_args(mesh, nx, ny, nz, lo, hi, out, outtri, opts, &a));
     if ((long long)nx * ny * nz == 0) return SSDF_OK;
-    if (!lo || !hi || !out) return fail(SSDF_ERR_INVALID_ARGUMENT, "null grid bounds or output array");
-    if (opts->output == SSDF_OUT_CLOSEST) return fail(SSDF_ERR_INVALID_ARGUMENT, "closest-point output is for point lists");
-    a.is_grid = 1;
-    a.nx = nx, a.ny = ny, a.nz = nz;
-    const long long n[3] = {nx, ny, nz};
-    for (int d = 0; d < 3; d++) {
-        // h = (max - min) / (n - 1) in G precision (serial/bvh/bvh.cpp:1665-1667)
-        a.lo64[d] = lo[d];
-        a.h64[d] = n[d] > 1 ? (hi[d] - lo[d]) / double(n[d] - 1) : 0.0;
-        a.lo32[d] = float(lo[d]);
-        a.h32[d] = n[d] > 1 ? (float(hi[d]) - float(lo[d])) / float(n[d] - 1) : 0.f;
-    }
-    a.out = out;
-    a.outtri = outtri;
     return launch_query(a, opts->precision, (cudaStream_t)stream);
 }
 

@@ -171,3 +171,19 @@ const char *env_str(const char *name);
 cudaStream_t library_stream();  // per-thread non-blocking stream for the blocking entry points
 
 }  // namespace ssdf_b200
+
+// The handle behind ssdf_mesh* (include/ssdf_b200.h).
+struct ssdf_mesh {
+    ssdf_b200::DeviceMesh m;
+    ssdf_b200::MeshStorage *storage = nullptr;
+    int device = 0;
+};
+
+namespace ssdf_b200 {
+// QueryArgs of one grid / point job (validation shared by the direct and the batch entry points).
+int fill_grid_args(ssdf_mesh *mesh, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, const double lo[3], const double hi[3],
+                   void *out, int *outtri, const ssdf_query_opts *opts, QueryArgs *a);
+int fill_point_args(ssdf_mesh *mesh, ptrdiff_t npoints, const void *x, const void *y, const void *z, void *out,
+                    int *outtri, void *outx, void *outy, void *outz, const ssdf_query_opts *opts, QueryArgs *a);
+}  // namespace ssdf_b200
+

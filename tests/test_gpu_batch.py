@@ -1,0 +1,125 @@
+"""GPU: many resident meshes in one persistent launch (ssdf_batch_*), replayed as a CUDA graph.
+
+Every job's output in the batch equals the same job queried alone (bitwise), whatever the
+composition, order or replay; and the alone results are the oracle's at sampled nodes.
+"""
+
+import numpy as np
+import pytest
+
+import oracle
+import ssdf_b200 as S
+from ssdf_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def mesh_set():
+    out = []
+    for k, (kind, size, side) in enumerate([("ico", 2, 20), ("torus", 24, 33), ("ico", 4, 17), ("torus", 96, 40),
+                                           ("ico", 3, 9), ("torus", 12, 26), ("ico", 1, 31), ("torus", 160, 12)]):
+        c = (k * 0.7, -k * 0.3, 0.2 * k)
+        if kind == "ico":
+            m = W.icosphere(size, radius=0.5 + 0.1 * k, seed=k, center=c)
+        else:
+            m = W.torus(0.8, 0.25, nu=size, nv=max(6, size // 3), jitter=0.01, seed=k, center=c)
+        out.append((m, W.Grid.padded_nodes(m, side, 0.1 * m.diagonal())))
+    return out
+
+
+@pytest.fixture(scope="module")
+def jobs():
+    import torch
+
+    res = []
+    for m, g in mesh_set():
+        dm = S.DeviceMesh(m)
+        out = torch.empty(g.size, dtype=torch.float64, device="cuda")
+        tri = torch.empty(g.size, dtype=torch.int32, device="cuda")
+        dm.query_grid(g, out, tri)
+        torch.cuda.synchronize()
+        res.append(dict(mesh=m, grid=g, dm=dm, alone=out.cpu().numpy(), alone_tri=tri.cpu().numpy()))
+    return res
+
+
+def test_alone_matches_oracle(jobs):
+    rng = np.random.default_rng(3)
+    for j in jobs[:4]:
+        ids = rng.choice(j["grid"].size, size=min(400, j["grid"].size), replace=False)
+        q = oracle.grid_points(j["grid"])[:, ids]
+        want, wtri = oracle.sdf_points(q, j["mesh"])
+        assert np.array_equal(j["alone"][ids], want) and np.array_equal(j["alone_tri"][ids], wtri)
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+@pytest.mark.parametrize("traversal", [0, 2])
+def test_batch_equals_alone(jobs, use_graph, traversal):
+    import torch
+
+    b = S.Batch(16, S.PREC_F32_FIXUP, traversal=traversal)
+    outs = []
+    for j in jobs:
+        out = torch.full((j["grid"].size,), -7.0, dtype=torch.float64, device="cuda")
+        tri = torch.full((j["grid"].size,), -7, dtype=torch.int32, device="cuda")
+        b.add_grid(j["dm"], j["grid"], out, tri)
+        outs.append((out, tri))
+    for rep in range(2):  # first run captures, second replays
+        for out, tri in outs:
+            out.fill_(-7.0)
+            tri.fill_(-7)
+        b.run(use_graph=use_graph)
+        torch.cuda.synchronize()
+        for j, (out, tri) in zip(jobs, outs):
+            assert np.array_equal(out.cpu().numpy(), j["alone"])
+            assert np.array_equal(tri.cpu().numpy(), j["alone_tri"])
+    # a different composition (subset, other order, plus a point-list job) replays the same graph
+    b.clear()
+    sub = [jobs[5], jobs[0], jobs[3]]
+    outs2 = []
+    for j in sub:
+        out = torch.empty(j["grid"].size, dtype=torch.float64, device="cuda")
+        b.add_grid(j["dm"], j["grid"], out)
+        outs2.append(out)
+    pts = torch.tensor(oracle.grid_points(jobs[2]["grid"]), dtype=torch.float64, device="cuda")
+    pout = torch.empty(pts.shape[1], dtype=torch.float64, device="cuda")
+    ptri = torch.empty(pts.shape[1], dtype=torch.int32, device="cuda")
+    b.add_points(jobs[2]["dm"], pts[0].contiguous(), pts[1].contiguous(), pts[2].contiguous(), pout, ptri)
+    b.run(use_graph=use_graph)
+    torch.cuda.synchronize()
+    for j, out in zip(sub, outs2):
+        assert np.array_equal(out.cpu().numpy(), j["alone"])
+    assert np.array_equal(pout.cpu().numpy(), jobs[2]["alone"])
+    assert np.array_equal(ptri.cpu().numpy(), jobs[2]["alone_tri"])
+    b.close()
+
+
+def test_batch_fp64(jobs):
+    import torch
+
+    b = S.Batch(16, S.PREC_F64)
+    outs = []
+    for j in jobs:
+        out = torch.empty(j["grid"].size, dtype=torch.float64, device="cuda")
+        b.add_grid(j["dm"], j["grid"], out)
+        outs.append(out)
+    b.run(use_graph=True)
+    torch.cuda.synchronize()
+    for j, out in zip(jobs, outs):
+        assert np.array_equal(out.cpu().numpy(), j["alone"])
+    b.close()
+
+
+def test_batch_rejects_mixed_precision(jobs):
+    import torch
+
+    b = S.Batch(4, S.PREC_F64)
+    out = torch.empty(jobs[0]["grid"].size, dtype=torch.float64, device="cuda")
+    bad = S.Batch(4, S.PREC_F32_FIXUP)
+    with pytest.raises(S.SsdfError):
+        o = S.QueryOpts(S.PREC_F32_FIXUP, S.OUT_SDF, S.F64, S.F64)
+        lo = (S.C.c_double * 3)(*jobs[0]["grid"].lo)
+        hi = (S.C.c_double * 3)(*jobs[0]["grid"].hi)
+        S._check(S.lib.ssdf_batch_add_grid(b._h, jobs[0]["dm"]._h, *jobs[0]["grid"].n, S.C.byref(lo), S.C.byref(hi),
+                                           out.data_ptr(), None, S.C.byref(o)), "ssdf_batch_add_grid")
+    b.close()
+    bad.close()
