@@ -225,6 +225,21 @@ int ssdf_batch_run(ssdf_batch *batch, int use_graph, void *stream);
 /* 128-query work items of the last run. */
 long long ssdf_batch_last_blocks(const ssdf_batch *batch);
 
+/* ---- allocation-free grid query (no counterpart in the reference) ----------------------------
+ * ssdf_query_grid with SSDF_PREC_F32_FIXUP, for callers that must not allocate device memory while
+ * they query: loops that reserve all memory up front, hosts that forbid the CUDA allocator or own
+ * every allocation. It allocates nothing: the fix-up overflow list lives in a fixed 8 MiB array
+ * inside the library, held by every GPU that loads the library until the process exits. Limits:
+ * at most ssdf_query_grid_noalloc_max() (1,048,576) nodes per call, larger grids are rejected with
+ * SSDF_ERR_NOT_SUPPORTED (query them slab by slab); SSDF_PREC_F32_FIXUP only. The mesh is built
+ * beforehand with ssdf_mesh_create. The first call on a device looks up the array's device address
+ * (once per device): make that first call before any stream capture. All calls share the array and
+ * each one resets it, so calls whose kernels overlap on the GPU (concurrent streams) race: order
+ * them on one stream. */
+int ssdf_query_grid_noalloc(ssdf_mesh *mesh, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, const double lo[3],
+                            const double hi[3], void *out, int *outtri, const ssdf_query_opts *opts, void *stream);
+long long ssdf_query_grid_noalloc_max(void);
+
 /* Diagnostics for measurement: per-query triangle and box test counts of the last query on this
  * thread when SSDF_B200_COUNT=1 was set at its launch (an untimed, instrumented launch). */
 int ssdf_last_query_counts(int64_t *triangle_tests, int64_t *box_tests, int64_t *fixup_queries,

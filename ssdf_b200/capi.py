@@ -101,6 +101,9 @@ _sig("ssdf_batch_add_grid", [_vp, _vp, _pd, _pd, _pd, C.POINTER(C.c_double * 3),
 _sig("ssdf_batch_add_points", [_vp, _vp, _pd, _vp, _vp, _vp, _vp, _ip, C.POINTER(QueryOpts)])
 _sig("ssdf_batch_run", [_vp, C.c_int, _vp])
 _sig("ssdf_batch_last_blocks", [_vp], C.c_longlong)
+_sig("ssdf_query_grid_noalloc", [_vp, _pd, _pd, _pd, C.POINTER(C.c_double * 3), C.POINTER(C.c_double * 3), _vp, _ip,
+                                 C.POINTER(QueryOpts), _vp])
+_sig("ssdf_query_grid_noalloc_max", [], C.c_longlong)
 
 EXPORTED = ["ssdf_status_string", "ssdf_last_error", "ssdf_b200_version", "ssdf_edf_f", "ssdf_edf_d",
             "ssdf_b200_edf_ff", "ssdf_b200_edf_dd", "ssdf_b200_edf_celllist_ff", "ssdf_b200_edf_celllist_dd",
@@ -111,7 +114,7 @@ EXPORTED = ["ssdf_status_string", "ssdf_last_error", "ssdf_b200_version", "ssdf_
             "ssdf_mesh_create", "ssdf_mesh_destroy", "ssdf_mesh_stats", "ssdf_query_points", "ssdf_query_grid",
             "ssdf_last_query_counts", "ssdf_b200_fma_peak", "ssdf_batch_create", "ssdf_batch_destroy", "ssdf_batch_clear",
             "ssdf_batch_size", "ssdf_batch_add_grid", "ssdf_batch_add_points", "ssdf_batch_run",
-            "ssdf_batch_last_blocks"]
+            "ssdf_batch_last_blocks", "ssdf_query_grid_noalloc", "ssdf_query_grid_noalloc_max"]
 
 
 def _status_name(status: int) -> str:

@@ -22,6 +22,8 @@
 
 #include <cfloat>
 #include <cstring>
+#include <mutex>
+#include <string>
 
 #include "device_geom.cuh"
 #include "internal.h"
@@ -1017,4 +1019,73 @@ bool default_warp(int is_grid) {
 
 bool default_wide() { return env_int("SSDF_B200_ARITY", 2) == 4; }
 
+// ---- allocation-free variant of the fix-up grid query ------------------------------------------------
+//
+// For callers that cannot allocate device memory while they query (a real-time loop whose memory is
+// reserved up front, an application that runs under a custom allocator and forbids the CUDA one, a
+// plugin host that owns all allocations): the FP32 + FP64 fix-up query keeps its overflow list
+// (count, query ids, window thresholds) in this fixed array instead of stream-ordered scratch. The
+// array is part of the library image, so every GPU that loads the library holds it (8 MiB) until
+// the process exits. All calls share it: each call clears the count it starts from, and two calls
+// whose kernels overlap on the GPU (different streams, no ordering between them) race on it.
+constexpr long long kNoAllocMaxQueries = 1ll << 20;  // queries per call
+static __device__ __align__(256) int g_noalloc_scratch[2 * kNoAllocMaxQueries + 1];
+
+static std::mutex g_noalloc_mutex;
+static int *g_noalloc_ptr[256];
+
+// Device address of g_noalloc_scratch on the current device, looked up once per device (the host
+// symbol is only a stand-in for it).
+static int noalloc_scratch(int **ptr) {
+    int dev = 0;
+    SSDF_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) return fail(SSDF_ERR_NOT_SUPPORTED, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
+        g_noalloc_ptr[dev] = static_cast<int *>(p);
+    }
+    *ptr = g_noalloc_ptr[dev];
+    return SSDF_OK;
+}
+
+long long noalloc_max_queries() { return kNoAllocMaxQueries; }
+
+// The fix-up query of `args` with its overflow list in g_noalloc_scratch: no allocation.
+int launch_query_noalloc(const QueryArgs &args_in, cudaStream_t stream) {
+    QueryArgs a = args_in;
+    const long long n = a.is_grid ? a.nx * a.ny * a.nz : a.npoints;
+    if (n <= 0) return SSDF_OK;
+    if (n > kNoAllocMaxQueries)
+        return fail(SSDF_ERR_NOT_SUPPORTED, "the allocation-free query takes at most " +
+                                                std::to_string(kNoAllocMaxQueries) + " queries per call, got " +
+                                                std::to_string(n) + ": split the grid into slabs");
+    if (!a.m.tris64 || !a.m.nodes64)
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "fix-up queries need the double triangles and BVH (keep_fp64=1)");
+    if (a.output == SSDF_OUT_SDF && !a.m.face_n)
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "signed queries need a mesh built with normals=1");
+    int *scratch = nullptr;
+    SSDF_CHECK(noalloc_scratch(&scratch));
+    a.counters = nullptr;
+    a.fallback_count = scratch;
+    a.fallback_ids = scratch + 1;
+    a.fallback_thr = reinterpret_cast<float *>(scratch + 1 + n);
+    const bool warp = use_warp(a), wide = use_wide();
+    const long long nblocks = query_blocks(a);
+    cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(int), stream);  // the count starts at zero
+    if (e == cudaSuccess) e = launch_prec<SSDF_PREC_F32_FIXUP>(a, warp, wide, false, unsigned(nblocks), stream);
+    if (e == cudaSuccess) {
+        if (wide)
+            k_window<true, false><<<296, kThreads, 0, stream>>>(a);
+        else
+            k_window<false, false><<<296, kThreads, 0, stream>>>(a);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "allocation-free query launch", __FILE__, __LINE__);
+    return SSDF_OK;
+}
+
 }  // namespace ssdf_b200
+

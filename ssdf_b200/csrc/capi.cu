@@ -516,6 +516,21 @@ int ssdf_query_grid(ssdf_mesh *mesh, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, c
     return launch_query(a, opts->precision, (cudaStream_t)stream);
 }
 
+// The fix-up grid query without any allocation (its overflow list lives in a fixed device array
+// of the library): for callers that must not allocate device memory while they query.
+int ssdf_query_grid_noalloc(ssdf_mesh *mesh, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, const double lo[3],
+                            const double hi[3], void *out, int *outtri, const ssdf_query_opts *opts, void *stream) {
+    QueryArgs a;
+    SSDF_CHECK(fill_grid_args(mesh, nx, ny, nz, lo, hi, out, outtri, opts, &a));
+    if (opts->precision != SSDF_PREC_F32_FIXUP)
+        return fail(SSDF_ERR_INVALID_ARGUMENT,
+                    "ssdf_query_grid_noalloc runs the fix-up arithmetic (SSDF_PREC_F32_FIXUP) only");
+    if ((long long)nx * ny * nz == 0) return SSDF_OK;
+    return launch_query_noalloc(a, (cudaStream_t)stream);
+}
+
+long long ssdf_query_grid_noalloc_max(void) { return noalloc_max_queries(); }
+
 int ssdf_last_query_counts(int64_t *triangle_tests, int64_t *box_tests, int64_t *fixup_queries,
                            int64_t *fallback_queries) {
     return query_counts(triangle_tests, box_tests, fixup_queries, fallback_queries);

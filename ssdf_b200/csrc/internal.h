@@ -146,6 +146,8 @@ int exclusive_scan_i32(const int *in, int *out, int n, cudaStream_t stream);
 
 // ---- queries (bvh_query.cu) ----------------------------------------------------------------------
 int launch_query(const QueryArgs &args, int precision, cudaStream_t stream);
+int launch_query_noalloc(const QueryArgs &args, cudaStream_t stream);
+long long noalloc_max_queries();
 int launch_batch(const BatchLaunch &b, int precision, cudaStream_t stream);
 int batch_blocks_per_sm(int precision, bool warp, bool wide);
 bool default_warp(int is_grid);
