@@ -54,6 +54,11 @@ def parse_args():
     p.add_argument("--cpu-sample", type=int, default=CPU_SAMPLE)
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-batch", action="store_true", help="skip the 256-mesh batched leg")
+    p.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    p.add_argument("--batch-meshes", type=int, default=256)
+    p.add_argument("--serve-meshes", type=int, default=128)
+    p.add_argument("--serve-seconds", type=float, default=3.0)
     return p.parse_args()
 
 
@@ -243,6 +248,16 @@ def main():
     }
     _attach_traffic(line)
 
+    if not args.no_batch and rank == 0:
+        try:
+            line["batched"] = batched_leg(S, args)
+        except Exception as ex:  # pragma: no cover - reported, not fatal
+            line["batched"] = {"error": repr(ex)}
+    if not args.no_serve and rank == 0:
+        try:
+            line["serving"] = serving_leg(S, args)
+        except Exception as ex:  # pragma: no cover - reported, not fatal
+            line["serving"] = {"error": repr(ex)}
     if not args.no_e2e:
         try:
             line["e2e"] = e2e(S, mesh, grid, args)
@@ -263,6 +278,98 @@ def main():
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def batched_leg(S, args):
+    """Config 4: uneven meshes (seeded icospheres / tori, 1e3..2e5 triangles, grid sides 32..160),
+    signed, FP32 + FP64 fix-up: one persistent launch (CUDA graph replay) against one launch per mesh."""
+    import torch
+
+    from ssdf_b200 import workloads as W
+
+    sets = W.multi_mesh_set(count=args.batch_meshes)
+    dms = [S.DeviceMesh(m) for m, _ in sets]
+    outs = [torch.empty(g.size, dtype=torch.float64, device="cuda") for _, g in sets]
+    nq = sum(g.size for _, g in sets)
+    ntri = sum(m.nt for m, _ in sets)
+    stream = torch.cuda.current_stream()
+    res = {"meshes": len(sets), "queries": nq, "triangles": ntri}
+    for prec, name in ((S.PREC_F32_FIXUP, "fixup"), (S.PREC_F64, "fp64")):
+        b = S.Batch(len(sets), prec)
+        for dm, (m, g), out in zip(dms, sets, outs):
+            b.add_grid(dm, g, out)
+        ms = []
+        for rep in range(4):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            b.run(use_graph=True, stream=stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if rep:
+                ms.append(e0.elapsed_time(e1))
+        res[name] = {"queries_per_s": nq / (statistics.median(ms) * 1e-3), "ms": statistics.median(ms)}
+        b.close()
+    ms = []
+    for rep in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for dm, (m, g), out in zip(dms, sets, outs):
+            dm.query_grid(g, out, None, precision=S.PREC_F32_FIXUP, output=S.OUT_SDF, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if rep:
+            ms.append(e0.elapsed_time(e1))
+    res["one_launch_per_mesh"] = {"queries_per_s": nq / (statistics.median(ms) * 1e-3), "ms": statistics.median(ms)}
+    res["speedup_fixup_vs_fp64"] = res["fixup"]["queries_per_s"] / res["fp64"]["queries_per_s"]
+    for dm in dms:
+        dm.close()
+    return res
+
+
+def serving_leg(S, args):
+    """Config 5 (reduced): resident meshes drawn as config 4, Poisson arrivals at swept rates; each
+    request a point list (log-uniform 1e3..1e6, uniform in the padded bbox) or a grid (32^3..128^3)."""
+    import threading
+
+    from ssdf_b200 import workloads as W
+
+    sets = W.multi_mesh_set(count=args.serve_meshes, seed=11)
+    rng = np.random.default_rng(5)
+    payloads = []
+    for k in range(48):
+        mid = int(rng.integers(len(sets)))
+        m, _ = sets[mid]
+        if rng.uniform() < 0.5:
+            side = int(np.exp(rng.uniform(np.log(32), np.log(128))))
+            payloads.append(("grid", mid, W.Grid.padded_nodes(m, side, 0.1 * m.diagonal()), side ** 3))
+        else:
+            n = int(np.exp(rng.uniform(np.log(1e3), np.log(1e6))))
+            lo, hi = m.bbox()
+            pad = 0.1 * m.diagonal()
+            payloads.append(("points", mid, W.uniform_points(n, lo - pad, hi + pad, seed=k), n))
+    srv = S.Server(memory_budget=120 << 30, max_batch_queries=1 << 22, max_batch_jobs=64)
+    ids = [srv.add_mesh(m) for m, _ in sets]
+    # admit every mesh once (building is not part of the latency being measured)
+    for mid in range(len(sets)):
+        srv.wait(srv.submit_points(ids[mid], np.zeros((3, 1))))
+    out = {"meshes": len(sets), "payloads": len(payloads), "seconds_per_rate": args.serve_seconds, "rates": []}
+    for lam in (50.0, 200.0, 800.0):
+        srv.reset_stats()
+        tickets = []
+        t_end = time.perf_counter() + args.serve_seconds
+        arrivals = np.random.default_rng(int(lam))
+        while time.perf_counter() < t_end:
+            kind, mid, q, n = payloads[int(arrivals.integers(len(payloads)))]
+            tickets.append(srv.submit_grid(ids[mid], q) if kind == "grid" else srv.submit_points(ids[mid], q))
+            time.sleep(float(arrivals.exponential(1.0 / lam)))
+        for t in tickets:
+            srv.wait(t, timeout=300)
+        st = srv.stats()
+        out["rates"].append({"lambda_per_s": lam, "requests": st["completed"], "p50_ms": st["p50_ms"],
+                             "p99_ms": st["p99_ms"], "queries_per_s": st["queries"] / max(st["seconds"], 1e-9),
+                             "batches": st["batches"]})
+    srv.close()
+    return out
 
 
 def e2e(S, mesh, grid, args):

@@ -225,6 +225,43 @@ int ssdf_batch_run(ssdf_batch *batch, int use_graph, void *stream);
 /* 128-query work items of the last run. */
 long long ssdf_batch_last_blocks(const ssdf_batch *batch);
 
+/* ---- serving loop: continuous batching over resident meshes (no reference counterpart) ------- */
+
+typedef struct ssdf_server ssdf_server;
+
+typedef struct {
+    size_t memory_budget;  /* bytes of device-resident mesh data; LRU eviction beyond it        */
+    int max_batch_queries; /* queries packed into one batch (also the largest request)         */
+    int max_batch_jobs;    /* requests packed into one batch                                   */
+    int precision;         /* SSDF_PREC_F32_FIXUP or SSDF_PREC_F64                             */
+    int leaf_size;         /* BVH leaf size of resident meshes (0: default)                    */
+} ssdf_server_opts;
+
+typedef struct {
+    long long completed;                  /* requests finished since the last reset            */
+    double p50_ms, p99_ms, max_ms;        /* submit -> result-in-caller-buffer latency          */
+    long long queries, batches, evictions, builds;
+    long long resident_bytes, resident_meshes;
+    double seconds;                       /* first submit -> last completion                   */
+} ssdf_server_report;
+
+/* A scheduler thread packs waiting requests into one persistent batch launch per free slot (two
+ * slots, so a batch's upload and kernels overlap the previous one's download); results are
+ * signed distances (double) and closest triangles written to the caller's HOST buffers. */
+int ssdf_server_create(ssdf_server **server, const ssdf_server_opts *opts);
+int ssdf_server_destroy(ssdf_server *server);
+/* Registers a mesh (host arrays, copied); it is built on the device when first queried. */
+int ssdf_server_add_mesh(ssdf_server *server, ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                         ptrdiff_t nspoints, const double *sx, const double *sy, const double *sz, int *mesh_id);
+/* Asynchronous requests; the host arrays must stay valid until ssdf_server_wait returns. */
+int ssdf_server_submit_points(ssdf_server *server, int mesh_id, ptrdiff_t npoints, const double *x, const double *y,
+                              const double *z, double *out, int *outtri, long long *ticket);
+int ssdf_server_submit_grid(ssdf_server *server, int mesh_id, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz,
+                            const double lo[3], const double hi[3], double *out, int *outtri, long long *ticket);
+int ssdf_server_wait(ssdf_server *server, long long ticket, double timeout_s);
+int ssdf_server_stats(ssdf_server *server, ssdf_server_report *stats);
+int ssdf_server_reset_stats(ssdf_server *server);
+
 /* ---- allocation-free grid query (no counterpart in the reference) ----------------------------
  * ssdf_query_grid with SSDF_PREC_F32_FIXUP, for callers that must not allocate device memory while
  * they query: loops that reserve all memory up front, hosts that forbid the CUDA allocator or own

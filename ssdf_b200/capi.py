@@ -105,6 +105,30 @@ _sig("ssdf_query_grid_noalloc", [_vp, _pd, _pd, _pd, C.POINTER(C.c_double * 3), 
                                  C.POINTER(QueryOpts), _vp])
 _sig("ssdf_query_grid_noalloc_max", [], C.c_longlong)
 
+
+class ServerOpts(C.Structure):
+    _fields_ = [("memory_budget", C.c_size_t), ("max_batch_queries", C.c_int), ("max_batch_jobs", C.c_int),
+                ("precision", C.c_int), ("leaf_size", C.c_int)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_longlong), ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double),
+                ("queries", C.c_longlong), ("batches", C.c_longlong), ("evictions", C.c_longlong),
+                ("builds", C.c_longlong), ("resident_bytes", C.c_longlong), ("resident_meshes", C.c_longlong),
+                ("seconds", C.c_double)]
+
+
+_dp_ = C.POINTER(C.c_double)
+_sig("ssdf_server_create", [C.POINTER(_vp), C.POINTER(ServerOpts)])
+_sig("ssdf_server_destroy", [_vp])
+_sig("ssdf_server_add_mesh", [_vp, _pd, _ip, _ip, _ip, _pd, _vp, _vp, _vp, _ip])
+_sig("ssdf_server_submit_points", [_vp, C.c_int, _pd, _vp, _vp, _vp, _vp, _ip, C.POINTER(C.c_longlong)])
+_sig("ssdf_server_submit_grid", [_vp, C.c_int, _pd, _pd, _pd, C.POINTER(C.c_double * 3), C.POINTER(C.c_double * 3),
+                                 _vp, _ip, C.POINTER(C.c_longlong)])
+_sig("ssdf_server_wait", [_vp, C.c_longlong, C.c_double])
+_sig("ssdf_server_stats", [_vp, C.POINTER(ServerStats)])
+_sig("ssdf_server_reset_stats", [_vp])
+
 EXPORTED = ["ssdf_status_string", "ssdf_last_error", "ssdf_b200_version", "ssdf_edf_f", "ssdf_edf_d",
             "ssdf_b200_edf_ff", "ssdf_b200_edf_dd", "ssdf_b200_edf_celllist_ff", "ssdf_b200_edf_celllist_dd",
             "ssdf_b200_edf_bvh_ff", "ssdf_b200_edf_bvh_fd", "ssdf_b200_edf_bvh_dd", "ssdf_b200_closest_point_bvh_ff",
@@ -114,7 +138,9 @@ EXPORTED = ["ssdf_status_string", "ssdf_last_error", "ssdf_b200_version", "ssdf_
             "ssdf_mesh_create", "ssdf_mesh_destroy", "ssdf_mesh_stats", "ssdf_query_points", "ssdf_query_grid",
             "ssdf_last_query_counts", "ssdf_b200_fma_peak", "ssdf_batch_create", "ssdf_batch_destroy", "ssdf_batch_clear",
             "ssdf_batch_size", "ssdf_batch_add_grid", "ssdf_batch_add_points", "ssdf_batch_run",
-            "ssdf_batch_last_blocks", "ssdf_query_grid_noalloc", "ssdf_query_grid_noalloc_max"]
+            "ssdf_batch_last_blocks", "ssdf_query_grid_noalloc", "ssdf_query_grid_noalloc_max", "ssdf_server_create",
+            "ssdf_server_destroy", "ssdf_server_add_mesh", "ssdf_server_submit_points", "ssdf_server_submit_grid",
+            "ssdf_server_wait", "ssdf_server_stats", "ssdf_server_reset_stats"]
 
 
 def _status_name(status: int) -> str:
@@ -401,4 +427,67 @@ class Batch:
 
     def last_blocks(self) -> int:
         return int(lib.ssdf_batch_last_blocks(self._h))
+
+
+class Server:
+    """Continuous-batching request loop over resident meshes (host arrays in and out)."""
+
+    def __init__(self, memory_budget=120 << 30, max_batch_queries=1 << 22, max_batch_jobs=64,
+                 precision=PREC_F32_FIXUP, leaf_size=0):
+        self._h = C.c_void_p()
+        o = ServerOpts(int(memory_budget), int(max_batch_queries), int(max_batch_jobs), int(precision),
+                       int(leaf_size))
+        _check(lib.ssdf_server_create(C.byref(self._h), C.byref(o)), "ssdf_server_create")
+        self._inflight = {}
+
+    def close(self):
+        if self._h:
+            lib.ssdf_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_mesh(self, mesh) -> int:
+        hm = _HostMesh(mesh, np.float64)
+        mid = C.c_int()
+        _check(lib.ssdf_server_add_mesh(self._h, *hm.args(), C.byref(mid)), "ssdf_server_add_mesh")
+        return mid.value
+
+    def submit_points(self, mesh_id, points):
+        x, y, z = _points(points, np.float64)
+        out = np.empty(len(x))
+        tri = np.empty(len(x), dtype=np.int32)
+        t = C.c_longlong()
+        _check(lib.ssdf_server_submit_points(self._h, int(mesh_id), len(x), _p(x), _p(y), _p(z), _p(out), _ipp(tri),
+                                             C.byref(t)), "ssdf_server_submit_points")
+        self._inflight[t.value] = (x, y, z, out, tri)
+        return t.value
+
+    def submit_grid(self, mesh_id, grid):
+        out = np.empty(grid.size)
+        tri = np.empty(grid.size, dtype=np.int32)
+        lo = (C.c_double * 3)(*grid.lo)
+        hi = (C.c_double * 3)(*grid.hi)
+        t = C.c_longlong()
+        _check(lib.ssdf_server_submit_grid(self._h, int(mesh_id), *(int(v) for v in grid.n), C.byref(lo), C.byref(hi),
+                                           _p(out), _ipp(tri), C.byref(t)), "ssdf_server_submit_grid")
+        self._inflight[t.value] = (out, tri)
+        return t.value
+
+    def wait(self, ticket, timeout=120.0):
+        _check(lib.ssdf_server_wait(self._h, int(ticket), float(timeout)), "ssdf_server_wait")
+        arrays = self._inflight.pop(ticket)
+        return arrays[-2], arrays[-1]
+
+    def stats(self):
+        st = ServerStats()
+        _check(lib.ssdf_server_stats(self._h, C.byref(st)), "ssdf_server_stats")
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_}
+
+    def reset_stats(self):
+        _check(lib.ssdf_server_reset_stats(self._h), "ssdf_server_reset_stats")
 

@@ -284,7 +284,7 @@ def multi_mesh_set(count: int = 256, tri_lo: float = 1e3, tri_hi: float = 2e5, s
         side = int(round(np.exp(rng.uniform(np.log(side_lo), np.log(side_hi)))))
         centre = rng.uniform(-2.0, 2.0, size=3)
         if rng.uniform() < 0.5:
-            sub = int(np.clip(np.round(np.log(target / 20.0) / np.log(4.0)), 2, 7))
+            sub = int(np.clip(np.floor(np.log(target / 20.0) / np.log(4.0)), 2, 6))  # 320 .. 81,920
             mesh = icosphere(sub, radius=float(rng.uniform(0.3, 1.0)), displacement=0.01,
                              seed=int(rng.integers(1 << 30)), center=centre)
         else:

@@ -1,0 +1,113 @@
+"""GPU: the serving loop (ssdf_server_*): continuous batching, LRU admission under a memory budget.
+
+Each request's result is the same alone and in the mix -- bitwise, since a batched job runs the
+same kernel as an alone query -- while requests from several threads arrive during other batches,
+meshes are evicted and rebuilt, and batches hold requests of very different sizes.
+"""
+
+import threading
+import time
+
+import numpy as np
+import pytest
+
+import ssdf_b200 as S
+from ssdf_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def meshes():
+    out = []
+    for k in range(6):
+        c = (0.3 * k, -0.2 * k, 0.1 * k)
+        if k % 2 == 0:
+            out.append(W.icosphere(2 + k // 2, radius=0.6, seed=k, center=c))
+        else:
+            out.append(W.torus(0.7, 0.2, nu=24 + 16 * k, nv=12 + 4 * k, jitter=0.01, seed=k, center=c))
+    return out
+
+
+def requests(ms, seed=0):
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for r in range(36):
+        mid = int(rng.integers(len(ms)))
+        m = ms[mid]
+        lo, hi = m.bbox()
+        if rng.uniform() < 0.5:
+            side = int(rng.integers(8, 40))
+            reqs.append(("grid", mid, W.Grid.padded_nodes(m, side, 0.1)))
+        else:
+            n = int(np.exp(rng.uniform(np.log(50), np.log(60000))))
+            reqs.append(("points", mid, W.uniform_points(n, lo - 0.1, hi + 0.1, seed=1000 + r)))
+    return reqs
+
+
+def alone(ms, req):
+    kind, mid, q = req
+    if kind == "grid":
+        return S.sample_sdf_bvh(ms[mid], q, with_index=True)
+    return S.sdf_points(q, ms[mid])
+
+
+def test_results_same_alone_and_in_the_mix():
+    ms = meshes()
+    reqs = requests(ms)
+    want = [alone(ms, r) for r in reqs]
+    sizes = []
+    for m in ms:
+        dm = S.DeviceMesh(m)
+        sizes.append(dm.stats()["bytes"])
+        dm.close()
+    # a budget of about two meshes forces evictions and rebuilds
+    srv = S.Server(memory_budget=int(sorted(sizes)[-1] * 2.2), max_batch_queries=1 << 20, max_batch_jobs=16)
+    ids = [srv.add_mesh(m) for m in ms]
+    got = [None] * len(reqs)
+    errors = []
+
+    def client(part):
+        try:
+            rng = np.random.default_rng(part)
+            tickets = []
+            for i in range(part, len(reqs), 4):
+                kind, mid, q = reqs[i]
+                t = srv.submit_grid(ids[mid], q) if kind == "grid" else srv.submit_points(ids[mid], q)
+                tickets.append((i, t))
+                time.sleep(float(rng.uniform(0, 0.004)))
+            for i, t in tickets:
+                got[i] = srv.wait(t)
+        except Exception as ex:  # surfaced below
+            errors.append(ex)
+
+    threads = [threading.Thread(target=client, args=(p,)) for p in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    for (d, tri), (wd, wtri) in zip(got, want):
+        assert np.array_equal(d, wd)
+        assert np.array_equal(tri, wtri)
+    st = srv.stats()
+    assert st["completed"] == len(reqs)
+    assert st["evictions"] > 0 and st["builds"] > len(ms)
+    assert 0 < st["p50_ms"] <= st["p99_ms"] <= st["max_ms"]
+    # a burst is packed: requests waiting while a batch runs share the next one
+    srv.reset_stats()
+    burst = [srv.submit_points(ids[1], reqs[i][2]) for i in range(len(reqs)) if reqs[i][0] == "points"]
+    for t in burst:
+        srv.wait(t)
+    st = srv.stats()
+    assert st["completed"] == len(burst) and st["batches"] < len(burst)
+    srv.close()
+
+
+def test_rejects_oversized_and_unknown():
+    srv = S.Server(max_batch_queries=1000, max_batch_jobs=4)
+    mid = srv.add_mesh(W.icosphere(1))
+    with pytest.raises(S.SsdfError):
+        srv.submit_grid(mid, W.Grid((20, 20, 20), (0, 0, 0), (1, 1, 1)))
+    with pytest.raises(S.SsdfError):
+        srv.submit_points(mid + 5, np.zeros((3, 10)))
+    srv.close()
