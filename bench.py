@@ -288,14 +288,27 @@ def batched_leg(S, args):
     from ssdf_b200 import workloads as W
 
     sets = W.multi_mesh_set(count=args.batch_meshes)
-    dms = [S.DeviceMesh(m) for m, _ in sets]
+    # autotune on representative meshes across the size range; each mesh takes the leaf size of the
+    # representative nearest in triangle count, the batch the query-weighted majority traversal/arity
+    order = sorted(range(len(sets)), key=lambda i: sets[i][0].nt)
+    reps = [order[int(k)] for k in np.linspace(0, len(order) - 1, 8)]
+    tuned = {i: S.autotune_grid(sets[i][0], sets[i][1]) for i in reps}
+    votes = {}
+    for i, t in tuned.items():
+        key = (t["traversal"], t["arity"])
+        votes[key] = votes.get(key, 0) + sets[i][1].size
+    trav, arity = max(votes, key=votes.get)
+    leaf_of = lambda m: tuned[min(reps, key=lambda i: abs(np.log(sets[i][0].nt) - np.log(m.nt)))]["leaf_size"]  # noqa
+    dms = [S.DeviceMesh(m, leaf_size=leaf_of(m)) for m, _ in sets]
     outs = [torch.empty(g.size, dtype=torch.float64, device="cuda") for _, g in sets]
     nq = sum(g.size for _, g in sets)
     ntri = sum(m.nt for m, _ in sets)
     stream = torch.cuda.current_stream()
-    res = {"meshes": len(sets), "queries": nq, "triangles": ntri}
+    res = {"meshes": len(sets), "queries": nq, "triangles": ntri,
+           "tuning": {"traversal": "warp" if trav == 1 else "thread", "arity": arity,
+                      "leaf_sizes": sorted({t["leaf_size"] for t in tuned.values()})}}
     for prec, name in ((S.PREC_F32_FIXUP, "fixup"), (S.PREC_F64, "fp64")):
-        b = S.Batch(len(sets), prec)
+        b = S.Batch(len(sets), prec, traversal=trav, arity=arity)
         for dm, (m, g), out in zip(dms, sets, outs):
             b.add_grid(dm, g, out)
         ms = []

@@ -172,7 +172,7 @@ typedef struct {
     int leaf_size;    /* triangles per BVH leaf, 1..16 (0: 4)                                 */
     int keep_fp64;    /* 1: also keep double triangles and nodes (F64 and fix-up queries)      */
     int normals;      /* 1: build pseudo-normals (signed queries)                             */
-    int treelet_opt;  /* 1: SAH treelet refinement of the LBVH (0: plain LBVH)                 */
+    int treelet_opt;  /* 1: SAH treelet refinement of the LBVH (0: plain LBVH); 1 by default    */
 } ssdf_build_opts;
 
 typedef struct {
@@ -224,6 +224,24 @@ int ssdf_batch_add_points(ssdf_batch *batch, ssdf_mesh *mesh, ptrdiff_t npoints,
 int ssdf_batch_run(ssdf_batch *batch, int use_graph, void *stream);
 /* 128-query work items of the last run. */
 long long ssdf_batch_last_blocks(const ssdf_batch *batch);
+
+/* ---- autotuner (no reference counterpart) ------------------------------------------------------ */
+
+typedef struct {
+    int leaf_size; /* BVH leaf size: 2, 4 or 8                                               */
+    int traversal; /* 1 warp packets, 2 thread per query                                      */
+    int arity;     /* 2 binary, 4 four-wide                                                   */
+    double ms;     /* measured time of the winner on the sample grid                         */
+} ssdf_tuning;
+
+/* Times leaf sizes {2, 4, 8} x traversal {warp, thread} x arity {2, 4} for this mesh (host double
+ * arrays) on a sample of the grid -- the same box at up to 2^21 nodes -- in the given arithmetic,
+ * and returns the fastest. With cache_path (a JSON file) the winner is stored per size class
+ * (log2 triangles, log2 nodes, arithmetic) and later calls of that class return it untimed. */
+int ssdf_autotune_grid(ptrdiff_t nselements, const int *s0, const int *s1, const int *s2, ptrdiff_t nspoints,
+                       const double *sx, const double *sy, const double *sz, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz,
+                       const double lo[3], const double hi[3], int precision, const char *cache_path,
+                       ssdf_tuning *best);
 
 /* ---- serving loop: continuous batching over resident meshes (no reference counterpart) ------- */
 

@@ -119,6 +119,14 @@ class ServerStats(C.Structure):
 
 
 _dp_ = C.POINTER(C.c_double)
+
+
+class Tuning(C.Structure):
+    _fields_ = [("leaf_size", C.c_int), ("traversal", C.c_int), ("arity", C.c_int), ("ms", C.c_double)]
+
+
+_sig("ssdf_autotune_grid", [_pd, _ip, _ip, _ip, _pd, _vp, _vp, _vp, _pd, _pd, _pd, C.POINTER(C.c_double * 3),
+                            C.POINTER(C.c_double * 3), C.c_int, C.c_char_p, C.POINTER(Tuning)])
 _sig("ssdf_server_create", [C.POINTER(_vp), C.POINTER(ServerOpts)])
 _sig("ssdf_server_destroy", [_vp])
 _sig("ssdf_server_add_mesh", [_vp, _pd, _ip, _ip, _ip, _pd, _vp, _vp, _vp, _ip])
@@ -140,7 +148,7 @@ EXPORTED = ["ssdf_status_string", "ssdf_last_error", "ssdf_b200_version", "ssdf_
             "ssdf_batch_size", "ssdf_batch_add_grid", "ssdf_batch_add_points", "ssdf_batch_run",
             "ssdf_batch_last_blocks", "ssdf_query_grid_noalloc", "ssdf_query_grid_noalloc_max", "ssdf_server_create",
             "ssdf_server_destroy", "ssdf_server_add_mesh", "ssdf_server_submit_points", "ssdf_server_submit_grid",
-            "ssdf_server_wait", "ssdf_server_stats", "ssdf_server_reset_stats"]
+            "ssdf_server_wait", "ssdf_server_stats", "ssdf_server_reset_stats", "ssdf_autotune_grid"]
 
 
 def _status_name(status: int) -> str:
@@ -331,7 +339,7 @@ def _stream_handle(stream) -> int:
 class DeviceMesh:
     """A mesh, its BVH and (optionally) pseudo-normals, resident on the current GPU."""
 
-    def __init__(self, mesh, coord_dtype=np.float64, leaf_size=0, keep_fp64=True, normals=True, treelet=False,
+    def __init__(self, mesh, coord_dtype=np.float64, leaf_size=0, keep_fp64=True, normals=True, treelet=True,
                  stream=None):
         hm = _HostMesh(mesh, coord_dtype)
         self._h = C.c_void_p()
@@ -490,4 +498,16 @@ class Server:
 
     def reset_stats(self):
         _check(lib.ssdf_server_reset_stats(self._h), "ssdf_server_reset_stats")
+
+
+def autotune_grid(mesh, grid, precision=PREC_F32_FIXUP, cache_path=None):
+    """Fastest (leaf_size, traversal, arity) for this mesh and grid; cached per size class."""
+    hm = _HostMesh(mesh, np.float64)
+    lo = (C.c_double * 3)(*grid.lo)
+    hi = (C.c_double * 3)(*grid.hi)
+    t = Tuning()
+    path = cache_path.encode() if cache_path else None
+    _check(lib.ssdf_autotune_grid(*hm.args(), *(int(v) for v in grid.n), C.byref(lo), C.byref(hi), int(precision),
+                                  path, C.byref(t)), "ssdf_autotune_grid")
+    return dict(leaf_size=t.leaf_size, traversal=t.traversal, arity=t.arity, ms=t.ms)
 

@@ -1,4 +1,4 @@
-// bvh_query.cu -- closest-triangle queries over the device BVH, one thread per query.
+// bvh_query.cu -- closest-triangle queries over the device BVH.
 //
 // Stands in for the reference's device query (serial/bvh/bvh.cu:60-76 + cuBQL CPAT) and its CPU
 // grid samplers (serial/bvh/bvh.cpp:1574-1798). Three arithmetics (SSDF_PREC_*):
@@ -12,9 +12,12 @@
 //         double winner is always in the window; a query whose window overflowed the K slots is
 //         walked again with the window fixed, re-evaluating every member in double (k_window).
 //         Result: bitwise the F64 result.
-// Traversal: nearest child first, the farther one pushed with its box distance on a per-thread
-// stack and culled on pop against the current threshold. Grid queries map a warp to a 4x4x2 brick
-// of nodes and a block to 8x4x4, so a warp's traversals stay coherent.
+// Traversal: nearest child first, the farther one pushed with its box distance on a per-lane stack
+// and culled on pop against the current thresholds. Each lane answers kQ queries (a build option;
+// 1 by default, 2 measured no faster: it shares each node and triangle load between two chains of
+// arithmetic but costs the registers of the second). Grid queries map a
+// warp to a 4 x 4 x 2kQ brick of nodes, so the warp's traversals stay coherent; by default a grid
+// warp walks the tree as one packet.
 // Outputs (SSDF_OUT_*): in/out distance (edf), in/out squared distance (sqedf), signed distance
 // with the pseudo-normal rule of serial/bvh/bvh.cpp:1751-1792, closest point + triangle
 // (closest_point_bvh, serial/bvh/bvh.cpp:178-194).
@@ -39,11 +42,13 @@ constexpr int kThreads = 128;
 #define SSDF_B200_WINDOW_SLOTS 8
 #endif
 constexpr int kCand = SSDF_B200_WINDOW_SLOTS;
-// Minimum resident blocks per SM the float query kernels are compiled for: 8 blocks of 128 caps
-// them at 64 registers. The traversal is latency-bound, so the occupancy this buys outweighs the
-// few spills (measured: -22 % time on the torus-knot grid); the double kernel keeps its registers.
+
+// Minimum resident blocks per SM the float query kernels are compiled for: 10 blocks of 128 caps
+// them at 48 registers (the fix-up window lives in shared memory). The traversal is issue-latency
+// bound, so the occupancy this buys outweighs the few spills (measured on the torus-knot grid:
+// 24.5 ms against 34 ms uncapped); the double kernel keeps its registers.
 #ifndef SSDF_B200_QUERY_MIN_BLOCKS
-#define SSDF_B200_QUERY_MIN_BLOCKS 8
+#define SSDF_B200_QUERY_MIN_BLOCKS 10
 #endif
 
 struct Counters {
@@ -55,11 +60,13 @@ __device__ __forceinline__ float finf() { return __int_as_float(0x7f800000); }
 
 // ---- query mapping ------------------------------------------------------------------------------
 
-// Grid brick: block = 8 (x) * 4 (y) * 4 (z) nodes, warp = 4 * 4 * 2.
-__device__ __forceinline__ bool map_thread(const QueryArgs &a, long long b, long long &q, long long &i,
-                                           long long &j, long long &k) {
+// Each lane answers kQ queries. Grid: a block covers 8 (x) x 4 (y) x 4 kQ (z) nodes and a warp
+// 4 x 4 x 2 kQ; lane (lx, ly, lz) takes kQ consecutive z nodes. Point lists: query
+// (block * kQ + s) * 128 + thread, so each of a lane's queries is a coalesced load.
+__device__ __forceinline__ bool map_query(const QueryArgs &a, long long b, int s, long long &q, long long &i,
+                                          long long &j, long long &k) {
     if (!a.is_grid) {
-        q = b * kThreads + threadIdx.x;
+        q = (b * kQ + s) * kThreads + threadIdx.x;
         return q < a.npoints;
     }
     const long long bxn = (a.nx + 7) >> 3, byn = (a.ny + 3) >> 2;
@@ -68,7 +75,7 @@ __device__ __forceinline__ bool map_thread(const QueryArgs &a, long long b, long
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     i = bx * 8 + (warp & 1) * 4 + (lane & 3);
     j = by * 4 + ((lane >> 2) & 3);
-    k = bz * 4 + (warp >> 1) * 2 + (lane >> 4);
+    k = (bz * 4 + (warp >> 1) * 2 + (lane >> 4)) * kQ + s;
     q = i + a.nx * (j + a.ny * k);
     return i < a.nx && j < a.ny && k < a.nz;
 }
@@ -218,101 +225,116 @@ __device__ __forceinline__ Tri64 load_tri64(const double2 *__restrict__ t, int p
 
 // ---- traversal policies ---------------------------------------------------------------------------
 //
-// A policy owns one query's state (point, incumbent, prune threshold `thr`) and knows how to test a
-// node's two child boxes and a leaf's triangles in its arithmetic. `want` tells a leaf which lanes
-// asked for it (in warp mode every lane walks every leaf the warp visits).
+// A policy owns a lane's kQ queries (points, incumbents, prune thresholds `thr`) and knows how to
+// test a node's child boxes and a leaf's triangles in its arithmetic. A node or leaf is wanted by a
+// lane when any of its queries wants it (`want` returns the per-query mask); a pushed node keeps the
+// smallest of its queries' box distances and is entered on pop while that is below the largest
+// threshold (conservative for every query of the lane).
 
 template <typename T>
 struct ExactData;
 template <>
 struct ExactData<double> {
+    using Tri = Tri64;
     static constexpr double rel = 1.0 + 1.0 / 65536.0;
     static __device__ __forceinline__ double abs_margin(float scale) {
         const double s = double(scale) * 0x1p-40;
         return s * s;
     }
-    static __device__ __forceinline__ void boxes(const DeviceMesh &m, int node, double px, double py, double pz,
-                                                 double &d0, double &d1, int &r0, int &r1) {
-        const Node64 n = load_node64(m.nodes64, node);
+    static __device__ __forceinline__ Node64 node(const DeviceMesh &m, int n) { return load_node64(m.nodes64, n); }
+    static __device__ __forceinline__ void boxes(const Node64 &n, double px, double py, double pz, double &d0,
+                                                 double &d1) {
         d0 = box_dist_sq<double>(px, py, pz, n.x0.x, n.x0.y, n.y0.x, n.y0.y, n.z0.x, n.z0.y);
         d1 = box_dist_sq<double>(px, py, pz, n.x1.x, n.x1.y, n.y1.x, n.y1.y, n.z1.x, n.z1.y);
-        r0 = n.r0;
-        r1 = n.r1;
     }
-    static __device__ __forceinline__ double tri(const DeviceMesh &m, int pos, double px, double py, double pz,
-                                                 int &id) {
-        const Tri64 t = load_tri64(m.tris64, pos);
-        id = t.id;
-        return tri_dist_sq_exact<double>(px, py, pz, t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
-    }
+    static __device__ __forceinline__ Tri tri(const DeviceMesh &m, int pos) { return load_tri64(m.tris64, pos); }
 };
 template <>
 struct ExactData<float> {
+    using Tri = Tri32;
     static constexpr float rel = 1.0f + 1.0f / 65536.0f;
     static __device__ __forceinline__ float abs_margin(float scale) {
         const float s = scale * 0x1p-16f;
         return s * s;
     }
-    static __device__ __forceinline__ void boxes(const DeviceMesh &m, int node, float px, float py, float pz,
-                                                 float &d0, float &d1, int &r0, int &r1) {
-        const Node32 n = load_node32(m.nodes32, node);
+    static __device__ __forceinline__ Node32 node(const DeviceMesh &m, int n) { return load_node32(m.nodes32, n); }
+    static __device__ __forceinline__ void boxes(const Node32 &n, float px, float py, float pz, float &d0, float &d1) {
         d0 = box_dist_sq<float>(px, py, pz, n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y);
         d1 = box_dist_sq<float>(px, py, pz, n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w);
-        r0 = n.r0;
-        r1 = n.r1;
     }
-    static __device__ __forceinline__ float tri(const DeviceMesh &m, int pos, float px, float py, float pz, int &id) {
-        const Tri32 t = load_tri32(m.tris32, pos);
-        id = t.id;
-        return tri_dist_sq_exact<float>(px, py, pz, t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
-    }
+    static __device__ __forceinline__ Tri tri(const DeviceMesh &m, int pos) { return load_tri32(m.tris32, pos); }
 };
 
 // Lexicographic (d^2, id) minimum over all triangles, starting from (best, -1): a triangle replaces
 // the incumbent if strictly closer, or equally close with a lower index (never the initial bound on
 // a tie). Boxes are kept while their distance is below best * (1 + 2^-16) + margin, so rounding in
 // box distances never drops a tie.
-template <typename T>
+template <typename T, int Q>
 struct ExactPolicy {
     using R = T;
+    static constexpr int kQn = Q;
     const DeviceMesh &m;
-    T px, py, pz, best, thr, margin;
-    int bid = -1, bpos = -1;
-    __device__ ExactPolicy(const DeviceMesh &mesh, T x, T y, T z, T init) : m(mesh), px(x), py(y), pz(z), best(init) {
+    T px[Q], py[Q], pz[Q], best[Q], thr[Q];
+    int bid[Q], bpos[Q];
+    T margin;
+    __device__ explicit ExactPolicy(const DeviceMesh &mesh) : m(mesh) {
         margin = ExactData<T>::abs_margin(m.coord_scale);
-        thr = best * ExactData<T>::rel + margin;
     }
-    __device__ __forceinline__ void boxes(int node, T &d0, T &d1, int &r0, int &r1) const {
-        ExactData<T>::boxes(m, node, px, py, pz, d0, d1, r0, r1);
+    __device__ __forceinline__ void set(int q, T x, T y, T z, T init) {
+        px[q] = x, py[q] = y, pz[q] = z, best[q] = init, bid[q] = -1, bpos[q] = -1;
+        thr[q] = init * ExactData<T>::rel + margin;
     }
-    __device__ __forceinline__ void boxes4(int node, T (&d)[4], int (&r)[4]) const {
-        boxes4_exact<T>(m, node, px, py, pz, d, r);
+    __device__ __forceinline__ void disable(int q) {
+        px[q] = py[q] = pz[q] = T(0), best[q] = T(0), bid[q] = -1, bpos[q] = -1;
+        thr[q] = T(-1);
+    }
+    __device__ __forceinline__ void boxes(int node, T (&d0)[Q], T (&d1)[Q], int &r0, int &r1) const {
+        const auto n = ExactData<T>::node(m, node);
+#pragma unroll
+        for (int q = 0; q < Q; q++) ExactData<T>::boxes(n, px[q], py[q], pz[q], d0[q], d1[q]);
+        r0 = n.r0;
+        r1 = n.r1;
+    }
+    __device__ __forceinline__ void boxes4(int node, T (&d)[4][Q], int (&r)[4]) const {
+#pragma unroll
+        for (int q = 0; q < Q; q++) {
+            T dq[4];
+            boxes4_exact<T>(m, node, px[q], py[q], pz[q], dq, r);
+#pragma unroll
+            for (int c = 0; c < 4; c++) d[c][q] = dq[c];
+        }
+    }
+    __device__ __forceinline__ T max_thr() const {
+        T t = thr[0];
+#pragma unroll
+        for (int q = 1; q < Q; q++) t = t > thr[q] ? t : thr[q];
+        return t;
     }
     template <bool COUNT>
-    __device__ __forceinline__ void leaf(int first, int n, bool want, Counters &cnt) {
+    __device__ __forceinline__ void leaf(int first, int n, unsigned mask, Counters &cnt) {
         for (int k = 0; k < n; k++) {
-            if (!want) continue;
-            int id;
-            const T d2 = ExactData<T>::tri(m, first + k, px, py, pz, id);
-            if (COUNT) cnt.tri++;
-            if (d2 < best || (d2 == best && bid >= 0 && id < bid)) {
-                best = d2;
-                bid = id;
-                bpos = first + k;
-                thr = best * ExactData<T>::rel + margin;
+            const auto t = ExactData<T>::tri(m, first + k);
+#pragma unroll
+            for (int q = 0; q < Q; q++) {
+                if (!((mask >> q) & 1u)) continue;
+                const T d2 = tri_dist_sq_exact<T>(px[q], py[q], pz[q], t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx,
+                                                  t.cy, t.cz);
+                if (COUNT) cnt.tri++;
+                if (d2 < best[q] || (d2 == best[q] && bid[q] >= 0 && t.id < bid[q])) {
+                    best[q] = d2;
+                    bid[q] = t.id;
+                    bpos[q] = first + k;
+                    thr[q] = best[q] * ExactData<T>::rel + margin;
+                }
             }
         }
     }
 };
 
-// F32X: float filter. Keeps the kCand smallest float d^2 inside the window
-// (sqrt(best) + tau)^2 and the smallest d^2 that was pushed out of the slots.
-struct Window {
-    float d[kCand];
-    int p[kCand];
-    float evicted;
-};
-
+// F32X: float filter. Per query, the kCand smallest float d^2 inside the window
+// (sqrt(best) + tau)^2 are kept, sorted, in shared memory (slot (q, s) of thread t at
+// [(q * kCand + s) * kThreads + t]: consecutive threads, consecutive banks), with the smallest d^2
+// pushed out of the slots.
 __device__ __forceinline__ float window_thr(float best, float tau_rel, float scale) {
     if (!(best < finf())) return finf();
     const float d = sqrtf(best);
@@ -320,53 +342,88 @@ __device__ __forceinline__ float window_thr(float best, float tau_rel, float sca
     return w * w * (1.0f + 1.0f / 65536.0f);
 }
 
+template <int Q>
 struct FastPolicy {
     using R = float;
+    static constexpr int kQn = Q;
     const DeviceMesh &m;
-    float px, py, pz, best, thr, tau_rel;
-    Window win;
-    __device__ FastPolicy(const DeviceMesh &mesh, float x, float y, float z, float init, float tau)
-        : m(mesh), px(x), py(y), pz(z), best(init), tau_rel(tau) {
+    float px[Q], py[Q], pz[Q], best[Q], thr[Q], evicted[Q], wmax[Q];
+    float tau_rel;
+    float *wd;
+    int *wp;
+    __device__ FastPolicy(const DeviceMesh &mesh, float tau, float *sd, int *sp)
+        : m(mesh), tau_rel(tau), wd(sd + threadIdx.x), wp(sp + threadIdx.x) {}
+    __device__ __forceinline__ int slot(int q, int s) const { return (q * kCand + s) * kThreads; }
+    __device__ __forceinline__ void set(int q, float x, float y, float z, float init) {
+        px[q] = x, py[q] = y, pz[q] = z, best[q] = init, evicted[q] = finf(), wmax[q] = finf();
+        thr[q] = window_thr(init, tau_rel, m.coord_scale);
 #pragma unroll
-        for (int s = 0; s < kCand; s++) win.d[s] = finf(), win.p[s] = -1;
-        win.evicted = finf();
-        thr = window_thr(best, tau_rel, m.coord_scale);
+        for (int s = 0; s < kCand; s++) wd[slot(q, s)] = finf(), wp[slot(q, s)] = -1;
     }
-    __device__ __forceinline__ void boxes(int node, float &d0, float &d1, int &r0, int &r1) const {
+    __device__ __forceinline__ void disable(int q) {
+        set(q, 0.f, 0.f, 0.f, finf());
+        thr[q] = -1.f;
+    }
+    __device__ __forceinline__ void boxes(int node, float (&d0)[Q], float (&d1)[Q], int &r0, int &r1) const {
         const Node32 n = load_node32(m.nodes32, node);
-        d0 = box_dist_sq_fast(px, py, pz, n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y);
-        d1 = box_dist_sq_fast(px, py, pz, n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w);
+#pragma unroll
+        for (int q = 0; q < Q; q++) {
+            d0[q] = box_dist_sq_fast(px[q], py[q], pz[q], n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y);
+            d1[q] = box_dist_sq_fast(px[q], py[q], pz[q], n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w);
+        }
         r0 = n.r0;
         r1 = n.r1;
     }
-    __device__ __forceinline__ void boxes4(int node, float (&d)[4], int (&r)[4]) const {
-        boxes4_fast(m, node, px, py, pz, d, r);
+    __device__ __forceinline__ void boxes4(int node, float (&d)[4][Q], int (&r)[4]) const {
+#pragma unroll
+        for (int q = 0; q < Q; q++) {
+            float dq[4];
+            boxes4_fast(m, node, px[q], py[q], pz[q], dq, r);
+#pragma unroll
+            for (int c = 0; c < 4; c++) d[c][q] = dq[c];
+        }
+    }
+    __device__ __forceinline__ float max_thr() const {
+        float t = thr[0];
+#pragma unroll
+        for (int q = 1; q < Q; q++) t = fmaxf(t, thr[q]);
+        return t;
+    }
+    __device__ __forceinline__ void insert(int q, float d, int p) {
+        if (!(d < wmax[q])) {
+            evicted[q] = fminf(evicted[q], d);
+            return;
+        }
+#pragma unroll
+        for (int s = 0; s < kCand; s++) {
+            const float cur = wd[slot(q, s)];
+            if (d < cur) {
+                const int cp = wp[slot(q, s)];
+                wd[slot(q, s)] = d;
+                wp[slot(q, s)] = p;
+                d = cur;
+                p = cp;
+            }
+        }
+        evicted[q] = fminf(evicted[q], d);
+        wmax[q] = wd[slot(q, kCand - 1)];
     }
     template <bool COUNT>
-    __device__ __forceinline__ void leaf(int first, int n, bool want, Counters &cnt) {
+    __device__ __forceinline__ void leaf(int first, int n, unsigned mask, Counters &cnt) {
         for (int k = 0; k < n; k++) {
-            if (!want) continue;
             const Tri32 t = load_tri32(m.tris32, first + k);
-            const float d2 = tri_dist_sq_fast(px, py, pz, t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
-            if (COUNT) cnt.tri++;
-            if (d2 < thr) {
-                float d = d2;
-                int p = first + k;
 #pragma unroll
-                for (int s = 0; s < kCand; s++) {
-                    if (d < win.d[s]) {
-                        const float td = win.d[s];
-                        const int tp = win.p[s];
-                        win.d[s] = d;
-                        win.p[s] = p;
-                        d = td;
-                        p = tp;
+            for (int q = 0; q < Q; q++) {
+                if (!((mask >> q) & 1u)) continue;
+                const float d2 =
+                    tri_dist_sq_fast(px[q], py[q], pz[q], t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
+                if (COUNT) cnt.tri++;
+                if (d2 < thr[q]) {
+                    insert(q, d2, first + k);
+                    if (d2 < best[q]) {
+                        best[q] = d2;
+                        thr[q] = window_thr(best[q], tau_rel, m.coord_scale);
                     }
-                }
-                win.evicted = fminf(win.evicted, d);
-                if (d2 < best) {
-                    best = d2;
-                    thr = window_thr(best, tau_rel, m.coord_scale);
                 }
             }
         }
@@ -378,30 +435,37 @@ struct FastPolicy {
 // the spot (the same float test decides membership, so the set is exactly the window).
 struct WindowPolicy {
     using R = float;
+    static constexpr int kQn = 1;
     const DeviceMesh &m;
-    float px, py, pz, thr;
+    float px[1], py[1], pz[1], thr[1];
     double qx, qy, qz, best;
     int bid = -1, bpos = -1;
     __device__ WindowPolicy(const DeviceMesh &mesh, double x, double y, double z, float window, double init)
-        : m(mesh), px(float(x)), py(float(y)), pz(float(z)), thr(window), qx(x), qy(y), qz(z), best(init) {}
-    __device__ __forceinline__ void boxes(int node, float &d0, float &d1, int &r0, int &r1) const {
+        : m(mesh), qx(x), qy(y), qz(z), best(init) {
+        px[0] = float(x), py[0] = float(y), pz[0] = float(z), thr[0] = window;
+    }
+    __device__ __forceinline__ void boxes(int node, float (&d0)[1], float (&d1)[1], int &r0, int &r1) const {
         const Node32 n = load_node32(m.nodes32, node);
-        d0 = box_dist_sq_fast(px, py, pz, n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y);
-        d1 = box_dist_sq_fast(px, py, pz, n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w);
+        d0[0] = box_dist_sq_fast(px[0], py[0], pz[0], n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y);
+        d1[0] = box_dist_sq_fast(px[0], py[0], pz[0], n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w);
         r0 = n.r0;
         r1 = n.r1;
     }
-    __device__ __forceinline__ void boxes4(int node, float (&d)[4], int (&r)[4]) const {
-        boxes4_fast(m, node, px, py, pz, d, r);
+    __device__ __forceinline__ void boxes4(int node, float (&d)[4][1], int (&r)[4]) const {
+        float dq[4];
+        boxes4_fast(m, node, px[0], py[0], pz[0], dq, r);
+#pragma unroll
+        for (int c = 0; c < 4; c++) d[c][0] = dq[c];
     }
+    __device__ __forceinline__ float max_thr() const { return thr[0]; }
     template <bool COUNT>
-    __device__ __forceinline__ void leaf(int first, int n, bool want, Counters &cnt) {
+    __device__ __forceinline__ void leaf(int first, int n, unsigned mask, Counters &cnt) {
+        if (!mask) return;
         for (int k = 0; k < n; k++) {
-            if (!want) continue;
             const Tri32 t = load_tri32(m.tris32, first + k);
-            const float d2 = tri_dist_sq_fast(px, py, pz, t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
+            const float d2 = tri_dist_sq_fast(px[0], py[0], pz[0], t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
             if (COUNT) cnt.tri++;
-            if (d2 < thr) {
+            if (d2 < thr[0]) {
                 const Tri64 u = load_tri64(m.tris64, first + k);
                 const double e2 =
                     tri_dist_sq_exact<double>(qx, qy, qz, u.ax, u.ay, u.az, u.bx, u.by, u.bz, u.cx, u.cy, u.cz);
@@ -416,28 +480,52 @@ struct WindowPolicy {
     }
 };
 
-// Nearest-child-first traversal with a per-lane stack of (node, box distance), culled on pop.
-// WARP = false: every thread walks its own query. WARP = true (packet): the 32 lanes of a warp walk
-// one path together -- a child is entered if any lane wants it, the nearer child is the one most
-// lanes rank first -- so node and triangle loads are warp-uniform (broadcast) and leaf work does
-// not diverge. Every lane must call it (warp-synchronous when WARP).
+template <class P, int Q = P::kQn>
+__device__ __forceinline__ unsigned want_mask(const P &p, const typename P::R (&d)[Q]) {
+    unsigned m = 0;
+#pragma unroll
+    for (int q = 0; q < Q; q++) m |= (d[q] < p.thr[q]) ? (1u << q) : 0u;
+    return m;
+}
+
+template <typename R, int Q>
+__device__ __forceinline__ R min_of(const R (&d)[Q]) {
+    R v = d[0];
+#pragma unroll
+    for (int q = 1; q < Q; q++) v = d[q] < v ? d[q] : v;
+    return v;
+}
+
+// Nearest-child-first traversal with a per-lane stack of (node, smallest box distance), culled on
+// pop. WARP = false: every thread walks its own queries. WARP = true (packet): the 32 lanes of a
+// warp walk one path together -- a child is entered if any lane wants it, the nearer child is the
+// one most lanes rank first -- so node and triangle loads are warp-uniform (broadcast) and leaf work
+// does not diverge. Every lane must call it (warp-synchronous when WARP).
 template <bool WARP, bool COUNT, class P>
 __device__ __forceinline__ void traverse(P &p, Counters &cnt) {
     using R = typename P::R;
+    constexpr int Q = P::kQn;
     int snode[kStackSize];
     R sdist[kStackSize];
     int sp = 0;
     int node = 0;
     while (true) {
-        R d0, d1;
+        R d0[Q], d1[Q];
         int r0, r1;
         p.boxes(node, d0, d1, r0, r1);
-        if (COUNT) cnt.box += 2;
-        const bool swap = WARP ? (__popc(__ballot_sync(0xffffffffu, d1 < d0)) > 16) : (d1 < d0);
+        if (COUNT) cnt.box += 2 * Q;
+        R k0 = min_of<R, Q>(d0), k1 = min_of<R, Q>(d1);
+        const bool swap = WARP ? (__popc(__ballot_sync(0xffffffffu, k1 < k0)) > 16) : (k1 < k0);
         if (swap) {
-            const R td = d0;
-            d0 = d1;
-            d1 = td;
+#pragma unroll
+            for (int q = 0; q < Q; q++) {
+                const R t = d0[q];
+                d0[q] = d1[q];
+                d1[q] = t;
+            }
+            const R tk = k0;
+            k0 = k1;
+            k1 = tk;
             const int tr = r0;
             r0 = r1;
             r1 = tr;
@@ -445,24 +533,24 @@ __device__ __forceinline__ void traverse(P &p, Counters &cnt) {
         int next = -1;
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-            const R dc = h ? d1 : d0;
             const int rc = h ? r1 : r0;
-            const bool want = dc < p.thr && rc != kEmptyRef;
-            if (WARP ? !__any_sync(0xffffffffu, want) : !want) continue;
+            const unsigned m = rc == kEmptyRef ? 0u : (h ? want_mask(p, d1) : want_mask(p, d0));
+            if (WARP ? !__any_sync(0xffffffffu, m != 0u) : m == 0u) continue;
             if (rc < 0) {
-                p.template leaf<COUNT>(leaf_first(rc), leaf_count(rc), want, cnt);
+                p.template leaf<COUNT>(leaf_first(rc), leaf_count(rc), m, cnt);
             } else if (next < 0) {
                 next = rc;
             } else if (sp < kStackSize) {
                 snode[sp] = rc;
-                sdist[sp] = dc;
+                sdist[sp] = h ? k1 : k0;
                 sp++;
             }
         }
         if (next < 0) {
+            const R tmax = p.max_thr();
             while (sp > 0) {
                 sp--;
-                const bool w = sdist[sp] < p.thr;
+                const bool w = sdist[sp] < tmax;
                 if (WARP ? __any_sync(0xffffffffu, w) : w) {
                     next = snode[sp];
                     break;
@@ -474,20 +562,24 @@ __device__ __forceinline__ void traverse(P &p, Counters &cnt) {
     }
 }
 
-// The same over the 4-wide BVH. Children are visited in ascending box distance -- the lane's own in
-// thread mode, a representative lane's (the brick centre) in warp mode -- leaves first in that
-// order, then the nearest wanted internal child is entered and the others pushed farthest-first.
+// The same over the 4-wide BVH. Children are visited in ascending box distance -- the lane's own
+// smallest in thread mode, a representative lane's (the brick centre) in warp mode -- leaves first
+// in that order, then the nearest wanted internal child is entered and the others pushed
+// farthest-first.
 constexpr int kRepLane = 21;  // (1, 1, 1) of the 4 x 4 x 2 brick
 
-template <typename R>
-__device__ __forceinline__ void cswap4(float (&k)[4], R (&d)[4], int (&r)[4], int i, int j) {
+template <typename R, int Q>
+__device__ __forceinline__ void cswap4(float (&k)[4], R (&d)[4][Q], int (&r)[4], int i, int j) {
     if (k[j] < k[i]) {
         const float tk = k[i];
         k[i] = k[j];
         k[j] = tk;
-        const R td = d[i];
-        d[i] = d[j];
-        d[j] = td;
+#pragma unroll
+        for (int q = 0; q < Q; q++) {
+            const R td = d[i][q];
+            d[i][q] = d[j][q];
+            d[j][q] = td;
+        }
         const int tr = r[i];
         r[i] = r[j];
         r[j] = tr;
@@ -497,49 +589,54 @@ __device__ __forceinline__ void cswap4(float (&k)[4], R (&d)[4], int (&r)[4], in
 template <bool WARP, bool COUNT, class P>
 __device__ __forceinline__ void traverse4(P &p, Counters &cnt) {
     using R = typename P::R;
+    constexpr int Q = P::kQn;
     int snode[kStackSize];
     R sdist[kStackSize];
     int sp = 0;
     int node = 0;
     while (true) {
-        R d[4];
+        R d[4][Q];
         int r[4];
         p.boxes4(node, d, r);
-        if (COUNT) cnt.box += 4;
+        if (COUNT) cnt.box += 4 * Q;
         float key[4];
 #pragma unroll
-        for (int c = 0; c < 4; c++) key[c] = WARP ? __shfl_sync(0xffffffffu, float(d[c]), kRepLane) : float(d[c]);
-        cswap4(key, d, r, 0, 1);
-        cswap4(key, d, r, 2, 3);
-        cswap4(key, d, r, 0, 2);
-        cswap4(key, d, r, 1, 3);
-        cswap4(key, d, r, 1, 2);
+        for (int c = 0; c < 4; c++) {
+            const float own = float(min_of<R, Q>(d[c]));
+            key[c] = WARP ? __shfl_sync(0xffffffffu, own, kRepLane) : own;
+        }
+        cswap4<R, Q>(key, d, r, 0, 1);
+        cswap4<R, Q>(key, d, r, 2, 3);
+        cswap4<R, Q>(key, d, r, 0, 2);
+        cswap4<R, Q>(key, d, r, 1, 3);
+        cswap4<R, Q>(key, d, r, 1, 2);
 #pragma unroll
         for (int c = 0; c < 4; c++) {
             if (r[c] >= 0 || r[c] == kEmptyRef) continue;
-            const bool want = d[c] < p.thr;
-            if (WARP ? !__any_sync(0xffffffffu, want) : !want) continue;
-            p.template leaf<COUNT>(leaf_first(r[c]), leaf_count(r[c]), want, cnt);
+            const unsigned m = want_mask(p, d[c]);
+            if (WARP ? !__any_sync(0xffffffffu, m != 0u) : m == 0u) continue;
+            p.template leaf<COUNT>(leaf_first(r[c]), leaf_count(r[c]), m, cnt);
         }
         int next = -1;
         R next_d = R(0);
 #pragma unroll
         for (int c = 3; c >= 0; c--) {
             if (r[c] < 0) continue;
-            const bool want = d[c] < p.thr;
-            if (WARP ? !__any_sync(0xffffffffu, want) : !want) continue;
+            const unsigned m = want_mask(p, d[c]);
+            if (WARP ? !__any_sync(0xffffffffu, m != 0u) : m == 0u) continue;
             if (next >= 0 && sp < kStackSize) {
                 snode[sp] = next;
                 sdist[sp] = next_d;
                 sp++;
             }
             next = r[c];
-            next_d = d[c];
+            next_d = min_of<R, Q>(d[c]);
         }
         if (next < 0) {
+            const R tmax = p.max_thr();
             while (sp > 0) {
                 sp--;
-                const bool w = sdist[sp] < p.thr;
+                const bool w = sdist[sp] < tmax;
                 if (WARP ? __any_sync(0xffffffffu, w) : w) {
                     next = snode[sp];
                     break;
@@ -681,76 +778,113 @@ __device__ __forceinline__ void flush_counters(const QueryArgs &a, const Counter
 
 // ---- kernels ----------------------------------------------------------------------------------------
 
-// One kernel per (arithmetic, traversal mode, instrumentation). Lanes without a query (the edge of
-// a grid brick, the tail of a point list) take part in warp-mode traversal with a negative
-// threshold, so they never ask for a node.
+// One block of 128 lanes x kQ queries. Lanes without a query (the edge of a grid brick, the tail of
+// a point list) take part in warp-mode traversal with a negative threshold, so they never ask for
+// a node.
 template <int PREC, bool WARP, bool WIDE, bool COUNT>
 __device__ __forceinline__ void query_block(const QueryArgs &a, long long block, Counters &cnt) {
-    long long q = 0, i = 0, j = 0, k = 0;
-    const bool valid = map_thread(a, block, q, i, j, k);
-    double qx = 0.0, qy = 0.0, qz = 0.0;
-    if (valid) query_point(a, q, i, j, k, qx, qy, qz);
+    constexpr int Q = kQ;
+    long long qid[Q], gi[Q], gj[Q], gk[Q];
+    bool valid[Q];
+    bool any = false;
+#pragma unroll
+    for (int s = 0; s < Q; s++) {
+        gi[s] = gj[s] = gk[s] = 0;
+        valid[s] = map_query(a, block, s, qid[s], gi[s], gj[s], gk[s]);
+        any |= valid[s];
+    }
     if (PREC == SSDF_PREC_F64) {
-        const double init = valid ? initial_bound(a, q) : 0.0;
-        ExactPolicy<double> p(a.m, qx, qy, qz, init);
-        if (!valid) p.thr = -1.0;
-        if (WARP || valid) walk<WARP, WIDE, COUNT>(p, cnt);
-        if (valid) write_result(a, q, qx, qy, qz, p.best, p.bid, p.bpos);
+        ExactPolicy<double, Q> p(a.m);
+#pragma unroll
+        for (int s = 0; s < Q; s++) {
+            if (valid[s]) {
+                double x, y, z;
+                query_point(a, qid[s], gi[s], gj[s], gk[s], x, y, z);
+                p.set(s, x, y, z, initial_bound(a, qid[s]));
+            } else {
+                p.disable(s);
+            }
+        }
+        if (WARP || any) walk<WARP, WIDE, COUNT>(p, cnt);
+#pragma unroll
+        for (int s = 0; s < Q; s++)
+            if (valid[s]) write_result(a, qid[s], p.px[s], p.py[s], p.pz[s], p.best[s], p.bid[s], p.bpos[s]);
     } else if (PREC == SSDF_PREC_F32) {
         // the reference's float arithmetic end to end (edf<float>'s value); edf and sqedf outputs
-        float init = 0.f;
-        if (valid) {
-            const float o = a.out_f64 ? float(((const double *)a.out)[q]) : ((const float *)a.out)[q];
-            init = a.output == SSDF_OUT_SQEDF ? o : o * o;
-        }
-        ExactPolicy<float> p(a.m, float(qx), float(qy), float(qz), init);
-        if (!valid) p.thr = -1.f;
-        if (WARP || valid) walk<WARP, WIDE, COUNT>(p, cnt);
-        if (valid) {
-            if (a.output == SSDF_OUT_SQEDF) {
-                store_out(a, q, double(p.best));
+        ExactPolicy<float, Q> p(a.m);
+#pragma unroll
+        for (int s = 0; s < Q; s++) {
+            if (valid[s]) {
+                double x, y, z;
+                query_point(a, qid[s], gi[s], gj[s], gk[s], x, y, z);
+                const long long q = qid[s];
+                const float o = a.out_f64 ? float(((const double *)a.out)[q]) : ((const float *)a.out)[q];
+                p.set(s, float(x), float(y), float(z), a.output == SSDF_OUT_SQEDF ? o : o * o);
             } else {
-                store_out(a, q, double(sqrtf(p.best)));
-                if (a.outtri && p.bid >= 0) a.outtri[q] = p.bid;
+                p.disable(s);
+            }
+        }
+        if (WARP || any) walk<WARP, WIDE, COUNT>(p, cnt);
+#pragma unroll
+        for (int s = 0; s < Q; s++) {
+            if (!valid[s]) continue;
+            const long long q = qid[s];
+            if (a.output == SSDF_OUT_SQEDF) {
+                store_out(a, q, double(p.best[s]));
+            } else {
+                store_out(a, q, double(sqrtf(p.best[s])));
+                if (a.outtri && p.bid[s] >= 0) a.outtri[q] = p.bid[s];
             }
         }
     } else {
-        // the double point and bound are recomputed after the walk rather than kept live through it
-        float finit = -1.f;
-        if (valid) {
-            const double init = initial_bound(a, q);
-            // float start bound rounded up, so no triangle closer in double is cut off
-            finit = init < dinf() ? __double2float_ru(init) : finf();
+        __shared__ float s_wd[kQ * kCand * kThreads];
+        __shared__ int s_wp[kQ * kCand * kThreads];
+        FastPolicy<Q> p(a.m, a.tau_rel, s_wd, s_wp);
+#pragma unroll
+        for (int s = 0; s < Q; s++) {
+            if (valid[s]) {
+                double x, y, z;
+                query_point(a, qid[s], gi[s], gj[s], gk[s], x, y, z);
+                const double init = initial_bound(a, qid[s]);
+                // float start bound rounded up, so no triangle closer in double is cut off
+                p.set(s, float(x), float(y), float(z), init < dinf() ? __double2float_ru(init) : finf());
+            } else {
+                p.disable(s);
+            }
         }
-        FastPolicy p(a.m, float(qx), float(qy), float(qz), finit, a.tau_rel);
-        if (!valid) p.thr = -1.f;
-        if (WARP || valid) walk<WARP, WIDE, COUNT>(p, cnt);
-        if (valid) {
-            if (p.win.evicted < p.thr) {
+        if (WARP || any) walk<WARP, WIDE, COUNT>(p, cnt);
+#pragma unroll
+        for (int s = 0; s < Q; s++) {
+            if (!valid[s]) continue;
+            const long long q = qid[s];
+            if (p.evicted[s] < p.thr[s]) {
                 const int slot = atomicAdd(a.fallback_count, 1);
                 a.fallback_ids[slot] = int(q);  // q < 2^31 is checked on the host
-                a.fallback_thr[slot] = p.thr;
-            } else {
-                double rx, ry, rz;
-                query_point(a, q, i, j, k, rx, ry, rz);
-                double b = initial_bound(a, q);
-                int bid = -1, bpos = -1;
+                a.fallback_thr[slot] = p.thr[s];
+                continue;
+            }
+            // the double point and bound are recomputed here rather than kept live through the walk
+            double rx, ry, rz;
+            query_point(a, q, gi[s], gj[s], gk[s], rx, ry, rz);
+            double b = initial_bound(a, q);
+            int bid = -1, bpos = -1;
 #pragma unroll
-                for (int s = 0; s < kCand; s++) {
-                    if (p.win.d[s] < p.thr) {
-                        const Tri64 t = load_tri64(a.m.tris64, p.win.p[s]);
-                        const double d2 = tri_dist_sq_exact<double>(rx, ry, rz, t.ax, t.ay, t.az, t.bx, t.by, t.bz,
-                                                                    t.cx, t.cy, t.cz);
-                        if (COUNT) cnt.fix++;
-                        if (d2 < b || (d2 == b && bid >= 0 && t.id < bid)) {
-                            b = d2;
-                            bid = t.id;
-                            bpos = p.win.p[s];
-                        }
+            for (int c = 0; c < kCand; c++) {
+                const int ix = p.slot(s, c);
+                if (p.wd[ix] < p.thr[s]) {
+                    const int pos = p.wp[ix];
+                    const Tri64 t = load_tri64(a.m.tris64, pos);
+                    const double d2 =
+                        tri_dist_sq_exact<double>(rx, ry, rz, t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
+                    if (COUNT) cnt.fix++;
+                    if (d2 < b || (d2 == b && bid >= 0 && t.id < bid)) {
+                        b = d2;
+                        bid = t.id;
+                        bpos = pos;
                     }
                 }
-                write_result(a, q, rx, ry, rz, b, bid, bpos);
             }
+            write_result(a, q, rx, ry, rz, b, bid, bpos);
         }
     }
 }
@@ -763,8 +897,6 @@ __global__ void __launch_bounds__(kThreads, PREC == SSDF_PREC_F64 ? 1 : SSDF_B20
     if (COUNT) flush_counters(a, cnt);
 }
 
-// Queries whose F32X window overflowed its slots, finished by the WindowPolicy walk (grid-stride
-// over the list, one thread per query: these are few and scattered).
 template <bool WIDE, bool COUNT>
 __device__ __forceinline__ void window_one(const QueryArgs &a, int idx, Counters &cnt) {
     const long long q = a.fallback_ids[idx];
@@ -896,9 +1028,13 @@ int query_counts(int64_t *tri, int64_t *box, int64_t *fix, int64_t *fallback) {
 // Traversal mode: SSDF_B200_TRAVERSAL=warp|thread overrides; by default grids (coherent bricks) walk
 // in warp packets and point lists thread by thread.
 // BVH arity: SSDF_B200_ARITY=2|4; binary by default (measured as fast as 4-wide on the torus knot).
-static bool use_wide() { return env_int("SSDF_B200_ARITY", 2) == 4; }
+static bool use_wide(const QueryArgs &a) {
+    if (a.force_arity) return a.force_arity == 4;
+    return env_int("SSDF_B200_ARITY", 2) == 4;
+}
 
 static bool use_warp(const QueryArgs &a) {
+    if (a.force_traversal) return a.force_traversal == 1;
     const char *v = env_str("SSDF_B200_TRAVERSAL");
     if (v && !strcmp(v, "warp")) return true;
     if (v && !strcmp(v, "thread")) return false;
@@ -923,12 +1059,8 @@ int launch_query(const QueryArgs &args_in, int precision, cudaStream_t stream) {
         return fail(SSDF_ERR_INVALID_ARGUMENT, "SSDF_PREC_F32 serves the edf and sqedf outputs");
     const bool count = env_int("SSDF_B200_COUNT", 0) != 0;
     const bool warp = use_warp(a);
-    const bool wide = use_wide();
-    long long nblocks;
-    if (a.is_grid)
-        nblocks = ((a.nx + 7) / 8) * ((a.ny + 3) / 4) * ((a.nz + 3) / 4);
-    else
-        nblocks = (n + kThreads - 1) / kThreads;
+    const bool wide = use_wide(a);
+    const long long nblocks = query_blocks(a);
     if (nblocks > 0x7fffffffll) return fail(SSDF_ERR_NOT_SUPPORTED, "too many queries in one launch");
     unsigned long long *counters = nullptr;
     int *fb = nullptr;
@@ -1072,7 +1204,7 @@ int launch_query_noalloc(const QueryArgs &args_in, cudaStream_t stream) {
     a.fallback_count = scratch;
     a.fallback_ids = scratch + 1;
     a.fallback_thr = reinterpret_cast<float *>(scratch + 1 + n);
-    const bool warp = use_warp(a), wide = use_wide();
+    const bool warp = use_warp(a), wide = use_wide(a);
     const long long nblocks = query_blocks(a);
     cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(int), stream);  // the count starts at zero
     if (e == cudaSuccess) e = launch_prec<SSDF_PREC_F32_FIXUP>(a, warp, wide, false, unsigned(nblocks), stream);

@@ -127,7 +127,7 @@ ssdf_build_opts build_opts_for(int precision, int output) {
     o.leaf_size = env_int("SSDF_B200_LEAF", 0);
     o.keep_fp64 = (precision != SSDF_PREC_F32 || output == SSDF_OUT_SDF || output == SSDF_OUT_CLOSEST) ? 1 : 0;
     o.normals = output == SSDF_OUT_SDF ? 1 : 0;
-    o.treelet_opt = env_int("SSDF_B200_TREELET", 0);
+    o.treelet_opt = env_int("SSDF_B200_TREELET", 1);
     return o;
 }
 
@@ -409,7 +409,7 @@ int ssdf_mesh_create(ssdf_mesh **mesh, ptrdiff_t nselements, const int *s0, cons
     if (opts) {
         o = *opts;
     } else {
-        o.leaf_size = 0, o.keep_fp64 = 1, o.normals = 1, o.treelet_opt = 0;
+        o.leaf_size = 0, o.keep_fp64 = 1, o.normals = 1, o.treelet_opt = 1;
     }
     if (!device_ptrs) SSDF_CHECK(check_mesh_host(nselements, s0, s1, s2, nspoints, sx, sy, sz));
     cudaStream_t s = (cudaStream_t)stream;

@@ -108,6 +108,9 @@ struct QueryArgs {
     int *fallback_count;
     // optional counters [4]: triangle tests, box tests, fix-up evaluations, fallbacks
     unsigned long long *counters;
+    // 0: environment / default; traversal 1 warp packets, 2 thread per query; arity 2 or 4
+    int force_traversal;
+    int force_arity;
 };
 
 // Job table header of a batch (device memory).
@@ -152,10 +155,16 @@ int launch_batch(const BatchLaunch &b, int precision, cudaStream_t stream);
 int batch_blocks_per_sm(int precision, bool warp, bool wide);
 bool default_warp(int is_grid);
 bool default_wide();
-// Blocks of 128 queries one job needs (grid bricks of 8x4x4 or 128 consecutive points).
+// Queries each lane of the query kernels answers (two independent arithmetic chains per node visit).
+#ifndef SSDF_B200_QUERIES_PER_LANE
+#define SSDF_B200_QUERIES_PER_LANE 1
+#endif
+constexpr int kQ = SSDF_B200_QUERIES_PER_LANE;
+// Blocks of 128 lanes x kQ queries one job needs (grid bricks of 8 x 4 x 4kQ nodes, or 128 kQ
+// consecutive points).
 inline long long query_blocks(const QueryArgs &a) {
-    if (a.is_grid) return ((a.nx + 7) / 8) * ((a.ny + 3) / 4) * ((a.nz + 3) / 4);
-    return (a.npoints + 127) / 128;
+    if (a.is_grid) return ((a.nx + 7) / 8) * ((a.ny + 3) / 4) * ((a.nz + 4 * kQ - 1) / (4 * kQ));
+    return (a.npoints + 128 * kQ - 1) / (128 * kQ);
 }
 
 // ---- brute force and cell list (brute_force.cu, celllist.cu) -------------------------------------

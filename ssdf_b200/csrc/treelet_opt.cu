@@ -1,11 +1,319 @@
-// treelet_opt.cu -- SAH treelet refinement of the LBVH (placeholder until implemented).
+// treelet_opt.cu -- SAH treelet refinement of the LBVH (after Karras and Aila, "Fast parallel
+// construction of high-quality bounding volume hierarchies", HPG 2013).
+//
+// One bottom-up pass with per-node arrival counters (the second thread to reach a node owns it, so
+// its subtree is final): every node with at least kTreeletLeaves triangles below it roots a treelet,
+// grown from its two children by opening the largest-area internal member until it has seven
+// members. The binary tree over those members with the lowest surface-area cost,
+//     cost(node) = area(node) + cost(left) + cost(right),   cost(triangle) = area(triangle),
+// is found exactly by dynamic programming over the 127 member subsets (each subset's best split
+// among its 2^k - 2 partitions), and replaces the old arrangement when it is cheaper, reusing the
+// treelet's six internal nodes (the root keeps its identity, so the walk continues upward). Boxes
+// and parent links inside the treelet are rewritten. The pass then re-derives the leaf order (a
+// depth-first numbering of the triangles), so every subtree is again a contiguous range of leaf
+// positions, as the leaf collapse and the node records require.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+
 #include "internal.h"
 
 namespace ssdf_b200 {
 
-int treelet_optimize(int, int *, int *, int *, int *, int *, float *, double *, const float *, const double *, int *,
-                     cudaStream_t) {
-    return fail(SSDF_ERR_NOT_SUPPORTED, "treelet refinement is not available in this build");
+namespace {
+
+constexpr int kTreeletLeaves = 7;
+constexpr int kSubsets = 1 << kTreeletLeaves;
+
+struct TreeArrays {
+    int *child_l, *child_r, *parent_int, *parent_leaf;
+    float *nbox32;
+    double *nbox64;
+    const float *pbox32;
+    const double *pbox64;
+    const int *ids;  // leaf position -> triangle
+    float *cost;     // per internal node: SAH cost of its subtree
+    int *count;      // per internal node: triangles below
+};
+
+__device__ __forceinline__ float area6(const float *b) {
+    const float dx = fmaxf(b[1] - b[0], 0.f), dy = fmaxf(b[3] - b[2], 0.f), dz = fmaxf(b[5] - b[4], 0.f);
+    return 2.f * (dx * dy + dy * dz + dz * dx);
+}
+
+// Box / cost / count of a child reference (internal >= 0, leaf -(pos + 1)); reads bypass L1 since
+// other threads wrote them.
+__device__ __forceinline__ void ref_box32(const TreeArrays &t, int ref, float *b) {
+    const float *s = ref >= 0 ? t.nbox32 + 6 * ref : t.pbox32 + 6 * t.ids[-ref - 1];
+    for (int k = 0; k < 6; k++) b[k] = __ldcg(s + k);
+}
+__device__ __forceinline__ void ref_box64(const TreeArrays &t, int ref, double *b) {
+    const double *s = ref >= 0 ? t.nbox64 + 6 * ref : t.pbox64 + 6 * t.ids[-ref - 1];
+    for (int k = 0; k < 6; k++) b[k] = __ldcg(s + k);
+}
+__device__ __forceinline__ float ref_cost(const TreeArrays &t, int ref) {
+    if (ref >= 0) return __ldcg(t.cost + ref);
+    float b[6];
+    ref_box32(t, ref, b);
+    return area6(b);
+}
+__device__ __forceinline__ int ref_count(const TreeArrays &t, int ref) { return ref >= 0 ? __ldcg(t.count + ref) : 1; }
+
+__device__ __forceinline__ void set_parent(const TreeArrays &t, int ref, int parent) {
+    if (ref >= 0)
+        __stcg(t.parent_int + ref, parent);
+    else
+        __stcg(t.parent_leaf + (-ref - 1), parent);
+}
+
+// Optimises the treelet rooted at internal node x (its subtree is final).
+__device__ void optimize_treelet(const TreeArrays &t, int x) {
+    int member[kTreeletLeaves];
+    int inner[kTreeletLeaves - 1];
+    int m = 2, ni = 1;
+    member[0] = __ldcg(t.child_l + x);
+    member[1] = __ldcg(t.child_r + x);
+    inner[0] = x;
+    float mb[kTreeletLeaves][6];
+    ref_box32(t, member[0], mb[0]);
+    ref_box32(t, member[1], mb[1]);
+    while (m < kTreeletLeaves) {
+        int pick = -1;
+        float best = -1.f;
+        for (int k = 0; k < m; k++) {
+            if (member[k] >= 0) {
+                const float a = area6(mb[k]);
+                if (a > best) best = a, pick = k;
+            }
+        }
+        if (pick < 0) break;
+        const int y = member[pick];
+        inner[ni++] = y;
+        member[pick] = __ldcg(t.child_l + y);
+        member[m] = __ldcg(t.child_r + y);
+        ref_box32(t, member[pick], mb[pick]);
+        ref_box32(t, member[m], mb[m]);
+        m++;
+    }
+    float mcost[kTreeletLeaves];
+    if (m < 3) {
+        float b[6];
+        for (int q = 0; q < 6; q++) b[q] = __ldcg(t.nbox32 + 6 * x + q);
+        __stcg(t.cost + x, area6(b) + ref_cost(t, member[0]) + ref_cost(t, member[1]));
+        return;
+    }
+    for (int k = 0; k < m; k++) mcost[k] = ref_cost(t, member[k]);
+    // current cost of the treelet: the old internal nodes' areas + members' costs
+    float old_cost = 0.f;
+    for (int k = 0; k < ni; k++) {
+        float b[6];
+        for (int q = 0; q < 6; q++) b[q] = __ldcg(t.nbox32 + 6 * inner[k] + q);
+        old_cost += area6(b);
+    }
+    for (int k = 0; k < m; k++) old_cost += mcost[k];
+    // dynamic programme over subsets
+    const int full = (1 << m) - 1;
+    float c[kSubsets];
+    unsigned char split[kSubsets];
+    for (int s = 1; s <= full; s++) {
+        float b[6] = {FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX};
+        int nbits = 0, only = 0;
+        for (int k = 0; k < m; k++) {
+            if (!((s >> k) & 1)) continue;
+            nbits++, only = k;
+            for (int q = 0; q < 6; q += 2) b[q] = fminf(b[q], mb[k][q]), b[q + 1] = fmaxf(b[q + 1], mb[k][q + 1]);
+        }
+        if (nbits == 1) {
+            c[s] = mcost[only];
+            split[s] = 0;
+            continue;
+        }
+        float best = FLT_MAX;
+        int bp = 0;
+        // partitions (p, s \ p) with p holding the lowest member of s: each split once
+        const int low = s & -s;
+        for (int p = (s - 1) & s; p > 0; p = (p - 1) & s) {
+            if (!(p & low)) continue;
+            const float v = c[p] + c[s ^ p];
+            if (v < best) best = v, bp = p;
+        }
+        c[s] = area6(b) + best;
+        split[s] = (unsigned char)bp;
+    }
+    if (!(c[full] < old_cost * (1.f - 1e-6f))) {
+        __stcg(t.cost + x, old_cost);
+        return;
+    }
+    // rebuild: internal nodes of the new tree take the treelet's internal ids, the root keeps x
+    int stack_set[kTreeletLeaves], stack_node[kTreeletLeaves];
+    int sp = 0, used = 1;
+    stack_set[sp] = full, stack_node[sp] = x, sp++;
+    // build top-down, then fix boxes and costs bottom-up in reverse creation order
+    int order_node[kTreeletLeaves - 1], order_set[kTreeletLeaves - 1], norder = 0;
+    while (sp > 0) {
+        sp--;
+        const int s = stack_set[sp], node = stack_node[sp];
+        order_node[norder] = node, order_set[norder] = s, norder++;
+        const int halves[2] = {split[s], s ^ split[s]};
+        int refs[2];
+        for (int h = 0; h < 2; h++) {
+            const int hs = halves[h];
+            if ((hs & (hs - 1)) == 0) {
+                refs[h] = member[__ffs(hs) - 1];
+            } else {
+                refs[h] = inner[used++];
+                stack_set[sp] = hs, stack_node[sp] = refs[h], sp++;
+            }
+        }
+        __stcg(t.child_l + node, refs[0]);
+        __stcg(t.child_r + node, refs[1]);
+        set_parent(t, refs[0], node);
+        set_parent(t, refs[1], node);
+    }
+    for (int k = norder - 1; k >= 0; k--) {
+        const int node = order_node[k];
+        const int l = __ldcg(t.child_l + node), r = __ldcg(t.child_r + node);
+        float bl[6], br[6];
+        double dl[6], dr[6];
+        ref_box32(t, l, bl);
+        ref_box32(t, r, br);
+        ref_box64(t, l, dl);
+        ref_box64(t, r, dr);
+        for (int q = 0; q < 6; q += 2) {
+            __stcg(t.nbox32 + 6 * node + q, fminf(bl[q], br[q]));
+            __stcg(t.nbox32 + 6 * node + q + 1, fmaxf(bl[q + 1], br[q + 1]));
+            __stcg(t.nbox64 + 6 * node + q, fmin(dl[q], dr[q]));
+            __stcg(t.nbox64 + 6 * node + q + 1, fmax(dl[q + 1], dr[q + 1]));
+        }
+        __stcg(t.count + node, ref_count(t, l) + ref_count(t, r));
+        __stcg(t.cost + node, c[order_set[k]] - 0.f);
+        __threadfence();
+    }
+}
+
+__global__ void k_treelets(int n, TreeArrays t, int *arrivals) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    int node = __ldcg(t.parent_leaf + p);
+    while (node >= 0) {
+        __threadfence();
+        if (atomicAdd(&arrivals[node], 1) == 0) return;
+        __threadfence();
+        const int l = __ldcg(t.child_l + node), r = __ldcg(t.child_r + node);
+        const int cnt = ref_count(t, l) + ref_count(t, r);
+        __stcg(t.count + node, cnt);
+        if (cnt >= kTreeletLeaves) {
+            optimize_treelet(t, node);
+        } else {
+            float b[6];
+            for (int q = 0; q < 6; q++) b[q] = __ldcg(t.nbox32 + 6 * node + q);
+            __stcg(t.cost + node, area6(b) + ref_cost(t, l) + ref_cost(t, r));
+        }
+        __threadfence();
+        node = __ldcg(t.parent_int + node);
+    }
+}
+
+// New leaf position of every triangle: its rank in a depth-first, left-first walk of the new tree,
+// found by walking up and adding the sizes of left siblings.
+__global__ void k_leaf_positions(int n, const int *__restrict__ child_l, const int *__restrict__ parent_int,
+                                 const int *__restrict__ parent_leaf, const int *__restrict__ count,
+                                 int *__restrict__ newpos) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    int ref = -(p + 1);
+    int node = parent_leaf[p];
+    int off = 0;
+    int guard = 0;
+    while (node >= 0 && guard++ < (1 << 20)) {
+        const int l = child_l[node];
+        if (l != ref) off += l >= 0 ? count[l] : 1;
+        ref = node;
+        node = parent_int[node];
+    }
+    newpos[p] = off;
+}
+
+__global__ void k_relabel(int n, const int *__restrict__ newpos, const int *__restrict__ ids_old,
+                          const int *__restrict__ parent_leaf_old, const int *__restrict__ child_l_old,
+                          const int *__restrict__ child_r_old, int *__restrict__ ids_new,
+                          int *__restrict__ parent_leaf_new, int *__restrict__ child_l_new,
+                          int *__restrict__ child_r_new) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const int q = newpos[p];
+    ids_new[q] = ids_old[p];
+    const int parent = parent_leaf_old[p];
+    parent_leaf_new[q] = parent;
+    if (child_l_old[parent] == -(p + 1)) child_l_new[parent] = -(q + 1);
+    if (child_r_old[parent] == -(p + 1)) child_r_new[parent] = -(q + 1);
+}
+
+// first_of: leaf position of the leftmost triangle below each internal node.
+__global__ void k_first_of(int nint, const int *__restrict__ child_l, int *__restrict__ first_of) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nint) return;
+    int ref = i;
+    int guard = 0;
+    while (ref >= 0 && guard++ < (1 << 20)) ref = child_l[ref];
+    first_of[i] = -ref - 1;
+}
+
+}  // namespace
+
+int treelet_optimize(int n, int *child_l, int *child_r, int *parent_int, int *parent_leaf, int *first_of,
+                     float *nbox32, double *nbox64, const float *pbox32, const double *pbox64, int *sorted_ids,
+                     cudaStream_t stream) {
+    const int nint = n - 1;
+    if (nint < kTreeletLeaves) return SSDF_OK;
+    float *cost = nullptr;
+    int *count = nullptr, *arrivals = nullptr, *newpos = nullptr, *ids2 = nullptr, *pl2 = nullptr, *cl2 = nullptr,
+        *cr2 = nullptr;
+    int st = SSDF_OK;
+    auto alloc = [&](void **p, size_t b) {
+        if (st == SSDF_OK && cudaMallocAsync(p, b, stream) != cudaSuccess) st = fail(SSDF_ERR_OUT_OF_MEMORY, "treelet scratch");
+    };
+    alloc((void **)&cost, sizeof(float) * nint);
+    alloc((void **)&count, sizeof(int) * nint);
+    alloc((void **)&arrivals, sizeof(int) * nint);
+    alloc((void **)&newpos, sizeof(int) * n);
+    alloc((void **)&ids2, sizeof(int) * n);
+    alloc((void **)&pl2, sizeof(int) * n);
+    alloc((void **)&cl2, sizeof(int) * nint);
+    alloc((void **)&cr2, sizeof(int) * nint);
+    cudaError_t e = cudaSuccess;
+    if (st == SSDF_OK) {
+        TreeArrays t{child_l, child_r, parent_int, parent_leaf, nbox32, nbox64, pbox32, pbox64, sorted_ids, cost, count};
+        e = cudaMemsetAsync(arrivals, 0, sizeof(int) * nint, stream);
+        if (e == cudaSuccess) {
+            k_treelets<<<grid_blocks(n, 128), 128, 0, stream>>>(n, t, arrivals);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) {
+            k_leaf_positions<<<grid_blocks(n, 256), 256, 0, stream>>>(n, child_l, parent_int, parent_leaf, count,
+                                                                       newpos);
+            e = cudaMemcpyAsync(cl2, child_l, sizeof(int) * nint, cudaMemcpyDeviceToDevice, stream);
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(cr2, child_r, sizeof(int) * nint, cudaMemcpyDeviceToDevice, stream);
+        if (e == cudaSuccess) {
+            k_relabel<<<grid_blocks(n, 256), 256, 0, stream>>>(n, newpos, sorted_ids, parent_leaf, child_l, child_r, ids2,
+                                                                pl2, cl2, cr2);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(sorted_ids, ids2, sizeof(int) * n, cudaMemcpyDeviceToDevice, stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(parent_leaf, pl2, sizeof(int) * n, cudaMemcpyDeviceToDevice, stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(child_l, cl2, sizeof(int) * nint, cudaMemcpyDeviceToDevice, stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(child_r, cr2, sizeof(int) * nint, cudaMemcpyDeviceToDevice, stream);
+        if (e == cudaSuccess) {
+            k_first_of<<<grid_blocks(nint, 256), 256, 0, stream>>>(nint, child_l, first_of);
+            e = cudaGetLastError();
+        }
+        if (e != cudaSuccess) st = cuda_fail(e, "treelet refinement", __FILE__, __LINE__);
+    }
+    for (void *p : {(void *)cost, (void *)count, (void *)arrivals, (void *)newpos, (void *)ids2, (void *)pl2,
+                    (void *)cl2, (void *)cr2})
+        if (p) cudaFreeAsync(p, stream);
+    return st;
 }
 
 }  // namespace ssdf_b200

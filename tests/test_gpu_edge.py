@@ -111,6 +111,21 @@ def test_leaf_sizes(leaf):
     assert np.array_equal(got, want) and np.array_equal(gtri, wtri)
 
 
+@pytest.mark.parametrize("leaf", [1, 4, 8])
+def test_treelet_refinement(leaf):
+    """SAH treelet refinement rearranges the tree; the values cannot change."""
+    mesh = W.torus_knot_tube(nu=256, nv=16)
+    g = W.Grid.padded_nodes(mesh, 24, 0.25)
+    want, wtri = oracle.sdf_points(oracle.grid_points(g), mesh)
+    for arity in (2, 4):
+        with env(SSDF_B200_LEAF=leaf, SSDF_B200_TREELET=1, SSDF_B200_ARITY=arity):
+            got, gtri = S.sample_sdf_bvh(mesh, g, with_index=True)
+        assert np.array_equal(got, want) and np.array_equal(gtri, wtri)
+    plain = S.DeviceMesh(mesh, leaf_size=leaf).stats()
+    tuned = S.DeviceMesh(mesh, leaf_size=leaf, treelet=True).stats()
+    assert tuned["leaves"] > 0 and tuned["depth"] < 64 and plain["leaves"] > 0
+
+
 def test_invalid_indices_are_rejected():
     mesh = W.icosphere(1)
     bad = W.Mesh(mesh.vertices, np.where(mesh.triangles == 5, mesh.nv + 3, mesh.triangles).astype(np.int32))
