@@ -62,6 +62,21 @@ def parse_args():
     return p.parse_args()
 
 
+def max_over_ranks(value, dist, device):
+    """The slowest rank's time: every rank takes the same collective step (MAX all-reduce)."""
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(queries_per_rank, steps, max_ms, world):
+    """Whole-job queries/s of `world` replicas, each doing `steps` steps, timed by the slowest."""
+    return world * queries_per_rank * steps / (max_ms * 1e-3)
+
+
 def workload(n=256):
     from ssdf_b200 import workloads as W
 
@@ -203,15 +218,12 @@ def main():
         torch.cuda.synchronize()
         barrier()
         ms = [e0.elapsed_time(e1) for e0, e1 in ev]
-        total = torch.tensor([sum(ms)], dtype=torch.float64, device="cuda")
-        if dist is not None:
-            dist.all_reduce(total, op=dist.ReduceOp.MAX)
-        return float(total.item()), ms
+        return max_over_ranks(sum(ms), dist, "cuda"), ms
 
     clocks = Clocks(local)
     t_x, ms_x = timed(S.PREC_F32_FIXUP, args.steps, args.warmup)
     clk = clocks.stop()
-    value = world * nq * args.steps / (t_x * 1e-3)
+    value = job_rate(nq, args.steps, t_x, world)
     t_64, ms_64 = timed(S.PREC_F64, max(2, args.steps // 2), 1)
     fp64_value = world * nq * max(2, args.steps // 2) / (t_64 * 1e-3)
 

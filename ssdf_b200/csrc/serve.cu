@@ -105,6 +105,25 @@ struct ssdf_server {
 
 namespace {
 
+// Host staging copies of large requests (tens of MB per batch at high load) split across threads:
+// one thread's memcpy bandwidth would otherwise cap the served query rate.
+void par_memcpy(void *dst, const void *src, size_t bytes) {
+    constexpr size_t kChunk = size_t(4) << 20;
+    if (bytes < 2 * kChunk) {
+        memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t parts = std::min<size_t>(8, bytes / kChunk);
+    const size_t step = (bytes + parts - 1) / parts;
+    std::vector<std::thread> th;
+    for (size_t k = 1; k < parts; k++) {
+        const size_t off = k * step, len = std::min(step, bytes - off);
+        th.emplace_back([=] { memcpy(static_cast<char *>(dst) + off, static_cast<const char *>(src) + off, len); });
+    }
+    memcpy(dst, src, std::min(step, bytes));
+    for (auto &t : th) t.join();
+}
+
 int build_resident(ssdf_server *s, int id, Resident *r) {
     const HostMeshCopy &h = s->meshes[id];
     ssdf_build_opts bo;
@@ -162,8 +181,8 @@ void finish(ssdf_server *s, Slot &sl, int status) {
         Request &r = *sl.reqs[k];
         const long long n = r.grid ? r.nx * r.ny * r.nz : r.n;
         if (status == SSDF_OK) {
-            memcpy(r.out, sl.h_out + sl.offsets[k], sizeof(double) * size_t(n));
-            if (r.outtri) memcpy(r.outtri, sl.h_tri + sl.offsets[k], sizeof(int) * size_t(n));
+            par_memcpy(r.out, sl.h_out + sl.offsets[k], sizeof(double) * size_t(n));
+            if (r.outtri) par_memcpy(r.outtri, sl.h_tri + sl.offsets[k], sizeof(int) * size_t(n));
         }
         r.status = status;
     }
@@ -243,9 +262,9 @@ void scheduler_loop(ssdf_server *s) {
                 st = ssdf_batch_add_grid(sl.batch, ms[k], r.nx, r.ny, r.nz, r.lo, r.hi, out, tri, &qo);
             } else {
                 double *hx = sl.h_pts + 3 * poff;
-                memcpy(hx, r.x, sizeof(double) * size_t(r.n));
-                memcpy(hx + r.n, r.y, sizeof(double) * size_t(r.n));
-                memcpy(hx + 2 * r.n, r.z, sizeof(double) * size_t(r.n));
+                par_memcpy(hx, r.x, sizeof(double) * size_t(r.n));
+                par_memcpy(hx + r.n, r.y, sizeof(double) * size_t(r.n));
+                par_memcpy(hx + 2 * r.n, r.z, sizeof(double) * size_t(r.n));
                 double *dx = sl.d_pts + 3 * poff;
                 st = ssdf_batch_add_points(sl.batch, ms[k], r.n, dx, dx + r.n, dx + 2 * r.n, out, tri, &qo);
                 poff += r.n;
