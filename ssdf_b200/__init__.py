@@ -11,9 +11,15 @@ from __future__ import annotations
 
 import importlib
 
+# submodules that import without the CUDA library (``from ssdf_b200 import build`` must work on a
+# fresh checkout, before the library exists)
+_LIBRARY_FREE = ("build", "workloads")
+
 
 def __getattr__(name):
     if name.startswith("__"):
         raise AttributeError(name)
+    if name in _LIBRARY_FREE:
+        return importlib.import_module("." + name, __name__)
     capi = importlib.import_module(".capi", __name__)
     return getattr(capi, name)

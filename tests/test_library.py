@@ -56,3 +56,15 @@ def test_cpp_header_compiles_against_c_abi(tmp_path):
     res = subprocess.run(["g++", "-std=c++17", f"-I{ROOT}/include", str(src), "-o", str(tmp_path / "use"),
                           f"-L{lib}", "-lssdf_b200", f"-Wl,-rpath,{lib}"], capture_output=True, text=True)
     assert res.returncode == 0, res.stderr
+
+
+def test_build_imports_without_the_library():
+    """``from ssdf_b200 import build`` (the first step of a fresh build) must not load the CUDA
+    binding, which needs the library it is about to build."""
+    import subprocess
+    import sys
+
+    code = ("import sys; from ssdf_b200 import build, workloads; "
+            "assert 'ssdf_b200.capi' not in sys.modules, 'binding loaded'")
+    res = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr
