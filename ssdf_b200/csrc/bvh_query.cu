@@ -23,6 +23,7 @@
 // (closest_point_bvh, serial/bvh/bvh.cpp:178-194).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cfloat>
 #include <cstring>
 #include <mutex>
@@ -972,10 +973,16 @@ cudaError_t launch_batch_main(const BatchLaunch &b, bool count, cudaStream_t str
         k_query_batch<PREC, WARP, WIDE, false><<<b.grid, kThreads, 0, stream>>>(b.hdr, b.jobs, b.first_block, b.next_item);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || PREC != SSDF_PREC_F32_FIXUP) return e;
+    static int per_sm = 0;  // resident blocks of the second stage, as for a single launch
+    if (per_sm == 0) {
+        int v = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_window_batch<WIDE, false>, kThreads, 0);
+        per_sm = v > 0 ? v : 1;
+    }
     if (count)
-        k_window_batch<WIDE, true><<<2 * b.sms, kThreads, 0, stream>>>(b.hdr, b.jobs);
+        k_window_batch<WIDE, true><<<per_sm * b.sms, kThreads, 0, stream>>>(b.hdr, b.jobs);
     else
-        k_window_batch<WIDE, false><<<2 * b.sms, kThreads, 0, stream>>>(b.hdr, b.jobs);
+        k_window_batch<WIDE, false><<<per_sm * b.sms, kThreads, 0, stream>>>(b.hdr, b.jobs);
     return cudaGetLastError();
 }
 
@@ -1041,6 +1048,24 @@ static bool use_warp(const QueryArgs &a) {
     return a.is_grid != 0;
 }
 
+// Blocks of the second fix-up stage: every SM filled to the kernel's occupancy. Its queries are
+// scattered and walk divergently, so it needs all the warps it can get to hide latency; the count
+// of overflowed queries is only known on the device, and the kernel strides over it.
+template <bool WIDE>
+unsigned window_grid() {
+    static int cached[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int &g = cached[dev & 63];
+    if (g == 0) {
+        int sms = 0, per_sm = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_window<WIDE, false>, kThreads, 0);
+        g = std::max(1, sms) * std::max(1, per_sm);
+    }
+    return unsigned(g);
+}
+
 int launch_query(const QueryArgs &args_in, int precision, cudaStream_t stream) {
     QueryArgs a = args_in;
     const long long n = a.is_grid ? a.nx * a.ny * a.nz : a.npoints;
@@ -1083,12 +1108,13 @@ int launch_query(const QueryArgs &args_in, int precision, cudaStream_t stream) {
             e = cudaMemsetAsync(fb, 0, sizeof(int), stream);
             if (e == cudaSuccess) e = launch_prec<SSDF_PREC_F32_FIXUP>(a, warp, wide, count, unsigned(nblocks), stream);
             if (e == cudaSuccess) {
+                const unsigned wg = wide ? window_grid<true>() : window_grid<false>();
                 if (wide)
-                    count ? k_window<true, true><<<296, kThreads, 0, stream>>>(a)
-                          : k_window<true, false><<<296, kThreads, 0, stream>>>(a);
+                    count ? k_window<true, true><<<wg, kThreads, 0, stream>>>(a)
+                          : k_window<true, false><<<wg, kThreads, 0, stream>>>(a);
                 else
-                    count ? k_window<false, true><<<296, kThreads, 0, stream>>>(a)
-                          : k_window<false, false><<<296, kThreads, 0, stream>>>(a);
+                    count ? k_window<false, true><<<wg, kThreads, 0, stream>>>(a)
+                          : k_window<false, false><<<wg, kThreads, 0, stream>>>(a);
                 e = cudaGetLastError();
             }
         }
@@ -1210,9 +1236,9 @@ int launch_query_noalloc(const QueryArgs &args_in, cudaStream_t stream) {
     if (e == cudaSuccess) e = launch_prec<SSDF_PREC_F32_FIXUP>(a, warp, wide, false, unsigned(nblocks), stream);
     if (e == cudaSuccess) {
         if (wide)
-            k_window<true, false><<<296, kThreads, 0, stream>>>(a);
+            k_window<true, false><<<window_grid<true>(), kThreads, 0, stream>>>(a);
         else
-            k_window<false, false><<<296, kThreads, 0, stream>>>(a);
+            k_window<false, false><<<window_grid<false>(), kThreads, 0, stream>>>(a);
         e = cudaGetLastError();
     }
     if (e != cudaSuccess) return cuda_fail(e, "allocation-free query launch", __FILE__, __LINE__);

@@ -142,6 +142,25 @@ int build_resident(ssdf_server *s, int id, Resident *r) {
     return SSDF_OK;
 }
 
+// Evicts least recently used meshes, other than `keep` and those an in-flight batch holds, while
+// the resident bytes exceed the budget (caller holds s->mu). Runs on every admission and again
+// whenever a batch releases its meshes, so a budget overrun while everything was pinned does not
+// outlive the batches that caused it.
+void evict_over_budget(ssdf_server *s, int keep) {
+    auto li = s->lru.end();
+    while (s->resident_bytes > s->opts.memory_budget && li != s->lru.begin()) {
+        --li;
+        const int victim = *li;
+        Resident &v = s->resident[victim];
+        if (victim == keep || v.pins > 0) continue;
+        s->resident_bytes -= v.bytes;
+        ssdf_mesh_destroy(v.mesh);
+        li = s->lru.erase(li);
+        s->resident.erase(victim);
+        s->evictions++;
+    }
+}
+
 // Makes mesh `id` resident (caller holds s->mu); evicts unpinned LRU meshes over the budget.
 int admit(ssdf_server *s, int id) {
     auto it = s->resident.find(id);
@@ -158,19 +177,7 @@ int admit(ssdf_server *s, int id) {
     s->lru.push_front(id);
     r.lru = s->lru.begin();
     s->resident[id] = r;
-    // evict from the back while over budget
-    auto li = s->lru.end();
-    while (s->resident_bytes > s->opts.memory_budget && li != s->lru.begin()) {
-        --li;
-        const int victim = *li;
-        Resident &v = s->resident[victim];
-        if (victim == id || v.pins > 0) continue;
-        s->resident_bytes -= v.bytes;
-        ssdf_mesh_destroy(v.mesh);
-        li = s->lru.erase(li);
-        s->resident.erase(victim);
-        s->evictions++;
-    }
+    evict_over_budget(s, id);
     return SSDF_OK;
 }
 
@@ -196,6 +203,7 @@ void finish(ssdf_server *s, Slot &sl, int status) {
         auto it = s->resident.find(id);
         if (it != s->resident.end()) it->second.pins--;
     }
+    evict_over_budget(s, -1);
     s->last_done = now;
     sl.reqs.clear();
     sl.offsets.clear();
