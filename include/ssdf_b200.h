@@ -129,6 +129,35 @@ int ssdf_b200_sample_sdf_bvh_dd(ptrdiff_t nselements, const int *s0, const int *
                                 ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, double xmin, double ymin, double zmin,
                                 double xmax, double ymax, double zmax, double *out);
 
+/* ---- drop-in: grid and box helpers ------------------------------------------------------------
+ * ssdf::compute_aabb<G, T> (serial/edf/edf.hpp:500-539): the bounding box of npoints (>= 1) points,
+ * each converted to T, written to the six scalars. Bitwise the reference's for NaN-free input (a
+ * NaN coordinate is skipped). Zero points: SSDF_ERR_INVALID_ARGUMENT (the reference reads x[0]). */
+int ssdf_b200_compute_aabb_ff(ptrdiff_t npoints, const float *x, const float *y, const float *z, float *xmin,
+                              float *xmax, float *ymin, float *ymax, float *zmin, float *zmax);
+int ssdf_b200_compute_aabb_fd(ptrdiff_t npoints, const float *x, const float *y, const float *z, double *xmin,
+                              double *xmax, double *ymin, double *ymax, double *zmin, double *zmax);
+int ssdf_b200_compute_aabb_df(ptrdiff_t npoints, const double *x, const double *y, const double *z, float *xmin,
+                              float *xmax, float *ymin, float *ymax, float *zmin, float *zmax);
+int ssdf_b200_compute_aabb_dd(ptrdiff_t npoints, const double *x, const double *y, const double *z, double *xmin,
+                              double *xmax, double *ymin, double *ymax, double *zmin, double *zmax);
+/* ssdf::all_points_aabb_signed_distance<G, T> (serial/edf/edf.hpp:541-557, point_aabb_signed_distance
+ * at 193-221): out[i] = signed distance of point i (converted to T) to the box, negative inside,
+ * bitwise the reference's T arithmetic. The reference's driver starts `out` at its absolute value
+ * over the query points' own box (drivers/sdf.exe.cpp:316-326). */
+int ssdf_b200_all_points_aabb_signed_distance_ff(ptrdiff_t npoints, const float *x, const float *y, const float *z,
+                                                 float minx, float maxx, float miny, float maxy, float minz,
+                                                 float maxz, float *out);
+int ssdf_b200_all_points_aabb_signed_distance_fd(ptrdiff_t npoints, const float *x, const float *y, const float *z,
+                                                 double minx, double maxx, double miny, double maxy, double minz,
+                                                 double maxz, double *out);
+int ssdf_b200_all_points_aabb_signed_distance_df(ptrdiff_t npoints, const double *x, const double *y,
+                                                 const double *z, float minx, float maxx, float miny, float maxy,
+                                                 float minz, float maxz, float *out);
+int ssdf_b200_all_points_aabb_signed_distance_dd(ptrdiff_t npoints, const double *x, const double *y,
+                                                 const double *z, double minx, double maxx, double miny,
+                                                 double maxy, double minz, double maxz, double *out);
+
 /* ---- additive entry points (no reference counterpart; patterned on closest_point_bvh) -------- */
 
 /* Unsigned distance (in/out, as edf_bvh) plus the closest triangle, written where it improves. */
@@ -199,6 +228,16 @@ int ssdf_query_points(ssdf_mesh *mesh, ptrdiff_t npoints, const void *x, const v
 /* Query at the node grid nx*ny*nz over [lo, hi] (ssdf's convention, G = coord_type precision). */
 int ssdf_query_grid(ssdf_mesh *mesh, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, const double lo[3],
                     const double hi[3], void *out, int *outtri, const ssdf_query_opts *opts, void *stream);
+
+/* Device-array forms of the box helpers, asynchronous on `stream` (x, y, z of coord_type; results
+ * of out_type, SSDF_F32 / SSDF_F64 each). ssdf_points_aabb writes xmin, xmax, ymin, ymax, zmin, zmax
+ * to the DEVICE array box6 (scratch is stream-ordered). ssdf_points_aabb_signed_distance takes the
+ * box from the HOST array box6 in the same order (converted to out_type) and writes out[npoints]; with
+ * absolute = 1 it writes |distance|, the reference driver's initial `out`. */
+int ssdf_points_aabb(ptrdiff_t npoints, const void *x, const void *y, const void *z, int coord_type, int out_type,
+                     void *box6, void *stream);
+int ssdf_points_aabb_signed_distance(ptrdiff_t npoints, const void *x, const void *y, const void *z, int coord_type,
+                                     const double box6[6], int absolute, void *out, int out_type, void *stream);
 
 /* ---- batches: many resident meshes and query sets in one persistent launch (no reference
  *      counterpart; ssdf answers one mesh per call) --------------------------------------------- */

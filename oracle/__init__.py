@@ -69,6 +69,12 @@ def lib() -> C.CDLL:
             f = getattr(_lib, "oracle_edf" + suf)
             f.restype = C.c_int
             f.argtypes = [_pd, fptr, fptr, fptr, _pd, _ip, _ip, _ip, _pd, fptr, fptr, fptr, fptr, _ip]
+            f = getattr(_lib, "oracle_compute_aabb" + suf)
+            f.restype = None
+            f.argtypes = [_pd, fptr, fptr, fptr, fptr]
+            f = getattr(_lib, "oracle_all_points_aabb_signed_distance" + suf)
+            f.restype = None
+            f.argtypes = [_pd, fptr, fptr, fptr, fptr, fptr]
             f = getattr(_lib, "oracle_grid_points" + suf)
             f.restype = None
             f.argtypes = [_pd, _pd, _pd] + [ft] * 6 + [_dp, _dp, _dp]
@@ -108,6 +114,13 @@ def ref() -> C.CDLL:
         for n in ("ref_point_aabb_distance_squared_d", "ref_point_aabb_signed_distance_d"):
             getattr(_ref, n).restype = C.c_double
             getattr(_ref, n).argtypes = [C.c_double] * 9
+        for suf, fptr in (("_d", _dp), ("_f", _fp)):
+            f = getattr(_ref, "ref_compute_aabb" + suf)
+            f.restype = None
+            f.argtypes = [_pd, fptr, fptr, fptr, fptr]
+            f = getattr(_ref, "ref_all_points_aabb_signed_distance" + suf)
+            f.restype = None
+            f.argtypes = [_pd, fptr, fptr, fptr, fptr, fptr]
         _ref.ref_set_quiet.restype = None
         _ref.ref_set_quiet.argtypes = [C.c_int]
         _ref.ref_set_quiet(1)
@@ -227,3 +240,26 @@ def grid_points(grid, dtype=np.float64):
     getattr(lib(), "oracle_grid_points" + suf)(nx, ny, nz, *lo, *hi, _ptr(q[0], C.c_double),
                                                _ptr(q[1], C.c_double), _ptr(q[2], C.c_double))
     return q
+
+
+def compute_aabb(points, dtype=np.float64, reference=False):
+    """(xmin, xmax, ymin, ymax, zmin, zmax) of the points converted to dtype -- the oracle's
+    restatement of ssdf::compute_aabb, or (reference=True) the reference's own template."""
+    ct, suf = _real(dtype)
+    x, y, z = (np.ascontiguousarray(a, dtype=dtype) for a in points)
+    b = np.empty(6, dtype=dtype)
+    fn = ("ref_compute_aabb" if reference else "oracle_compute_aabb") + suf
+    getattr(ref() if reference else lib(), fn)(len(x), _ptr(x, ct), _ptr(y, ct), _ptr(z, ct), _ptr(b, ct))
+    return b
+
+
+def all_points_aabb_signed_distance(points, box, dtype=np.float64, reference=False):
+    """Signed distance of each point (converted to dtype) to box (minx, maxx, miny, maxy, minz, maxz)."""
+    ct, suf = _real(dtype)
+    x, y, z = (np.ascontiguousarray(a, dtype=dtype) for a in points)
+    b = np.ascontiguousarray(box, dtype=dtype)
+    out = np.empty(len(x), dtype=dtype)
+    fn = ("ref_all_points_aabb_signed_distance" if reference else "oracle_all_points_aabb_signed_distance") + suf
+    getattr(ref() if reference else lib(), fn)(len(x), _ptr(x, ct), _ptr(y, ct), _ptr(z, ct), _ptr(b, ct),
+                                               _ptr(out, ct))
+    return out

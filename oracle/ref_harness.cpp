@@ -62,4 +62,15 @@ double ref_point_aabb_signed_distance_d(double px, double py, double pz, double 
                                         double maxy, double minz, double maxz) {
     return ssdf::point_aabb_signed_distance<double>(px, py, pz, minx, maxx, miny, maxy, minz, maxz);
 }
+
+#define REF_BOX(T, SUF)                                                                                       \
+    void ref_compute_aabb##SUF(const ptrdiff_t n, const T *x, const T *y, const T *z, T *b) {                 \
+        ssdf::compute_aabb<T, T>(n, x, y, z, b, b + 1, b + 2, b + 3, b + 4, b + 5);                           \
+    }                                                                                                         \
+    void ref_all_points_aabb_signed_distance##SUF(const ptrdiff_t n, const T *x, const T *y, const T *z,      \
+                                                 const T *b, T *out) {                                        \
+        ssdf::all_points_aabb_signed_distance<T, T>(n, x, y, z, b[0], b[1], b[2], b[3], b[4], b[5], out);      \
+    }
+REF_BOX(double, _d)
+REF_BOX(float, _f)
 }

@@ -175,6 +175,31 @@ REAL OR_NAME(oracle_point_aabb_signed_distance)(const REAL px, const REAL py, co
     return outside + inside;
 }
 
+/* Bounding box of n >= 1 points as six extremes (xmin, xmax, ymin, ymax, zmin, zmax): the scalar
+ * reduction of serial/edf/edf.hpp:500-539 with std::min(m, v) = (v < m ? v : m), seeded with the
+ * first point. */
+void OR_NAME(oracle_compute_aabb)(const ptrdiff_t n, const REAL *x, const REAL *y, const REAL *z, REAL *box6) {
+    REAL b[6] = {x[0], x[0], y[0], y[0], z[0], z[0]};
+    for (ptrdiff_t i = 0; i < n; i++) {
+        b[0] = x[i] < b[0] ? x[i] : b[0];
+        b[1] = b[1] < x[i] ? x[i] : b[1];
+        b[2] = y[i] < b[2] ? y[i] : b[2];
+        b[3] = b[3] < y[i] ? y[i] : b[3];
+        b[4] = z[i] < b[4] ? z[i] : b[4];
+        b[5] = b[5] < z[i] ? z[i] : b[5];
+    }
+    for (int k = 0; k < 6; k++) box6[k] = b[k];
+}
+
+/* out[i] = signed distance of point i to box6 (minx, maxx, miny, maxy, minz, maxz):
+ * serial/edf/edf.hpp:541-557. */
+void OR_NAME(oracle_all_points_aabb_signed_distance)(const ptrdiff_t n, const REAL *x, const REAL *y,
+                                                     const REAL *z, const REAL *box6, REAL *out) {
+    for (ptrdiff_t i = 0; i < n; i++)
+        out[i] = OR_NAME(oracle_point_aabb_signed_distance)(x[i], y[i], z[i], box6[0], box6[1], box6[2], box6[3],
+                                                            box6[4], box6[5]);
+}
+
 /*
  * Unsigned distance with the in/out `out` of ssdf::edf / edf_celllist
  * (serial/ssdf.hpp:447-619, 642-963): on entry out[p] is the current best distance, on exit

@@ -25,6 +25,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("SSDF_B200_LIBRARY") or os.path.join(HERE, "_lib", "libssdf_b200.so")
 
 SSDF_OK = 0
+SSDF_ERR_INVALID_ARGUMENT, SSDF_ERR_OUT_OF_MEMORY, SSDF_ERR_CUDA, SSDF_ERR_NOT_SUPPORTED, SSDF_ERR_INTERNAL = 1, 2, 3, 4, 5
 F32, F64 = 0, 1
 PREC_F32, PREC_F64, PREC_F32_FIXUP = 0, 1, 2
 OUT_EDF, OUT_SQEDF, OUT_SDF, OUT_CLOSEST = 0, 1, 2, 3
@@ -104,6 +105,13 @@ _sig("ssdf_batch_last_blocks", [_vp], C.c_longlong)
 _sig("ssdf_query_grid_noalloc", [_vp, _pd, _pd, _pd, C.POINTER(C.c_double * 3), C.POINTER(C.c_double * 3), _vp, _ip,
                                  C.POINTER(QueryOpts), _vp])
 _sig("ssdf_query_grid_noalloc_max", [], C.c_longlong)
+for _g, _gc in (("f", C.c_float), ("d", C.c_double)):
+    for _t, _tc in (("f", C.c_float), ("d", C.c_double)):
+        _sig(f"ssdf_b200_compute_aabb_{_g}{_t}", [_pd, _vp, _vp, _vp] + [C.POINTER(_tc)] * 6)
+        _sig(f"ssdf_b200_all_points_aabb_signed_distance_{_g}{_t}", [_pd, _vp, _vp, _vp] + [_tc] * 6 + [_vp])
+_sig("ssdf_points_aabb", [_pd, _vp, _vp, _vp, C.c_int, C.c_int, _vp, _vp])
+_sig("ssdf_points_aabb_signed_distance", [_pd, _vp, _vp, _vp, C.c_int, C.POINTER(C.c_double * 6), C.c_int, _vp,
+                                          C.c_int, _vp])
 
 
 class ServerOpts(C.Structure):
@@ -148,7 +156,9 @@ EXPORTED = ["ssdf_status_string", "ssdf_last_error", "ssdf_b200_version", "ssdf_
             "ssdf_batch_size", "ssdf_batch_add_grid", "ssdf_batch_add_points", "ssdf_batch_run",
             "ssdf_batch_last_blocks", "ssdf_query_grid_noalloc", "ssdf_query_grid_noalloc_max", "ssdf_server_create",
             "ssdf_server_destroy", "ssdf_server_add_mesh", "ssdf_server_submit_points", "ssdf_server_submit_grid",
-            "ssdf_server_wait", "ssdf_server_stats", "ssdf_server_reset_stats", "ssdf_autotune_grid"]
+            "ssdf_server_wait", "ssdf_server_stats", "ssdf_server_reset_stats", "ssdf_autotune_grid",
+            "ssdf_points_aabb", "ssdf_points_aabb_signed_distance"] + \
+    [f"ssdf_b200_{k}_{g}{t}" for k in ("compute_aabb", "all_points_aabb_signed_distance") for g in "fd" for t in "fd"]
 
 
 def _status_name(status: int) -> str:
@@ -272,6 +282,29 @@ def closest_point_bvh(points, mesh, outd=None, dtype=np.float64):
     return d, ox, oy, oz, tri
 
 
+def compute_aabb(points, gdtype=np.float64, tdtype=None):
+    """ssdf::compute_aabb<G, T> (serial/edf/edf.hpp:500-539) on the GPU: the bounding box of the points
+    as (xmin, xmax, ymin, ymax, zmin, zmax) in T."""
+    tdtype = gdtype if tdtype is None else tdtype
+    x, y, z = _points(points, gdtype)
+    tc = C.c_double if np.dtype(tdtype) == np.float64 else C.c_float
+    v = [tc() for _ in range(6)]
+    fn = f"ssdf_b200_compute_aabb_{_suffix(gdtype)}{_suffix(tdtype)}"
+    _check(getattr(lib, fn)(len(x), _p(x), _p(y), _p(z), *[C.byref(a) for a in v]), fn)
+    return tuple(np.dtype(tdtype).type(a.value) for a in v)
+
+
+def all_points_aabb_signed_distance(points, box, gdtype=np.float64, tdtype=None):
+    """ssdf::all_points_aabb_signed_distance<G, T> (serial/edf/edf.hpp:541-557) on the GPU: each point's
+    signed distance to box = (minx, maxx, miny, maxy, minz, maxz), negative inside."""
+    tdtype = gdtype if tdtype is None else tdtype
+    x, y, z = _points(points, gdtype)
+    out = np.empty(len(x), dtype=tdtype)
+    fn = f"ssdf_b200_all_points_aabb_signed_distance_{_suffix(gdtype)}{_suffix(tdtype)}"
+    _check(getattr(lib, fn)(len(x), _p(x), _p(y), _p(z), *[float(b) for b in box], _p(out)), fn)
+    return out
+
+
 def _grid_call(fn, mesh, grid, out, dtype, extra=()):
     nx, ny, nz = (int(v) for v in grid.n)
     hm = _HostMesh(mesh, dtype)
@@ -334,6 +367,32 @@ def _stream_handle(stream) -> int:
     if isinstance(stream, int):
         return stream
     return stream.cuda_stream
+
+
+def _dtype_code(t) -> int:
+    import torch
+
+    if t.dtype == torch.float64:
+        return F64
+    if t.dtype == torch.float32:
+        return F32
+    raise TypeError(f"unsupported dtype {t.dtype}")
+
+
+def points_aabb_device(x, y, z, box6, stream=None):
+    """Device form of compute_aabb: torch tensors x, y, z (one float dtype) in, the six extremes
+    (xmin, xmax, ymin, ymax, zmin, zmax) written to the device tensor box6 (its dtype is T)."""
+    _check(lib.ssdf_points_aabb(x.numel(), _dptr(x), _dptr(y), _dptr(z), _dtype_code(x), _dtype_code(box6),
+                                _dptr(box6), _stream_handle(stream)), "ssdf_points_aabb")
+
+
+def points_aabb_signed_distance_device(x, y, z, box, out, absolute=False, stream=None):
+    """Device form of all_points_aabb_signed_distance: out (device, T) gets each point's signed (or,
+    with absolute, unsigned) distance to box = (minx, maxx, miny, maxy, minz, maxz)."""
+    b = (C.c_double * 6)(*[float(v) for v in box])
+    _check(lib.ssdf_points_aabb_signed_distance(x.numel(), _dptr(x), _dptr(y), _dptr(z), _dtype_code(x), C.byref(b),
+                                                int(bool(absolute)), _dptr(out), _dtype_code(out),
+                                                _stream_handle(stream)), "ssdf_points_aabb_signed_distance")
 
 
 class DeviceMesh:

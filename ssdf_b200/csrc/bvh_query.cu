@@ -10,7 +10,8 @@
 //         window (sqrt(best) + tau)^2; the window's members are re-evaluated in double and the
 //         lexicographic minimum taken. tau bounds twice the float error of one distance, so the
 //         double winner is always in the window; a query whose window overflowed the K slots is
-//         walked again with the window fixed, re-evaluating every member in double (k_window).
+//         walked again with the window fixed, re-evaluating every member in double (k_window, a
+//         warp per query).
 //         Result: bitwise the F64 result.
 // Traversal: nearest child first, the farther one pushed with its box distance on a per-lane stack
 // and culled on pop against the current thresholds. Each lane answers kQ queries (a build option;
@@ -37,10 +38,11 @@ namespace ssdf_b200 {
 namespace {
 
 constexpr int kThreads = 128;
-// F32X window slots: candidates kept per query in registers. A window that overflows them sends
-// its query to the second stage (k_window); fewer slots means fewer registers, more second stage.
+// F32X window slots: candidates kept per query in shared memory. A window that overflows them sends
+// its query to the second stage (k_window). On the torus-knot 256^3 grid: 8 slots overflow 0.72% of
+// the queries (22.9 ms), 12 slots 0.01% (21.6 ms), 16 slots none (23.2 ms: the longer insertion).
 #ifndef SSDF_B200_WINDOW_SLOTS
-#define SSDF_B200_WINDOW_SLOTS 8
+#define SSDF_B200_WINDOW_SLOTS 12
 #endif
 constexpr int kCand = SSDF_B200_WINDOW_SLOTS;
 
@@ -425,56 +427,6 @@ struct FastPolicy {
                         best[q] = d2;
                         thr[q] = window_thr(best[q], tau_rel, m.coord_scale);
                     }
-                }
-            }
-        }
-    }
-};
-
-// Second stage of F32X for queries whose window overflowed its slots: the float walk again, now
-// with the window fixed at its final extent, and every triangle inside it re-evaluated in double on
-// the spot (the same float test decides membership, so the set is exactly the window).
-struct WindowPolicy {
-    using R = float;
-    static constexpr int kQn = 1;
-    const DeviceMesh &m;
-    float px[1], py[1], pz[1], thr[1];
-    double qx, qy, qz, best;
-    int bid = -1, bpos = -1;
-    __device__ WindowPolicy(const DeviceMesh &mesh, double x, double y, double z, float window, double init)
-        : m(mesh), qx(x), qy(y), qz(z), best(init) {
-        px[0] = float(x), py[0] = float(y), pz[0] = float(z), thr[0] = window;
-    }
-    __device__ __forceinline__ void boxes(int node, float (&d0)[1], float (&d1)[1], int &r0, int &r1) const {
-        const Node32 n = load_node32(m.nodes32, node);
-        d0[0] = box_dist_sq_fast(px[0], py[0], pz[0], n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y);
-        d1[0] = box_dist_sq_fast(px[0], py[0], pz[0], n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w);
-        r0 = n.r0;
-        r1 = n.r1;
-    }
-    __device__ __forceinline__ void boxes4(int node, float (&d)[4][1], int (&r)[4]) const {
-        float dq[4];
-        boxes4_fast(m, node, px[0], py[0], pz[0], dq, r);
-#pragma unroll
-        for (int c = 0; c < 4; c++) d[c][0] = dq[c];
-    }
-    __device__ __forceinline__ float max_thr() const { return thr[0]; }
-    template <bool COUNT>
-    __device__ __forceinline__ void leaf(int first, int n, unsigned mask, Counters &cnt) {
-        if (!mask) return;
-        for (int k = 0; k < n; k++) {
-            const Tri32 t = load_tri32(m.tris32, first + k);
-            const float d2 = tri_dist_sq_fast(px[0], py[0], pz[0], t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
-            if (COUNT) cnt.tri++;
-            if (d2 < thr[0]) {
-                const Tri64 u = load_tri64(m.tris64, first + k);
-                const double e2 =
-                    tri_dist_sq_exact<double>(qx, qy, qz, u.ax, u.ay, u.az, u.bx, u.by, u.bz, u.cx, u.cy, u.cz);
-                if (COUNT) cnt.fix++;
-                if (e2 < best || (e2 == best && bid >= 0 && u.id < bid)) {
-                    best = e2;
-                    bid = u.id;
-                    bpos = first + k;
                 }
             }
         }
@@ -898,24 +850,145 @@ __global__ void __launch_bounds__(kThreads, PREC == SSDF_PREC_F64 ? 1 : SSDF_B20
     if (COUNT) flush_counters(a, cnt);
 }
 
-template <bool WIDE, bool COUNT>
-__device__ __forceinline__ void window_one(const QueryArgs &a, int idx, Counters &cnt) {
+// ---- second fix-up stage: one warp per overflowed query --------------------------------------------
+//
+// A query whose window overflowed its slots is walked again with the window fixed at its final
+// extent: every triangle whose float distance is inside it is re-evaluated in double. With the
+// window fixed the visiting order is free, so the warp walks the tree breadth-parallel: each step
+// the 32 lanes take up to 32 nodes from the warp's shared stack, test their children, run the
+// wanted leaves, and push the wanted internal children (ballot-compacted). A lane keeps the
+// lexicographic (d^2, index) minimum of the triangles it evaluated (the incoming bound ranks -1, so
+// it wins ties, as in the sequential rule) and a warp reduction takes the minimum of those: the
+// same value as the sequential walk, since each triangle's double distance does not depend on the
+// order. The boxes and the float test are the first stage's, on the binary tree: the double winner
+// lies inside the window by the margin tau, so its boxes pass under either arity.
+constexpr int kWinStack = 1024;  // node slots of a warp's shared stack
+#ifndef SSDF_B200_WINDOW_BLOCKS_PER_SM
+#define SSDF_B200_WINDOW_BLOCKS_PER_SM 4
+#endif
+constexpr int kWindowBlocksPerSm = SSDF_B200_WINDOW_BLOCKS_PER_SM;
+
+struct WindowBest {
+    double d2;
+    int id, pos;
+};
+
+__device__ __forceinline__ void window_leaf(const DeviceMesh &m, int ref, float px, float py, float pz, float thr,
+                                            double qx, double qy, double qz, WindowBest &b, Counters &cnt,
+                                            bool count) {
+    const int first = leaf_first(ref), n = leaf_count(ref);
+    for (int k = 0; k < n; k++) {
+        const Tri32 t = load_tri32(m.tris32, first + k);
+        const float f = tri_dist_sq_fast(px, py, pz, t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
+        if (count) cnt.tri++;
+        if (f < thr) {
+            const Tri64 u = load_tri64(m.tris64, first + k);
+            const double e2 =
+                tri_dist_sq_exact<double>(qx, qy, qz, u.ax, u.ay, u.az, u.bx, u.by, u.bz, u.cx, u.cy, u.cz);
+            if (count) cnt.fix++;
+            if (e2 < b.d2 || (e2 == b.d2 && u.id < b.id)) b = WindowBest{e2, u.id, first + k};
+        }
+    }
+}
+
+// A lane's own depth-first walk of the subtree under `root` (when the warp's stack is full). Depth
+// below kStackSize is checked when the mesh is built, and a depth-first walk that pushes both
+// children holds at most depth + 1 entries.
+__device__ __noinline__ void window_subtree(const DeviceMesh &m, int root, float px, float py, float pz, float thr,
+                                            double qx, double qy, double qz, WindowBest &b, Counters &cnt,
+                                            bool count) {
+    int st[kStackSize];
+    int sp = 0;
+    st[sp++] = root;
+    while (sp > 0) {
+        const Node32 n = load_node32(m.nodes32, st[--sp]);
+        const float d0 = box_dist_sq_fast(px, py, pz, n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y);
+        const float d1 = box_dist_sq_fast(px, py, pz, n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w);
+        if (count) cnt.box += 2;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int c = h ? n.r1 : n.r0;
+            if (c == kEmptyRef || !((h ? d1 : d0) < thr)) continue;
+            if (c < 0)
+                window_leaf(m, c, px, py, pz, thr, qx, qy, qz, b, cnt, count);
+            else if (sp < kStackSize)
+                st[sp++] = c;
+        }
+    }
+}
+
+// The whole warp answers overflowed query `idx` of job `a`; lane 0 writes the result.
+template <bool COUNT>
+__device__ void window_warp(const QueryArgs &a, int idx, int *__restrict__ stack, int cap, Counters &cnt) {
+    const unsigned kAll = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
     const long long q = a.fallback_ids[idx];
     long long i = 0, j = 0, k = 0;
     if (a.is_grid) grid_ijk(a, q, i, j, k);
     double qx, qy, qz;
     query_point(a, q, i, j, k, qx, qy, qz);
-    WindowPolicy p(a.m, qx, qy, qz, a.fallback_thr[idx], initial_bound(a, q));
-    walk<false, WIDE, COUNT>(p, cnt);
-    write_result(a, q, qx, qy, qz, p.best, p.bid, p.bpos);
+    const float px = float(qx), py = float(qy), pz = float(qz);
+    const float thr = a.fallback_thr[idx];
+    const DeviceMesh &m = a.m;
+    WindowBest b{initial_bound(a, q), -1, -1};
+    if (lane == 0) stack[0] = 0;
+    int sp = 1;  // warp-uniform
+    __syncwarp();
+    while (sp > 0) {
+        const int take = sp < 32 ? sp : 32;
+        const int node = lane < take ? stack[sp - take + lane] : -1;
+        sp -= take;
+        __syncwarp();  // the slots just read are free for the pushes below
+        int c0 = kEmptyRef, c1 = kEmptyRef;
+        bool w0 = false, w1 = false;
+        if (node >= 0) {
+            const Node32 n = load_node32(m.nodes32, node);
+            const float d0 = box_dist_sq_fast(px, py, pz, n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y);
+            const float d1 = box_dist_sq_fast(px, py, pz, n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w);
+            if (COUNT) cnt.box += 2;
+            c0 = n.r0, c1 = n.r1;
+            w0 = c0 != kEmptyRef && d0 < thr;
+            w1 = c1 != kEmptyRef && d1 < thr;
+            if (w0 && c0 < 0) {
+                window_leaf(m, c0, px, py, pz, thr, qx, qy, qz, b, cnt, COUNT);
+                w0 = false;
+            }
+            if (w1 && c1 < 0) {
+                window_leaf(m, c1, px, py, pz, thr, qx, qy, qz, b, cnt, COUNT);
+                w1 = false;
+            }
+        }
+        const unsigned m0 = __ballot_sync(kAll, w0), m1 = __ballot_sync(kAll, w1);
+        const int n0 = __popc(m0), total = n0 + __popc(m1);
+        if (sp + total <= cap) {
+            const unsigned below = (1u << lane) - 1u;
+            if (w0) stack[sp + __popc(m0 & below)] = c0;
+            if (w1) stack[sp + n0 + __popc(m1 & below)] = c1;
+            sp += total;
+        } else {
+            if (w0) window_subtree(m, c0, px, py, pz, thr, qx, qy, qz, b, cnt, COUNT);
+            if (w1) window_subtree(m, c1, px, py, pz, thr, qx, qy, qz, b, cnt, COUNT);
+        }
+        __syncwarp();
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double od = __shfl_xor_sync(kAll, b.d2, o);
+        const int oid = __shfl_xor_sync(kAll, b.id, o), opos = __shfl_xor_sync(kAll, b.pos, o);
+        if (od < b.d2 || (od == b.d2 && oid < b.id)) b = WindowBest{od, oid, opos};
+    }
+    if (lane == 0) write_result(a, q, qx, qy, qz, b.d2, b.id, b.pos);
 }
 
-template <bool WIDE, bool COUNT>
-__global__ void __launch_bounds__(kThreads) k_window(const QueryArgs a) {
+// Overflowed queries of one launch, a warp each. `cap` (<= kWinStack) is the shared stack's usable
+// depth: kWinStack, lowered only to test the per-lane subtree walk.
+template <bool COUNT>
+__global__ void __launch_bounds__(kThreads) k_window(const QueryArgs a, int cap) {
+    __shared__ int s_stack[kThreads / 32][kWinStack];
     const int n = *a.fallback_count;
+    const int w = (blockIdx.x * kThreads + threadIdx.x) >> 5, nw = (gridDim.x * kThreads) >> 5;
     Counters cnt;
-    for (int idx = blockIdx.x * kThreads + threadIdx.x; idx < n; idx += gridDim.x * kThreads)
-        window_one<WIDE, COUNT>(a, idx, cnt);
+    for (int idx = w; idx < n; idx += nw) window_warp<COUNT>(a, idx, s_stack[threadIdx.x >> 5], cap, cnt);
     if (COUNT) flush_counters(a, cnt);
 }
 
@@ -950,19 +1023,32 @@ __global__ void __launch_bounds__(kThreads, PREC == SSDF_PREC_F64 ? 1 : SSDF_B20
     if (COUNT && njobs > 0) flush_counters(jobs[0], cnt);
 }
 
-template <bool WIDE, bool COUNT>
+// Overflowed queries of every job: the jobs' lists laid end to end and dealt to the warps in turn,
+// so no warp takes the same position of every list.
+template <bool COUNT>
 __global__ void __launch_bounds__(kThreads) k_window_batch(const BatchHeader *__restrict__ hdr,
-                                                           const QueryArgs *__restrict__ jobs) {
+                                                           const QueryArgs *__restrict__ jobs, int cap) {
+    __shared__ int s_stack[kThreads / 32][kWinStack];
     const int njobs = hdr->njobs;
+    const long long w = (blockIdx.x * kThreads + threadIdx.x) >> 5, nw = (gridDim.x * kThreads) >> 5;
     Counters cnt;
+    long long base = 0;  // overflowed queries of the jobs before jb
     for (int jb = 0; jb < njobs; jb++) {
         const QueryArgs &a = jobs[jb];
         if (!a.fallback_count) continue;
         const int n = *a.fallback_count;
-        for (int idx = blockIdx.x * kThreads + threadIdx.x; idx < n; idx += gridDim.x * kThreads)
-            window_one<WIDE, COUNT>(a, idx, cnt);
+        for (long long idx = ((w - base) % nw + nw) % nw; idx < n; idx += nw)
+            window_warp<COUNT>(a, int(idx), s_stack[threadIdx.x >> 5], cap, cnt);
+        base += n;
     }
     if (COUNT && njobs > 0) flush_counters(jobs[0], cnt);
+}
+
+// Usable depth of the second stage's shared stack: kWinStack, or SSDF_B200_WINDOW_STACK (1 ..
+// kWinStack) to exercise the per-lane subtree walk in tests.
+int window_stack_cap() {
+    const int v = env_int("SSDF_B200_WINDOW_STACK", kWinStack);
+    return v < 1 ? 1 : (v > kWinStack ? kWinStack : v);
 }
 
 template <int PREC, bool WARP, bool WIDE>
@@ -973,16 +1059,10 @@ cudaError_t launch_batch_main(const BatchLaunch &b, bool count, cudaStream_t str
         k_query_batch<PREC, WARP, WIDE, false><<<b.grid, kThreads, 0, stream>>>(b.hdr, b.jobs, b.first_block, b.next_item);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || PREC != SSDF_PREC_F32_FIXUP) return e;
-    static int per_sm = 0;  // resident blocks of the second stage, as for a single launch
-    if (per_sm == 0) {
-        int v = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_window_batch<WIDE, false>, kThreads, 0);
-        per_sm = v > 0 ? v : 1;
-    }
     if (count)
-        k_window_batch<WIDE, true><<<per_sm * b.sms, kThreads, 0, stream>>>(b.hdr, b.jobs);
+        k_window_batch<true><<<kWindowBlocksPerSm * b.sms, kThreads, 0, stream>>>(b.hdr, b.jobs, window_stack_cap());
     else
-        k_window_batch<WIDE, false><<<per_sm * b.sms, kThreads, 0, stream>>>(b.hdr, b.jobs);
+        k_window_batch<false><<<kWindowBlocksPerSm * b.sms, kThreads, 0, stream>>>(b.hdr, b.jobs, window_stack_cap());
     return cudaGetLastError();
 }
 
@@ -1048,20 +1128,17 @@ static bool use_warp(const QueryArgs &a) {
     return a.is_grid != 0;
 }
 
-// Blocks of the second fix-up stage: every SM filled to the kernel's occupancy. Its queries are
-// scattered and walk divergently, so it needs all the warps it can get to hide latency; the count
-// of overflowed queries is only known on the device, and the kernel strides over it.
-template <bool WIDE>
+// Blocks of the second fix-up stage (kWindowBlocksPerSm per SM, four warps each). The warps stride
+// over the overflow count, which is only known on the device.
 unsigned window_grid() {
     static int cached[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
     int &g = cached[dev & 63];
     if (g == 0) {
-        int sms = 0, per_sm = 0;
+        int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_window<WIDE, false>, kThreads, 0);
-        g = std::max(1, sms) * std::max(1, per_sm);
+        g = kWindowBlocksPerSm * std::max(1, sms);
     }
     return unsigned(g);
 }
@@ -1108,13 +1185,10 @@ int launch_query(const QueryArgs &args_in, int precision, cudaStream_t stream) {
             e = cudaMemsetAsync(fb, 0, sizeof(int), stream);
             if (e == cudaSuccess) e = launch_prec<SSDF_PREC_F32_FIXUP>(a, warp, wide, count, unsigned(nblocks), stream);
             if (e == cudaSuccess) {
-                const unsigned wg = wide ? window_grid<true>() : window_grid<false>();
-                if (wide)
-                    count ? k_window<true, true><<<wg, kThreads, 0, stream>>>(a)
-                          : k_window<true, false><<<wg, kThreads, 0, stream>>>(a);
-                else
-                    count ? k_window<false, true><<<wg, kThreads, 0, stream>>>(a)
-                          : k_window<false, false><<<wg, kThreads, 0, stream>>>(a);
+                const unsigned wg = window_grid();
+                const int cap = window_stack_cap();
+                count ? k_window<true><<<wg, kThreads, 0, stream>>>(a, cap)
+                      : k_window<false><<<wg, kThreads, 0, stream>>>(a, cap);
                 e = cudaGetLastError();
             }
         }
@@ -1235,10 +1309,7 @@ int launch_query_noalloc(const QueryArgs &args_in, cudaStream_t stream) {
     cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(int), stream);  // the count starts at zero
     if (e == cudaSuccess) e = launch_prec<SSDF_PREC_F32_FIXUP>(a, warp, wide, false, unsigned(nblocks), stream);
     if (e == cudaSuccess) {
-        if (wide)
-            k_window<true, false><<<window_grid<true>(), kThreads, 0, stream>>>(a);
-        else
-            k_window<false, false><<<window_grid<false>(), kThreads, 0, stream>>>(a);
+        k_window<false><<<window_grid(), kThreads, 0, stream>>>(a, kWinStack);
         e = cudaGetLastError();
     }
     if (e != cudaSuccess) return cuda_fail(e, "allocation-free query launch", __FILE__, __LINE__);

@@ -293,6 +293,53 @@ int edf_select_host(ptrdiff_t npoints, const T *x, const T *y, const T *z, ptrdi
                          out, nullptr);
 }
 
+// ssdf::compute_aabb over host arrays (serial/edf/edf.hpp:500-539).
+template <typename G, typename T>
+int compute_aabb_host(ptrdiff_t n, const G *x, const G *y, const G *z, T *xmin, T *xmax, T *ymin, T *ymax, T *zmin,
+                      T *zmax) {
+    if (n <= 0) return fail(SSDF_ERR_INVALID_ARGUMENT, "compute_aabb of no points");
+    if (!x || !y || !z || !xmin || !xmax || !ymin || !ymax || !zmin || !zmax)
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "compute_aabb: null pointer");
+    cudaStream_t stream;
+    SSDF_CHECK(ready_stream(&stream));
+    T box[6];
+    {
+        Scratch sc(stream);
+        void *dx, *dy, *dz, *db;
+        SSDF_CHECK(sc.upload(&dx, x, sizeof(G) * size_t(n)));
+        SSDF_CHECK(sc.upload(&dy, y, sizeof(G) * size_t(n)));
+        SSDF_CHECK(sc.upload(&dz, z, sizeof(G) * size_t(n)));
+        SSDF_CHECK(sc.alloc(&db, sizeof(box)));
+        SSDF_CHECK((points_aabb_device<G, T>)(n, (const G *)dx, (const G *)dy, (const G *)dz, (T *)db, stream));
+        SSDF_CUDA(cudaMemcpyAsync(box, db, sizeof(box), cudaMemcpyDeviceToHost, stream));
+        SSDF_CUDA(cudaStreamSynchronize(stream));
+    }
+    *xmin = box[0], *xmax = box[1], *ymin = box[2], *ymax = box[3], *zmin = box[4], *zmax = box[5];
+    return SSDF_OK;
+}
+
+// ssdf::all_points_aabb_signed_distance over host arrays (serial/edf/edf.hpp:541-557).
+template <typename G, typename T>
+int box_sdf_host(ptrdiff_t n, const G *x, const G *y, const G *z, T minx, T maxx, T miny, T maxy, T minz, T maxz,
+                 T *out) {
+    if (n < 0) return fail(SSDF_ERR_INVALID_ARGUMENT, "negative point count");
+    if (n == 0) return SSDF_OK;
+    if (!x || !y || !z || !out) return fail(SSDF_ERR_INVALID_ARGUMENT, "all_points_aabb_signed_distance: null pointer");
+    cudaStream_t stream;
+    SSDF_CHECK(ready_stream(&stream));
+    Scratch sc(stream);
+    void *dx, *dy, *dz, *dout;
+    SSDF_CHECK(sc.upload(&dx, x, sizeof(G) * size_t(n)));
+    SSDF_CHECK(sc.upload(&dy, y, sizeof(G) * size_t(n)));
+    SSDF_CHECK(sc.upload(&dz, z, sizeof(G) * size_t(n)));
+    SSDF_CHECK(sc.alloc(&dout, sizeof(T) * size_t(n)));
+    const T box[6] = {minx, maxx, miny, maxy, minz, maxz};
+    SSDF_CHECK((points_box_sdf_device<G, T>)(n, (const G *)dx, (const G *)dy, (const G *)dz, box, 0, (T *)dout, stream));
+    SSDF_CUDA(cudaMemcpyAsync(out, dout, sizeof(T) * size_t(n), cudaMemcpyDeviceToHost, stream));
+    SSDF_CUDA(cudaStreamSynchronize(stream));
+    return SSDF_OK;
+}
+
 }  // namespace
 }  // namespace ssdf_b200
 
@@ -395,6 +442,70 @@ int ssdf_b200_sample_sdf_bvh_dd(GRID_ARGS(double, double)) {
 }
 int ssdf_b200_sample_sdf_index_bvh_dd(GRID_ARGS(double, double), int *outtri) {
     return bvh_grid_host<double, double>(GRID_PASS, outtri, SSDF_OUT_SDF, precision_from_env(SSDF_PREC_F32_FIXUP));
+}
+
+// ---- grid and box helpers (serial/edf/edf.hpp:500-557) ---------------------------------------------
+
+#define AABB_ARGS(G, T)                                                                                            \
+    ptrdiff_t npoints, const G *x, const G *y, const G *z, T *xmin, T *xmax, T *ymin, T *ymax, T *zmin, T *zmax
+#define AABB_PASS npoints, x, y, z, xmin, xmax, ymin, ymax, zmin, zmax
+int ssdf_b200_compute_aabb_ff(AABB_ARGS(float, float)) { return compute_aabb_host<float, float>(AABB_PASS); }
+int ssdf_b200_compute_aabb_fd(AABB_ARGS(float, double)) { return compute_aabb_host<float, double>(AABB_PASS); }
+int ssdf_b200_compute_aabb_df(AABB_ARGS(double, float)) { return compute_aabb_host<double, float>(AABB_PASS); }
+int ssdf_b200_compute_aabb_dd(AABB_ARGS(double, double)) { return compute_aabb_host<double, double>(AABB_PASS); }
+
+#define BOXSDF_ARGS(G, T)                                                                                          \
+    ptrdiff_t npoints, const G *x, const G *y, const G *z, T minx, T maxx, T miny, T maxy, T minz, T maxz, T *out
+#define BOXSDF_PASS npoints, x, y, z, minx, maxx, miny, maxy, minz, maxz, out
+int ssdf_b200_all_points_aabb_signed_distance_ff(BOXSDF_ARGS(float, float)) {
+    return box_sdf_host<float, float>(BOXSDF_PASS);
+}
+int ssdf_b200_all_points_aabb_signed_distance_fd(BOXSDF_ARGS(float, double)) {
+    return box_sdf_host<float, double>(BOXSDF_PASS);
+}
+int ssdf_b200_all_points_aabb_signed_distance_df(BOXSDF_ARGS(double, float)) {
+    return box_sdf_host<double, float>(BOXSDF_PASS);
+}
+int ssdf_b200_all_points_aabb_signed_distance_dd(BOXSDF_ARGS(double, double)) {
+    return box_sdf_host<double, double>(BOXSDF_PASS);
+}
+
+int ssdf_points_aabb(ptrdiff_t npoints, const void *x, const void *y, const void *z, int coord_type, int out_type,
+                     void *box6, void *stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    const int g64 = coord_type == SSDF_F64, t64 = out_type == SSDF_F64;
+    if ((coord_type != SSDF_F32 && !g64) || (out_type != SSDF_F32 && !t64))
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "ssdf_points_aabb: bad coord_type / out_type");
+    if (g64)
+        return t64 ? points_aabb_device<double, double>(npoints, (const double *)x, (const double *)y, (const double *)z,
+                                                        (double *)box6, s)
+                   : points_aabb_device<double, float>(npoints, (const double *)x, (const double *)y, (const double *)z,
+                                                       (float *)box6, s);
+    return t64 ? points_aabb_device<float, double>(npoints, (const float *)x, (const float *)y, (const float *)z,
+                                                   (double *)box6, s)
+               : points_aabb_device<float, float>(npoints, (const float *)x, (const float *)y, (const float *)z,
+                                                  (float *)box6, s);
+}
+
+int ssdf_points_aabb_signed_distance(ptrdiff_t npoints, const void *x, const void *y, const void *z, int coord_type,
+                                     const double box6[6], int absolute, void *out, int out_type, void *stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    const int g64 = coord_type == SSDF_F64, t64 = out_type == SSDF_F64;
+    if ((coord_type != SSDF_F32 && !g64) || (out_type != SSDF_F32 && !t64))
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "ssdf_points_aabb_signed_distance: bad coord_type / out_type");
+    if (!box6) return fail(SSDF_ERR_INVALID_ARGUMENT, "ssdf_points_aabb_signed_distance: null box");
+    if (t64) {
+        return g64 ? points_box_sdf_device<double, double>(npoints, (const double *)x, (const double *)y,
+                                                           (const double *)z, box6, absolute, (double *)out, s)
+                   : points_box_sdf_device<float, double>(npoints, (const float *)x, (const float *)y,
+                                                          (const float *)z, box6, absolute, (double *)out, s);
+    }
+    float b[6];
+    for (int k = 0; k < 6; k++) b[k] = float(box6[k]);
+    return g64 ? points_box_sdf_device<double, float>(npoints, (const double *)x, (const double *)y, (const double *)z,
+                                                      b, absolute, (float *)out, s)
+               : points_box_sdf_device<float, float>(npoints, (const float *)x, (const float *)y, (const float *)z, b,
+                                                     absolute, (float *)out, s);
 }
 
 // ---- handle API ---------------------------------------------------------------------------------------

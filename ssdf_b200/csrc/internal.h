@@ -175,6 +175,15 @@ int celllist_edf(int f64, ptrdiff_t npoints, const void *x, const void *y, const
                  const int *s0, const int *s1, const int *s2, ptrdiff_t nv, const void *sx, const void *sy,
                  const void *sz, void *out, int *outtri, cudaStream_t stream);
 
+// ---- box helpers (box_helpers.cu) ----------------------------------------------------------------
+// Bounding box of n device points as T (xmin, xmax, ymin, ymax, zmin, zmax into device box6).
+template <typename G, typename T>
+int points_aabb_device(long long n, const G *x, const G *y, const G *z, T *box6, cudaStream_t stream);
+// Signed distance of n device points to the box given as host box6 (|.| when absolute).
+template <typename G, typename T>
+int points_box_sdf_device(long long n, const G *x, const G *y, const G *z, const T box6[6], int absolute, T *out,
+                          cudaStream_t stream);
+
 // ---- small helpers -------------------------------------------------------------------------------
 inline int grid_blocks(long long n, int threads) { return int((n + threads - 1) / threads); }
 int env_int(const char *name, int dflt);

@@ -1,0 +1,87 @@
+"""GPU: the fix-up path's second stage -- queries whose float window holds more near-tied triangles
+than the window slots -- bitwise against the plain double result and the oracle.
+
+Grid nodes within 2e-5 of the centre of an undisplaced icosphere are nearly equidistant from
+dozens of triangles (the icosahedral symmetry makes exact ties), so every one of them overflows
+and is answered by the warp-per-query walk. SSDF_B200_WINDOW_STACK lowers that walk's shared stack
+so the lanes' own subtree walks run too. In a batch, such jobs sit among ordinary ones.
+"""
+
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+import ssdf_b200 as S
+from ssdf_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def centre_grid(n=16, r=2e-5):
+    return W.Grid((n, n, n), (-r, -r, -r), (r, r, r))
+
+
+def run(dm, grid, prec, stack=None):
+    out = torch.empty(grid.size, dtype=torch.float64, device="cuda")
+    tri = torch.empty(grid.size, dtype=torch.int32, device="cuda")
+    env = {"SSDF_B200_COUNT": "1"}
+    if stack is not None:
+        env["SSDF_B200_WINDOW_STACK"] = str(stack)
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
+    try:
+        dm.query_grid(grid, out, tri, precision=prec, output=S.OUT_SDF)
+        torch.cuda.synchronize()
+        counts = S.last_query_counts()
+    finally:
+        for k, v in old.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v
+    return out.cpu().numpy(), tri.cpu().numpy(), counts
+
+
+@pytest.mark.parametrize("sub", [2, 4])
+@pytest.mark.parametrize("stack", [None, 40, 1])
+def test_overflowed_windows_match_double(sub, stack):
+    mesh = W.icosphere(sub, radius=1.0, displacement=0.0)
+    grid = centre_grid()
+    dm = S.DeviceMesh(mesh)
+    d, t, c = run(dm, grid, S.PREC_F32_FIXUP, stack)
+    d64, t64, _ = run(dm, grid, S.PREC_F64)
+    dm.close()
+    assert c["fallback_queries"] > grid.size // 2, c  # the second stage answered most of them
+    assert np.array_equal(d, d64) and np.array_equal(t, t64)
+    want, wtri = oracle.sdf_points(oracle.grid_points(grid), mesh)
+    assert np.array_equal(d, want) and np.array_equal(t, wtri)
+    assert np.all(d < 0)  # the centre is inside
+
+
+def test_batch_with_overflowing_jobs():
+    jobs = []
+    for k in range(12):
+        if k % 3 == 0:
+            m = W.icosphere(2 + k % 4, radius=0.5 + 0.1 * k, displacement=0.0)
+            jobs.append((m, centre_grid(8 + k)))
+        else:
+            m = W.torus(0.7, 0.2, nu=24 + 8 * k, nv=12 + 2 * k, jitter=0.01, seed=k)
+            jobs.append((m, W.Grid.padded_nodes(m, 20 + 3 * k, 0.1)))
+    dms = [S.DeviceMesh(m) for m, _ in jobs]
+    outs = [torch.empty(g.size, dtype=torch.float64, device="cuda") for _, g in jobs]
+    tris = [torch.empty(g.size, dtype=torch.int32, device="cuda") for _, g in jobs]
+    for use_graph in (False, True):
+        b = S.Batch(len(jobs), S.PREC_F32_FIXUP)
+        for dm, (m, g), o, t in zip(dms, jobs, outs, tris):
+            b.add_grid(dm, g, o, t)
+        b.run(use_graph=use_graph)
+        torch.cuda.synchronize()
+        b.close()
+        for dm, (m, g), o, t in zip(dms, jobs, outs, tris):
+            d64, t64, _ = run(dm, g, S.PREC_F64)
+            assert np.array_equal(o.cpu().numpy(), d64) and np.array_equal(t.cpu().numpy(), t64)
+    for dm in dms:
+        dm.close()

@@ -182,3 +182,28 @@ def test_pseudonormals_manifold_edges():
             g = g[g != f][0]
             assert np.allclose(en[f, e], fn[f] + fn[g], atol=0, rtol=0) or np.array_equal(en[f, e], fn[g] + fn[f])
     assert np.all(np.linalg.norm(vn.reshape(-1, 3), axis=1) > 0)
+
+
+def _box_points(n, seed, dtype):
+    """Points inside, outside, on faces and on edges of a box spanning [-1, 2] x [0, 3] x [-2, 1]."""
+    rng = np.random.default_rng(seed)
+    p = rng.uniform(-3.0, 4.0, size=(3, n))
+    p[:, : n // 4] = np.round(p[:, : n // 4])  # exact face / edge / corner coordinates
+    return p.astype(dtype)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_box_helpers_golden_and_reference(dtype):
+    g = load_golden_json()["box_sdf"]
+    pts = np.array([g["x"], g["y"], g["z"]], dtype=np.float64)
+    if dtype == np.float64:
+        assert np.array_equal(oracle.all_points_aabb_signed_distance(pts, g["box"]), np.array(g["reference"]))
+    if not oracle.ref_available():
+        pytest.skip("the reference was not compiled here")
+    p = _box_points(4099, 7, dtype)
+    b = oracle.compute_aabb(p, dtype)
+    assert np.array_equal(b, oracle.compute_aabb(p, dtype, reference=True))
+    assert np.array_equal(b, np.array([p[0].min(), p[0].max(), p[1].min(), p[1].max(), p[2].min(), p[2].max()]))
+    box = np.array([-1, 2, 0, 3, -2, 1], dtype=dtype)
+    d = oracle.all_points_aabb_signed_distance(p, box, dtype)
+    assert np.array_equal(d, oracle.all_points_aabb_signed_distance(p, box, dtype, reference=True))
