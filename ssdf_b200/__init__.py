@@ -22,4 +22,4 @@ def __getattr__(name):
     if name in _LIBRARY_FREE:
         return importlib.import_module("." + name, __name__)
     capi = importlib.import_module(".capi", __name__)
-    return getattr(capi, name)
+    return capi if name == "capi" else getattr(capi, name)

@@ -68,3 +68,7 @@ def test_build_imports_without_the_library():
             "assert 'ssdf_b200.capi' not in sys.modules, 'binding loaded'")
     res = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True)
     assert res.returncode == 0, res.stderr
+    # the binding module itself is reachable as an attribute on first use
+    code = "import ssdf_b200 as S; assert S.capi.lib is not None; assert S.version() == S.capi.version()"
+    res = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr
