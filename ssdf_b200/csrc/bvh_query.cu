@@ -449,6 +449,83 @@ __device__ __forceinline__ R min_of(const R (&d)[Q]) {
     return v;
 }
 
+// Stack entries of a packet walk hold a float: distances round down and thresholds up, so the
+// float comparison never culls what the exact one would keep.
+__device__ __forceinline__ float stack_key_lo(float d) { return d; }
+__device__ __forceinline__ float stack_key_lo(double d) { return __double2float_rd(d); }
+__device__ __forceinline__ float stack_key_hi(float t) { return t; }
+__device__ __forceinline__ float stack_key_hi(double t) { return __double2float_ru(t); }
+
+// Packet walk (a grid warp as one packet): the node ids on the stack are the same in every lane, so
+// the warp keeps one stack in shared memory instead of 32 copies in local memory. An entry keeps
+// the smallest box distance over the warp's lanes (one redux.sync on the float bits, which order
+// like the values for non-negative floats) and is entered on pop while that is below the largest
+// lane threshold: a superset of "some lane's distance below its own threshold", so never a miss.
+template <bool COUNT, class P>
+__device__ __forceinline__ void traverse_packet(P &p, Counters &cnt) {
+    using R = typename P::R;
+    constexpr int Q = P::kQn;
+    constexpr unsigned kAll = 0xffffffffu;
+    __shared__ int s_node[kThreads / 32][kStackSize];
+    __shared__ float s_dist[kThreads / 32][kStackSize];
+    int *snode = s_node[threadIdx.x >> 5];
+    float *sdist = s_dist[threadIdx.x >> 5];
+    const bool live = p.max_thr() >= R(0);  // lanes without a query take no part in the keys
+    int sp = 0;
+    int node = 0;
+    while (true) {
+        R d0[Q], d1[Q];
+        int r0, r1;
+        p.boxes(node, d0, d1, r0, r1);
+        if (COUNT) cnt.box += 2 * Q;
+        R k0 = min_of<R, Q>(d0), k1 = min_of<R, Q>(d1);
+        if (__popc(__ballot_sync(kAll, k1 < k0)) > 16) {
+#pragma unroll
+            for (int q = 0; q < Q; q++) {
+                const R t = d0[q];
+                d0[q] = d1[q];
+                d1[q] = t;
+            }
+            const R tk = k0;
+            k0 = k1;
+            k1 = tk;
+            const int tr = r0;
+            r0 = r1;
+            r1 = tr;
+        }
+        int next = -1;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int rc = h ? r1 : r0;
+            const unsigned m = rc == kEmptyRef ? 0u : (h ? want_mask(p, d1) : want_mask(p, d0));
+            if (!__any_sync(kAll, m != 0u)) continue;
+            if (rc < 0) {
+                p.template leaf<COUNT>(leaf_first(rc), leaf_count(rc), m, cnt);
+            } else if (next < 0) {
+                next = rc;
+            } else if (sp < kStackSize) {
+                const float key = live ? stack_key_lo(h ? k1 : k0) : finf();
+                snode[sp] = rc;  // every lane stores the same values
+                sdist[sp] = __uint_as_float(__reduce_min_sync(kAll, __float_as_uint(key)));
+                sp++;
+            }
+        }
+        if (next < 0) {
+            const float tl = live ? stack_key_hi(p.max_thr()) : 0.f;
+            const float tmax = __uint_as_float(__reduce_max_sync(kAll, __float_as_uint(tl)));
+            while (sp > 0) {
+                sp--;
+                if (sdist[sp] < tmax) {
+                    next = snode[sp];
+                    break;
+                }
+            }
+            if (next < 0) break;
+        }
+        node = next;
+    }
+}
+
 // Nearest-child-first traversal with a per-lane stack of (node, smallest box distance), culled on
 // pop. WARP = false: every thread walks its own queries. WARP = true (packet): the 32 lanes of a
 // warp walk one path together -- a child is entered if any lane wants it, the nearer child is the
@@ -456,6 +533,10 @@ __device__ __forceinline__ R min_of(const R (&d)[Q]) {
 // does not diverge. Every lane must call it (warp-synchronous when WARP).
 template <bool WARP, bool COUNT, class P>
 __device__ __forceinline__ void traverse(P &p, Counters &cnt) {
+    if constexpr (WARP) {
+        traverse_packet<COUNT>(p, cnt);
+        return;
+    }
     using R = typename P::R;
     constexpr int Q = P::kQn;
     int snode[kStackSize];
