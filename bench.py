@@ -39,6 +39,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "grid SDF queries/s (FP32+FP64 fixup vs plain FP64 GPU); served p50/p99 latency"
+BEAMS_METRIC = "unsigned edf queries/s (FP32, reference float arithmetic) + closest triangle"
 WORKLOAD = "torus-knot tube (2,3), 131072 triangles, 256^3 node grid over bbox+0.25, signed, double"
 REF_SAMPLE = 262144       # reference arm: grid nodes per step
 CPU_SAMPLE = 1048576      # cpu_baseline leg of our arm
@@ -50,7 +51,10 @@ def parse_args():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--grid", type=int, default=256)
+    p.add_argument("--workload", choices=["knot", "icosphere", "beams"], default="knot",
+                   help="knot (default): the headline line; icosphere / beams: the other single-mesh "
+                        "configurations, one line each, without the batched and serving legs")
+    p.add_argument("--grid", type=int, default=None, help="grid side (default 256 knot, 64 icosphere, 512 beams)")
     p.add_argument("--cpu-sample", type=int, default=CPU_SAMPLE)
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     p.add_argument("--no-e2e", action="store_true")
@@ -59,7 +63,10 @@ def parse_args():
     p.add_argument("--batch-meshes", type=int, default=256)
     p.add_argument("--serve-meshes", type=int, default=128)
     p.add_argument("--serve-seconds", type=float, default=3.0)
-    return p.parse_args()
+    a = p.parse_args()
+    if a.grid is None:
+        a.grid = DEFAULT_GRID[a.workload]
+    return a
 
 
 def max_over_ranks(value, dist, device):
@@ -77,9 +84,22 @@ def job_rate(queries_per_rank, steps, max_ms, world):
     return world * queries_per_rank * steps / (max_ms * 1e-3)
 
 
-def workload(n=256):
+WORKLOADS = {
+    "knot": WORKLOAD,
+    "icosphere": "icosphere r=1 subdivided 4x (5120 triangles, 0.02 radial jitter), 64^3 cell-centred grid over "
+                 "bbox+0.2, signed, double, closest triangle",
+    "beams": "beam lattice (20000 beams, 240000 triangles), 8e6 uniform points in [-0.1,1.1]^3 + 512^3 grid over "
+             "the same cube, unsigned float distance + int32 closest triangle",
+}
+DEFAULT_GRID = {"knot": 256, "icosphere": 64, "beams": 512}
+
+
+def workload(n=256, name="knot"):
     from ssdf_b200 import workloads as W
 
+    if name == "icosphere":
+        mesh = W.icosphere(4)
+        return mesh, W.Grid.cell_centred(mesh, n, 0.2)
     mesh = W.torus_knot_tube()
     grid = W.Grid.padded_nodes(mesh, n, 0.25)
     return mesh, grid
@@ -147,21 +167,171 @@ def cpu_reference_rate(mesh, grid, nsample, seed=17, steps=1):
     return len(ids), times
 
 
+def beams_workload(n=512, npoints=8_000_000):
+    """Config 3: the beam lattice, seeded uniform points in [-0.1, 1.1]^3 and an n^3 node grid there."""
+    from ssdf_b200 import workloads as W
+
+    mesh = W.beam_lattice()
+    pts = W.uniform_points(npoints, -0.1, 1.1, seed=23).astype(np.float32)
+    grid = W.Grid((n, n, n), (-0.1, -0.1, -0.1), (1.1, 1.1, 1.1))
+    return mesh, (pts, grid)
+
+
+def cpu_reference_points(mesh, pts_grid, nsample, dtype, seed=17, steps=1):
+    """The reference's edf_celllist<float> (oracle/_ref) on a seeded sample of the beam-lattice queries."""
+    import oracle
+
+    if not oracle.ref_available():
+        raise RuntimeError("reference CPU library (oracle/_ref) is not built")
+    pts, grid = pts_grid
+    rng = np.random.default_rng(seed)
+    half = nsample // 2
+    a = pts[:, np.sort(rng.choice(pts.shape[1], size=half, replace=False))]
+    ids = np.sort(rng.choice(grid.size, size=nsample - half, replace=False))
+    b = oracle.grid_points(grid)[:, ids].astype(dtype)
+    q = np.concatenate([a, b], axis=1).astype(dtype)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        oracle.ref_edf(q, mesh, dtype=dtype, which="celllist")
+        times.append(time.perf_counter() - t0)
+    return q.shape[1], times
+
+
+def run_beams(S, args, rank, world, dist):
+    """Config 3 line: unsigned float distance + closest triangle (the reference's float arithmetic,
+    SSDF_PREC_F32) at 8e6 scattered points and a 512^3 grid, one step = both sets."""
+    import torch
+
+    mesh, (pts, grid) = beams_workload(args.grid)
+    dm = S.DeviceMesh(mesh, keep_fp64=False, normals=False)
+    x, y, z = (torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in pts)
+    npts, ng = x.numel(), grid.size
+    nq = npts + ng
+    out = torch.empty(nq, dtype=torch.float32, device="cuda")
+    tri = torch.empty(nq, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    big = float(np.finfo(np.float32).max)
+
+    def step():
+        out.fill_(big)  # the in/out start value of edf (drivers/sdf.exe.cpp:330-333)
+        dm.query_points(x, y, z, out[:npts], tri[:npts], precision=S.PREC_F32, output=S.OUT_EDF, coord_type=S.F32,
+                        out_type=S.F32, stream=stream)
+        dm.query_grid(grid, out[npts:], tri[npts:], precision=S.PREC_F32, output=S.OUT_EDF, coord_type=S.F32,
+                      out_type=S.F32, stream=stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for e0, e1 in ev:
+        flush.zero_()
+        e0.record(stream)
+        step()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = [e0.elapsed_time(e1) for e0, e1 in ev]
+    t = max_over_ranks(sum(ms), dist, "cuda")
+    value = job_rate(nq, args.steps, t, world)
+    os.environ["SSDF_B200_COUNT"] = "1"
+    dm.query_points(x, y, z, out[:npts], tri[:npts], precision=S.PREC_F32, output=S.OUT_EDF, coord_type=S.F32,
+                    out_type=S.F32, stream=stream)
+    torch.cuda.synchronize()
+    c1 = S.last_query_counts()
+    dm.query_grid(grid, out[npts:], tri[npts:], precision=S.PREC_F32, output=S.OUT_EDF, coord_type=S.F32,
+                  out_type=S.F32, stream=stream)
+    torch.cuda.synchronize()
+    c2 = S.last_query_counts()
+    del os.environ["SSDF_B200_COUNT"]
+    counts = {k: c1[k] + c2[k] for k in c1}
+    flops = 79.0 * counts["triangle_tests"] + 8.0 * counts["box_tests"]
+    step_s = statistics.median(ms) * 1e-3
+    peak = S.fma_peak_tflops(False)
+    stats = dm.stats()
+    alg_bytes = npts * 12 + nq * 8 + stats["bytes"]
+    line = {
+        "metric": BEAMS_METRIC, "value": value,
+        "unit": "queries/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOADS["beams"], "queries_per_step": nq, "points": npts, "grid_nodes": ng,
+                   "triangles": mesh.nt, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "l2": "flushed between steps (256 MiB write); outputs 1.1 GB exceed L2"},
+        "gpu_launches": 3 * args.steps,
+        "roofline": {"bound": "fp32", "achieved": flops / step_s / 1e12, "peak": peak, "unit": "TFLOP/s",
+                     "frac": flops / step_s / 1e12 / peak, "traffic": None,
+                     "peak_source": "measured FP32 FMA microbenchmark on this GPU (ssdf_b200_fma_peak)",
+                     "flops_per_step": flops, "counts": counts,
+                     "hbm": {"algorithmic_bytes": alg_bytes, "achieved_gbs": alg_bytes / step_s / 1e9,
+                             "peak_gbs": _hbm_peak()}},
+        "clocks": clk,
+        "mesh": stats,
+    }
+    if not args.no_e2e:
+        # the drop-in host-array entry point on the scattered points (mesh upload + build + query + download)
+        hx, hy, hz = (np.ascontiguousarray(a) for a in pts)
+        hm = S.capi._HostMesh(mesh, np.float32)
+        hout = torch.empty(npts, dtype=torch.float32, pin_memory=True).numpy()
+        htri = torch.empty(npts, dtype=torch.int32, pin_memory=True).numpy()
+        import ctypes as C
+
+        def call():
+            hout.fill(big)
+            st = S.lib.ssdf_b200_edf_index_ff(npts, S.capi._p(hx), S.capi._p(hy), S.capi._p(hz), *hm.args(),
+                                              S.capi._p(hout), htri.ctypes.data_as(C.POINTER(C.c_int)))
+            if st != 0:
+                raise RuntimeError(S.last_error())
+
+        call()
+        t0 = time.perf_counter()
+        for _ in range(max(2, args.steps)):
+            call()
+        dt = (time.perf_counter() - t0) / max(2, args.steps)
+        line["e2e"] = {"value": npts / dt, "unit": "queries/s", "h2d_bytes_per_step": int(3 * 4 * npts),
+                       "d2h_bytes_per_step": int(8 * npts), "ms_per_call": dt * 1e3,
+                       "api": "ssdf_b200_edf_index_ff on the 8e6 points (host arrays, blocking; wall clock)"}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            n, times = cpu_reference_points(mesh, (pts, grid), min(args.cpu_sample, REF_SAMPLE), np.float32)
+            line["cpu_baseline"] = {"value": n / times[0], "unit": "queries/s", "cores": os.cpu_count(),
+                                    "kind": "reference",
+                                    "sample": f"{n} seeded queries (half points, half grid nodes), "
+                                              f"ssdf::edf_celllist<float>, oracle/_ref built from the reference's sources"}
+        except Exception as ex:
+            line["cpu_baseline"] = {"error": repr(ex)}
+    dm.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    mesh, grid = workload(args.grid)
     cores = os.cpu_count()
-    n, times = cpu_reference_rate(mesh, grid, REF_SAMPLE, steps=args.warmup + args.steps)
+    if args.workload == "beams":
+        mesh, pts = beams_workload(args.grid)
+        n, times = cpu_reference_points(mesh, pts, REF_SAMPLE, np.float32, steps=args.warmup + args.steps)
+        sample = f"{n} seeded queries of the beam-lattice set per step, ssdf::edf_celllist<float,float,int>"
+    else:
+        mesh, grid = workload(args.grid, args.workload)
+        n, times = cpu_reference_rate(mesh, grid, REF_SAMPLE, steps=args.warmup + args.steps)
+        sample = (f"{n} seeded nodes of the {args.grid}^3 grid per step, ssdf::edf_celllist<double,double,int> "
+                  f"(unsigned; the reference has no CPU signed grid sampler without cuBQL)")
     timed = times[args.warmup:]
     t = sum(timed)
     value = n * len(timed) / t
-    sample = (f"{n} seeded nodes of the 256^3 grid per step, ssdf::edf_celllist<double,double,int> "
-              f"(unsigned; the reference has no CPU signed grid sampler without cuBQL)")
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
+    line = {"impl": "reference", "metric": BEAMS_METRIC if args.workload == "beams" else METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / len(timed),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "queries_per_step": n, "parallelism": "host threads"},
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.workload == "beams" else "f64", "data": "synthetic",
+            "config": {"workload": WORKLOADS[args.workload], "queries_per_step": n, "parallelism": "host threads"},
             "cpu_baseline": {"value": value, "unit": "queries/s", "cores": cores, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -189,7 +359,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
     import ssdf_b200 as S
 
-    mesh, grid = workload(args.grid)
+    if args.workload == "beams":
+        run_beams(S, args, rank, world, dist)
+        return
+    mesh, grid = workload(args.grid, args.workload)
     nq = grid.size
     dm = S.DeviceMesh(mesh)
     stream = torch.cuda.current_stream()
@@ -244,7 +417,7 @@ def main():
         "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_x / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "queries_per_step": nq, "triangles": mesh.nt, "parallelism":
+        "config": {"workload": WORKLOADS[args.workload], "queries_per_step": nq, "triangles": mesh.nt, "parallelism":
                    f"replicas x{world}" if world > 1 else "1 GPU", "l2": "flushed between steps (256 MiB write)",
                    "precision": "FP32 traversal + FP64 fix-up (bitwise the FP64 result)"},
         "fp64_plain": {"value": fp64_value, "unit": "queries/s", "ms_per_step": t_64 / max(2, args.steps // 2),
@@ -258,8 +431,11 @@ def main():
         "clocks": clk,
         "mesh": stats,
     }
-    _attach_traffic(line)
+    if args.workload == "knot":
+        _attach_traffic(line)
 
+    if args.workload != "knot":
+        args.no_batch = args.no_serve = True
     if not args.no_batch and rank == 0:
         try:
             line["batched"] = batched_leg(S, args)

@@ -248,6 +248,10 @@ typedef struct ssdf_batch ssdf_batch;
  * arity: 0 automatic (binary), 2, 4. One arithmetic (precision) per batch. */
 int ssdf_batch_create(ssdf_batch **batch, int max_jobs, int precision, int traversal, int arity);
 int ssdf_batch_destroy(ssdf_batch *batch);
+/* Pre-sizes the batch's fix-up overflow lists for runs of up to max_queries queries in total, so
+ * that ssdf_batch_run never grows them (growing frees and allocates device memory, which waits for
+ * all work on the device). Optional; runs grow the lists themselves when needed. */
+int ssdf_batch_reserve(ssdf_batch *batch, long long max_queries, void *stream);
 /* Removes every job (the device table is rewritten on the next run). */
 int ssdf_batch_clear(ssdf_batch *batch);
 int ssdf_batch_size(const ssdf_batch *batch);

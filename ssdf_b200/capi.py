@@ -95,6 +95,7 @@ _sig("ssdf_last_query_counts", [C.POINTER(C.c_int64)] * 4)
 _sig("ssdf_b200_fma_peak", [C.c_int, C.POINTER(C.c_double)])
 _sig("ssdf_batch_create", [C.POINTER(_vp), C.c_int, C.c_int, C.c_int, C.c_int])
 _sig("ssdf_batch_destroy", [_vp])
+_sig("ssdf_batch_reserve", [_vp, C.c_longlong, _vp])
 _sig("ssdf_batch_clear", [_vp])
 _sig("ssdf_batch_size", [_vp])
 _sig("ssdf_batch_add_grid", [_vp, _vp, _pd, _pd, _pd, C.POINTER(C.c_double * 3), C.POINTER(C.c_double * 3), _vp, _ip,
@@ -157,7 +158,7 @@ EXPORTED = ["ssdf_status_string", "ssdf_last_error", "ssdf_b200_version", "ssdf_
             "ssdf_batch_last_blocks", "ssdf_query_grid_noalloc", "ssdf_query_grid_noalloc_max", "ssdf_server_create",
             "ssdf_server_destroy", "ssdf_server_add_mesh", "ssdf_server_submit_points", "ssdf_server_submit_grid",
             "ssdf_server_wait", "ssdf_server_stats", "ssdf_server_reset_stats", "ssdf_autotune_grid",
-            "ssdf_points_aabb", "ssdf_points_aabb_signed_distance"] + \
+            "ssdf_points_aabb", "ssdf_points_aabb_signed_distance", "ssdf_batch_reserve"] + \
     [f"ssdf_b200_{k}_{g}{t}" for k in ("compute_aabb", "all_points_aabb_signed_distance") for g in "fd" for t in "fd"]
 
 
@@ -464,6 +465,10 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+    def reserve(self, max_queries, stream=None):
+        """Pre-size the fix-up overflow lists for runs of up to max_queries queries."""
+        _check(lib.ssdf_batch_reserve(self._h, int(max_queries), _stream_handle(stream)), "ssdf_batch_reserve")
 
     def clear(self):
         _check(lib.ssdf_batch_clear(self._h), "ssdf_batch_clear")

@@ -36,15 +36,15 @@ struct ssdf_batch {
     BatchHeader *h_hdr = nullptr;
     QueryArgs *h_jobs = nullptr;
     long long *h_first = nullptr;
-    // captured graph for (warp, wide)
-    cudaGraphExec_t exec = nullptr;
-    int exec_key = -1;
+    // captured graphs, one per (warp, wide) key: a run reuses the graph of its key
+    cudaGraphExec_t exec[4] = {nullptr, nullptr, nullptr, nullptr};
     int sms = 0;
     long long last_total = 0;
 };
 
 static void batch_free(ssdf_batch *b) {
-    if (b->exec) cudaGraphExecDestroy(b->exec);
+    for (auto &g : b->exec)
+        if (g) cudaGraphExecDestroy(g);
     cudaFree(b->d_hdr);
     cudaFree(b->d_jobs);
     cudaFree(b->d_first);
@@ -138,6 +138,21 @@ int ssdf_batch_add_points(ssdf_batch *b, ssdf_mesh *mesh, ptrdiff_t npoints, con
     return batch_add(b, a, opts);
 }
 
+// Sizes the fix-up overflow lists for runs of up to max_queries queries, so that such runs never
+// reallocate them (a reallocation synchronises the device).
+int ssdf_batch_reserve(ssdf_batch *b, long long max_queries, void *stream_) {
+    if (!b || max_queries < 0) return fail(SSDF_ERR_INVALID_ARGUMENT, "ssdf_batch_reserve: bad arguments");
+    const size_t need = b->precision == SSDF_PREC_F32_FIXUP ? 2 * size_t(max_queries) : 0;
+    if (need <= b->fb_cap) return SSDF_OK;
+    SSDF_CUDA(cudaStreamSynchronize((cudaStream_t)stream_));
+    cudaFree(b->d_fb);
+    b->d_fb = nullptr;
+    b->fb_cap = 0;
+    SSDF_CUDA(cudaMalloc(&b->d_fb, sizeof(int) * need));
+    b->fb_cap = need;
+    return SSDF_OK;
+}
+
 // One persistent launch over every job (+ the fix-up window stage). use_graph: capture the launch
 // sequence once (per traversal mode and arity) and replay it afterwards.
 int ssdf_batch_run(ssdf_batch *b, int use_graph, void *stream_) {
@@ -158,14 +173,7 @@ int ssdf_batch_run(ssdf_batch *b, int use_graph, void *stream_) {
     size_t need = 0;
     if (b->precision == SSDF_PREC_F32_FIXUP)
         for (const auto &j : b->jobs) need += 2 * size_t(j.is_grid ? j.nx * j.ny * j.nz : j.npoints);
-    if (need > b->fb_cap) {
-        SSDF_CUDA(cudaStreamSynchronize(stream));
-        cudaFree(b->d_fb);
-        b->d_fb = nullptr;
-        b->fb_cap = 0;
-        SSDF_CUDA(cudaMalloc(&b->d_fb, sizeof(int) * need));
-        b->fb_cap = need;
-    }
+    if (need > b->fb_cap) SSDF_CHECK(ssdf_batch_reserve(b, (long long)(need / 2), stream));
     // the staging buffers may still feed the previous run's copies
     SSDF_CUDA(cudaStreamSynchronize(stream));
     long long total = 0;
@@ -213,11 +221,7 @@ int ssdf_batch_run(ssdf_batch *b, int use_graph, void *stream_) {
     };
     if (!use_graph || count) return enqueue(stream);
     const int key = (warp ? 1 : 0) | (wide ? 2 : 0);
-    if (!b->exec || b->exec_key != key) {
-        if (b->exec) {
-            cudaGraphExecDestroy(b->exec);
-            b->exec = nullptr;
-        }
+    if (!b->exec[key]) {
         cudaStream_t cap;
         SSDF_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
         cudaGraph_t g = nullptr;
@@ -227,14 +231,13 @@ int ssdf_batch_run(ssdf_batch *b, int use_graph, void *stream_) {
             st = enqueue(cap);
             e = cudaStreamEndCapture(cap, &g);
         }
-        if (e == cudaSuccess && st == SSDF_OK) e = cudaGraphInstantiate(&b->exec, g, 0);
+        if (e == cudaSuccess && st == SSDF_OK) e = cudaGraphInstantiate(&b->exec[key], g, 0);
         if (g) cudaGraphDestroy(g);
         cudaStreamDestroy(cap);
         if (st != SSDF_OK) return st;
         if (e != cudaSuccess) return cuda_fail(e, "batch graph capture", __FILE__, __LINE__);
-        b->exec_key = key;
     }
-    SSDF_CUDA(cudaGraphLaunch(b->exec, stream));
+    SSDF_CUDA(cudaGraphLaunch(b->exec[key], stream));
     return SSDF_OK;
 }
 

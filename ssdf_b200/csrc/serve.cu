@@ -11,7 +11,10 @@
 //     stream and buffers; requests that arrive while a batch runs go into the next one, whose
 //     upload and kernels overlap the previous batch's download;
 //   * completion: a second thread waits for each slot's event, copies results to the callers'
-//     buffers, stamps latencies and wakes waiters.
+//     buffers, stamps latencies and wakes waiters;
+//   * tracing: with SSDF_B200_SERVE_TRACE=<file> every batch appends one line -- its slot, request and
+//     query counts, and the times (ms since creation) its oldest request was submitted, packing
+//     began, the launch was enqueued, the GPU finished and the results were delivered.
 // Each result is computed by the same kernel as an alone query, so it is bitwise the same in any mix.
 #include <cuda_runtime.h>
 
@@ -19,6 +22,7 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
 #include <cstring>
 #include <deque>
 #include <list>
@@ -75,6 +79,9 @@ struct Slot {
     std::vector<long long> offsets;
     std::vector<int> meshes;
     bool busy = false;
+    // trace stamps of the batch in flight
+    Clock::time_point t_pack, t_launch, t_gpu;
+    long long queries = 0;
 };
 
 }  // namespace
@@ -101,6 +108,9 @@ struct ssdf_server {
     long long queries_done = 0, batches = 0, evictions = 0, builds = 0;
     Clock::time_point first_submit, last_done;
     bool any_submit = false;
+    // optional per-batch trace (SSDF_B200_SERVE_TRACE = file path): one line per batch
+    FILE *trace = nullptr;
+    Clock::time_point t0;
 };
 
 namespace {
@@ -203,6 +213,15 @@ void finish(ssdf_server *s, Slot &sl, int status) {
         auto it = s->resident.find(id);
         if (it != s->resident.end()) it->second.pins--;
     }
+    if (s->trace) {
+        auto ms = [&](Clock::time_point t) { return std::chrono::duration<double, std::milli>(t - s->t0).count(); };
+        Clock::time_point oldest = now;
+        for (auto &rp : sl.reqs) oldest = std::min(oldest, rp->submitted);
+        fprintf(s->trace, "slot %d reqs %zu queries %lld oldest_submit %.3f pack %.3f launched %.3f gpu_done %.3f "
+                          "delivered %.3f\n",
+                int(&sl - s->slots), sl.reqs.size(), sl.queries, ms(oldest), ms(sl.t_pack), ms(sl.t_launch),
+                ms(sl.t_gpu), ms(Clock::now()));
+    }
     evict_over_budget(s, -1);
     s->last_done = now;
     sl.reqs.clear();
@@ -225,6 +244,7 @@ void scheduler_loop(ssdf_server *s) {
         if (s->stop) return;
         Slot &sl = !s->slots[0].busy ? s->slots[0] : s->slots[1];
         const int slot_index = &sl == &s->slots[0] ? 0 : 1;
+        sl.t_pack = Clock::now();
         // pack waiting requests (FIFO) up to the query and job budgets
         long long used = 0, used_pts = 0;
         while (!s->pending.empty() && int(sl.reqs.size()) < s->opts.max_batch_jobs) {
@@ -289,6 +309,8 @@ void scheduler_loop(ssdf_server *s) {
             e = cudaMemcpyAsync(sl.h_tri, sl.d_tri, sizeof(int) * size_t(used), cudaMemcpyDeviceToHost, sl.stream);
         if (st == SSDF_OK && e == cudaSuccess) e = cudaEventRecord(sl.event, sl.stream);
         if (e != cudaSuccess && st == SSDF_OK) st = cuda_fail(e, "serving batch", __FILE__, __LINE__);
+        sl.t_launch = Clock::now();
+        sl.queries = used;
         lock.lock();
         s->batches++;
         if (st != SSDF_OK) {
@@ -314,6 +336,7 @@ void completer_loop(ssdf_server *s) {
         }
         Slot &sl = s->slots[idx];
         const cudaError_t e = cudaEventSynchronize(sl.event);
+        sl.t_gpu = Clock::now();
         finish(s, sl, e == cudaSuccess ? SSDF_OK : SSDF_ERR_CUDA);
     }
 }
@@ -345,11 +368,15 @@ int ssdf_server_create(ssdf_server **out, const ssdf_server_opts *opts) {
         if (e == cudaSuccess) e = cudaMallocHost(&sl.h_tri, sizeof(int) * cap);
         if (e != cudaSuccess) st = cuda_fail(e, "ssdf_server_create", __FILE__, __LINE__);
         if (st == SSDF_OK) st = ssdf_batch_create(&sl.batch, opts->max_batch_jobs, opts->precision, 0, 0);
+        // overflow lists sized once: a run that grew them would wait for the other slot's batch
+        if (st == SSDF_OK) st = ssdf_batch_reserve(sl.batch, (long long)cap, sl.stream);
     }
     if (st != SSDF_OK) {
         ssdf_server_destroy(s);
         return st;
     }
+    s->t0 = Clock::now();
+    if (const char *tp = env_str("SSDF_B200_SERVE_TRACE")) s->trace = fopen(tp, "w");
     s->scheduler = std::thread(scheduler_loop, s);
     s->completer = std::thread(completer_loop, s);
     *out = s;
@@ -380,6 +407,7 @@ int ssdf_server_destroy(ssdf_server *s) {
         if (sl.stream) cudaStreamDestroy(sl.stream);
     }
     if (s->build_stream) cudaStreamDestroy(s->build_stream);
+    if (s->trace) fclose(s->trace);
     delete s;
     return SSDF_OK;
 }

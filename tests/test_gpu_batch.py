@@ -123,3 +123,30 @@ def test_batch_rejects_mixed_precision(jobs):
                                            out.data_ptr(), None, S.C.byref(o)), "ssdf_batch_add_grid")
     b.close()
     bad.close()
+
+
+def test_alternating_graph_keys_after_reserve(jobs):
+    """Point-only runs (thread traversal) alternating with grid runs (warp packets): each key keeps its
+    own captured graph, and lists reserved up front are large enough for every run."""
+    import torch
+
+    b = S.Batch(16, S.PREC_F32_FIXUP)
+    b.reserve(sum(j["grid"].size for j in jobs))
+    pts = torch.tensor(oracle.grid_points(jobs[1]["grid"]), dtype=torch.float64, device="cuda")
+    for rep in range(3):
+        b.clear()
+        if rep % 2 == 0:
+            out = torch.empty(pts.shape[1], dtype=torch.float64, device="cuda")
+            tri = torch.empty(pts.shape[1], dtype=torch.int32, device="cuda")
+            b.add_points(jobs[1]["dm"], pts[0].contiguous(), pts[1].contiguous(), pts[2].contiguous(), out, tri)
+            want = jobs[1]
+        else:
+            out = torch.empty(jobs[3]["grid"].size, dtype=torch.float64, device="cuda")
+            tri = torch.empty(jobs[3]["grid"].size, dtype=torch.int32, device="cuda")
+            b.add_grid(jobs[3]["dm"], jobs[3]["grid"], out, tri)
+            want = jobs[3]
+        b.run(use_graph=True)
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy(), want["alone"])
+        assert np.array_equal(tri.cpu().numpy(), want["alone_tri"])
+    b.close()
