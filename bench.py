@@ -554,7 +554,7 @@ def serving_leg(S, args):
     for mid in range(len(sets)):
         srv.wait(srv.submit_points(ids[mid], np.zeros((3, 1))))
     out = {"meshes": len(sets), "payloads": len(payloads), "seconds_per_rate": args.serve_seconds, "rates": []}
-    for lam in (50.0, 200.0, 800.0):
+    for lam in (50.0, 200.0, 800.0, 3200.0):
         srv.reset_stats()
         tickets = []
         t_end = time.perf_counter() + args.serve_seconds

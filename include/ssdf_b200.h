@@ -296,6 +296,7 @@ typedef struct {
     int max_batch_jobs;    /* requests packed into one batch                                   */
     int precision;         /* SSDF_PREC_F32_FIXUP or SSDF_PREC_F64                             */
     int leaf_size;         /* BVH leaf size of resident meshes (0: default)                    */
+    int slots;             /* batches in flight at once, 1..16 (0: 4); each holds its buffers  */
 } ssdf_server_opts;
 
 typedef struct {
@@ -306,8 +307,9 @@ typedef struct {
     double seconds;                       /* first submit -> last completion                   */
 } ssdf_server_report;
 
-/* A scheduler thread packs waiting requests into one persistent batch launch per free slot (two
- * slots, so a batch's upload and kernels overlap the previous one's download); results are
+/* A scheduler thread packs waiting requests into one persistent batch launch per free slot (several
+ * slots, so one batch's upload, kernels and download overlap the others' and a batch's slow tail
+ * leaves the SMs to the next); one completer thread per slot delivers its results. Results are
  * signed distances (double) and closest triangles written to the caller's HOST buffers. */
 int ssdf_server_create(ssdf_server **server, const ssdf_server_opts *opts);
 int ssdf_server_destroy(ssdf_server *server);

@@ -117,7 +117,7 @@ _sig("ssdf_points_aabb_signed_distance", [_pd, _vp, _vp, _vp, C.c_int, C.POINTER
 
 class ServerOpts(C.Structure):
     _fields_ = [("memory_budget", C.c_size_t), ("max_batch_queries", C.c_int), ("max_batch_jobs", C.c_int),
-                ("precision", C.c_int), ("leaf_size", C.c_int)]
+                ("precision", C.c_int), ("leaf_size", C.c_int), ("slots", C.c_int)]
 
 
 class ServerStats(C.Structure):
@@ -505,10 +505,10 @@ class Server:
     """Continuous-batching request loop over resident meshes (host arrays in and out)."""
 
     def __init__(self, memory_budget=120 << 30, max_batch_queries=1 << 22, max_batch_jobs=64,
-                 precision=PREC_F32_FIXUP, leaf_size=0):
+                 precision=PREC_F32_FIXUP, leaf_size=0, slots=0):
         self._h = C.c_void_p()
         o = ServerOpts(int(memory_budget), int(max_batch_queries), int(max_batch_jobs), int(precision),
-                       int(leaf_size))
+                       int(leaf_size), int(slots))
         _check(lib.ssdf_server_create(C.byref(self._h), C.byref(o)), "ssdf_server_create")
         self._inflight = {}
 

@@ -7,11 +7,12 @@
 //     no in-flight batch holds are evicted (and rebuilt if asked for again);
 //   * continuous batching: a scheduler thread packs the requests that are waiting into one batch
 //     (ssdf_batch_* -- one persistent launch, replayed as a CUDA graph) up to a query budget, stages
-//     the point lists through pinned memory, and launches it on one of two slots, each with its own
-//     stream and buffers; requests that arrive while a batch runs go into the next one, whose
-//     upload and kernels overlap the previous batch's download;
-//   * completion: a second thread waits for each slot's event, copies results to the callers'
-//     buffers, stamps latencies and wakes waiters;
+//     the point lists through pinned memory, and launches it on a free slot (4 by default), each
+//     with its own stream and buffers; requests that arrive while batches run go into the next
+//     one, whose upload and kernels overlap the others' (a batch whose last packets still walk
+//     leaves the rest of the GPU to the next batch);
+//   * completion: one thread per slot waits for that slot's event, copies results to the callers'
+//     buffers, stamps latencies and wakes waiters, so no batch waits behind a slower one;
 //   * tracing: with SSDF_B200_SERVE_TRACE=<file> every batch appends one line -- its slot, request and
 //     query counts, and the times (ms since creation) its oldest request was submitted, packing
 //     began, the launch was enqueued, the GPU finished and the results were delivered.
@@ -78,7 +79,8 @@ struct Slot {
     std::vector<std::shared_ptr<Request>> reqs;
     std::vector<long long> offsets;
     std::vector<int> meshes;
-    bool busy = false;
+    bool busy = false;      // packed or in flight
+    bool inflight = false;  // launched; its completer waits on the event
     // trace stamps of the batch in flight
     Clock::time_point t_pack, t_launch, t_gpu;
     long long queries = 0;
@@ -97,12 +99,12 @@ struct ssdf_server {
     std::deque<std::shared_ptr<Request>> pending;
     std::unordered_map<long long, std::shared_ptr<Request>> tickets;
     long long next_ticket = 1;
-    Slot slots[2];
-    std::thread scheduler, completer;
+    std::vector<Slot> slots;
+    std::thread scheduler;
+    std::vector<std::thread> completers;  // one per slot
     cudaStream_t build_stream = nullptr;  // mesh builds, apart from the two batch slots
     bool stop = false;
     int device = 0;
-    std::deque<int> launched;  // slot order of in-flight batches
     // stats
     std::vector<double> latencies_ms;
     long long queries_done = 0, batches = 0, evictions = 0, builds = 0;
@@ -219,7 +221,7 @@ void finish(ssdf_server *s, Slot &sl, int status) {
         for (auto &rp : sl.reqs) oldest = std::min(oldest, rp->submitted);
         fprintf(s->trace, "slot %d reqs %zu queries %lld oldest_submit %.3f pack %.3f launched %.3f gpu_done %.3f "
                           "delivered %.3f\n",
-                int(&sl - s->slots), sl.reqs.size(), sl.queries, ms(oldest), ms(sl.t_pack), ms(sl.t_launch),
+                int(&sl - s->slots.data()), sl.reqs.size(), sl.queries, ms(oldest), ms(sl.t_pack), ms(sl.t_launch),
                 ms(sl.t_gpu), ms(Clock::now()));
     }
     evict_over_budget(s, -1);
@@ -228,6 +230,7 @@ void finish(ssdf_server *s, Slot &sl, int status) {
     sl.offsets.clear();
     sl.meshes.clear();
     sl.busy = false;
+    sl.inflight = false;
     s->cv_done.notify_all();
     s->cv_slot.notify_all();
     s->cv_work.notify_all();
@@ -238,12 +241,14 @@ void scheduler_loop(ssdf_server *s) {
     const long long cap = s->opts.max_batch_queries;
     while (true) {
         std::unique_lock<std::mutex> lock(s->mu);
-        s->cv_work.wait(lock, [&] {
-            return s->stop || (!s->pending.empty() && (!s->slots[0].busy || !s->slots[1].busy));
-        });
+        auto free_slot = [&]() -> Slot * {
+            for (auto &x : s->slots)
+                if (!x.busy) return &x;
+            return nullptr;
+        };
+        s->cv_work.wait(lock, [&] { return s->stop || (!s->pending.empty() && free_slot()); });
         if (s->stop) return;
-        Slot &sl = !s->slots[0].busy ? s->slots[0] : s->slots[1];
-        const int slot_index = &sl == &s->slots[0] ? 0 : 1;
+        Slot &sl = *free_slot();
         sl.t_pack = Clock::now();
         // pack waiting requests (FIFO) up to the query and job budgets
         long long used = 0, used_pts = 0;
@@ -318,23 +323,21 @@ void scheduler_loop(ssdf_server *s) {
             finish(s, sl, st);
             continue;
         }
-        s->launched.push_back(slot_index);
+        sl.inflight = true;
         s->cv_slot.notify_all();
     }
 }
 
-void completer_loop(ssdf_server *s) {
+// Delivers the batches of one slot: waits for its launch, then for its event.
+void completer_loop(ssdf_server *s, int idx) {
     cudaSetDevice(s->device);
+    Slot &sl = s->slots[idx];
     while (true) {
-        int idx;
         {
             std::unique_lock<std::mutex> lock(s->mu);
-            s->cv_slot.wait(lock, [&] { return s->stop || !s->launched.empty(); });
-            if (s->launched.empty()) return;
-            idx = s->launched.front();
-            s->launched.pop_front();
+            s->cv_slot.wait(lock, [&] { return s->stop || sl.inflight; });
+            if (!sl.inflight) return;
         }
-        Slot &sl = s->slots[idx];
         const cudaError_t e = cudaEventSynchronize(sl.event);
         sl.t_gpu = Clock::now();
         finish(s, sl, e == cudaSuccess ? SSDF_OK : SSDF_ERR_CUDA);
@@ -353,10 +356,15 @@ int ssdf_server_create(ssdf_server **out, const ssdf_server_opts *opts) {
     s->opts = *opts;
     cudaGetDevice(&s->device);
     const size_t cap = size_t(opts->max_batch_queries);
+    if (opts->slots < 0 || opts->slots > 16) {
+        delete s;
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "ssdf_server_create: slots must be 0 (default 4) or 1..16");
+    }
+    s->slots = std::vector<Slot>(opts->slots ? opts->slots : 4);
     int st = SSDF_OK;
     if (cudaStreamCreateWithFlags(&s->build_stream, cudaStreamNonBlocking) != cudaSuccess)
         st = fail(SSDF_ERR_CUDA, "ssdf_server_create: build stream");
-    for (int k = 0; k < 2 && st == SSDF_OK; k++) {
+    for (size_t k = 0; k < s->slots.size() && st == SSDF_OK; k++) {
         Slot &sl = s->slots[k];
         cudaError_t e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.event, cudaEventDisableTiming);
@@ -378,7 +386,7 @@ int ssdf_server_create(ssdf_server **out, const ssdf_server_opts *opts) {
     s->t0 = Clock::now();
     if (const char *tp = env_str("SSDF_B200_SERVE_TRACE")) s->trace = fopen(tp, "w");
     s->scheduler = std::thread(scheduler_loop, s);
-    s->completer = std::thread(completer_loop, s);
+    for (int k = 0; k < int(s->slots.size()); k++) s->completers.emplace_back(completer_loop, s, k);
     *out = s;
     return SSDF_OK;
 }
@@ -392,7 +400,8 @@ int ssdf_server_destroy(ssdf_server *s) {
     s->cv_work.notify_all();
     s->cv_slot.notify_all();
     if (s->scheduler.joinable()) s->scheduler.join();
-    if (s->completer.joinable()) s->completer.join();
+    for (auto &t : s->completers)
+        if (t.joinable()) t.join();
     cudaDeviceSynchronize();
     for (auto &kv : s->resident) ssdf_mesh_destroy(kv.second.mesh);
     for (auto &sl : s->slots) {

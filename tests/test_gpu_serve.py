@@ -111,3 +111,21 @@ def test_rejects_oversized_and_unknown():
     with pytest.raises(S.SsdfError):
         srv.submit_points(mid + 5, np.zeros((3, 10)))
     srv.close()
+    with pytest.raises(S.SsdfError):
+        S.Server(slots=17)
+
+
+@pytest.mark.parametrize("slots", [1, 2, 6])
+def test_slot_counts_give_the_same_results(slots):
+    ms = meshes()[:3]
+    reqs = requests(ms, seed=4)[:12]
+    want = [alone(ms, r) for r in reqs]
+    srv = S.Server(max_batch_queries=1 << 18, max_batch_jobs=4, slots=slots)
+    ids = [srv.add_mesh(m) for m in ms]
+    tickets = [srv.submit_grid(ids[mid], q) if kind == "grid" else srv.submit_points(ids[mid], q)
+               for kind, mid, q in reqs]
+    for t, (wd, wtri) in zip(tickets, want):
+        d, tri = srv.wait(t)
+        assert np.array_equal(d, wd) and np.array_equal(tri, wtri)
+    assert srv.stats()["completed"] == len(reqs)
+    srv.close()
