@@ -61,7 +61,7 @@ def parse_args():
     p.add_argument("--no-batch", action="store_true", help="skip the 256-mesh batched leg")
     p.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     p.add_argument("--batch-meshes", type=int, default=256)
-    p.add_argument("--serve-meshes", type=int, default=128)
+    p.add_argument("--serve-meshes", type=int, default=512)
     p.add_argument("--serve-seconds", type=float, default=3.0)
     a = p.parse_args()
     if a.grid is None:
