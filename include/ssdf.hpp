@@ -1,7 +1,8 @@
 // ssdf.hpp -- the reference's C++ template API (namespace ssdf), served by the B200 library.
 //
 // A drop-in for zulianp/ssdf's serial/ssdf.hpp (edf, edf_celllist, edf_select) and
-// serial/bvh/bvh.hpp (edf_bvh, closest_point_bvh, sample_sqedf_bvh, sample_sdf_bvh): same names,
+// serial/bvh/bvh.hpp (edf_bvh, closest_point_bvh, sample_sqedf_bvh, sample_sdf_bvh) and the grid
+// helpers of serial/edf/edf.hpp (compute_aabb, all_points_aabb_signed_distance): same names,
 // template parameters <G coordinates, T outputs, I indices>, argument order, in/out semantics and
 // int return (0 on success). Each instantiation the reference provides maps onto one C symbol of
 // libssdf_b200.so (include/ssdf_b200.h); other type combinations do not compile.
@@ -142,6 +143,44 @@ int sample_sdf_bvh(SSDF_B200_GRID_SIG(G, T)) {
 #undef SSDF_B200_EDF_PASS
 #undef SSDF_B200_GRID_SIG
 #undef SSDF_B200_GRID_PASS
+
+// serial/edf/edf.hpp:500-539. The reference returns void; this returns the status (a discarded
+// int return compiles at the same call sites).
+template <typename G, typename T>
+int compute_aabb(const ptrdiff_t npoints, const G *const SSDF_RESTRICT x, const G *const SSDF_RESTRICT y,
+                 const G *const SSDF_RESTRICT z, T *const SSDF_RESTRICT xmin, T *const SSDF_RESTRICT xmax,
+                 T *const SSDF_RESTRICT ymin, T *const SSDF_RESTRICT ymax, T *const SSDF_RESTRICT zmin,
+                 T *const SSDF_RESTRICT zmax) {
+    if constexpr (std::is_same<G, float>::value && std::is_same<T, float>::value)
+        return ssdf_b200_compute_aabb_ff(npoints, x, y, z, xmin, xmax, ymin, ymax, zmin, zmax);
+    else if constexpr (std::is_same<G, float>::value && std::is_same<T, double>::value)
+        return ssdf_b200_compute_aabb_fd(npoints, x, y, z, xmin, xmax, ymin, ymax, zmin, zmax);
+    else if constexpr (std::is_same<G, double>::value && std::is_same<T, float>::value)
+        return ssdf_b200_compute_aabb_df(npoints, x, y, z, xmin, xmax, ymin, ymax, zmin, zmax);
+    else if constexpr (std::is_same<G, double>::value && std::is_same<T, double>::value)
+        return ssdf_b200_compute_aabb_dd(npoints, x, y, z, xmin, xmax, ymin, ymax, zmin, zmax);
+    else
+        static_assert(detail::always_false<G, T>::value, "compute_aabb: G and T are float or double");
+}
+
+// serial/edf/edf.hpp:541-557 (void in the reference; the status here, as compute_aabb).
+template <typename G, typename T>
+int all_points_aabb_signed_distance(const ptrdiff_t npoints, const G *const SSDF_RESTRICT x,
+                                    const G *const SSDF_RESTRICT y, const G *const SSDF_RESTRICT z, const T minx,
+                                    const T maxx, const T miny, const T maxy, const T minz, const T maxz,
+                                    T *const SSDF_RESTRICT out) {
+    if constexpr (std::is_same<G, float>::value && std::is_same<T, float>::value)
+        return ssdf_b200_all_points_aabb_signed_distance_ff(npoints, x, y, z, minx, maxx, miny, maxy, minz, maxz, out);
+    else if constexpr (std::is_same<G, float>::value && std::is_same<T, double>::value)
+        return ssdf_b200_all_points_aabb_signed_distance_fd(npoints, x, y, z, minx, maxx, miny, maxy, minz, maxz, out);
+    else if constexpr (std::is_same<G, double>::value && std::is_same<T, float>::value)
+        return ssdf_b200_all_points_aabb_signed_distance_df(npoints, x, y, z, minx, maxx, miny, maxy, minz, maxz, out);
+    else if constexpr (std::is_same<G, double>::value && std::is_same<T, double>::value)
+        return ssdf_b200_all_points_aabb_signed_distance_dd(npoints, x, y, z, minx, maxx, miny, maxy, minz, maxz, out);
+    else
+        static_assert(detail::always_false<G, T>::value,
+                      "all_points_aabb_signed_distance: G and T are float or double");
+}
 
 }  // namespace ssdf
 

@@ -51,6 +51,8 @@ def test_cpp_header_compiles_against_c_abi(tmp_path):
         "  (void)ssdf::closest_point_bvh<double, double, int>;\n"
         "  (void)ssdf::sample_sdf_bvh<float, float, int>;\n"
         "  (void)ssdf::sample_sqedf_bvh<double, double, int>;\n"
+        "  (void)ssdf::compute_aabb<float, double>;\n"
+        "  (void)ssdf::all_points_aabb_signed_distance<double, double>;\n"
         "  return 0;\n}\n")
     lib = os.path.join(ROOT, "ssdf_b200", "_lib")
     res = subprocess.run(["g++", "-std=c++17", f"-I{ROOT}/include", str(src), "-o", str(tmp_path / "use"),
