@@ -54,7 +54,27 @@ def build(verbose: bool = False) -> str:
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stderr}")
+    _build_cli(verbose)
     return LIB
+
+
+CLI_SRC = os.path.join(HERE, "cli", "ssdf_sdf.cpp")
+CLI = os.path.join(OUT_DIR, "ssdf_sdf")
+
+
+def _build_cli(verbose: bool) -> str:
+    """The command-line driver (drivers/sdf.exe.cpp's arguments and files) over the library."""
+    deps = [CLI_SRC, LIB, os.path.join(HERE, "..", "include", "ssdf_b200.h")]
+    if os.path.exists(CLI) and all(os.path.getmtime(CLI) >= os.path.getmtime(d) for d in deps):
+        return CLI
+    cmd = [NVCC, "-O2", "-std=c++17", "-I", os.path.join(HERE, "..", "include"), CLI_SRC, "-o", CLI,
+           "-L", OUT_DIR, "-lssdf_b200", "-Xlinker", "-rpath,$ORIGIN"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"nvcc failed on {CLI_SRC}:\n{res.stderr}")
+    if verbose and res.stderr:
+        sys.stderr.write(res.stderr)
+    return CLI
 
 
 if __name__ == "__main__":
