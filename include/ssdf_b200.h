@@ -158,6 +158,43 @@ int ssdf_b200_all_points_aabb_signed_distance_dd(ptrdiff_t npoints, const double
                                                  const double *z, double minx, double maxx, double miny,
                                                  double maxy, double minz, double maxz, double *out);
 
+/* ---- drop-in: level sets and field rebuilds (serial/bvh/sdf_rebuild.hpp) ---------------------
+ * A grid is ssdf::GridGeometry<G> (sdf_rebuild.hpp:10-21) as three arrays: n[3] samples along each
+ * axis at o[d] + i h[d], x fastest. Host arrays, blocking. */
+
+/* ssdf::level_set_triangles (sdf_rebuild.hpp:23-37): the triangles of {f = level} by marching
+ * tetrahedra (six per cell about the corner-0-to-7 diagonal; crossings interpolated from the lower
+ * grid index; triangles with two vertices equal in G dropped), in the reference's order, each
+ * vertex bitwise its value. *ntriangles receives the count; with x non-null and capacity >= count
+ * the soup (three vertices per triangle) is written to x, y, z [3 * count]. */
+int ssdf_b200_level_set_triangles_ff(const ptrdiff_t n[3], const float o[3], const float h[3], const float *f,
+                                     float level, ptrdiff_t capacity, float *x, float *y, float *z,
+                                     ptrdiff_t *ntriangles);
+int ssdf_b200_level_set_triangles_dd(const ptrdiff_t n[3], const double o[3], const double h[3], const double *f,
+                                     double level, ptrdiff_t capacity, double *x, double *y, double *z,
+                                     ptrdiff_t *ntriangles);
+/* ssdf::rebuild_sdf (sdf_rebuild.hpp:38-50, sdf_rebuild.cpp:252-299): out[strided(stride).size()] =
+ * sign(f - level) * min(band, distance to those triangles), 0 on the level set; samples with
+ * |f - level| >= band get +-band unsearched. The distance is the double one from the sample (the
+ * reference searches in float with cuBQL from the float-rounded sample). */
+int ssdf_b200_rebuild_sdf_ff(const ptrdiff_t n[3], const float o[3], const float h[3], const float *f, float level,
+                             float band, ptrdiff_t stride, float *out);
+int ssdf_b200_rebuild_sdf_dd(const ptrdiff_t n[3], const double o[3], const double h[3], const double *f,
+                             double level, double band, ptrdiff_t stride, double *out);
+/* ssdf::refine_field (sdf_rebuild.hpp:52-56): fine[refined(factor).size()], the cubic through the four
+ * nearest samples along each axis in turn, bitwise the reference's double arithmetic. */
+int ssdf_b200_refine_field_ff(const ptrdiff_t n[3], const float o[3], const float h[3], const float *f,
+                              ptrdiff_t factor, float *fine);
+int ssdf_b200_refine_field_dd(const ptrdiff_t n[3], const double o[3], const double h[3], const double *f,
+                              ptrdiff_t factor, double *fine);
+/* ssdf::round_sdf (sdf_rebuild.hpp:57-78): the region f > 0 rounded by radius (opening and / or
+ * closing, each a rebuild), its signed distance on every stride-th sample; f0 (may be NULL) gets
+ * the first rebuild R(f, 0) on the full grid. */
+int ssdf_b200_round_sdf_ff(const ptrdiff_t n[3], const float o[3], const float h[3], const float *f, float radius,
+                           float band, int open, int close, ptrdiff_t stride, float *out, float *f0);
+int ssdf_b200_round_sdf_dd(const ptrdiff_t n[3], const double o[3], const double h[3], const double *f, double radius,
+                           double band, int open, int close, ptrdiff_t stride, double *out, double *f0);
+
 /* ---- additive entry points (no reference counterpart; patterned on closest_point_bvh) -------- */
 
 /* Unsigned distance (in/out, as edf_bvh) plus the closest triangle, written where it improves. */
@@ -217,7 +254,11 @@ typedef struct {
 int ssdf_mesh_create(ssdf_mesh **mesh, ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
                      ptrdiff_t nspoints, const void *sx, const void *sy, const void *sz, int coord_type,
                      int device_ptrs, const ssdf_build_opts *opts, void *stream);
+/* Frees the mesh after waiting for all work on its device (queries on any stream may still read it). */
 int ssdf_mesh_destroy(ssdf_mesh *mesh);
+/* Frees the mesh in stream order: after the work already queued on `stream`, without waiting. Only
+ * for a mesh whose queries were all queued on that stream. */
+int ssdf_mesh_destroy_async(ssdf_mesh *mesh, void *stream);
 /* BVH statistics: nodes, leaves, depth, bytes resident on the device. */
 int ssdf_mesh_stats(const ssdf_mesh *mesh, int64_t *nodes, int64_t *leaves, int64_t *depth, int64_t *bytes);
 

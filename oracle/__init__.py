@@ -78,6 +78,17 @@ def lib() -> C.CDLL:
             f = getattr(_lib, "oracle_grid_points" + suf)
             f.restype = None
             f.argtypes = [_pd, _pd, _pd] + [ft] * 6 + [_dp, _dp, _dp]
+        for suf, fptr, ft in (("_d", _dp, C.c_double), ("_f", _fp, C.c_float)):
+            n3 = C.POINTER(C.c_ssize_t)
+            f = getattr(_lib, "oracle_level_set_triangles" + suf)
+            f.restype = C.c_ssize_t
+            f.argtypes = [n3, fptr, fptr, fptr, ft, fptr, fptr, fptr]
+            f = getattr(_lib, "oracle_refine_field" + suf)
+            f.restype = None
+            f.argtypes = [n3, fptr, C.c_ssize_t, fptr]
+            f = getattr(_lib, "oracle_rebuild_sdf" + suf)
+            f.restype = None
+            f.argtypes = [n3, fptr, fptr, fptr, ft, ft, C.c_ssize_t, fptr]
         _lib.oracle_pseudonormals_d.restype = C.c_int
         _lib.oracle_pseudonormals_d.argtypes = [_pd, _ip, _ip, _ip, _pd, _dp, _dp, _dp, _dp, _dp, _dp]
         _lib.oracle_sdf_points_d.restype = C.c_int
@@ -263,3 +274,55 @@ def all_points_aabb_signed_distance(points, box, dtype=np.float64, reference=Fal
     getattr(ref() if reference else lib(), fn)(len(x), _ptr(x, ct), _ptr(y, ct), _ptr(z, ct), _ptr(b, ct),
                                                _ptr(out, ct))
     return out
+
+
+# ---- level sets (serial/bvh/sdf_rebuild.cpp) -----------------------------------------------------
+
+def _grid_args(n, o, h, dtype):
+    ct, suf = _real(dtype)
+    na = (C.c_ssize_t * 3)(*[int(v) for v in n])
+    oa = np.ascontiguousarray(o, dtype=dtype)
+    ha = np.ascontiguousarray(h, dtype=dtype)
+    return ct, suf, na, oa, ha
+
+
+def level_set_triangles(n, o, h, f, level, dtype=np.float64):
+    """The oracle's marching-tetrahedra soup (3, 3 * ntri) of {f = level}."""
+    ct, suf, na, oa, ha = _grid_args(n, o, h, dtype)
+    fa = np.ascontiguousarray(f, dtype=dtype)
+    fn = getattr(lib(), "oracle_level_set_triangles" + suf)
+    nt = fn(na, _ptr(oa, ct), _ptr(ha, ct), _ptr(fa, ct), dtype(level), None, None, None)
+    x, y, z = (np.empty(3 * nt, dtype=dtype) for _ in range(3))
+    fn(na, _ptr(oa, ct), _ptr(ha, ct), _ptr(fa, ct), dtype(level), _ptr(x, ct), _ptr(y, ct), _ptr(z, ct))
+    return np.stack([x, y, z])
+
+
+def refine_field(n, f, factor, dtype=np.float64):
+    ct, suf, na, _, _ = _grid_args(n, (0, 0, 0), (0, 0, 0), dtype)
+    fa = np.ascontiguousarray(f, dtype=dtype)
+    rn = [(int(v) - 1) * factor + 1 for v in n]
+    fine = np.empty(rn[0] * rn[1] * rn[2], dtype=dtype)
+    getattr(lib(), "oracle_refine_field" + suf)(na, _ptr(fa, ct), int(factor), _ptr(fine, ct))
+    return fine
+
+
+def rebuild_sdf(n, o, h, f, level, band, stride=1, dtype=np.float64):
+    ct, suf, na, oa, ha = _grid_args(n, o, h, dtype)
+    fa = np.ascontiguousarray(f, dtype=dtype)
+    on = [(int(v) - 1) // stride + 1 for v in n]
+    out = np.empty(on[0] * on[1] * on[2], dtype=dtype)
+    getattr(lib(), "oracle_rebuild_sdf" + suf)(na, _ptr(oa, ct), _ptr(ha, ct), _ptr(fa, ct), dtype(level),
+                                               dtype(band), int(stride), _ptr(out, ct))
+    return out
+
+
+def round_sdf(n, o, h, f, radius, band, open=True, close=True, stride=1, dtype=np.float64):
+    """serial/bvh/sdf_rebuild.cpp:300-336 composed from the oracle's rebuilds (shifts in REAL)."""
+    t = np.dtype(dtype).type
+    r0 = rebuild_sdf(n, o, h, f, 0, band, 1, dtype)
+    cur = r0
+    if open:
+        cur = (rebuild_sdf(n, o, h, cur, radius, band, 1, dtype) + t(radius)).astype(dtype)
+    if close:
+        cur = (rebuild_sdf(n, o, h, cur, -t(radius), band, 1, dtype) - t(radius)).astype(dtype)
+    return rebuild_sdf(n, o, h, cur, 0, band, stride, dtype), r0

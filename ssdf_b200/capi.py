@@ -87,6 +87,7 @@ _sig("ssdf_b200_sample_sdf_index_bvh_dd", _GRID + [C.c_double] * 6 + [_vp, _ip])
 _sig("ssdf_mesh_create", [C.POINTER(_vp), _pd, _ip, _ip, _ip, _pd, _vp, _vp, _vp, C.c_int, C.c_int,
                           C.POINTER(BuildOpts), _vp])
 _sig("ssdf_mesh_destroy", [_vp])
+_sig("ssdf_mesh_destroy_async", [_vp, _vp])
 _sig("ssdf_mesh_stats", [_vp] + [C.POINTER(C.c_int64)] * 4)
 _sig("ssdf_query_points", [_vp, _pd, _vp, _vp, _vp, _vp, _ip, _vp, _vp, _vp, C.POINTER(QueryOpts), _vp])
 _sig("ssdf_query_grid", [_vp, _pd, _pd, _pd, C.POINTER(C.c_double * 3), C.POINTER(C.c_double * 3), _vp, _ip,
@@ -111,6 +112,12 @@ for _g, _gc in (("f", C.c_float), ("d", C.c_double)):
         _sig(f"ssdf_b200_compute_aabb_{_g}{_t}", [_pd, _vp, _vp, _vp] + [C.POINTER(_tc)] * 6)
         _sig(f"ssdf_b200_all_points_aabb_signed_distance_{_g}{_t}", [_pd, _vp, _vp, _vp] + [_tc] * 6 + [_vp])
 _sig("ssdf_points_aabb", [_pd, _vp, _vp, _vp, C.c_int, C.c_int, _vp, _vp])
+for _g, _gc in (("ff", C.c_float), ("dd", C.c_double)):
+    _GP = [C.POINTER(C.c_ssize_t * 3), C.POINTER(_gc * 3), C.POINTER(_gc * 3), _vp]
+    _sig(f"ssdf_b200_level_set_triangles_{_g}", _GP + [_gc, _pd, _vp, _vp, _vp, C.POINTER(C.c_ssize_t)])
+    _sig(f"ssdf_b200_rebuild_sdf_{_g}", _GP + [_gc, _gc, _pd, _vp])
+    _sig(f"ssdf_b200_refine_field_{_g}", _GP + [_pd, _vp])
+    _sig(f"ssdf_b200_round_sdf_{_g}", _GP + [_gc, _gc, C.c_int, C.c_int, _pd, _vp, _vp])
 _sig("ssdf_points_aabb_signed_distance", [_pd, _vp, _vp, _vp, C.c_int, C.POINTER(C.c_double * 6), C.c_int, _vp,
                                           C.c_int, _vp])
 
@@ -158,8 +165,9 @@ EXPORTED = ["ssdf_status_string", "ssdf_last_error", "ssdf_b200_version", "ssdf_
             "ssdf_batch_last_blocks", "ssdf_query_grid_noalloc", "ssdf_query_grid_noalloc_max", "ssdf_server_create",
             "ssdf_server_destroy", "ssdf_server_add_mesh", "ssdf_server_submit_points", "ssdf_server_submit_grid",
             "ssdf_server_wait", "ssdf_server_stats", "ssdf_server_reset_stats", "ssdf_autotune_grid",
-            "ssdf_points_aabb", "ssdf_points_aabb_signed_distance", "ssdf_batch_reserve"] + \
-    [f"ssdf_b200_{k}_{g}{t}" for k in ("compute_aabb", "all_points_aabb_signed_distance") for g in "fd" for t in "fd"]
+            "ssdf_points_aabb", "ssdf_points_aabb_signed_distance", "ssdf_batch_reserve", "ssdf_mesh_destroy_async"] + \
+    [f"ssdf_b200_{k}_{g}{t}" for k in ("compute_aabb", "all_points_aabb_signed_distance") for g in "fd" for t in "fd"] + \
+    [f"ssdf_b200_{k}_{g}" for k in ("level_set_triangles", "rebuild_sdf", "refine_field", "round_sdf") for g in ("ff", "dd")]
 
 
 def _status_name(status: int) -> str:
@@ -304,6 +312,76 @@ def all_points_aabb_signed_distance(points, box, gdtype=np.float64, tdtype=None)
     fn = f"ssdf_b200_all_points_aabb_signed_distance_{_suffix(gdtype)}{_suffix(tdtype)}"
     _check(getattr(lib, fn)(len(x), _p(x), _p(y), _p(z), *[float(b) for b in box], _p(out)), fn)
     return out
+
+
+class GridGeometry:
+    """ssdf::GridGeometry<G> (serial/bvh/sdf_rebuild.hpp:10-21): n[d] samples at o[d] + i h[d], x fastest."""
+
+    def __init__(self, n, o, h, dtype=np.float64):
+        self.n = tuple(int(v) for v in n)
+        self.dtype = np.dtype(dtype)
+        self.o = tuple(self.dtype.type(v) for v in o)
+        self.h = tuple(self.dtype.type(v) for v in h)
+
+    @property
+    def size(self):
+        return self.n[0] * self.n[1] * self.n[2]
+
+    def strided(self, stride):
+        t = self.dtype.type
+        return GridGeometry([(v - 1) // stride + 1 for v in self.n], self.o, [t(v * t(stride)) for v in self.h], self.dtype)
+
+    def refined(self, factor):
+        return GridGeometry([(v - 1) * factor + 1 for v in self.n], self.o,
+                            [self.dtype.type(float(v) / float(factor)) for v in self.h], self.dtype)
+
+    def _args(self):
+        ct = C.c_double if self.dtype == np.float64 else C.c_float
+        return [C.byref((C.c_ssize_t * 3)(*self.n)), C.byref((ct * 3)(*self.o)), C.byref((ct * 3)(*self.h))]
+
+    def _suffix(self):
+        return "dd" if self.dtype == np.float64 else "ff"
+
+
+def level_set_triangles(grid: GridGeometry, f, level):
+    """ssdf::level_set_triangles on the GPU: the triangle soup (3, 3 * ntri) of {f = level}."""
+    fa = _arr(f, grid.dtype)
+    fn = f"ssdf_b200_level_set_triangles_{grid._suffix()}"
+    nt = C.c_ssize_t(0)
+    _check(getattr(lib, fn)(*grid._args(), _p(fa), float(level), 0, None, None, None, C.byref(nt)), fn)
+    x, y, z = (np.empty(3 * nt.value, dtype=grid.dtype) for _ in range(3))
+    if nt.value:
+        _check(getattr(lib, fn)(*grid._args(), _p(fa), float(level), nt.value, _p(x), _p(y), _p(z), C.byref(nt)), fn)
+    return np.stack([x, y, z])
+
+
+def rebuild_sdf(grid: GridGeometry, f, level, band, stride=1):
+    """ssdf::rebuild_sdf on the GPU: signed distance to {f = level} within band on grid.strided(stride)."""
+    fa = _arr(f, grid.dtype)
+    out = np.empty(grid.strided(stride).size, dtype=grid.dtype)
+    fn = f"ssdf_b200_rebuild_sdf_{grid._suffix()}"
+    _check(getattr(lib, fn)(*grid._args(), _p(fa), float(level), float(band), int(stride), _p(out)), fn)
+    return out
+
+
+def refine_field(grid: GridGeometry, f, factor):
+    """ssdf::refine_field on the GPU: f on grid.refined(factor), cubic along each axis in turn."""
+    fa = _arr(f, grid.dtype)
+    fine = np.empty(grid.refined(factor).size, dtype=grid.dtype)
+    fn = f"ssdf_b200_refine_field_{grid._suffix()}"
+    _check(getattr(lib, fn)(*grid._args(), _p(fa), int(factor), _p(fine)), fn)
+    return fine
+
+
+def round_sdf(grid: GridGeometry, f, radius, band, open=True, close=True, stride=1, with_f0=False):
+    """ssdf::round_sdf on the GPU: the region f > 0 rounded by radius, its signed distance strided."""
+    fa = _arr(f, grid.dtype)
+    out = np.empty(grid.strided(stride).size, dtype=grid.dtype)
+    f0 = np.empty(grid.size, dtype=grid.dtype) if with_f0 else None
+    fn = f"ssdf_b200_round_sdf_{grid._suffix()}"
+    _check(getattr(lib, fn)(*grid._args(), _p(fa), float(radius), float(band), int(open), int(close), int(stride),
+                            _p(out), _p(f0) if with_f0 else None), fn)
+    return (out, f0) if with_f0 else out
 
 
 def _grid_call(fn, mesh, grid, out, dtype, extra=()):

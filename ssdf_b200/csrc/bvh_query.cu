@@ -210,10 +210,11 @@ __device__ __forceinline__ void boxes4_fast(const DeviceMesh &m, int node, float
 struct Tri32 {
     float ax, ay, az, bx, by, bz, cx, cy, cz;
     int id;
+    bool ill;  // ill-conditioned: the fix-up path keys it by its double distance
 };
 __device__ __forceinline__ Tri32 load_tri32(const float4 *__restrict__ t, int p) {
     const float4 u = __ldg(t + 3 * p), v = __ldg(t + 3 * p + 1), w = __ldg(t + 3 * p + 2);
-    return Tri32{u.x, u.y, u.z, u.w, v.x, v.y, v.z, v.w, w.x, __float_as_int(w.y)};
+    return Tri32{u.x, u.y, u.z, u.w, v.x, v.y, v.z, v.w, w.x, __float_as_int(w.y), w.z != 0.f};
 }
 
 struct Tri64 {
@@ -337,7 +338,10 @@ struct ExactPolicy {
 // F32X: float filter. Per query, the kCand smallest float d^2 inside the window
 // (sqrt(best) + tau)^2 are kept, sorted, in shared memory (slot (q, s) of thread t at
 // [(q * kCand + s) * kThreads + t]: consecutive threads, consecutive banks), with the smallest d^2
-// pushed out of the slots.
+// pushed out of the slots. The float filter's error is second order in its error along the
+// triangle's plane, which stays small unless the triangle is ill-conditioned (a needle or a
+// sliver: the face-region solve divides by its area); those triangles (flagged at build time) are
+// keyed instead by their double distance, from the query's double point kept in shared memory.
 __device__ __forceinline__ float window_thr(float best, float tau_rel, float scale) {
     if (!(best < finf())) return finf();
     const float d = sqrtf(best);
@@ -354,8 +358,20 @@ struct FastPolicy {
     float tau_rel;
     float *wd;
     int *wp;
-    __device__ FastPolicy(const DeviceMesh &mesh, float tau, float *sd, int *sp)
-        : m(mesh), tau_rel(tau), wd(sd + threadIdx.x), wp(sp + threadIdx.x) {}
+    double *wq;  // the queries' double points, [(q * 3 + axis) * kThreads + t]
+    __device__ FastPolicy(const DeviceMesh &mesh, float tau, float *sd, int *sp, double *sq)
+        : m(mesh), tau_rel(tau), wd(sd + threadIdx.x), wp(sp + threadIdx.x), wq(sq + threadIdx.x) {}
+    __device__ __forceinline__ void set_point(int q, double x, double y, double z) {
+        wq[(3 * q + 0) * kThreads] = x, wq[(3 * q + 1) * kThreads] = y, wq[(3 * q + 2) * kThreads] = z;
+    }
+    // key of an ill-conditioned triangle: its double distance, rounded to float
+    __device__ __forceinline__ float exact_key(int q, int pos) const {
+        const Tri64 u = load_tri64(m.tris64, pos);
+        const double e2 = tri_dist_sq_exact<double>(wq[(3 * q + 0) * kThreads], wq[(3 * q + 1) * kThreads],
+                                                    wq[(3 * q + 2) * kThreads], u.ax, u.ay, u.az, u.bx, u.by, u.bz,
+                                                    u.cx, u.cy, u.cz);
+        return float(e2);
+    }
     __device__ __forceinline__ int slot(int q, int s) const { return (q * kCand + s) * kThreads; }
     __device__ __forceinline__ void set(int q, float x, float y, float z, float init) {
         px[q] = x, py[q] = y, pz[q] = z, best[q] = init, evicted[q] = finf(), wmax[q] = finf();
@@ -418,8 +434,9 @@ struct FastPolicy {
 #pragma unroll
             for (int q = 0; q < Q; q++) {
                 if (!((mask >> q) & 1u)) continue;
-                const float d2 =
-                    tri_dist_sq_fast(px[q], py[q], pz[q], t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
+                const float d2 = t.ill ? exact_key(q, first + k)
+                                       : tri_dist_sq_fast(px[q], py[q], pz[q], t.ax, t.ay, t.az, t.bx, t.by, t.bz,
+                                                          t.cx, t.cy, t.cz);
                 if (COUNT) cnt.tri++;
                 if (d2 < thr[q]) {
                     insert(q, d2, first + k);
@@ -873,7 +890,8 @@ __device__ __forceinline__ void query_block(const QueryArgs &a, long long block,
     } else {
         __shared__ float s_wd[kQ * kCand * kThreads];
         __shared__ int s_wp[kQ * kCand * kThreads];
-        FastPolicy<Q> p(a.m, a.tau_rel, s_wd, s_wp);
+        __shared__ double s_wq[3 * kQ * kThreads];
+        FastPolicy<Q> p(a.m, a.tau_rel, s_wd, s_wp, s_wq);
 #pragma unroll
         for (int s = 0; s < Q; s++) {
             if (valid[s]) {
@@ -882,6 +900,7 @@ __device__ __forceinline__ void query_block(const QueryArgs &a, long long block,
                 const double init = initial_bound(a, qid[s]);
                 // float start bound rounded up, so no triangle closer in double is cut off
                 p.set(s, float(x), float(y), float(z), init < dinf() ? __double2float_ru(init) : finf());
+                p.set_point(s, x, y, z);
             } else {
                 p.disable(s);
             }
@@ -960,12 +979,20 @@ __device__ __forceinline__ void window_leaf(const DeviceMesh &m, int ref, float 
     const int first = leaf_first(ref), n = leaf_count(ref);
     for (int k = 0; k < n; k++) {
         const Tri32 t = load_tri32(m.tris32, first + k);
-        const float f = tri_dist_sq_fast(px, py, pz, t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
+        double e2 = 0.0;
+        float f;
+        if (t.ill) {  // keyed by its double distance, as in the first stage
+            const Tri64 u = load_tri64(m.tris64, first + k);
+            e2 = tri_dist_sq_exact<double>(qx, qy, qz, u.ax, u.ay, u.az, u.bx, u.by, u.bz, u.cx, u.cy, u.cz);
+            f = float(e2);
+        } else {
+            f = tri_dist_sq_fast(px, py, pz, t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
+        }
         if (count) cnt.tri++;
         if (f < thr) {
             const Tri64 u = load_tri64(m.tris64, first + k);
-            const double e2 =
-                tri_dist_sq_exact<double>(qx, qy, qz, u.ax, u.ay, u.az, u.bx, u.by, u.bz, u.cx, u.cy, u.cz);
+            if (!t.ill)
+                e2 = tri_dist_sq_exact<double>(qx, qy, qz, u.ax, u.ay, u.az, u.bx, u.by, u.bz, u.cx, u.cy, u.cz);
             if (count) cnt.fix++;
             if (e2 < b.d2 || (e2 == b.d2 && u.id < b.id)) b = WindowBest{e2, u.id, first + k};
         }

@@ -538,7 +538,22 @@ int ssdf_mesh_create(ssdf_mesh **mesh, ptrdiff_t nselements, const int *s0, cons
 
 int ssdf_mesh_destroy(ssdf_mesh *mesh) {
     if (!mesh) return SSDF_OK;
+    // queries still running on any stream may read the mesh: wait for its device first (its storage is
+    // pool memory, which cudaFree releases without waiting)
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != mesh->device) cudaSetDevice(mesh->device);
+    const cudaError_t e = cudaDeviceSynchronize();
     mesh_free(mesh->storage);
+    if (prev != mesh->device) cudaSetDevice(prev);
+    delete mesh;
+    if (e != cudaSuccess) return cuda_fail(e, "ssdf_mesh_destroy", __FILE__, __LINE__);
+    return SSDF_OK;
+}
+
+int ssdf_mesh_destroy_async(ssdf_mesh *mesh, void *stream) {
+    if (!mesh) return SSDF_OK;
+    mesh_free_async(mesh->storage, (cudaStream_t)stream);
     delete mesh;
     return SSDF_OK;
 }

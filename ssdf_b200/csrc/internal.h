@@ -44,7 +44,8 @@ int cuda_fail(cudaError_t err, const char *what, const char *file, int line);
 // A reference >= 0 is an internal node; < 0 is a leaf ~((first << 5) | (count - 1)) over the
 // triangle records in leaf order; kEmptyRef is an empty slot (its box is inverted).
 // Triangles in leaf order:
-//   FP32 record (3 x float4): (ax, ay, az, bx), (by, bz, cx, cy), (cz, id bits, -, -)
+//   FP32 record (3 x float4): (ax, ay, az, bx), (by, bz, cx, cy), (cz, id bits, ill, -) with ill = 1
+//                             for a triangle whose height is below 1/8 of its longest edge
 //   FP64 record (5 x double2): (ax, ay), (az, bx), (by, bz), (cx, cy), (cz, id)
 // where id is the triangle's index in the caller's s0/s1/s2 and a, b, c its vertices s0, s1, s2.
 constexpr int kEmptyRef = -2147483647 - 1;  // INT_MIN
@@ -136,7 +137,8 @@ struct MeshStorage;  // owns the device allocations behind a DeviceMesh
 int mesh_build(MeshStorage **storage, DeviceMesh *mesh, ptrdiff_t nt, const int *s0, const int *s1, const int *s2,
                ptrdiff_t nv, const void *sx, const void *sy, const void *sz, int coord_f64, int device_ptrs,
                const ssdf_build_opts &opts, cudaStream_t stream);
-void mesh_free(MeshStorage *storage);
+void mesh_free(MeshStorage *storage);                            // after the work using it completed
+void mesh_free_async(MeshStorage *storage, cudaStream_t stream);  // in stream order
 size_t mesh_bytes(const MeshStorage *storage);
 
 // ---- radix sort (radix_sort.cu) ------------------------------------------------------------------
@@ -183,6 +185,25 @@ int points_aabb_device(long long n, const G *x, const G *y, const G *z, T *box6,
 template <typename G, typename T>
 int points_box_sdf_device(long long n, const G *x, const G *y, const G *z, const T box6[6], int absolute, T *out,
                           cudaStream_t stream);
+
+// ---- level sets and field rebuilds (sdf_rebuild.cu) ----------------------------------------------
+// A uniform grid: n[d] samples along axis d at o[d] + i h[d], x fastest (G's o and h, widened).
+struct GridDesc {
+    long long n[3];
+    double o[3], h[3];
+};
+GridDesc grid_strided(const GridDesc &g, long long stride, bool g64);
+GridDesc grid_refined(const GridDesc &g, long long factor, bool g64);
+template <typename G, typename T>
+int level_set_device(const GridDesc &gd, const T *d_f, T level, long long *ntri, G *x, G *y, G *z, int **d_offsets,
+                     cudaStream_t stream);
+template <typename G, typename T>
+int rebuild_device(const GridDesc &gd, const T *d_f, T level, T band, long long stride, T *d_out, cudaStream_t stream);
+template <typename G, typename T>
+int refine_device(const GridDesc &gd, const T *d_f, long long factor, T *d_fine, cudaStream_t stream);
+template <typename G, typename T>
+int round_device(const GridDesc &gd, const T *d_f, T radius, T band, bool open, bool close, long long stride, T *d_out,
+                 T *d_f0, cudaStream_t stream);
 
 // ---- small helpers -------------------------------------------------------------------------------
 inline int grid_blocks(long long n, int threads) { return int((n + threads - 1) / threads); }

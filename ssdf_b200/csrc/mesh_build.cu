@@ -446,7 +446,15 @@ __global__ void k_tri_records(int nt, const int *__restrict__ sorted_ids, const 
     const double cx = vx[c], cy = vy[c], cz = vz[c];
     t32[3 * p + 0] = make_float4(float(ax), float(ay), float(az), float(bx));
     t32[3 * p + 1] = make_float4(float(by), float(bz), float(cx), float(cy));
-    t32[3 * p + 2] = make_float4(float(cz), __int_as_float(t), 0.f, 0.f);
+    // ill-conditioned (height below 1/8 of the longest edge, or degenerate): the fix-up path keys it
+    // by its double distance instead of the float filter (see bvh_query.cu)
+    const double abx = bx - ax, aby = by - ay, abz = bz - az, acx = cx - ax, acy = cy - ay, acz = cz - az;
+    const double bcx = cx - bx, bcy = cy - by, bcz = cz - bz;
+    const double l2 = fmax(fmax(abx * abx + aby * aby + abz * abz, acx * acx + acy * acy + acz * acz),
+                           bcx * bcx + bcy * bcy + bcz * bcz);
+    const double nx = aby * acz - abz * acy, ny = abz * acx - abx * acz, nz = abx * acy - aby * acx;
+    const bool ill = !(64.0 * (nx * nx + ny * ny + nz * nz) >= l2 * l2) || !(l2 > 0.0);
+    t32[3 * p + 2] = make_float4(float(cz), __int_as_float(t), ill ? 1.f : 0.f, 0.f);
     if (t64) {
         t64[5 * p + 0] = make_double2(ax, ay);
         t64[5 * p + 1] = make_double2(az, bx);
@@ -586,9 +594,18 @@ int build_normals(MeshStorage *s, DeviceMesh *m, const int *s0, const int *s1, c
 
 }  // namespace
 
+// The storage comes from the stream-ordered pool (cudaMallocAsync): cudaFree on it does not wait for
+// work that still reads it, so the caller has ensured that none does (ssdf_mesh_destroy waits for the
+// device) -- or frees it in stream order behind that work with mesh_free_async.
 void mesh_free(MeshStorage *storage) {
     if (!storage) return;
     for (void *p : storage->blocks) cudaFree(p);
+    delete storage;
+}
+
+void mesh_free_async(MeshStorage *storage, cudaStream_t stream) {
+    if (!storage) return;
+    for (void *p : storage->blocks) cudaFreeAsync(p, stream);
     delete storage;
 }
 

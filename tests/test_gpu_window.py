@@ -85,3 +85,41 @@ def test_batch_with_overflowing_jobs():
             assert np.array_equal(o.cpu().numpy(), d64) and np.array_equal(t.cpu().numpy(), t64)
     for dm in dms:
         dm.close()
+
+
+def sliver_mesh(sub, height):
+    """An icosphere whose every triangle (a, b, c) is split at a point m just off the middle of ab:
+    (a, m, c), (m, b, c) and the sliver (a, b, m) of relative height `height`."""
+    base = W.icosphere(sub, radius=1.0, displacement=0.01, seed=4)
+    v = list(base.vertices)
+    tris = []
+    for a, b, c in base.triangles:
+        pa, pb, pc = base.vertices[a], base.vertices[b], base.vertices[c]
+        m = 0.5 * (pa + pb) + height * np.linalg.norm(pb - pa) * (pc - 0.5 * (pa + pb)) / np.linalg.norm(pc - 0.5 * (pa + pb))
+        v.append(m)
+        im = len(v) - 1
+        tris += [(a, im, c), (im, b, c), (a, b, im)]
+    return W.Mesh(np.array(v), np.array(tris, dtype=np.int32))
+
+
+@pytest.mark.parametrize("height", [1e-3, 1e-6, 0.0])
+def test_slivers_fixup_equals_double(height):
+    """Ill-conditioned triangles (needles, slivers, collinear) are keyed by their double distance in the
+    fix-up path, so its result stays the double one at every query."""
+    mesh = sliver_mesh(2, height)
+    dm = S.DeviceMesh(mesh)
+    lo, hi = mesh.bbox()
+    grid = W.Grid((40, 40, 40), tuple(lo - 0.3), tuple(hi + 0.3))
+    res = {}
+    for prec in (S.PREC_F32_FIXUP, S.PREC_F64):
+        out = torch.full((grid.size,), np.finfo(np.float64).max, dtype=torch.float64, device="cuda")
+        tri = torch.full((grid.size,), -1, dtype=torch.int32, device="cuda")
+        dm.query_grid(grid, out, tri, precision=prec, output=S.OUT_EDF)
+        torch.cuda.synchronize()
+        res[prec] = (out.cpu().numpy(), tri.cpu().numpy())
+    dm.close()
+    assert np.array_equal(res[S.PREC_F32_FIXUP][0], res[S.PREC_F64][0])
+    assert np.array_equal(res[S.PREC_F32_FIXUP][1], res[S.PREC_F64][1])
+    ids = np.random.default_rng(0).choice(grid.size, 500, replace=False)
+    want, wtri = oracle.edf(oracle.grid_points(grid)[:, ids], mesh, with_index=True)
+    assert np.array_equal(res[S.PREC_F64][0][ids], want) and np.array_equal(res[S.PREC_F64][1][ids], wtri)
