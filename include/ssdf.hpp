@@ -14,6 +14,7 @@
 #include <stddef.h>
 
 #include <type_traits>
+#include <vector>
 
 #include "ssdf_b200.h"
 
@@ -180,6 +181,93 @@ int all_points_aabb_signed_distance(const ptrdiff_t npoints, const G *const SSDF
     else
         static_assert(detail::always_false<G, T>::value,
                       "all_points_aabb_signed_distance: G and T are float or double");
+}
+
+// ---- level sets and field rebuilds (serial/bvh/sdf_rebuild.hpp) ----------------------------------
+
+// serial/bvh/sdf_rebuild.hpp:10-21: n[d] samples along axis d at o[d] + i h[d], x fastest.
+template <typename G>
+struct GridGeometry {
+    ptrdiff_t n[3];
+    G o[3];
+    G h[3];
+
+    ptrdiff_t size() const { return n[0] * n[1] * n[2]; }
+    GridGeometry strided(const ptrdiff_t stride) const {
+        GridGeometry s = *this;
+        for (int d = 0; d < 3; ++d) {
+            s.n[d] = (n[d] - 1) / stride + 1;
+            s.h[d] = h[d] * G(stride);
+        }
+        return s;
+    }
+    GridGeometry refined(const ptrdiff_t factor) const {
+        GridGeometry r = *this;
+        for (int d = 0; d < 3; ++d) {
+            r.n[d] = (n[d] - 1) * factor + 1;
+            r.h[d] = G(double(h[d]) / double(factor));
+        }
+        return r;
+    }
+};
+
+// serial/bvh/sdf_rebuild.hpp:23-37: appends the soup to x, y, z; returns the triangle count (or a
+// negative status).
+template <typename G, typename T>
+ptrdiff_t level_set_triangles(const GridGeometry<G> &grid, const T *const f, const T level, std::vector<G> &x,
+                              std::vector<G> &y, std::vector<G> &z) {
+    static_assert(std::is_same<G, T>::value && (std::is_same<G, float>::value || std::is_same<G, double>::value),
+                  "level_set_triangles is instantiated for <float,float> and <double,double>");
+    ptrdiff_t nt = 0;
+    auto call = [&](ptrdiff_t cap, G *px, G *py, G *pz) {
+        if constexpr (std::is_same<G, float>::value)
+            return ssdf_b200_level_set_triangles_ff(grid.n, grid.o, grid.h, f, level, cap, px, py, pz, &nt);
+        else
+            return ssdf_b200_level_set_triangles_dd(grid.n, grid.o, grid.h, f, level, cap, px, py, pz, &nt);
+    };
+    int st = call(0, nullptr, nullptr, nullptr);
+    if (st != SSDF_OK) return -ptrdiff_t(st);
+    const size_t first = x.size();
+    x.resize(first + 3 * size_t(nt));
+    y.resize(first + 3 * size_t(nt));
+    z.resize(first + 3 * size_t(nt));
+    if (nt > 0) st = call(nt, x.data() + first, y.data() + first, z.data() + first);
+    return st == SSDF_OK ? nt : -ptrdiff_t(st);
+}
+
+// serial/bvh/sdf_rebuild.hpp:38-50
+template <typename G, typename T>
+int rebuild_sdf(const GridGeometry<G> &grid, const T *const f, const T level, const T band, const ptrdiff_t stride,
+                T *const out) {
+    if constexpr (std::is_same<G, float>::value && std::is_same<T, float>::value)
+        return ssdf_b200_rebuild_sdf_ff(grid.n, grid.o, grid.h, f, level, band, stride, out);
+    else if constexpr (std::is_same<G, double>::value && std::is_same<T, double>::value)
+        return ssdf_b200_rebuild_sdf_dd(grid.n, grid.o, grid.h, f, level, band, stride, out);
+    else
+        static_assert(detail::always_false<G, T>::value, "rebuild_sdf is instantiated for <float,float> and <double,double>");
+}
+
+// serial/bvh/sdf_rebuild.hpp:52-56 (void in the reference; the status here)
+template <typename G, typename T>
+int refine_field(const GridGeometry<G> &grid, const T *const f, const ptrdiff_t factor, T *const fine) {
+    if constexpr (std::is_same<G, float>::value && std::is_same<T, float>::value)
+        return ssdf_b200_refine_field_ff(grid.n, grid.o, grid.h, f, factor, fine);
+    else if constexpr (std::is_same<G, double>::value && std::is_same<T, double>::value)
+        return ssdf_b200_refine_field_dd(grid.n, grid.o, grid.h, f, factor, fine);
+    else
+        static_assert(detail::always_false<G, T>::value, "refine_field is instantiated for <float,float> and <double,double>");
+}
+
+// serial/bvh/sdf_rebuild.hpp:57-78
+template <typename G, typename T>
+int round_sdf(const GridGeometry<G> &grid, const T *const f, const T radius, const T band, const bool open,
+              const bool close, const ptrdiff_t stride, T *const out, T *const f0) {
+    if constexpr (std::is_same<G, float>::value && std::is_same<T, float>::value)
+        return ssdf_b200_round_sdf_ff(grid.n, grid.o, grid.h, f, radius, band, open, close, stride, out, f0);
+    else if constexpr (std::is_same<G, double>::value && std::is_same<T, double>::value)
+        return ssdf_b200_round_sdf_dd(grid.n, grid.o, grid.h, f, radius, band, open, close, stride, out, f0);
+    else
+        static_assert(detail::always_false<G, T>::value, "round_sdf is instantiated for <float,float> and <double,double>");
 }
 
 }  // namespace ssdf

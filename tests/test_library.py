@@ -39,6 +39,7 @@ def test_cpp_header_compiles_against_c_abi(tmp_path):
 
     src = tmp_path / "use.cpp"
     src.write_text(
+        '#include "bvh/sdf_rebuild.hpp"\n'
         '#include "ssdf.hpp"\n'
         "int main() {\n"
         "  double x[1] = {0}, y[1] = {0}, z[1] = {2}, sx[3] = {0, 1, 0}, sy[3] = {0, 0, 1}, sz[3] = {0, 0, 0};\n"
@@ -53,6 +54,13 @@ def test_cpp_header_compiles_against_c_abi(tmp_path):
         "  (void)ssdf::sample_sqedf_bvh<double, double, int>;\n"
         "  (void)ssdf::compute_aabb<float, double>;\n"
         "  (void)ssdf::all_points_aabb_signed_distance<double, double>;\n"
+        "  ssdf::GridGeometry<float> g{{4, 4, 4}, {0, 0, 0}, {0.5f, 0.5f, 0.5f}};\n"
+        "  std::vector<float> vx, vy, vz;\n"
+        "  (void)&ssdf::level_set_triangles<float, float>;\n"
+        "  (void)ssdf::rebuild_sdf<double, double>;\n"
+        "  (void)ssdf::refine_field<float, float>;\n"
+        "  (void)ssdf::round_sdf<double, double>;\n"
+        "  (void)g.strided(2).refined(2).size();\n"
         "  return 0;\n}\n")
     lib = os.path.join(ROOT, "ssdf_b200", "_lib")
     res = subprocess.run(["g++", "-std=c++17", f"-I{ROOT}/include", str(src), "-o", str(tmp_path / "use"),
