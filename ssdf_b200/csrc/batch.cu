@@ -110,7 +110,7 @@ static int batch_add(ssdf_batch *b, const QueryArgs &a, const ssdf_query_opts *o
     if (int(b->jobs.size()) >= b->max_jobs) return fail(SSDF_ERR_INVALID_ARGUMENT, "batch is full");
     if (b->precision == SSDF_PREC_F64 && !a.m.nodes64)
         return fail(SSDF_ERR_INVALID_ARGUMENT, "mesh built without double data (keep_fp64=0)");
-    if (b->precision == SSDF_PREC_F32_FIXUP && (!a.m.tris64 || !a.m.nodes64))
+    if (b->precision == SSDF_PREC_F32_FIXUP && (!a.m.tris64 || !a.m.nodes64 || !a.m.filt32))
         return fail(SSDF_ERR_INVALID_ARGUMENT, "fix-up queries need the double triangles and BVH (keep_fp64=1)");
     if (a.output == SSDF_OUT_SDF && (!a.m.face_n || !a.m.tris64))
         return fail(SSDF_ERR_INVALID_ARGUMENT, "signed queries need a mesh built with normals=1 and keep_fp64=1");

@@ -210,11 +210,11 @@ __device__ __forceinline__ void boxes4_fast(const DeviceMesh &m, int node, float
 struct Tri32 {
     float ax, ay, az, bx, by, bz, cx, cy, cz;
     int id;
-    bool ill;  // ill-conditioned: the fix-up path keys it by its double distance
+    float pen;  // fix-up filter records: 0, or +inf for a proxy (never the window's centre)
 };
 __device__ __forceinline__ Tri32 load_tri32(const float4 *__restrict__ t, int p) {
     const float4 u = __ldg(t + 3 * p), v = __ldg(t + 3 * p + 1), w = __ldg(t + 3 * p + 2);
-    return Tri32{u.x, u.y, u.z, u.w, v.x, v.y, v.z, v.w, w.x, __float_as_int(w.y), w.z != 0.f};
+    return Tri32{u.x, u.y, u.z, u.w, v.x, v.y, v.z, v.w, w.x, __float_as_int(w.y), w.z};
 }
 
 struct Tri64 {
@@ -340,8 +340,11 @@ struct ExactPolicy {
 // [(q * kCand + s) * kThreads + t]: consecutive threads, consecutive banks), with the smallest d^2
 // pushed out of the slots. The float filter's error is second order in its error along the
 // triangle's plane, which stays small unless the triangle is ill-conditioned (a needle or a
-// sliver: the face-region solve divides by its area); those triangles (flagged at build time) are
-// keyed instead by their double distance, from the query's double point kept in shared memory.
+// sliver: the face-region solve divides by its area). Such a triangle is filtered through a
+// well-conditioned proxy that contains it (DeviceMesh::filt32): a lower bound of its distance,
+// within the float filter's error, which may enter the window but, with its +inf penalty, never
+// moves its centre; the member is re-evaluated in double like any other, so the double winner,
+// whose key is at most its distance plus that error, stays inside the window.
 __device__ __forceinline__ float window_thr(float best, float tau_rel, float scale) {
     if (!(best < finf())) return finf();
     const float d = sqrtf(best);
@@ -358,20 +361,8 @@ struct FastPolicy {
     float tau_rel;
     float *wd;
     int *wp;
-    double *wq;  // the queries' double points, [(q * 3 + axis) * kThreads + t]
-    __device__ FastPolicy(const DeviceMesh &mesh, float tau, float *sd, int *sp, double *sq)
-        : m(mesh), tau_rel(tau), wd(sd + threadIdx.x), wp(sp + threadIdx.x), wq(sq + threadIdx.x) {}
-    __device__ __forceinline__ void set_point(int q, double x, double y, double z) {
-        wq[(3 * q + 0) * kThreads] = x, wq[(3 * q + 1) * kThreads] = y, wq[(3 * q + 2) * kThreads] = z;
-    }
-    // key of an ill-conditioned triangle: its double distance, rounded to float
-    __device__ __forceinline__ float exact_key(int q, int pos) const {
-        const Tri64 u = load_tri64(m.tris64, pos);
-        const double e2 = tri_dist_sq_exact<double>(wq[(3 * q + 0) * kThreads], wq[(3 * q + 1) * kThreads],
-                                                    wq[(3 * q + 2) * kThreads], u.ax, u.ay, u.az, u.bx, u.by, u.bz,
-                                                    u.cx, u.cy, u.cz);
-        return float(e2);
-    }
+    __device__ FastPolicy(const DeviceMesh &mesh, float tau, float *sd, int *sp)
+        : m(mesh), tau_rel(tau), wd(sd + threadIdx.x), wp(sp + threadIdx.x) {}
     __device__ __forceinline__ int slot(int q, int s) const { return (q * kCand + s) * kThreads; }
     __device__ __forceinline__ void set(int q, float x, float y, float z, float init) {
         px[q] = x, py[q] = y, pz[q] = z, best[q] = init, evicted[q] = finf(), wmax[q] = finf();
@@ -430,17 +421,16 @@ struct FastPolicy {
     template <bool COUNT>
     __device__ __forceinline__ void leaf(int first, int n, unsigned mask, Counters &cnt) {
         for (int k = 0; k < n; k++) {
-            const Tri32 t = load_tri32(m.tris32, first + k);
+            const Tri32 t = load_tri32(m.filt32, first + k);
 #pragma unroll
             for (int q = 0; q < Q; q++) {
                 if (!((mask >> q) & 1u)) continue;
-                const float d2 = t.ill ? exact_key(q, first + k)
-                                       : tri_dist_sq_fast(px[q], py[q], pz[q], t.ax, t.ay, t.az, t.bx, t.by, t.bz,
-                                                          t.cx, t.cy, t.cz);
+                const float d2 =
+                    tri_dist_sq_fast(px[q], py[q], pz[q], t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
                 if (COUNT) cnt.tri++;
                 if (d2 < thr[q]) {
                     insert(q, d2, first + k);
-                    if (d2 < best[q]) {
+                    if (d2 + t.pen < best[q]) {
                         best[q] = d2;
                         thr[q] = window_thr(best[q], tau_rel, m.coord_scale);
                     }
@@ -890,8 +880,7 @@ __device__ __forceinline__ void query_block(const QueryArgs &a, long long block,
     } else {
         __shared__ float s_wd[kQ * kCand * kThreads];
         __shared__ int s_wp[kQ * kCand * kThreads];
-        __shared__ double s_wq[3 * kQ * kThreads];
-        FastPolicy<Q> p(a.m, a.tau_rel, s_wd, s_wp, s_wq);
+        FastPolicy<Q> p(a.m, a.tau_rel, s_wd, s_wp);
 #pragma unroll
         for (int s = 0; s < Q; s++) {
             if (valid[s]) {
@@ -900,7 +889,6 @@ __device__ __forceinline__ void query_block(const QueryArgs &a, long long block,
                 const double init = initial_bound(a, qid[s]);
                 // float start bound rounded up, so no triangle closer in double is cut off
                 p.set(s, float(x), float(y), float(z), init < dinf() ? __double2float_ru(init) : finf());
-                p.set_point(s, x, y, z);
             } else {
                 p.disable(s);
             }
@@ -978,21 +966,13 @@ __device__ __forceinline__ void window_leaf(const DeviceMesh &m, int ref, float 
                                             bool count) {
     const int first = leaf_first(ref), n = leaf_count(ref);
     for (int k = 0; k < n; k++) {
-        const Tri32 t = load_tri32(m.tris32, first + k);
-        double e2 = 0.0;
-        float f;
-        if (t.ill) {  // keyed by its double distance, as in the first stage
-            const Tri64 u = load_tri64(m.tris64, first + k);
-            e2 = tri_dist_sq_exact<double>(qx, qy, qz, u.ax, u.ay, u.az, u.bx, u.by, u.bz, u.cx, u.cy, u.cz);
-            f = float(e2);
-        } else {
-            f = tri_dist_sq_fast(px, py, pz, t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
-        }
+        const Tri32 t = load_tri32(m.filt32, first + k);  // the first stage's key
+        const float f = tri_dist_sq_fast(px, py, pz, t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
         if (count) cnt.tri++;
         if (f < thr) {
             const Tri64 u = load_tri64(m.tris64, first + k);
-            if (!t.ill)
-                e2 = tri_dist_sq_exact<double>(qx, qy, qz, u.ax, u.ay, u.az, u.bx, u.by, u.bz, u.cx, u.cy, u.cz);
+            const double e2 =
+                tri_dist_sq_exact<double>(qx, qy, qz, u.ax, u.ay, u.az, u.bx, u.by, u.bz, u.cx, u.cy, u.cz);
             if (count) cnt.fix++;
             if (e2 < b.d2 || (e2 == b.d2 && u.id < b.id)) b = WindowBest{e2, u.id, first + k};
         }
@@ -1257,7 +1237,7 @@ int launch_query(const QueryArgs &args_in, int precision, cudaStream_t stream) {
     if (n <= 0) return SSDF_OK;
     if (precision == SSDF_PREC_F64 && !a.m.nodes64)
         return fail(SSDF_ERR_INVALID_ARGUMENT, "mesh built without double data (keep_fp64=0)");
-    if (precision == SSDF_PREC_F32_FIXUP && (!a.m.tris64 || !a.m.nodes64))
+    if (precision == SSDF_PREC_F32_FIXUP && (!a.m.tris64 || !a.m.nodes64 || !a.m.filt32))
         return fail(SSDF_ERR_INVALID_ARGUMENT, "fix-up queries need the double triangles and BVH (keep_fp64=1)");
     if (a.output == SSDF_OUT_SDF && !a.m.face_n)
         return fail(SSDF_ERR_INVALID_ARGUMENT, "signed queries need a mesh built with normals=1");
@@ -1402,7 +1382,7 @@ int launch_query_noalloc(const QueryArgs &args_in, cudaStream_t stream) {
         return fail(SSDF_ERR_NOT_SUPPORTED, "the allocation-free query takes at most " +
                                                 std::to_string(kNoAllocMaxQueries) + " queries per call, got " +
                                                 std::to_string(n) + ": split the grid into slabs");
-    if (!a.m.tris64 || !a.m.nodes64)
+    if (!a.m.tris64 || !a.m.nodes64 || !a.m.filt32)
         return fail(SSDF_ERR_INVALID_ARGUMENT, "fix-up queries need the double triangles and BVH (keep_fp64=1)");
     if (a.output == SSDF_OUT_SDF && !a.m.face_n)
         return fail(SSDF_ERR_INVALID_ARGUMENT, "signed queries need a mesh built with normals=1");

@@ -434,10 +434,61 @@ __global__ void k_depth(int n, int L, const int *__restrict__ count, const int *
     atomicAdd(&stats[1], leaves);
 }
 
+// The fix-up path's FP32 filter record of one triangle: the triangle itself, or, when it is
+// ill-conditioned (height below 1/8 of its longest edge PQ, third corner R), a proxy triangle that
+// contains it: PQ widened by L/4 at both ends (L = |PQ|) and an apex L/2 off its middle, towards R in
+// the triangle's plane. R projects inside PQ (PQ is the longest edge) at height below L/8, and the
+// proxy is at least L/6 high over all of PQ, so it contains P, Q and R; its distance is a lower
+// bound of the triangle's, and its height (1/3 of its base) keeps the float test accurate. The
+// record's w.z is 0, or +inf for a proxy (whose key may enter the window but never move its centre).
+__device__ void filter_record(double ax, double ay, double az, double bx, double by, double bz, double cx,
+                              double cy, double cz, int t, float4 *__restrict__ out) {
+    const double abx = bx - ax, aby = by - ay, abz = bz - az, acx = cx - ax, acy = cy - ay, acz = cz - az;
+    const double bcx = cx - bx, bcy = cy - by, bcz = cz - bz;
+    const double lab = abx * abx + aby * aby + abz * abz, lac = acx * acx + acy * acy + acz * acz;
+    const double lbc = bcx * bcx + bcy * bcy + bcz * bcz;
+    const double l2 = fmax(fmax(lab, lac), lbc);
+    const double nx = aby * acz - abz * acy, ny = abz * acx - abx * acz, nz = abx * acy - aby * acx;
+    const bool ill = l2 > 0.0 && !(64.0 * (nx * nx + ny * ny + nz * nz) >= l2 * l2);
+    double v[3][3] = {{ax, ay, az}, {bx, by, bz}, {cx, cy, cz}};
+    if (ill) {
+        // P, Q: the longest edge; R: the third corner
+        int ip = 0, iq = 1, ir = 2;
+        if (lac >= lab && lac >= lbc) ip = 0, iq = 2, ir = 1;
+        else if (lbc >= lab && lbc >= lac) ip = 1, iq = 2, ir = 0;
+        const double *P = v[ip], *Q = v[iq], *R = v[ir];
+        const double L = sqrt(l2);
+        double e[3] = {(Q[0] - P[0]) / L, (Q[1] - P[1]) / L, (Q[2] - P[2]) / L};
+        const double rp[3] = {R[0] - P[0], R[1] - P[1], R[2] - P[2]};
+        const double x = rp[0] * e[0] + rp[1] * e[1] + rp[2] * e[2];
+        double u[3] = {rp[0] - x * e[0], rp[1] - x * e[1], rp[2] - x * e[2]};  // R's offset off PQ
+        double lu = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+        if (!(lu > 1e-9 * L)) {  // collinear to rounding: any direction across PQ
+            const double w[3] = {fabs(e[0]) < 0.9 ? 1.0 : 0.0, fabs(e[0]) < 0.9 ? 0.0 : 1.0, 0.0};
+            u[0] = e[1] * w[2] - e[2] * w[1], u[1] = e[2] * w[0] - e[0] * w[2], u[2] = e[0] * w[1] - e[1] * w[0];
+        }
+        const double ue = u[0] * e[0] + u[1] * e[1] + u[2] * e[2];  // re-orthogonalised against PQ
+        for (int d = 0; d < 3; d++) u[d] -= ue * e[d];
+        lu = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+        for (int d = 0; d < 3; d++) u[d] /= lu;
+        double pr[3][3];
+        for (int d = 0; d < 3; d++) {
+            pr[0][d] = P[d] - 0.25 * L * e[d];
+            pr[1][d] = Q[d] + 0.25 * L * e[d];
+            pr[2][d] = 0.5 * (P[d] + Q[d]) + 0.5 * L * u[d];
+        }
+        for (int a = 0; a < 3; a++)
+            for (int d = 0; d < 3; d++) v[a][d] = pr[a][d];
+    }
+    out[0] = make_float4(float(v[0][0]), float(v[0][1]), float(v[0][2]), float(v[1][0]));
+    out[1] = make_float4(float(v[1][1]), float(v[1][2]), float(v[2][0]), float(v[2][1]));
+    out[2] = make_float4(float(v[2][2]), __int_as_float(t), ill ? __int_as_float(0x7f800000) : 0.f, 0.f);
+}
+
 __global__ void k_tri_records(int nt, const int *__restrict__ sorted_ids, const int *__restrict__ s0,
                               const int *__restrict__ s1, const int *__restrict__ s2, const double *__restrict__ vx,
                               const double *__restrict__ vy, const double *__restrict__ vz, float4 *__restrict__ t32,
-                              double2 *__restrict__ t64) {
+                              double2 *__restrict__ t64, float4 *__restrict__ filt) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= nt) return;
     const int t = sorted_ids[p];
@@ -446,15 +497,8 @@ __global__ void k_tri_records(int nt, const int *__restrict__ sorted_ids, const 
     const double cx = vx[c], cy = vy[c], cz = vz[c];
     t32[3 * p + 0] = make_float4(float(ax), float(ay), float(az), float(bx));
     t32[3 * p + 1] = make_float4(float(by), float(bz), float(cx), float(cy));
-    // ill-conditioned (height below 1/8 of the longest edge, or degenerate): the fix-up path keys it
-    // by its double distance instead of the float filter (see bvh_query.cu)
-    const double abx = bx - ax, aby = by - ay, abz = bz - az, acx = cx - ax, acy = cy - ay, acz = cz - az;
-    const double bcx = cx - bx, bcy = cy - by, bcz = cz - bz;
-    const double l2 = fmax(fmax(abx * abx + aby * aby + abz * abz, acx * acx + acy * acy + acz * acz),
-                           bcx * bcx + bcy * bcy + bcz * bcz);
-    const double nx = aby * acz - abz * acy, ny = abz * acx - abx * acz, nz = abx * acy - aby * acx;
-    const bool ill = !(64.0 * (nx * nx + ny * ny + nz * nz) >= l2 * l2) || !(l2 > 0.0);
-    t32[3 * p + 2] = make_float4(float(cz), __int_as_float(t), ill ? 1.f : 0.f, 0.f);
+    t32[3 * p + 2] = make_float4(float(cz), __int_as_float(t), 0.f, 0.f);
+    if (filt) filter_record(ax, ay, az, bx, by, bz, cx, cy, cz, t, filt + 3 * size_t(p));
     if (t64) {
         t64[5 * p + 0] = make_double2(ax, ay);
         t64[5 * p + 1] = make_double2(az, bx);
@@ -773,11 +817,12 @@ static int mesh_build_impl(MeshStorage *s, MeshStorage *tmp, DeviceMesh *m, int 
         }
     }
     // triangle records in leaf order
-    float4 *t32;
+    float4 *t32, *filt = nullptr;
     double2 *t64 = nullptr;
     SSDF_CHECK(dalloc(s, &t32, 3 * size_t(nt), stream));
     if (keep64) SSDF_CHECK(dalloc(s, &t64, 5 * size_t(nt), stream));
-    k_tri_records<<<grid_blocks(nt, 256), 256, 0, stream>>>(nt, ids, s0, s1, s2, vx, vy, vz, t32, t64);
+    if (keep64) SSDF_CHECK(dalloc(s, &filt, 3 * size_t(nt), stream));  // the fix-up path's filter records
+    k_tri_records<<<grid_blocks(nt, 256), 256, 0, stream>>>(nt, ids, s0, s1, s2, vx, vy, vz, t32, t64, filt);
     LAUNCH_CHECK("k_tri_records");
     int scale_bits = 0;
     SSDF_CUDA(cudaMemcpyAsync(&scale_bits, flags + 7, sizeof(int), cudaMemcpyDeviceToHost, stream));
@@ -796,6 +841,7 @@ static int mesh_build_impl(MeshStorage *s, MeshStorage *tmp, DeviceMesh *m, int 
     m->depth4 = depth4;
     m->tris32 = t32;
     m->tris64 = t64;
+    m->filt32 = filt;
     if (m->depth >= kStackSize || 3 * m->depth4 >= kStackSize)
         return fail(SSDF_ERR_NOT_SUPPORTED,
                     "BVH depth " + std::to_string(m->depth) + " exceeds the traversal stack (" +
