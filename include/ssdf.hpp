@@ -183,6 +183,40 @@ int all_points_aabb_signed_distance(const ptrdiff_t npoints, const G *const SSDF
                       "all_points_aabb_signed_distance: G and T are float or double");
 }
 
+// serial/bvh/bvh.hpp:54-66
+template <typename G, typename I>
+int points_inside_bvh(const ptrdiff_t npoints, const G *const SSDF_RESTRICT x, const G *const SSDF_RESTRICT y,
+                      const G *const SSDF_RESTRICT z, const ptrdiff_t nselements, const I *const SSDF_RESTRICT s0,
+                      const I *const SSDF_RESTRICT s1, const I *const SSDF_RESTRICT s2, const ptrdiff_t nspoints,
+                      const G *const SSDF_RESTRICT sx, const G *const SSDF_RESTRICT sy,
+                      const G *const SSDF_RESTRICT sz, uint8_t *const SSDF_RESTRICT out) {
+    static_assert(std::is_same<I, int>::value, "ssdf_b200 indices are int");
+    if constexpr (std::is_same<G, float>::value)
+        return ssdf_b200_points_inside_bvh_f(npoints, x, y, z, nselements, s0, s1, s2, nspoints, sx, sy, sz, out);
+    else if constexpr (std::is_same<G, double>::value)
+        return ssdf_b200_points_inside_bvh_d(npoints, x, y, z, nselements, s0, s1, s2, nspoints, sx, sy, sz, out);
+    else
+        static_assert(detail::always_false<G>::value, "points_inside_bvh: G is float or double");
+}
+
+// serial/bvh/bvh.hpp:230-247
+template <typename G, typename I>
+int sample_inside_bvh(const ptrdiff_t nselements, const I *const SSDF_RESTRICT s0, const I *const SSDF_RESTRICT s1,
+                      const I *const SSDF_RESTRICT s2, const ptrdiff_t nspoints, const G *const SSDF_RESTRICT sx,
+                      const G *const SSDF_RESTRICT sy, const G *const SSDF_RESTRICT sz, const ptrdiff_t nx,
+                      const ptrdiff_t ny, const ptrdiff_t nz, const G xmin, const G ymin, const G zmin, const G xmax,
+                      const G ymax, const G zmax, uint8_t *const SSDF_RESTRICT out) {
+    static_assert(std::is_same<I, int>::value, "ssdf_b200 indices are int");
+    if constexpr (std::is_same<G, float>::value)
+        return ssdf_b200_sample_inside_bvh_f(nselements, s0, s1, s2, nspoints, sx, sy, sz, nx, ny, nz, xmin, ymin,
+                                             zmin, xmax, ymax, zmax, out);
+    else if constexpr (std::is_same<G, double>::value)
+        return ssdf_b200_sample_inside_bvh_d(nselements, s0, s1, s2, nspoints, sx, sy, sz, nx, ny, nz, xmin, ymin,
+                                             zmin, xmax, ymax, zmax, out);
+    else
+        static_assert(detail::always_false<G>::value, "sample_inside_bvh: G is float or double");
+}
+
 // ---- level sets and field rebuilds (serial/bvh/sdf_rebuild.hpp) ----------------------------------
 
 // serial/bvh/sdf_rebuild.hpp:10-21: n[d] samples along axis d at o[d] + i h[d], x fastest.

@@ -129,6 +129,28 @@ int ssdf_b200_sample_sdf_bvh_dd(ptrdiff_t nselements, const int *s0, const int *
                                 ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, double xmin, double ymin, double zmin,
                                 double xmax, double ymax, double zmax, double *out);
 
+/* ---- drop-in: inside flags --------------------------------------------------------------------
+ * ssdf::points_inside_bvh<G, int> (serial/bvh/bvh.hpp:54-66, bvh.cpp:318-365) and
+ * ssdf::sample_inside_bvh<G, int> (bvh.hpp:230-247, bvh.cpp:1800-1866): out = 1 inside the closed
+ * surface, 0 outside, one byte per point / grid node. Inside is where sample_sdf_bvh's signed
+ * distance (pseudo-normal rule, in double) is negative; the reference asks cuBQL's
+ * pointIsInsideSurface, which cannot be built here. */
+int ssdf_b200_points_inside_bvh_f(ptrdiff_t npoints, const float *x, const float *y, const float *z,
+                                  ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                  ptrdiff_t nspoints, const float *sx, const float *sy, const float *sz, uint8_t *out);
+int ssdf_b200_points_inside_bvh_d(ptrdiff_t npoints, const double *x, const double *y, const double *z,
+                                  ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                  ptrdiff_t nspoints, const double *sx, const double *sy, const double *sz,
+                                  uint8_t *out);
+int ssdf_b200_sample_inside_bvh_f(ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                  ptrdiff_t nspoints, const float *sx, const float *sy, const float *sz, ptrdiff_t nx,
+                                  ptrdiff_t ny, ptrdiff_t nz, float xmin, float ymin, float zmin, float xmax,
+                                  float ymax, float zmax, uint8_t *out);
+int ssdf_b200_sample_inside_bvh_d(ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                  ptrdiff_t nspoints, const double *sx, const double *sy, const double *sz,
+                                  ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, double xmin, double ymin, double zmin,
+                                  double xmax, double ymax, double zmax, uint8_t *out);
+
 /* ---- drop-in: grid and box helpers ------------------------------------------------------------
  * ssdf::compute_aabb<G, T> (serial/edf/edf.hpp:500-539): the bounding box of npoints (>= 1) points,
  * each converted to T, written to the six scalars. Bitwise the reference's for NaN-free input (a

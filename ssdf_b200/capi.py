@@ -112,6 +112,9 @@ for _g, _gc in (("f", C.c_float), ("d", C.c_double)):
         _sig(f"ssdf_b200_compute_aabb_{_g}{_t}", [_pd, _vp, _vp, _vp] + [C.POINTER(_tc)] * 6)
         _sig(f"ssdf_b200_all_points_aabb_signed_distance_{_g}{_t}", [_pd, _vp, _vp, _vp] + [_tc] * 6 + [_vp])
 _sig("ssdf_points_aabb", [_pd, _vp, _vp, _vp, C.c_int, C.c_int, _vp, _vp])
+for _g, _gc in (("f", C.c_float), ("d", C.c_double)):
+    _sig(f"ssdf_b200_points_inside_bvh_{_g}", _EDF[:-1] + [_vp])
+    _sig(f"ssdf_b200_sample_inside_bvh_{_g}", _GRID + [_gc] * 6 + [_vp])
 for _g, _gc in (("ff", C.c_float), ("dd", C.c_double)):
     _GP = [C.POINTER(C.c_ssize_t * 3), C.POINTER(_gc * 3), C.POINTER(_gc * 3), _vp]
     _sig(f"ssdf_b200_level_set_triangles_{_g}", _GP + [_gc, _pd, _vp, _vp, _vp, C.POINTER(C.c_ssize_t)])
@@ -165,7 +168,9 @@ EXPORTED = ["ssdf_status_string", "ssdf_last_error", "ssdf_b200_version", "ssdf_
             "ssdf_batch_last_blocks", "ssdf_query_grid_noalloc", "ssdf_query_grid_noalloc_max", "ssdf_server_create",
             "ssdf_server_destroy", "ssdf_server_add_mesh", "ssdf_server_submit_points", "ssdf_server_submit_grid",
             "ssdf_server_wait", "ssdf_server_stats", "ssdf_server_reset_stats", "ssdf_autotune_grid",
-            "ssdf_points_aabb", "ssdf_points_aabb_signed_distance", "ssdf_batch_reserve", "ssdf_mesh_destroy_async"] + \
+            "ssdf_points_aabb", "ssdf_points_aabb_signed_distance", "ssdf_batch_reserve", "ssdf_mesh_destroy_async",
+            "ssdf_b200_points_inside_bvh_f", "ssdf_b200_points_inside_bvh_d", "ssdf_b200_sample_inside_bvh_f",
+            "ssdf_b200_sample_inside_bvh_d"] + \
     [f"ssdf_b200_{k}_{g}{t}" for k in ("compute_aabb", "all_points_aabb_signed_distance") for g in "fd" for t in "fd"] + \
     [f"ssdf_b200_{k}_{g}" for k in ("level_set_triangles", "rebuild_sdf", "refine_field", "round_sdf") for g in ("ff", "dd")]
 
@@ -289,6 +294,27 @@ def closest_point_bvh(points, mesh, outd=None, dtype=np.float64):
     fn = f"ssdf_b200_closest_point_bvh_{s}{s}"
     _check(getattr(lib, fn)(n, _p(x), _p(y), _p(z), *hm.args(), _p(d), _p(ox), _p(oy), _p(oz), _ipp(tri)), fn)
     return d, ox, oy, oz, tri
+
+
+def points_inside_bvh(points, mesh, dtype=np.float64):
+    """ssdf::points_inside_bvh on the GPU: uint8 flags, 1 inside the closed surface."""
+    x, y, z = _points(points, dtype)
+    out = np.empty(len(x), dtype=np.uint8)
+    hm = _HostMesh(mesh, dtype)
+    fn = f"ssdf_b200_points_inside_bvh_{_suffix(dtype)}"
+    _check(getattr(lib, fn)(len(x), _p(x), _p(y), _p(z), *hm.args(), _p(out)), fn)
+    return out
+
+
+def sample_inside_bvh(mesh, grid, dtype=np.float64):
+    """ssdf::sample_inside_bvh on the GPU: uint8 flags on the node grid."""
+    hm = _HostMesh(mesh, dtype)
+    out = np.empty(grid.size, dtype=np.uint8)
+    fn = f"ssdf_b200_sample_inside_bvh_{_suffix(dtype)}"
+    ct = C.c_double if np.dtype(dtype) == np.float64 else C.c_float
+    nx, ny, nz = grid.n
+    _check(getattr(lib, fn)(*hm.args(), nx, ny, nz, *[ct(v) for v in grid.lo], *[ct(v) for v in grid.hi], _p(out)), fn)
+    return out
 
 
 def compute_aabb(points, gdtype=np.float64, tdtype=None):

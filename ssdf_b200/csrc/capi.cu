@@ -363,6 +363,9 @@ const char *ssdf_last_error(void) { return t_error.c_str(); }
 
 const char *ssdf_b200_version(void) { return "ssdf_b200 0.1 (sm_100a)"; }
 
+#define EDF_ARGS_NOOUT(G)                                                                                         \
+    ptrdiff_t npoints, const G *x, const G *y, const G *z, ptrdiff_t nselements, const int *s0, const int *s1,      \
+        const int *s2, ptrdiff_t nspoints, const G *sx, const G *sy, const G *sz
 #define EDF_ARGS(G, T)                                                                                            \
     ptrdiff_t npoints, const G *x, const G *y, const G *z, ptrdiff_t nselements, const int *s0, const int *s1,    \
         const int *s2, ptrdiff_t nspoints, const G *sx, const G *sy, const G *sz, T *out
@@ -442,6 +445,65 @@ int ssdf_b200_sample_sdf_bvh_dd(GRID_ARGS(double, double)) {
 }
 int ssdf_b200_sample_sdf_index_bvh_dd(GRID_ARGS(double, double), int *outtri) {
     return bvh_grid_host<double, double>(GRID_PASS, outtri, SSDF_OUT_SDF, precision_from_env(SSDF_PREC_F32_FIXUP));
+}
+
+// ---- inside flags (serial/bvh/bvh.cpp:318-365, 1800-1866) ------------------------------------------
+// 1 where the signed distance (sample_sdf_bvh's pseudo-normal rule, in double) is negative.
+
+int ssdf_b200_points_inside_bvh_f(EDF_ARGS_NOOUT(float), uint8_t *out) {
+    if (npoints > 0 && !out) return fail(SSDF_ERR_INVALID_ARGUMENT, "null output array");
+    std::vector<double> d(static_cast<size_t>(npoints > 0 ? npoints : 0));
+    SSDF_CHECK((bvh_points_host<float, double>(npoints, x, y, z, nselements, s0, s1, s2, nspoints, sx, sy, sz,
+                                               d.data(), nullptr, nullptr, nullptr, nullptr, SSDF_OUT_SDF,
+                                               precision_from_env(SSDF_PREC_F32_FIXUP))));
+    if (nselements == 0 || nspoints == 0) return SSDF_OK;
+    for (ptrdiff_t i = 0; i < npoints; i++) out[i] = d[size_t(i)] < 0 ? 1 : 0;
+    return SSDF_OK;
+}
+int ssdf_b200_points_inside_bvh_d(EDF_ARGS_NOOUT(double), uint8_t *out) {
+    if (npoints > 0 && !out) return fail(SSDF_ERR_INVALID_ARGUMENT, "null output array");
+    std::vector<double> d(static_cast<size_t>(npoints > 0 ? npoints : 0));
+    SSDF_CHECK((bvh_points_host<double, double>(npoints, x, y, z, nselements, s0, s1, s2, nspoints, sx, sy, sz,
+                                                d.data(), nullptr, nullptr, nullptr, nullptr, SSDF_OUT_SDF,
+                                                precision_from_env(SSDF_PREC_F32_FIXUP))));
+    if (nselements == 0 || nspoints == 0) return SSDF_OK;
+    for (ptrdiff_t i = 0; i < npoints; i++) out[i] = d[size_t(i)] < 0 ? 1 : 0;
+    return SSDF_OK;
+}
+
+}  // extern "C"
+
+template <typename G>
+static int sample_inside_host(ptrdiff_t nselements, const int *s0, const int *s1, const int *s2, ptrdiff_t nspoints,
+                       const G *sx, const G *sy, const G *sz, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, G xmin, G ymin,
+                       G zmin, G xmax, G ymax, G zmax, uint8_t *out) {
+    if (nx < 0 || ny < 0 || nz < 0) return fail(SSDF_ERR_INVALID_ARGUMENT, "negative grid size");
+    const long long n = (long long)nx * ny * nz;
+    if (n > 0 && !out) return fail(SSDF_ERR_INVALID_ARGUMENT, "null output array");
+    std::vector<double> d(static_cast<size_t>(n));
+    SSDF_CHECK((bvh_grid_host<G, double>(nselements, s0, s1, s2, nspoints, sx, sy, sz, nx, ny, nz, xmin, ymin, zmin,
+                                         xmax, ymax, zmax, d.data(), nullptr, SSDF_OUT_SDF,
+                                         precision_from_env(SSDF_PREC_F32_FIXUP))));
+    if (nselements == 0 || nspoints == 0) return SSDF_OK;
+    for (long long i = 0; i < n; i++) out[i] = d[size_t(i)] < 0 ? 1 : 0;
+    return SSDF_OK;
+}
+
+extern "C" {
+
+int ssdf_b200_sample_inside_bvh_f(ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                  ptrdiff_t nspoints, const float *sx, const float *sy, const float *sz, ptrdiff_t nx,
+                                  ptrdiff_t ny, ptrdiff_t nz, float xmin, float ymin, float zmin, float xmax,
+                                  float ymax, float zmax, uint8_t *out) {
+    return sample_inside_host<float>(nselements, s0, s1, s2, nspoints, sx, sy, sz, nx, ny, nz, xmin, ymin, zmin, xmax,
+                                     ymax, zmax, out);
+}
+int ssdf_b200_sample_inside_bvh_d(ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                  ptrdiff_t nspoints, const double *sx, const double *sy, const double *sz,
+                                  ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, double xmin, double ymin, double zmin,
+                                  double xmax, double ymax, double zmax, uint8_t *out) {
+    return sample_inside_host<double>(nselements, s0, s1, s2, nspoints, sx, sy, sz, nx, ny, nz, xmin, ymin, zmin, xmax,
+                                      ymax, zmax, out);
 }
 
 // ---- grid and box helpers (serial/edf/edf.hpp:500-557) ---------------------------------------------
