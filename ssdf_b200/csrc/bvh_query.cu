@@ -1232,6 +1232,7 @@ unsigned window_grid() {
 }
 
 int launch_query(const QueryArgs &args_in, int precision, cudaStream_t stream) {
+    retain_pool_memory();
     QueryArgs a = args_in;
     const long long n = a.is_grid ? a.nx * a.ny * a.nz : a.npoints;
     if (n <= 0) return SSDF_OK;

@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -48,7 +49,29 @@ int env_int(const char *name, int dflt) {
 
 const char *env_str(const char *name) { return getenv(name); }
 
+// The library's scratch (overflow lists, staging buffers, mesh storage) comes from the device's
+// default stream-ordered pool. With the pool's default release threshold of 0, memory freed back to it
+// is returned to the device at every synchronisation, so the next query maps it again (134 MB of
+// overflow list for a 256^3 grid), at a cost that varied from run to run by up to half the query.
+// The library keeps freed memory in the pool instead (once per device); it stays reusable by any
+// cudaMallocAsync of the process and is released by cudaMemPoolTrimTo or at exit.
+void retain_pool_memory() {
+    static std::mutex mu;
+    static bool done[64] = {false};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = ~uint64_t(0);
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    done[dev] = true;
+}
+
 cudaStream_t library_stream() {
+    retain_pool_memory();
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
     if (!t_stream || t_stream_device != dev) {

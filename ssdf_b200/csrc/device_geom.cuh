@@ -170,12 +170,14 @@ __device__ __forceinline__ T box_dist_sq(const T px, const T py, const T pz, con
     return dx * dx + dy * dy + dz * dz;
 }
 
+// The same distance as p - clamp(p, lo, hi) per axis: bitwise the magnitude of max(lo - p, p - hi, 0)
+// (and +inf for an inverted, empty box) in three instructions per axis instead of four.
 __device__ __forceinline__ float box_dist_sq_fast(const float px, const float py, const float pz, const float lox,
                                                   const float hix, const float loy, const float hiy,
                                                   const float loz, const float hiz) {
-    const float dx = fmaxf(fmaxf(lox - px, px - hix), 0.f);
-    const float dy = fmaxf(fmaxf(loy - py, py - hiy), 0.f);
-    const float dz = fmaxf(fmaxf(loz - pz, pz - hiz), 0.f);
+    const float dx = px - fminf(fmaxf(px, lox), hix);
+    const float dy = py - fminf(fmaxf(py, loy), hiy);
+    const float dz = pz - fminf(fmaxf(pz, loz), hiz);
     return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
 }
 

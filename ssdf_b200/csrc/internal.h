@@ -213,6 +213,7 @@ inline int grid_blocks(long long n, int threads) { return int((n + threads - 1) 
 int env_int(const char *name, int dflt);
 const char *env_str(const char *name);
 cudaStream_t library_stream();  // per-thread non-blocking stream for the blocking entry points
+void retain_pool_memory();      // keep freed scratch in the device's default pool (once per device)
 
 }  // namespace ssdf_b200
 

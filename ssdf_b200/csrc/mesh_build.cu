@@ -858,6 +858,7 @@ int mesh_build(MeshStorage **storage, DeviceMesh *mesh, ptrdiff_t nt, const int 
     if (opts.leaf_size < 0 || opts.leaf_size > kMaxLeafSize)
         return fail(SSDF_ERR_INVALID_ARGUMENT, "leaf_size must be 0 (default) or 1.." + std::to_string(kMaxLeafSize));
     if (!s0 || !s1 || !s2 || !sx || !sy || !sz) return fail(SSDF_ERR_INVALID_ARGUMENT, "null mesh array");
+    retain_pool_memory();
     MeshStorage *s = new MeshStorage();
     MeshStorage tmp;
     *mesh = DeviceMesh();
