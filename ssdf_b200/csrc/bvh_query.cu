@@ -69,8 +69,10 @@ __device__ __forceinline__ float finf() { return __int_as_float(0x7f800000); }
 __device__ __forceinline__ bool map_query(const QueryArgs &a, long long b, int s, long long &q, long long &i,
                                           long long &j, long long &k) {
     if (!a.is_grid) {
-        q = (b * kQ + s) * kThreads + threadIdx.x;
-        return q < a.npoints;
+        const long long slot = (b * kQ + s) * kThreads + threadIdx.x;
+        if (slot >= a.npoints) return false;
+        q = a.order ? (long long)__ldg(a.order + slot) : slot;
+        return true;
     }
     const long long bxn = (a.nx + 7) >> 3, byn = (a.ny + 3) >> 2;
     const long long bx = b % bxn, r = b / bxn;
@@ -1213,8 +1215,44 @@ static bool use_warp(const QueryArgs &a) {
     const char *v = env_str("SSDF_B200_TRAVERSAL");
     if (v && !strcmp(v, "warp")) return true;
     if (v && !strcmp(v, "thread")) return false;
-    return a.is_grid != 0;
+    return a.is_grid != 0 || a.order != nullptr;  // sorted point lists are coherent enough for packets
 }
+
+// Point lists in Morton order: a warp's 32 slots then hold neighbouring points, which the packet walk
+// needs (in input order a warp of scattered queries keeps about 5 of its lanes busy). Keys are 30-bit
+// Morton codes of the points in the mesh's bounding box (the union of the root's two child boxes),
+// points outside it clamped to its faces; the stable radix sort makes the order deterministic.
+__global__ void k_point_keys(long long n, const void *__restrict__ x, const void *__restrict__ y,
+                             const void *__restrict__ z, int f64, const float4 *__restrict__ root,
+                             uint32_t *__restrict__ keys, int *__restrict__ vals) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 c0 = __ldg(root), c1 = __ldg(root + 1), c2 = __ldg(root + 2);
+    // child boxes: (lox, hix, loy, hiy) of each, then (loz, hiz) of both; an empty child is inverted
+    const float lo[3] = {fminf(c0.x, c1.x), fminf(c0.z, c1.z), fminf(c2.x, c2.z)};
+    const float hi[3] = {fmaxf(c0.y, c1.y), fmaxf(c0.w, c1.w), fmaxf(c2.y, c2.w)};
+    const float p[3] = {f64 ? float(((const double *)x)[i]) : ((const float *)x)[i],
+                        f64 ? float(((const double *)y)[i]) : ((const float *)y)[i],
+                        f64 ? float(((const double *)z)[i]) : ((const float *)z)[i]};
+    uint32_t key = 0;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const float ext = hi[d] - lo[d];
+        float u = ext > 0.f ? (p[d] - lo[d]) / ext : 0.5f;
+        u = fminf(fmaxf(u, 0.f), 1.f);  // NaN -> 0
+        uint32_t v = uint32_t(fminf(u * 1024.f, 1023.f));
+        v = (v * 0x00010001u) & 0xFF0000FFu;
+        v = (v * 0x00000101u) & 0x0F00F00Fu;
+        v = (v * 0x00000011u) & 0xC30C30C3u;
+        v = (v * 0x00000005u) & 0x49249249u;
+        key |= v << (2 - d);
+    }
+    keys[i] = key;
+    vals[i] = int(i);
+}
+
+// Point lists of at least this many queries are sorted (SSDF_B200_SORT_POINTS=0 keeps input order).
+constexpr long long kSortMinPoints = 4096;
 
 // Blocks of the second fix-up stage (kWindowBlocksPerSm per SM, four warps each). The warps stride
 // over the overflow count, which is only known on the device.
@@ -1249,6 +1287,28 @@ int launch_query(const QueryArgs &args_in, int precision, cudaStream_t stream) {
     if (precision == SSDF_PREC_F32 && (a.output == SSDF_OUT_SDF || a.output == SSDF_OUT_CLOSEST))
         return fail(SSDF_ERR_INVALID_ARGUMENT, "SSDF_PREC_F32 serves the edf and sqedf outputs");
     const bool count = env_int("SSDF_B200_COUNT", 0) != 0;
+    // large point lists: visit them in Morton order, as warp packets (results are per query, so the
+    // order changes nothing but the time); the order array is freed behind the launches
+    struct StreamFree {  // stream-ordered frees when the launch returns, on every path
+        void *p[2];
+        cudaStream_t s;
+        ~StreamFree() {
+            for (void *q : p)
+                if (q) cudaFreeAsync(q, s);
+        }
+    } sorted{{nullptr, nullptr}, stream};
+    if (!a.is_grid && !a.force_traversal && n >= kSortMinPoints && n < 0x7fffffffll &&
+        env_int("SSDF_B200_SORT_POINTS", 1) != 0) {
+        SSDF_CUDA(cudaMallocAsync(&sorted.p[0], sizeof(uint32_t) * size_t(n), stream));
+        SSDF_CUDA(cudaMallocAsync(&sorted.p[1], sizeof(int) * size_t(n), stream));
+        uint32_t *keys = static_cast<uint32_t *>(sorted.p[0]);
+        int *order = static_cast<int *>(sorted.p[1]);
+        k_point_keys<<<unsigned((n + 255) / 256), 256, 0, stream>>>(n, a.x, a.y, a.z, a.coord_f64, a.m.nodes32,
+                                                                   keys, order);
+        SSDF_CUDA(cudaGetLastError());
+        SSDF_CHECK(radix_sort_pairs_u32(keys, order, int(n), 30, stream));
+        a.order = order;
+    }
     const bool warp = use_warp(a);
     const bool wide = use_wide(a);
     const long long nblocks = query_blocks(a);

@@ -115,6 +115,8 @@ struct QueryArgs {
     // 0: environment / default; traversal 1 warp packets, 2 thread per query; arity 2 or 4
     int force_traversal;
     int force_arity;
+    // point lists: the visiting order (query index per slot, Morton-sorted), or null (input order)
+    const int *order;
 };
 
 // Job table header of a batch (device memory).
