@@ -1,7 +1,8 @@
 // ssdf.hpp -- the reference's C++ template API (namespace ssdf), served by the B200 library.
 //
 // A drop-in for zulianp/ssdf's serial/ssdf.hpp (edf, edf_celllist, edf_select) and
-// serial/bvh/bvh.hpp (edf_bvh, closest_point_bvh, sample_sqedf_bvh, sample_sdf_bvh) and the grid
+// serial/bvh/bvh.hpp (edf_bvh, closest_point_bvh, sample_sqedf_bvh, sample_sdf_bvh, inside flags,
+// closest_within_radius_*) and the grid
 // helpers of serial/edf/edf.hpp (compute_aabb, all_points_aabb_signed_distance): same names,
 // template parameters <G coordinates, T outputs, I indices>, argument order, in/out semantics and
 // int return (0 on success). Each instantiation the reference provides maps onto one C symbol of
@@ -302,6 +303,64 @@ int round_sdf(const GridGeometry<G> &grid, const T *const f, const T radius, con
         return ssdf_b200_round_sdf_dd(grid.n, grid.o, grid.h, f, radius, band, open, close, stride, out, f0);
     else
         static_assert(detail::always_false<G, T>::value, "round_sdf is instantiated for <float,float> and <double,double>");
+}
+
+// serial/bvh/bvh.hpp:68-154: the closest primitive within a radius. Instantiations
+// <float, float>, <float, double>, <double, double> (serial/bvh/bvh.cpp:1272-1521).
+#define SSDF_B200_RADIUS_SIG(G, T)                                                                                \
+    const ptrdiff_t npoints, const G *const SSDF_RESTRICT x, const G *const SSDF_RESTRICT y,                      \
+        const G *const SSDF_RESTRICT z, const ptrdiff_t nselements, const I *const SSDF_RESTRICT s0,               \
+        const I *const SSDF_RESTRICT s1, const I *const SSDF_RESTRICT s2
+#define SSDF_B200_RADIUS_TAIL(G, T)                                                                               \
+    const ptrdiff_t nspoints, const G *const SSDF_RESTRICT sx, const G *const SSDF_RESTRICT sy,                   \
+        const G *const SSDF_RESTRICT sz, const ptrdiff_t radius_stride, const T *const SSDF_RESTRICT radius_squared, \
+        I *const SSDF_RESTRICT outtri, T *const SSDF_RESTRICT out_sqr_dist
+#define SSDF_B200_RADIUS_DISPATCH(NAME, ...)                                                                      \
+    static_assert(std::is_same<I, int>::value, "ssdf_b200 indices are int");                                     \
+    if constexpr (std::is_same<G, float>::value && std::is_same<T, float>::value)                                 \
+        return ssdf_b200_##NAME##_ff(__VA_ARGS__);                                                                \
+    else if constexpr (std::is_same<G, float>::value && std::is_same<T, double>::value)                           \
+        return ssdf_b200_##NAME##_fd(__VA_ARGS__);                                                                \
+    else if constexpr (std::is_same<G, double>::value && std::is_same<T, double>::value)                          \
+        return ssdf_b200_##NAME##_dd(__VA_ARGS__);                                                                \
+    else                                                                                                          \
+        static_assert(detail::always_false<G, T>::value, #NAME ": <float,float>, <float,double>, <double,double>")
+
+template <typename G, typename T, typename I>
+int closest_within_radius_bvh(SSDF_B200_RADIUS_SIG(G, T), SSDF_B200_RADIUS_TAIL(G, T),
+                              T *const SSDF_RESTRICT closest_x, T *const SSDF_RESTRICT closest_y,
+                              T *const SSDF_RESTRICT closest_z, const bool skip_self = false) {
+    SSDF_B200_RADIUS_DISPATCH(closest_within_radius_bvh, npoints, x, y, z, nselements, s0, s1, s2, nspoints, sx, sy,
+                              sz, radius_stride, radius_squared, outtri, out_sqr_dist, closest_x, closest_y, closest_z,
+                              skip_self ? 1 : 0);
+}
+
+template <typename G, typename T, typename I>
+int closest_within_radius_local_bvh(SSDF_B200_RADIUS_SIG(G, T), SSDF_B200_RADIUS_TAIL(G, T),
+                                    T *const SSDF_RESTRICT closest_s, T *const SSDF_RESTRICT closest_t,
+                                    const bool skip_self = false) {
+    SSDF_B200_RADIUS_DISPATCH(closest_within_radius_local_bvh, npoints, x, y, z, nselements, s0, s1, s2, nspoints, sx,
+                              sy, sz, radius_stride, radius_squared, outtri, out_sqr_dist, closest_s, closest_t,
+                              skip_self ? 1 : 0);
+}
+
+template <typename G, typename T, typename I>
+int closest_within_radius_quads_bvh(SSDF_B200_RADIUS_SIG(G, T), const I *const SSDF_RESTRICT s3,
+                                    SSDF_B200_RADIUS_TAIL(G, T), T *const SSDF_RESTRICT closest_x,
+                                    T *const SSDF_RESTRICT closest_y, T *const SSDF_RESTRICT closest_z,
+                                    const bool skip_self = false) {
+    SSDF_B200_RADIUS_DISPATCH(closest_within_radius_quads_bvh, npoints, x, y, z, nselements, s0, s1, s2, s3, nspoints,
+                              sx, sy, sz, radius_stride, radius_squared, outtri, out_sqr_dist, closest_x, closest_y,
+                              closest_z, skip_self ? 1 : 0);
+}
+
+template <typename G, typename T, typename I>
+int closest_within_radius_quads_local_bvh(SSDF_B200_RADIUS_SIG(G, T), const I *const SSDF_RESTRICT s3,
+                                          SSDF_B200_RADIUS_TAIL(G, T), T *const SSDF_RESTRICT closest_s,
+                                          T *const SSDF_RESTRICT closest_t, const bool skip_self = false) {
+    SSDF_B200_RADIUS_DISPATCH(closest_within_radius_quads_local_bvh, npoints, x, y, z, nselements, s0, s1, s2, s3,
+                              nspoints, sx, sy, sz, radius_stride, radius_squared, outtri, out_sqr_dist, closest_s,
+                              closest_t, skip_self ? 1 : 0);
 }
 
 }  // namespace ssdf

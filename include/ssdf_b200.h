@@ -151,6 +151,100 @@ int ssdf_b200_sample_inside_bvh_d(ptrdiff_t nselements, const int *s0, const int
                                   ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, double xmin, double ymin, double zmin,
                                   double xmax, double ymax, double zmax, uint8_t *out);
 
+/* ---- drop-in: closest primitive within a radius ----------------------------------------------
+ * ssdf::closest_within_radius_bvh, _local_bvh, _quads_bvh, _quads_local_bvh<G, T, int>
+ * (serial/bvh/bvh.hpp:68-154, bvh.cpp:367-832), for (G, T) = (float, float) _ff, (float, double) _fd
+ * and (double, double) _dd. Per point pid: the primitive (triangle s0/s1/s2, or quad s0/s1/s2/s3)
+ * whose float closest point is nearest, among those at squared distance at most
+ * radius_squared[pid * radius_stride] (stride 0: one radius for all), skipping primitives that have
+ * pid as a corner when skip_self != 0 (node-to-surface self contact). Outputs, written for every
+ * point: outtri (-1 when none), out_sqr_dist (the float squared distance, or the float radius
+ * squared when none), and the closest point (closest_x/y/z; zeros when none) or its local
+ * coordinates (closest_s/t: triangle_local_coordinates_st in T for triangles, the clamped bilinear
+ * parameters for quads; zeros when none). Arithmetic is float as in the reference; cuBQL's triangle
+ * closest point is replaced by the reference's point_triangle_closest_point<float>, and among
+ * primitives at the same squared distance the lowest index wins. The reference's skip_self defaults
+ * to false; here it is an explicit argument. */
+int ssdf_b200_closest_within_radius_bvh_ff(ptrdiff_t npoints, const float *x, const float *y, const float *z,
+                                           ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                           ptrdiff_t nspoints, const float *sx, const float *sy, const float *sz,
+                                           ptrdiff_t radius_stride, const float *radius_squared, int *outtri,
+                                           float *out_sqr_dist, float *closest_x, float *closest_y,
+                                           float *closest_z, int skip_self);
+int ssdf_b200_closest_within_radius_bvh_fd(ptrdiff_t npoints, const float *x, const float *y, const float *z,
+                                           ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                           ptrdiff_t nspoints, const float *sx, const float *sy, const float *sz,
+                                           ptrdiff_t radius_stride, const double *radius_squared, int *outtri,
+                                           double *out_sqr_dist, double *closest_x, double *closest_y,
+                                           double *closest_z, int skip_self);
+int ssdf_b200_closest_within_radius_bvh_dd(ptrdiff_t npoints, const double *x, const double *y, const double *z,
+                                           ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                           ptrdiff_t nspoints, const double *sx, const double *sy, const double *sz,
+                                           ptrdiff_t radius_stride, const double *radius_squared, int *outtri,
+                                           double *out_sqr_dist, double *closest_x, double *closest_y,
+                                           double *closest_z, int skip_self);
+int ssdf_b200_closest_within_radius_local_bvh_ff(ptrdiff_t npoints, const float *x, const float *y, const float *z,
+                                                 ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                                 ptrdiff_t nspoints, const float *sx, const float *sy,
+                                                 const float *sz, ptrdiff_t radius_stride,
+                                                 const float *radius_squared, int *outtri, float *out_sqr_dist,
+                                                 float *closest_s, float *closest_t, int skip_self);
+int ssdf_b200_closest_within_radius_local_bvh_fd(ptrdiff_t npoints, const float *x, const float *y, const float *z,
+                                                 ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                                 ptrdiff_t nspoints, const float *sx, const float *sy,
+                                                 const float *sz, ptrdiff_t radius_stride,
+                                                 const double *radius_squared, int *outtri, double *out_sqr_dist,
+                                                 double *closest_s, double *closest_t, int skip_self);
+int ssdf_b200_closest_within_radius_local_bvh_dd(ptrdiff_t npoints, const double *x, const double *y,
+                                                 const double *z, ptrdiff_t nselements, const int *s0, const int *s1,
+                                                 const int *s2, ptrdiff_t nspoints, const double *sx,
+                                                 const double *sy, const double *sz, ptrdiff_t radius_stride,
+                                                 const double *radius_squared, int *outtri, double *out_sqr_dist,
+                                                 double *closest_s, double *closest_t, int skip_self);
+int ssdf_b200_closest_within_radius_quads_bvh_ff(ptrdiff_t npoints, const float *x, const float *y, const float *z,
+                                                 ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                                 const int *s3, ptrdiff_t nspoints, const float *sx, const float *sy,
+                                                 const float *sz, ptrdiff_t radius_stride,
+                                                 const float *radius_squared, int *outtri, float *out_sqr_dist,
+                                                 float *closest_x, float *closest_y, float *closest_z, int skip_self);
+int ssdf_b200_closest_within_radius_quads_bvh_fd(ptrdiff_t npoints, const float *x, const float *y, const float *z,
+                                                 ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                                 const int *s3, ptrdiff_t nspoints, const float *sx, const float *sy,
+                                                 const float *sz, ptrdiff_t radius_stride,
+                                                 const double *radius_squared, int *outtri, double *out_sqr_dist,
+                                                 double *closest_x, double *closest_y, double *closest_z,
+                                                 int skip_self);
+int ssdf_b200_closest_within_radius_quads_bvh_dd(ptrdiff_t npoints, const double *x, const double *y,
+                                                 const double *z, ptrdiff_t nselements, const int *s0, const int *s1,
+                                                 const int *s2, const int *s3, ptrdiff_t nspoints, const double *sx,
+                                                 const double *sy, const double *sz, ptrdiff_t radius_stride,
+                                                 const double *radius_squared, int *outtri, double *out_sqr_dist,
+                                                 double *closest_x, double *closest_y, double *closest_z,
+                                                 int skip_self);
+int ssdf_b200_closest_within_radius_quads_local_bvh_ff(ptrdiff_t npoints, const float *x, const float *y,
+                                                       const float *z, ptrdiff_t nselements, const int *s0,
+                                                       const int *s1, const int *s2, const int *s3,
+                                                       ptrdiff_t nspoints, const float *sx, const float *sy,
+                                                       const float *sz, ptrdiff_t radius_stride,
+                                                       const float *radius_squared, int *outtri, float *out_sqr_dist,
+                                                       float *closest_s, float *closest_t, int skip_self);
+int ssdf_b200_closest_within_radius_quads_local_bvh_fd(ptrdiff_t npoints, const float *x, const float *y,
+                                                       const float *z, ptrdiff_t nselements, const int *s0,
+                                                       const int *s1, const int *s2, const int *s3,
+                                                       ptrdiff_t nspoints, const float *sx, const float *sy,
+                                                       const float *sz, ptrdiff_t radius_stride,
+                                                       const double *radius_squared, int *outtri,
+                                                       double *out_sqr_dist, double *closest_s, double *closest_t,
+                                                       int skip_self);
+int ssdf_b200_closest_within_radius_quads_local_bvh_dd(ptrdiff_t npoints, const double *x, const double *y,
+                                                       const double *z, ptrdiff_t nselements, const int *s0,
+                                                       const int *s1, const int *s2, const int *s3,
+                                                       ptrdiff_t nspoints, const double *sx, const double *sy,
+                                                       const double *sz, ptrdiff_t radius_stride,
+                                                       const double *radius_squared, int *outtri,
+                                                       double *out_sqr_dist, double *closest_s, double *closest_t,
+                                                       int skip_self);
+
 /* ---- drop-in: grid and box helpers ------------------------------------------------------------
  * ssdf::compute_aabb<G, T> (serial/edf/edf.hpp:500-539): the bounding box of npoints (>= 1) points,
  * each converted to T, written to the six scalars. Bitwise the reference's for NaN-free input (a

@@ -97,6 +97,18 @@ def lib() -> C.CDLL:
         _lib.oracle_closest_point_d.restype = C.c_int
         _lib.oracle_closest_point_d.argtypes = [_pd, _dp, _dp, _dp, _pd, _ip, _ip, _ip, _pd, _dp, _dp, _dp,
                                                 _dp, _dp, _dp, _dp, _ip]
+        for suf, (gp, tp) in (("_ff", (_fp, _fp)), ("_fd", (_fp, _dp)), ("_dd", (_dp, _dp))):
+            f = getattr(_lib, "oracle_within_radius" + suf)
+            f.restype = C.c_int
+            f.argtypes = [_pd, gp, gp, gp, _pd, _ip, _ip, _ip, _ip, gp, gp, gp, _pd, tp, C.c_int, C.c_int, _ip,
+                          tp, tp, tp, tp]
+        for suf, fptr, ft in (("_d", _dp, C.c_double), ("_f", _fp, C.c_float)):
+            f = getattr(_lib, "oracle_point_to_quad_closest_point" + suf)
+            f.restype = None
+            f.argtypes = [ft] * 15 + [fptr, fptr]
+            f = getattr(_lib, "oracle_point_triangle_barycentric" + suf)
+            f.restype = ft
+            f.argtypes = [ft] * 12 + [fptr] * 3
         _lib.oracle_sqedf_points_d.restype = C.c_int
         _lib.oracle_sqedf_points_d.argtypes = [_pd, _dp, _dp, _dp, _pd, _ip, _ip, _ip, _pd, _dp, _dp, _dp, _dp]
     return _lib
@@ -132,6 +144,13 @@ def ref() -> C.CDLL:
             f = getattr(_ref, "ref_all_points_aabb_signed_distance" + suf)
             f.restype = None
             f.argtypes = [_pd, fptr, fptr, fptr, fptr, fptr]
+        for suf, fptr, ft in (("_d", _dp, C.c_double), ("_f", _fp, C.c_float)):
+            f = getattr(_ref, "ref_point_to_quad_closest_point" + suf)
+            f.restype = None
+            f.argtypes = [fptr, fptr, fptr]
+            f = getattr(_ref, "ref_point_triangle_barycentric" + suf)
+            f.restype = ft
+            f.argtypes = [ft] * 12 + [fptr]
         _ref.ref_set_quiet.restype = None
         _ref.ref_set_quiet.argtypes = [C.c_int]
         _ref.ref_set_quiet(1)
@@ -326,3 +345,64 @@ def round_sdf(n, o, h, f, radius, band, open=True, close=True, stride=1, dtype=n
     if close:
         cur = (rebuild_sdf(n, o, h, cur, -t(radius), band, 1, dtype) - t(radius)).astype(dtype)
     return rebuild_sdf(n, o, h, cur, 0, band, stride, dtype), r0
+
+
+# ----------------------------------------------------------------------------------------------
+# closest primitive within a radius (serial/bvh/bvh.cpp:367-832)
+# ----------------------------------------------------------------------------------------------
+
+def quad_closest_st(p, quad, dtype=np.float64, reference=False):
+    """(s, t) of point p on the quad (4 x 3 corners): point_to_quad_closest_point
+    (serial/edf/edf.hpp:388-489), the restatement or (reference=True) the reference's own."""
+    ct, suf = _real(dtype)
+    p = np.asarray(p, dtype=dtype)
+    v = np.asarray(quad, dtype=dtype).reshape(12)
+    if reference:
+        st = np.zeros(2, dtype=dtype)
+        getattr(ref(), "ref_point_to_quad_closest_point" + suf)(_ptr(np.ascontiguousarray(p), ct), _ptr(np.ascontiguousarray(v), ct),
+                                                       _ptr(st, ct))
+        return float(st[0]), float(st[1])
+    s, t = ct(), ct()
+    getattr(lib(), "oracle_point_to_quad_closest_point" + suf)(*[ct(float(a)) for a in p], *[ct(float(a)) for a in v],
+                                                      C.byref(s), C.byref(t))
+    return s.value, t.value
+
+
+def triangle_barycentric(q, tri, dtype=np.float64, reference=False):
+    """(d2, wa, wb, wc): point_triangle_barycentric (serial/edf/edf.hpp:251-386)."""
+    ct, suf = _real(dtype)
+    args = [ct(float(a)) for a in np.asarray(q, dtype=dtype)] + [ct(float(a)) for a in np.asarray(tri, dtype=dtype).reshape(9)]
+    w = np.zeros(3, dtype=dtype)
+    if reference:
+        d2 = getattr(ref(), "ref_point_triangle_barycentric" + suf)(*args, _ptr(w, ct))
+        return d2, float(w[0]), float(w[1]), float(w[2])
+    wa, wb, wc = ct(), ct(), ct()
+    d2 = getattr(lib(), "oracle_point_triangle_barycentric" + suf)(*args, C.byref(wa), C.byref(wb), C.byref(wc))
+    return d2, wa.value, wb.value, wc.value
+
+
+def within_radius(points, elements, vertices, radius_squared, stride=1, skip_self=False, local=False,
+                  gdtype=np.float64, tdtype=None):
+    """Brute-force closest primitive within a radius: closest_within_radius_bvh (elements = 3
+    index arrays, triangles) or closest_within_radius_quads_bvh (4 arrays, quads), with local=True
+    their _local_ variants. Returns (outtri, out_sqr_dist, o0, o1[, o2])."""
+    tdtype = gdtype if tdtype is None else tdtype
+    suf = {(np.float32, np.float32): "_ff", (np.float32, np.float64): "_fd",
+           (np.float64, np.float64): "_dd"}[(np.dtype(gdtype).type, np.dtype(tdtype).type)]
+    gct = C.c_float if np.dtype(gdtype) == np.float32 else C.c_double
+    tct = C.c_float if np.dtype(tdtype) == np.float32 else C.c_double
+    x, y, z = (np.ascontiguousarray(a, dtype=gdtype) for a in points)
+    sx, sy, sz = (np.ascontiguousarray(a, dtype=gdtype) for a in vertices)
+    idx = [np.ascontiguousarray(a, dtype=np.int32) for a in elements]
+    quads = len(idx) == 4
+    r2 = np.ascontiguousarray(radius_squared, dtype=tdtype)
+    n = len(x)
+    outtri = np.empty(n, dtype=np.int32)
+    outs = [np.empty(n, dtype=tdtype) for _ in range(4)]
+    getattr(lib(), "oracle_within_radius" + suf)(n, _ptr(x, gct), _ptr(y, gct), _ptr(z, gct), len(idx[0]),
+                                        *[_ptr(a, C.c_int) for a in idx[:3]],
+                                        _ptr(idx[3], C.c_int) if quads else None,
+                                        _ptr(sx, gct), _ptr(sy, gct), _ptr(sz, gct), int(stride), _ptr(r2, tct),
+                                        int(bool(skip_self)), int(bool(local)), _ptr(outtri, C.c_int),
+                                        *[_ptr(a, tct) for a in outs])
+    return (outtri, outs[0], outs[1], outs[2]) if local else (outtri, *outs)

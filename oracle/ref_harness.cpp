@@ -73,4 +73,19 @@ double ref_point_aabb_signed_distance_d(double px, double py, double pz, double 
     }
 REF_BOX(double, _d)
 REF_BOX(float, _f)
+
+// point_triangle_barycentric / point_to_quad_closest_point (serial/edf/edf.hpp:251-489), the
+// primitives of the closest-within-radius queries.
+#define REF_QUAD(T, SUF)                                                                                      \
+    T ref_point_triangle_barycentric##SUF(T qx, T qy, T qz, T ax, T ay, T az, T bx, T by, T bz, T cx, T cy,    \
+                                          T cz, T *w) {                                                       \
+        return ssdf::point_triangle_barycentric<T>(qx, qy, qz, ax, ay, az, bx, by, bz, cx, cy, cz, w, w + 1,   \
+                                                   w + 2);                                                    \
+    }                                                                                                         \
+    void ref_point_to_quad_closest_point##SUF(const T *p, const T *v, T *st) {                                \
+        ssdf::point_to_quad_closest_point<T>(p[0], p[1], p[2], v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7],  \
+                                             v[8], v[9], v[10], v[11], st, st + 1);                           \
+    }
+REF_QUAD(double, _d)
+REF_QUAD(float, _f)
 }

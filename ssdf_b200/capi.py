@@ -121,6 +121,12 @@ for _g, _gc in (("ff", C.c_float), ("dd", C.c_double)):
     _sig(f"ssdf_b200_rebuild_sdf_{_g}", _GP + [_gc, _gc, _pd, _vp])
     _sig(f"ssdf_b200_refine_field_{_g}", _GP + [_pd, _vp])
     _sig(f"ssdf_b200_round_sdf_{_g}", _GP + [_gc, _gc, C.c_int, C.c_int, _pd, _vp, _vp])
+for _g in ("ff", "fd", "dd"):
+    _sig(f"ssdf_b200_closest_within_radius_bvh_{_g}", _EDF[:-1] + [_pd, _vp, _ip] + [_vp] * 4 + [C.c_int])
+    _sig(f"ssdf_b200_closest_within_radius_local_bvh_{_g}", _EDF[:-1] + [_pd, _vp, _ip] + [_vp] * 3 + [C.c_int])
+    _QE = [_pd, _vp, _vp, _vp, _pd, _ip, _ip, _ip, _ip, _pd, _vp, _vp, _vp]
+    _sig(f"ssdf_b200_closest_within_radius_quads_bvh_{_g}", _QE + [_pd, _vp, _ip] + [_vp] * 4 + [C.c_int])
+    _sig(f"ssdf_b200_closest_within_radius_quads_local_bvh_{_g}", _QE + [_pd, _vp, _ip] + [_vp] * 3 + [C.c_int])
 _sig("ssdf_points_aabb_signed_distance", [_pd, _vp, _vp, _vp, C.c_int, C.POINTER(C.c_double * 6), C.c_int, _vp,
                                           C.c_int, _vp])
 
@@ -172,7 +178,9 @@ EXPORTED = ["ssdf_status_string", "ssdf_last_error", "ssdf_b200_version", "ssdf_
             "ssdf_b200_points_inside_bvh_f", "ssdf_b200_points_inside_bvh_d", "ssdf_b200_sample_inside_bvh_f",
             "ssdf_b200_sample_inside_bvh_d"] + \
     [f"ssdf_b200_{k}_{g}{t}" for k in ("compute_aabb", "all_points_aabb_signed_distance") for g in "fd" for t in "fd"] + \
-    [f"ssdf_b200_{k}_{g}" for k in ("level_set_triangles", "rebuild_sdf", "refine_field", "round_sdf") for g in ("ff", "dd")]
+    [f"ssdf_b200_{k}_{g}" for k in ("level_set_triangles", "rebuild_sdf", "refine_field", "round_sdf") for g in ("ff", "dd")] + \
+    [f"ssdf_b200_closest_within_radius_{k}_{g}" for k in ("bvh", "local_bvh", "quads_bvh", "quads_local_bvh")
+     for g in ("ff", "fd", "dd")]
 
 
 def _status_name(status: int) -> str:
@@ -294,6 +302,32 @@ def closest_point_bvh(points, mesh, outd=None, dtype=np.float64):
     fn = f"ssdf_b200_closest_point_bvh_{s}{s}"
     _check(getattr(lib, fn)(n, _p(x), _p(y), _p(z), *hm.args(), _p(d), _p(ox), _p(oy), _p(oz), _ipp(tri)), fn)
     return d, ox, oy, oz, tri
+
+
+def closest_within_radius(points, elements, vertices, radius_squared, stride=1, skip_self=False, local=False,
+                          gdtype=np.float64, tdtype=None):
+    """ssdf::closest_within_radius_bvh / _local_bvh (elements = three index arrays, triangles) and
+    _quads_bvh / _quads_local_bvh (four arrays, quads) on the GPU. Returns (outtri, out_sqr_dist,
+    closest_x, closest_y, closest_z), or (outtri, out_sqr_dist, closest_s, closest_t) when local."""
+    tdtype = gdtype if tdtype is None else tdtype
+    x, y, z = _points(points, gdtype)
+    sx, sy, sz = (_arr(a, gdtype) for a in vertices)
+    idx = [_arr(a, np.int32) for a in elements]
+    if len(idx) not in (3, 4):
+        raise ValueError("elements: three (triangles) or four (quads) index arrays")
+    r2 = _arr(radius_squared, tdtype)
+    n = len(x)
+    need = (stride * (n - 1) + 1) if n else 0
+    if stride < 0 or len(r2) < need:
+        raise ValueError(f"radius_squared holds {len(r2)} values; stride {stride} over {n} points needs {need}")
+    outtri = np.empty(n, dtype=np.int32)
+    outs = [np.empty(n, dtype=tdtype) for _ in range(3 if local else 4)]
+    kind = ("quads_" if len(idx) == 4 else "") + ("local_" if local else "") + "bvh"
+    fn = f"ssdf_b200_closest_within_radius_{kind}_{_suffix(gdtype)}{_suffix(tdtype)}"
+    _check(getattr(lib, fn)(n, _p(x), _p(y), _p(z), len(idx[0]), *[_ipp(a) for a in idx], len(sx), _p(sx), _p(sy),
+                            _p(sz), int(stride), _p(r2), _ipp(outtri), *[_p(a) for a in outs], int(bool(skip_self))),
+           fn)
+    return (outtri, *outs)
 
 
 def points_inside_bvh(points, mesh, dtype=np.float64):

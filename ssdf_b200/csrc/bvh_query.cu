@@ -1254,6 +1254,28 @@ __global__ void k_point_keys(long long n, const void *__restrict__ x, const void
 // Point lists of at least this many queries are sorted (SSDF_B200_SORT_POINTS=0 keeps input order).
 constexpr long long kSortMinPoints = 4096;
 
+int morton_point_order(long long n, const void *x, const void *y, const void *z, int f64, const float4 *nodes32,
+                       int **order, cudaStream_t stream) {
+    *order = nullptr;
+    if (n <= 0 || n >= 0x7fffffffll) return fail(SSDF_ERR_INVALID_ARGUMENT, "point count out of range for sorting");
+    uint32_t *keys = nullptr;
+    SSDF_CUDA(cudaMallocAsync(&keys, sizeof(uint32_t) * size_t(n), stream));
+    cudaError_t e = cudaMallocAsync(order, sizeof(int) * size_t(n), stream);
+    int st = e == cudaSuccess ? SSDF_OK : cuda_fail(e, "sort order", __FILE__, __LINE__);
+    if (st == SSDF_OK) {
+        k_point_keys<<<unsigned((n + 255) / 256), 256, 0, stream>>>(n, x, y, z, f64, nodes32, keys, *order);
+        e = cudaGetLastError();
+        st = e == cudaSuccess ? radix_sort_pairs_u32(keys, *order, int(n), 30, stream)
+                              : cuda_fail(e, "point keys", __FILE__, __LINE__);
+    }
+    cudaFreeAsync(keys, stream);
+    if (st != SSDF_OK && *order) {
+        cudaFreeAsync(*order, stream);
+        *order = nullptr;
+    }
+    return st;
+}
+
 // Blocks of the second fix-up stage (kWindowBlocksPerSm per SM, four warps each). The warps stride
 // over the overflow count, which is only known on the device.
 unsigned window_grid() {
@@ -1289,25 +1311,17 @@ int launch_query(const QueryArgs &args_in, int precision, cudaStream_t stream) {
     const bool count = env_int("SSDF_B200_COUNT", 0) != 0;
     // large point lists: visit them in Morton order, as warp packets (results are per query, so the
     // order changes nothing but the time); the order array is freed behind the launches
-    struct StreamFree {  // stream-ordered frees when the launch returns, on every path
-        void *p[2];
+    struct StreamFree {  // stream-ordered free when the launch returns, on every path
+        int *p;
         cudaStream_t s;
         ~StreamFree() {
-            for (void *q : p)
-                if (q) cudaFreeAsync(q, s);
+            if (p) cudaFreeAsync(p, s);
         }
-    } sorted{{nullptr, nullptr}, stream};
+    } sorted{nullptr, stream};
     if (!a.is_grid && !a.force_traversal && n >= kSortMinPoints && n < 0x7fffffffll &&
         env_int("SSDF_B200_SORT_POINTS", 1) != 0) {
-        SSDF_CUDA(cudaMallocAsync(&sorted.p[0], sizeof(uint32_t) * size_t(n), stream));
-        SSDF_CUDA(cudaMallocAsync(&sorted.p[1], sizeof(int) * size_t(n), stream));
-        uint32_t *keys = static_cast<uint32_t *>(sorted.p[0]);
-        int *order = static_cast<int *>(sorted.p[1]);
-        k_point_keys<<<unsigned((n + 255) / 256), 256, 0, stream>>>(n, a.x, a.y, a.z, a.coord_f64, a.m.nodes32,
-                                                                   keys, order);
-        SSDF_CUDA(cudaGetLastError());
-        SSDF_CHECK(radix_sort_pairs_u32(keys, order, int(n), 30, stream));
-        a.order = order;
+        SSDF_CHECK(morton_point_order(n, a.x, a.y, a.z, a.coord_f64, a.m.nodes32, &sorted.p, stream));
+        a.order = sorted.p;
     }
     const bool warp = use_warp(a);
     const bool wide = use_wide(a);

@@ -212,6 +212,10 @@ int round_device(const GridDesc &gd, const T *d_f, T radius, T band, bool open, 
 
 // ---- small helpers -------------------------------------------------------------------------------
 inline int grid_blocks(long long n, int threads) { return int((n + threads - 1) / threads); }
+// Morton order of n (< 2^31) points over the mesh's root box: *order (n ints, stream-ordered
+// allocation the caller frees with cudaFreeAsync) lists the point indices in key order (bvh_query.cu).
+int morton_point_order(long long n, const void *x, const void *y, const void *z, int f64, const float4 *nodes32,
+                       int **order, cudaStream_t stream);
 int env_int(const char *name, int dflt);
 const char *env_str(const char *name);
 cudaStream_t library_stream();  // per-thread non-blocking stream for the blocking entry points

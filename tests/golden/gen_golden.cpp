@@ -8,6 +8,8 @@
 //                        20 points, edf<double> and edf_select<double> (= edf_celllist without cuBQL)
 //   point_aabb           tests/point_aabb_distance_test.cpp:24-35   seven points, unit box
 //   box_sdf              tests/signed_distance_box_test.cpp:23-38   eleven points
+//   quad_closest         tests/point_quad_closest_point_test.cpp:8-160   segment, triangle and five
+//                        quads (basic, warped, concave, concave notch, degenerate), double
 //
 // Doubles are printed with 17 significant digits and floats with 9, which round-trip exactly.
 #include <cmath>
@@ -135,6 +137,38 @@ int main(int argc, char **argv) {
         put_d(f, "x", px), put_d(f, "y", py), put_d(f, "z", pz);
         put_d(f, "expected", expected);
         put_d(f, "reference", got, true);
+        std::fprintf(f, "  },\n");
+    }
+
+    {  // tests/point_quad_closest_point_test.cpp: rows (point, 4 corners, expected s, t)
+        const double c[5][17] = {
+            {0.25, 0.75, 1, 0, 0, 0, 1, 0, 0, 1, 1, 0, 0, 1, 0, 0.25, 0.75},
+            {0.7, 0.2, 0.225, 0, 0, 0, 1, 0, 0.25, 1, 1, 0.5, 0, 1, -0.25, 0.7, 0.2},
+            {0.3, 1.0, 0, 0, 0, 0, 2, 0, 0, 0.75, 0.5, 0, 0, 2, 0, 0.4, 0.8},
+            {11.0 / 12.0, 5.0 / 6.0, 0, 0, 0, 0, 2, 0, 0, 0.75, 0.5, 0, 0, 2, 0, 13.0 / 15.0, 1},
+            {1.5, 1, 0, 0, 0, 0, 1, 0, 0, 2, 0, 0, 3, 0, 0, 1, 0.5}};
+        std::vector<double> rows, expected, got;
+        for (auto &r : c) {
+            double s = -1, t = -1;
+            ssdf::point_to_quad_closest_point<double>(r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7], r[8], r[9], r[10],
+                                                      r[11], r[12], r[13], r[14], &s, &t);
+            for (int k = 0; k < 15; k++) rows.push_back(r[k]);
+            expected.push_back(r[15]), expected.push_back(r[16]);
+            got.push_back(s), got.push_back(t);
+        }
+        double u = -1, wa = -1, wb = -1, wc = -1;
+        const double dseg = ssdf::point_segment_parameter(0.25, 1.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, &u);
+        const double dtri = ssdf::point_triangle_barycentric(0.25, 0.25, 1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0,
+                                                             0.0, &wa, &wb, &wc);
+        std::fprintf(f, "  \"quad_closest\": {\n    \"tolerance\": 1e-12,\n");
+        std::fprintf(f, "    \"names\": [\"basic\", \"warped\", \"concave\", \"concave notch\", \"degenerate\"],\n");
+        put_d(f, "rows", rows);
+        put_d(f, "expected", expected);
+        put_d(f, "reference", got);
+        put_d(f, "triangle", {0.25, 0.25, 1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0, 0.0});
+        put_d(f, "triangle_expected", {1.0, 0.5, 0.25, 0.25});
+        put_d(f, "triangle_reference", {dtri, wa, wb, wc});
+        put_d(f, "segment_reference", {dseg, u}, true);
         std::fprintf(f, "  }\n");
     }
 

@@ -61,6 +61,17 @@ def test_cpp_header_compiles_against_c_abi(tmp_path):
         "  (void)ssdf::refine_field<float, float>;\n"
         "  (void)ssdf::round_sdf<double, double>;\n"
         "  (void)g.strided(2).refined(2).size();\n"
+        "  int q3[1] = {2}, tri[1];\n"
+        "  double r2[1] = {1.0}, d2[1], cx[1], cy[1], cz[1];\n"
+        "  float fx[1] = {0}, fy[1] = {0}, fz[1] = {2}, fsx[3] = {0, 1, 0}, fsy[3] = {0, 0, 1}, fsz[3] = {0, 0, 0};\n"
+        "  (void)ssdf::closest_within_radius_bvh<double, double, int>(1, x, y, z, 1, s0, s1, s2, 3, sx, sy, sz, 1, r2,\n"
+        "      tri, d2, cx, cy, cz);\n"
+        "  (void)ssdf::closest_within_radius_local_bvh<float, double, int>(1, fx, fy, fz, 1, s0, s1, s2, 3, fsx, fsy,\n"
+        "      fsz, 0, r2, tri, d2, cx, cy, true);\n"
+        "  (void)ssdf::closest_within_radius_quads_bvh<float, double, int>(1, fx, fy, fz, 1, s0, s1, s2, q3, 3, fsx,\n"
+        "      fsy, fsz, 1, r2, tri, d2, cx, cy, cz);\n"
+        "  (void)ssdf::closest_within_radius_quads_local_bvh<double, double, int>(1, x, y, z, 1, s0, s1, s2, q3, 3, sx,\n"
+        "      sy, sz, 1, r2, tri, d2, cx, cy);\n"
         "  return 0;\n}\n")
     lib = os.path.join(ROOT, "ssdf_b200", "_lib")
     res = subprocess.run(["g++", "-std=c++17", f"-I{ROOT}/include", str(src), "-o", str(tmp_path / "use"),
@@ -82,3 +93,25 @@ def test_build_imports_without_the_library():
     code = "import ssdf_b200 as S; assert S.capi.lib is not None; assert S.version() == S.capi.version()"
     res = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True)
     assert res.returncode == 0, res.stderr
+
+
+def test_radius_queries_validate_on_the_host():
+    """closest_within_radius_*: bad indices and sizes are rejected before any device work, and an
+    empty point set returns at once (neither needs a GPU)."""
+    import numpy as np
+
+    import ssdf_b200 as S
+
+    pts = np.zeros((3, 4))
+    verts = np.zeros((3, 3))
+    tri = [np.array([0]), np.array([1]), np.array([3])]
+    with pytest.raises(S.SsdfError) as e:
+        S.closest_within_radius(pts, tri, verts, np.ones(4))
+    assert e.value.status == S.SSDF_ERR_INVALID_ARGUMENT
+    quad = [np.array([0]), np.array([1]), np.array([2]), np.array([-1])]
+    with pytest.raises(S.SsdfError):
+        S.closest_within_radius(pts, quad, verts, np.ones(4), local=True, gdtype=np.float32)
+    out = S.closest_within_radius(np.zeros((3, 0)), [np.array([0]), np.array([1]), np.array([2])], verts, np.ones(0))
+    assert len(out) == 5 and len(out[0]) == 0
+    with pytest.raises(ValueError):
+        S.closest_within_radius(pts, [np.array([0]), np.array([1]), np.array([2])], verts, np.ones(2))

@@ -10,6 +10,7 @@
   tests/sample_sdf_bvh_test.cpp), restated.
 """
 
+import ctypes
 import os
 
 import numpy as np
@@ -207,3 +208,99 @@ def test_box_helpers_golden_and_reference(dtype):
     box = np.array([-1, 2, 0, 3, -2, 1], dtype=dtype)
     d = oracle.all_points_aabb_signed_distance(p, box, dtype)
     assert np.array_equal(d, oracle.all_points_aabb_signed_distance(p, box, dtype, reference=True))
+
+
+# ---- closest primitive within a radius (serial/bvh/bvh.cpp:367-832) ----------------------------
+
+def test_golden_quad_closest_point():
+    g = load_golden_json()["quad_closest"]
+    rows = np.array(g["rows"]).reshape(-1, 15)
+    for k, name in enumerate(g["names"]):
+        s, t = oracle.quad_closest_st(rows[k, :3], rows[k, 3:])
+        assert (s, t) == tuple(g["reference"][2 * k: 2 * k + 2]), name
+        assert abs(s - g["expected"][2 * k]) < g["tolerance"] and abs(t - g["expected"][2 * k + 1]) < g["tolerance"]
+    tri = g["triangle"]
+    assert oracle.triangle_barycentric(tri[:3], tri[3:]) == tuple(g["triangle_reference"])
+
+
+def _random_quads(rng, n, dtype):
+    base = rng.uniform(-1, 1, size=(n, 1, 3))
+    quads = base + rng.uniform(-0.5, 0.5, size=(n, 4, 3))
+    quads[: n // 8, 3] = quads[: n // 8, 2]  # a repeated corner
+    quads[n // 8: n // 4] = quads[n // 8: n // 4, :1] + np.linspace(0, 1, 4)[None, :, None] * rng.normal(size=(n // 8, 1, 3))
+    quads[n // 4: n // 3, :, 2] = 0.25  # planar
+    return quads.astype(dtype)
+
+
+@needs_ref
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_quad_and_barycentric_against_reference(dtype):
+    """The restated primitives equal the reference's own templates bit for bit on random, planar,
+    collinear and repeated-corner inputs."""
+    rng = np.random.default_rng(17)
+    quads = _random_quads(rng, 800, dtype)
+    pts = rng.uniform(-2, 2, size=(800, 3)).astype(dtype)
+    for p, q in zip(pts, quads):
+        assert oracle.quad_closest_st(p, q, dtype) == oracle.quad_closest_st(p, q, dtype, reference=True)
+        tri = q[:3]
+        a, b = oracle.triangle_barycentric(p, tri, dtype), oracle.triangle_barycentric(p, tri, dtype, reference=True)
+        assert a == b or all((x == y) or (np.isnan(x) and np.isnan(y)) for x, y in zip(a, b))
+
+
+def _brute_within(points, quads_or_tris, verts, r2, skip_self):
+    """Independent float restatement of the per-point loop, on top of the pinned primitives."""
+    n = points.shape[1]
+    out = []
+    for pid in range(n):
+        q = points[:, pid].astype(np.float32)
+        best, bt = np.float32(r2[pid]), -1
+        for e, idx in enumerate(quads_or_tris):
+            if skip_self and pid in idx:
+                continue
+            c = verts[:, idx].T.astype(np.float32)
+            if len(idx) == 4:
+                s, t = oracle.quad_closest_st(q, c, np.float32)
+                s, t = np.float32(s), np.float32(t)
+                w = [(1 - s) * (1 - t), s * (1 - t), s * t, (1 - s) * t]
+                cp = ((c[0] * w[0] + c[1] * w[1]) + c[2] * w[2]) + c[3] * w[3]
+            else:
+                o = [ctypes.c_float() for _ in range(3)]
+                oracle.lib().oracle_point_triangle_closest_point_f(*q, *c.reshape(9), *[ctypes.byref(v) for v in o])
+                cp = np.array([v.value for v in o], np.float32)
+            d = q - cp
+            d2 = np.float32(np.float32(d[0] * d[0] + d[1] * d[1]) + d[2] * d[2])
+            if d2 != np.inf and (d2 < best or (d2 == best and bt < 0)):
+                best, bt = d2, e
+        out.append((bt, best))
+    return out
+
+
+@pytest.mark.parametrize("quads", [False, True])
+def test_within_radius_oracle_semantics(quads):
+    rng = np.random.default_rng(3 + quads)
+    verts = rng.uniform(0, 1, size=(3, 40))
+    k = 4 if quads else 3
+    elems = [rng.choice(40, size=k, replace=False) for _ in range(30)]
+    pts = verts[:, :25] + rng.normal(0, 0.05, size=(3, 25))
+    pts[:, 20:] = verts[:, 20:25]  # on corners: skip_self matters
+    r2 = np.where(np.arange(25) % 3 == 0, 1e-4, 0.05)
+    r2[5] = np.inf
+    r2[6] = -1.0
+    for skip in (False, True):
+        got = oracle.within_radius(pts.astype(np.float32), [np.array([e[j] for e in elems]) for j in range(k)],
+                                   verts.astype(np.float32), r2.astype(np.float32), skip_self=skip,
+                                   gdtype=np.float32)
+        want = _brute_within(pts, elems, verts, r2.astype(np.float32), skip)
+        assert [int(t) for t in got[0]] == [w[0] for w in want]
+        assert np.array_equal(got[1], np.array([w[1] for w in want], np.float32))
+        none = got[0] < 0
+        assert np.all(got[2][none] == 0) and np.all(got[3][none] == 0) and np.all(got[4][none] == 0)
+        assert got[1][6] == -1.0 and got[0][6] == -1
+    # stride 0: one radius for every point; the local variant carries the same index and distance
+    a = oracle.within_radius(pts, [np.array([e[j] for e in elems]) for j in range(k)], verts, np.array([0.01]),
+                             stride=0)
+    b = oracle.within_radius(pts, [np.array([e[j] for e in elems]) for j in range(k)], verts, np.array([0.01]),
+                             stride=0, local=True)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    if quads:
+        assert np.all((b[2] >= 0) & (b[2] <= 1) & (b[3] >= 0) & (b[3] <= 1))
