@@ -160,9 +160,15 @@ int ssdf_batch_run(ssdf_batch *b, int use_graph, void *stream_) {
     cudaStream_t stream = (cudaStream_t)stream_;
     const int njobs = int(b->jobs.size());
     if (njobs == 0) return SSDF_OK;
-    bool any_grid = false;
-    for (const auto &j : b->jobs) any_grid |= j.is_grid != 0;
-    const bool warp = b->traversal == 1 ? true : b->traversal == 2 ? false : default_warp(any_grid);
+    // point jobs of kSortMinPoints or more are visited in Morton order (computed before the launch,
+    // outside any graph; freed in stream order behind it), which lets them walk as warp packets
+    const bool sort_points = b->traversal != 2 && env_int("SSDF_B200_SORT_POINTS", 1) != 0;
+    bool any_grid = false, any_sorted = false;
+    for (const auto &j : b->jobs) {
+        any_grid |= j.is_grid != 0;
+        any_sorted |= sort_points && !j.is_grid && j.npoints >= kSortMinPoints;
+    }
+    const bool warp = b->traversal == 1 ? true : b->traversal == 2 ? false : default_warp(any_grid || any_sorted);
     const bool wide = b->arity == 4 ? true : b->arity == 2 ? false : default_wide();
     // largest jobs first: the tail of the launch is then made of small items
     std::vector<int> order(njobs);
@@ -176,10 +182,23 @@ int ssdf_batch_run(ssdf_batch *b, int use_graph, void *stream_) {
     if (need > b->fb_cap) SSDF_CHECK(ssdf_batch_reserve(b, (long long)(need / 2), stream));
     // the staging buffers may still feed the previous run's copies
     SSDF_CUDA(cudaStreamSynchronize(stream));
+    struct Orders {  // the runs' visiting orders, freed in stream order when the call returns
+        std::vector<int *> p;
+        cudaStream_t s;
+        ~Orders() {
+            for (int *q : p) cudaFreeAsync(q, s);
+        }
+    } orders{{}, stream};
     long long total = 0;
     size_t off = 0;
     for (int k = 0; k < njobs; k++) {
         QueryArgs a = b->jobs[order[k]];
+        if (sort_points && !a.is_grid && a.npoints >= kSortMinPoints) {
+            int *ord = nullptr;
+            SSDF_CHECK(morton_point_order(a.npoints, a.x, a.y, a.z, a.coord_f64, a.m.nodes32, &ord, stream));
+            orders.p.push_back(ord);
+            a.order = ord;
+        }
         if (b->precision == SSDF_PREC_F32_FIXUP) {
             const size_t n = size_t(a.is_grid ? a.nx * a.ny * a.nz : a.npoints);
             a.fallback_count = b->d_fbcount + k;

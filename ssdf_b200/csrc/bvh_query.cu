@@ -1251,8 +1251,18 @@ __global__ void k_point_keys(long long n, const void *__restrict__ x, const void
     vals[i] = int(i);
 }
 
-// Point lists of at least this many queries are sorted (SSDF_B200_SORT_POINTS=0 keeps input order).
-constexpr long long kSortMinPoints = 4096;
+// Measured on B200: the torus knot with 29 % of its triangles slivers still runs 1.4x faster on the
+// fix-up path than on FP64; the beam lattice (64 % slivers, in parallel bundles) runs 5x slower.
+constexpr double kIllMaxFraction = 0.5;
+
+// The fix-up path hands a mesh to the FP64 kernel when more than this fraction of its triangles are
+// ill-conditioned (SSDF_B200_ILL_MAX overrides; above 1 never).
+bool sliver_heavy(const DeviceMesh &m) {
+    const char *v = env_str("SSDF_B200_ILL_MAX");
+    const double f = v ? atof(v) : kIllMaxFraction;
+    return m.nt > 0 && double(m.nill) > f * double(m.nt);
+}
+
 
 int morton_point_order(long long n, const void *x, const void *y, const void *z, int f64, const float4 *nodes32,
                        int **order, cudaStream_t stream) {
@@ -1304,6 +1314,10 @@ int launch_query(const QueryArgs &args_in, int precision, cudaStream_t stream) {
         return fail(SSDF_ERR_INVALID_ARGUMENT, "signed queries need a mesh built with normals=1");
     if (a.output == SSDF_OUT_SDF && !a.m.tris64)
         return fail(SSDF_ERR_INVALID_ARGUMENT, "signed queries need the double triangles (keep_fp64=1)");
+    // A mesh made mostly of ill-conditioned triangles (needles, slivers) is answered faster by the
+    // plain FP64 kernel: the fix-up filter sees each such triangle through a wide proxy, whose keys
+    // crowd the window. Both give the same bits.
+    if (precision == SSDF_PREC_F32_FIXUP && sliver_heavy(a.m)) precision = SSDF_PREC_F64;
     if (a.output == SSDF_OUT_CLOSEST && (!a.m.tris64 || !a.outx || !a.outy || !a.outz || !a.outtri))
         return fail(SSDF_ERR_INVALID_ARGUMENT, "closest-point queries need outx/outy/outz/outtri and double data");
     if (precision == SSDF_PREC_F32 && (a.output == SSDF_OUT_SDF || a.output == SSDF_OUT_CLOSEST))

@@ -84,6 +84,8 @@ struct DeviceMesh {
     const double *vertex_n = nullptr;  // [3 * nv]
     // scale of the coordinates (max |coordinate| over the mesh), for the fix-up window
     float coord_scale = 0.f;
+    // triangles the fix-up filter sees through a proxy (ill-conditioned; 0 without the double data)
+    int nill = 0;
 };
 
 // Everything a query launch needs; built by the host entry points.
@@ -212,6 +214,9 @@ int round_device(const GridDesc &gd, const T *d_f, T radius, T band, bool open, 
 
 // ---- small helpers -------------------------------------------------------------------------------
 inline int grid_blocks(long long n, int threads) { return int((n + threads - 1) / threads); }
+// Point lists of at least this many queries are visited in Morton order (SSDF_B200_SORT_POINTS=0
+// keeps input order).
+constexpr long long kSortMinPoints = 4096;
 // Morton order of n (< 2^31) points over the mesh's root box: *order (n ints, stream-ordered
 // allocation the caller frees with cudaFreeAsync) lists the point indices in key order (bvh_query.cu).
 int morton_point_order(long long n, const void *x, const void *y, const void *z, int f64, const float4 *nodes32,

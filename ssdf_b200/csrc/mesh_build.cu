@@ -441,7 +441,7 @@ __global__ void k_depth(int n, int L, const int *__restrict__ count, const int *
 // proxy is at least L/6 high over all of PQ, so it contains P, Q and R; its distance is a lower
 // bound of the triangle's, and its height (1/3 of its base) keeps the float test accurate. The
 // record's w.z is 0, or +inf for a proxy (whose key may enter the window but never move its centre).
-__device__ void filter_record(double ax, double ay, double az, double bx, double by, double bz, double cx,
+__device__ bool filter_record(double ax, double ay, double az, double bx, double by, double bz, double cx,
                               double cy, double cz, int t, float4 *__restrict__ out) {
     const double abx = bx - ax, aby = by - ay, abz = bz - az, acx = cx - ax, acy = cy - ay, acz = cz - az;
     const double bcx = cx - bx, bcy = cy - by, bcz = cz - bz;
@@ -483,12 +483,13 @@ __device__ void filter_record(double ax, double ay, double az, double bx, double
     out[0] = make_float4(float(v[0][0]), float(v[0][1]), float(v[0][2]), float(v[1][0]));
     out[1] = make_float4(float(v[1][1]), float(v[1][2]), float(v[2][0]), float(v[2][1]));
     out[2] = make_float4(float(v[2][2]), __int_as_float(t), ill ? __int_as_float(0x7f800000) : 0.f, 0.f);
+    return ill;
 }
 
 __global__ void k_tri_records(int nt, const int *__restrict__ sorted_ids, const int *__restrict__ s0,
                               const int *__restrict__ s1, const int *__restrict__ s2, const double *__restrict__ vx,
                               const double *__restrict__ vy, const double *__restrict__ vz, float4 *__restrict__ t32,
-                              double2 *__restrict__ t64, float4 *__restrict__ filt) {
+                              double2 *__restrict__ t64, float4 *__restrict__ filt, int *__restrict__ nill) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= nt) return;
     const int t = sorted_ids[p];
@@ -498,7 +499,7 @@ __global__ void k_tri_records(int nt, const int *__restrict__ sorted_ids, const 
     t32[3 * p + 0] = make_float4(float(ax), float(ay), float(az), float(bx));
     t32[3 * p + 1] = make_float4(float(by), float(bz), float(cx), float(cy));
     t32[3 * p + 2] = make_float4(float(cz), __int_as_float(t), 0.f, 0.f);
-    if (filt) filter_record(ax, ay, az, bx, by, bz, cx, cy, cz, t, filt + 3 * size_t(p));
+    if (filt && filter_record(ax, ay, az, bx, by, bz, cx, cy, cz, t, filt + 3 * size_t(p))) atomicAdd(nill, 1);
     if (t64) {
         t64[5 * p + 0] = make_double2(ax, ay);
         t64[5 * p + 1] = make_double2(az, bx);
@@ -697,7 +698,7 @@ static int mesh_build_impl(MeshStorage *s, MeshStorage *tmp, DeviceMesh *m, int 
                                                                  (const float *)gz, vx, vy, vz);
     LAUNCH_CHECK("k_widen");
     // validation + per-triangle boxes
-    int *flags;  // [0] first bad triangle, [1..6] scene, [7] scale, [8..9] depth / leaves
+    int *flags;  // [0] first bad triangle, [1..6] scene, [7] scale, [8..9] depth / leaves, [10] ill
     SSDF_CHECK(dalloc(tmp, &flags, 16, stream));
     {
         // ordered-int encodings (f2o) of +FLT_MAX and -FLT_MAX seed the scene min / max
@@ -822,15 +823,18 @@ static int mesh_build_impl(MeshStorage *s, MeshStorage *tmp, DeviceMesh *m, int 
     SSDF_CHECK(dalloc(s, &t32, 3 * size_t(nt), stream));
     if (keep64) SSDF_CHECK(dalloc(s, &t64, 5 * size_t(nt), stream));
     if (keep64) SSDF_CHECK(dalloc(s, &filt, 3 * size_t(nt), stream));  // the fix-up path's filter records
-    k_tri_records<<<grid_blocks(nt, 256), 256, 0, stream>>>(nt, ids, s0, s1, s2, vx, vy, vz, t32, t64, filt);
+    k_tri_records<<<grid_blocks(nt, 256), 256, 0, stream>>>(nt, ids, s0, s1, s2, vx, vy, vz, t32, t64, filt,
+                                                            flags + 10);
     LAUNCH_CHECK("k_tri_records");
-    int scale_bits = 0;
+    int scale_bits = 0, nill = 0;
     SSDF_CUDA(cudaMemcpyAsync(&scale_bits, flags + 7, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    SSDF_CUDA(cudaMemcpyAsync(&nill, flags + 10, sizeof(int), cudaMemcpyDeviceToHost, stream));
     if (opts.normals) SSDF_CHECK(build_normals(s, m, s0, s1, s2, vx, vy, vz, stream));
     SSDF_CUDA(cudaStreamSynchronize(stream));
     float scale;
     memcpy(&scale, &scale_bits, sizeof(float));
     m->coord_scale = scale;
+    m->nill = nill;
     m->depth = depth_leaves[0];
     m->nleaves = depth_leaves[1];
     m->nodes32 = nodes32;

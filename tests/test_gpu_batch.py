@@ -10,6 +10,7 @@ import pytest
 import oracle
 import ssdf_b200 as S
 from ssdf_b200 import workloads as W
+from test_gpu_golden import env
 
 pytestmark = pytest.mark.gpu
 
@@ -126,8 +127,8 @@ def test_batch_rejects_mixed_precision(jobs):
 
 
 def test_alternating_graph_keys_after_reserve(jobs):
-    """Point-only runs (thread traversal) alternating with grid runs (warp packets): each key keeps its
-    own captured graph, and lists reserved up front are large enough for every run."""
+    """Point-only runs in input order (thread traversal) alternating with grid runs (warp packets): each
+    key keeps its own captured graph, and lists reserved up front are large enough for every run."""
     import torch
 
     b = S.Batch(16, S.PREC_F32_FIXUP)
@@ -145,8 +146,38 @@ def test_alternating_graph_keys_after_reserve(jobs):
             tri = torch.empty(jobs[3]["grid"].size, dtype=torch.int32, device="cuda")
             b.add_grid(jobs[3]["dm"], jobs[3]["grid"], out, tri)
             want = jobs[3]
-        b.run(use_graph=True)
+        with env(SSDF_B200_SORT_POINTS=0):
+            b.run(use_graph=True)
         torch.cuda.synchronize()
         assert np.array_equal(out.cpu().numpy(), want["alone"])
         assert np.array_equal(tri.cpu().numpy(), want["alone_tri"])
     b.close()
+
+
+def test_sorted_point_jobs_in_a_batch(jobs):
+    """Point jobs of 4096 queries or more are visited in Morton order inside a batch (warp packets,
+    also beside grid jobs); every result equals the same query alone, with and without the sort."""
+    import torch
+
+    rng = np.random.default_rng(11)
+    for sort in (1, 0):
+        b = S.Batch(16, S.PREC_F32_FIXUP)
+        outs = []
+        for k, n in ((1, 5000), (2, 4095), (4, 20000)):
+            lo, hi = jobs[k]["mesh"].bbox()
+            pts = rng.uniform(lo - 0.2, hi + 0.2, size=(n, 3)).T.copy()
+            want, wtri = S.sdf_points(pts, jobs[k]["mesh"])
+            p = torch.tensor(pts, dtype=torch.float64, device="cuda")
+            out = torch.empty(n, dtype=torch.float64, device="cuda")
+            tri = torch.empty(n, dtype=torch.int32, device="cuda")
+            b.add_points(jobs[k]["dm"], p[0].contiguous(), p[1].contiguous(), p[2].contiguous(), out, tri)
+            outs.append((out, tri, want, wtri))
+        gout = torch.empty(jobs[3]["grid"].size, dtype=torch.float64, device="cuda")
+        b.add_grid(jobs[3]["dm"], jobs[3]["grid"], gout)
+        with env(SSDF_B200_SORT_POINTS=sort):
+            b.run(use_graph=True)
+        torch.cuda.synchronize()
+        for out, tri, want, wtri in outs:
+            assert np.array_equal(out.cpu().numpy(), want) and np.array_equal(tri.cpu().numpy(), wtri)
+        assert np.array_equal(gout.cpu().numpy(), jobs[3]["alone"])
+        b.close()

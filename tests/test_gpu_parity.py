@@ -125,6 +125,11 @@ def test_beam_lattice_points():
     with env(SSDF_B200_PRECISION="f64"):
         g64, t64 = S.edf_index(pts, mesh)
     assert np.array_equal(g64, got) and np.array_equal(t64, gtri)
+    # most beam triangles are slivers, so fix-up requests run the FP64 kernel; the fix-up kernel's
+    # proxy path, forced, gives the same bits
+    with env(SSDF_B200_ILL_MAX=2):
+        gx, tx = S.edf_index(pts, mesh)
+    assert np.array_equal(gx, got) and np.array_equal(tx, gtri)
 
 
 def test_closest_point_bvh():

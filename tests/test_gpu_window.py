@@ -16,6 +16,7 @@ import torch
 import oracle
 import ssdf_b200 as S
 from ssdf_b200 import workloads as W
+from test_gpu_golden import env
 
 pytestmark = pytest.mark.gpu
 
@@ -104,8 +105,9 @@ def sliver_mesh(sub, height):
 
 @pytest.mark.parametrize("height", [1e-3, 1e-6, 0.0])
 def test_slivers_fixup_equals_double(height):
-    """Ill-conditioned triangles (needles, slivers, collinear) are keyed by their double distance in the
-    fix-up path, so its result stays the double one at every query."""
+    """Ill-conditioned triangles (needles, slivers, collinear) are filtered through well-conditioned
+    proxies in the fix-up path, so its result stays the double one at every query. A third of this
+    mesh is slivers, so the proxy path is forced (SSDF_B200_ILL_MAX above 1)."""
     mesh = sliver_mesh(2, height)
     dm = S.DeviceMesh(mesh)
     lo, hi = mesh.bbox()
@@ -114,8 +116,11 @@ def test_slivers_fixup_equals_double(height):
     for prec in (S.PREC_F32_FIXUP, S.PREC_F64):
         out = torch.full((grid.size,), np.finfo(np.float64).max, dtype=torch.float64, device="cuda")
         tri = torch.full((grid.size,), -1, dtype=torch.int32, device="cuda")
-        dm.query_grid(grid, out, tri, precision=prec, output=S.OUT_EDF)
-        torch.cuda.synchronize()
+        with env(SSDF_B200_ILL_MAX=2, SSDF_B200_COUNT=1):
+            dm.query_grid(grid, out, tri, precision=prec, output=S.OUT_EDF)
+            torch.cuda.synchronize()
+        if prec == S.PREC_F32_FIXUP:
+            assert S.last_query_counts()["fixup_evaluations"] > 0  # the fix-up kernel ran
         res[prec] = (out.cpu().numpy(), tri.cpu().numpy())
     dm.close()
     assert np.array_equal(res[S.PREC_F32_FIXUP][0], res[S.PREC_F64][0])
@@ -123,3 +128,25 @@ def test_slivers_fixup_equals_double(height):
     ids = np.random.default_rng(0).choice(grid.size, 500, replace=False)
     want, wtri = oracle.edf(oracle.grid_points(grid)[:, ids], mesh, with_index=True)
     assert np.array_equal(res[S.PREC_F64][0][ids], want) and np.array_equal(res[S.PREC_F64][1][ids], wtri)
+
+
+def test_sliver_heavy_mesh_is_handed_to_fp64():
+    """A mesh with more than the limit's share of ill-conditioned triangles (a third here; the limit is
+    a half by default, set to a fifth) answers fix-up requests with the FP64 kernel (no fix-up
+    evaluations), with the same bits; below the limit the fix-up kernel runs."""
+    mesh = sliver_mesh(2, 1e-3)
+    dm = S.DeviceMesh(mesh)
+    lo, hi = mesh.bbox()
+    grid = W.Grid((32, 32, 32), tuple(lo - 0.3), tuple(hi + 0.3))
+    outs = []
+    for limit in (0.2, None):
+        out = torch.empty(grid.size, dtype=torch.float64, device="cuda")
+        kw = dict(SSDF_B200_COUNT=1) if limit is None else dict(SSDF_B200_COUNT=1, SSDF_B200_ILL_MAX=limit)
+        with env(**kw):
+            dm.query_grid(grid, out, None, precision=S.PREC_F32_FIXUP, output=S.OUT_SDF)
+            torch.cuda.synchronize()
+        outs.append(out.cpu().numpy())
+        c = S.last_query_counts()["fixup_evaluations"]
+        assert (c == 0) if limit is not None else (c > 0)
+    dm.close()
+    assert np.array_equal(outs[0], outs[1])
