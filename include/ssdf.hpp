@@ -2,7 +2,7 @@
 //
 // A drop-in for zulianp/ssdf's serial/ssdf.hpp (edf, edf_celllist, edf_select) and
 // serial/bvh/bvh.hpp (edf_bvh, closest_point_bvh, sample_sqedf_bvh, sample_sdf_bvh, inside flags,
-// closest_within_radius_*) and the grid
+// closest_within_radius_*, potential_contact_*) and the grid
 // helpers of serial/edf/edf.hpp (compute_aabb, all_points_aabb_signed_distance): same names,
 // template parameters <G coordinates, T outputs, I indices>, argument order, in/out semantics and
 // int return (0 on success). Each instantiation the reference provides maps onto one C symbol of
@@ -361,6 +361,43 @@ int closest_within_radius_quads_local_bvh(SSDF_B200_RADIUS_SIG(G, T), const I *c
     SSDF_B200_RADIUS_DISPATCH(closest_within_radius_quads_local_bvh, npoints, x, y, z, nselements, s0, s1, s2, s3,
                               nspoints, sx, sy, sz, radius_stride, radius_squared, outtri, out_sqr_dist, closest_s,
                               closest_t, skip_self ? 1 : 0);
+}
+
+// serial/bvh/bvh.hpp:156-181: candidate contact pairs, CSR with a malloc'd index array.
+// Instantiations <float, float, int, int>, <double, double, int, int> (serial/bvh/bvh.cpp:1524-1572).
+template <typename G, typename T, typename I, typename F>
+int potential_contact_triangles_bvh(const ptrdiff_t nselements, const I *const SSDF_RESTRICT s0,
+                                    const I *const SSDF_RESTRICT s1, const I *const SSDF_RESTRICT s2,
+                                    const ptrdiff_t nspoints, const G *const SSDF_RESTRICT sx,
+                                    const G *const SSDF_RESTRICT sy, const G *const SSDF_RESTRICT sz, const T extrusion,
+                                    ptrdiff_t *const SSDF_RESTRICT pc_ptr, F **const SSDF_RESTRICT out_pc_idx) {
+    static_assert(std::is_same<I, int>::value && std::is_same<F, int>::value, "ssdf_b200 indices are int");
+    if constexpr (std::is_same<G, float>::value && std::is_same<T, float>::value)
+        return ssdf_b200_potential_contact_triangles_bvh_ff(nselements, s0, s1, s2, nspoints, sx, sy, sz, extrusion,
+                                                            pc_ptr, out_pc_idx);
+    else if constexpr (std::is_same<G, double>::value && std::is_same<T, double>::value)
+        return ssdf_b200_potential_contact_triangles_bvh_dd(nselements, s0, s1, s2, nspoints, sx, sy, sz, extrusion,
+                                                            pc_ptr, out_pc_idx);
+    else
+        static_assert(detail::always_false<G, T>::value, "potential_contact_triangles_bvh: <float,float>, <double,double>");
+}
+
+template <typename G, typename T, typename I, typename F>
+int potential_contact_quads_bvh(const ptrdiff_t nselements, const I *const SSDF_RESTRICT s0,
+                                const I *const SSDF_RESTRICT s1, const I *const SSDF_RESTRICT s2,
+                                const I *const SSDF_RESTRICT s3, const ptrdiff_t nspoints,
+                                const G *const SSDF_RESTRICT sx, const G *const SSDF_RESTRICT sy,
+                                const G *const SSDF_RESTRICT sz, const T extrusion, ptrdiff_t *const SSDF_RESTRICT pc_ptr,
+                                F **const SSDF_RESTRICT out_pc_idx) {
+    static_assert(std::is_same<I, int>::value && std::is_same<F, int>::value, "ssdf_b200 indices are int");
+    if constexpr (std::is_same<G, float>::value && std::is_same<T, float>::value)
+        return ssdf_b200_potential_contact_quads_bvh_ff(nselements, s0, s1, s2, s3, nspoints, sx, sy, sz, extrusion,
+                                                        pc_ptr, out_pc_idx);
+    else if constexpr (std::is_same<G, double>::value && std::is_same<T, double>::value)
+        return ssdf_b200_potential_contact_quads_bvh_dd(nselements, s0, s1, s2, s3, nspoints, sx, sy, sz, extrusion,
+                                                        pc_ptr, out_pc_idx);
+    else
+        static_assert(detail::always_false<G, T>::value, "potential_contact_quads_bvh: <float,float>, <double,double>");
 }
 
 }  // namespace ssdf

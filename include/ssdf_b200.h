@@ -245,6 +245,34 @@ int ssdf_b200_closest_within_radius_quads_local_bvh_dd(ptrdiff_t npoints, const 
                                                        double *out_sqr_dist, double *closest_s, double *closest_t,
                                                        int skip_self);
 
+/* ---- drop-in: candidate contact pairs -----------------------------------------------------------
+ * ssdf::potential_contact_triangles_bvh / potential_contact_quads_bvh<G, G, int, int>
+ * (serial/bvh/bvh.hpp:156-181, bvh.cpp:834-1196), for G = float _ff and double _dd. For each
+ * element (triangle s0/s1/s2 or quad s0/s1/s2/s3), the other elements whose tight float box meets
+ * its own box grown by `extrusion` along its unit normal(s) and by a tenth of it against them, and
+ * which share no corner index with it. pc_ptr[nselements + 1] receives the CSR offsets and
+ * *out_pc_idx a malloc'd array of pc_ptr[nselements] element indices (the caller frees it with
+ * free(), or ssdf_b200_free), each row in the order of the BVH walk (deterministic; the reference's
+ * is its threads' order). The triangle normal is taken as the unit
+ * normal (cuBQL's Triangle::normal(), not available to this build); quads use the reference's
+ * per-corner normals. */
+int ssdf_b200_potential_contact_triangles_bvh_ff(ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                                 ptrdiff_t nspoints, const float *sx, const float *sy, const float *sz,
+                                                 float extrusion, ptrdiff_t *pc_ptr, int **out_pc_idx);
+int ssdf_b200_potential_contact_triangles_bvh_dd(ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                                 ptrdiff_t nspoints, const double *sx, const double *sy,
+                                                 const double *sz, double extrusion, ptrdiff_t *pc_ptr,
+                                                 int **out_pc_idx);
+int ssdf_b200_potential_contact_quads_bvh_ff(ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                             const int *s3, ptrdiff_t nspoints, const float *sx, const float *sy,
+                                             const float *sz, float extrusion, ptrdiff_t *pc_ptr, int **out_pc_idx);
+int ssdf_b200_potential_contact_quads_bvh_dd(ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                             const int *s3, ptrdiff_t nspoints, const double *sx, const double *sy,
+                                             const double *sz, double extrusion, ptrdiff_t *pc_ptr,
+                                             int **out_pc_idx);
+/* free() from the library's C runtime, for callers (ctypes and the like) that cannot call it. */
+void ssdf_b200_free(void *p);
+
 /* ---- drop-in: grid and box helpers ------------------------------------------------------------
  * ssdf::compute_aabb<G, T> (serial/edf/edf.hpp:500-539): the bounding box of npoints (>= 1) points,
  * each converted to T, written to the six scalars. Bitwise the reference's for NaN-free input (a

@@ -109,6 +109,9 @@ def lib() -> C.CDLL:
             f = getattr(_lib, "oracle_point_triangle_barycentric" + suf)
             f.restype = ft
             f.argtypes = [ft] * 12 + [fptr] * 3
+        _lib.oracle_potential_contact.restype = C.c_ssize_t
+        _lib.oracle_potential_contact.argtypes = [_pd, _ip, _ip, _ip, _ip, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                                  C.c_float, C.c_float, C.POINTER(C.c_ssize_t), _ip, _pd]
         _lib.oracle_sqedf_points_d.restype = C.c_int
         _lib.oracle_sqedf_points_d.argtypes = [_pd, _dp, _dp, _dp, _pd, _ip, _ip, _ip, _pd, _dp, _dp, _dp, _dp]
     return _lib
@@ -406,3 +409,22 @@ def within_radius(points, elements, vertices, radius_squared, stride=1, skip_sel
                                         int(bool(skip_self)), int(bool(local)), _ptr(outtri, C.c_int),
                                         *[_ptr(a, tct) for a in outs])
     return (outtri, outs[0], outs[1], outs[2]) if local else (outtri, *outs)
+
+
+def potential_contact(elements, vertices, extrusion, dtype=np.float64):
+    """Brute-force candidate contact pairs (potential_contact_triangles_bvh / _quads_bvh,
+    serial/bvh/bvh.cpp:834-1196): (pc_ptr int64, idx int32), rows ascending."""
+    sx, sy, sz = (np.ascontiguousarray(a, dtype=dtype) for a in vertices)
+    idx = [np.ascontiguousarray(a, dtype=np.int32) for a in elements]
+    n = len(idx[0])
+    t = np.dtype(dtype).type
+    ext = float(np.float32(extrusion))
+    inner = float(np.float32(t(0.1) * t(extrusion)))
+    ptr = np.zeros(n + 1, dtype=np.int64)
+    pp = ptr.ctypes.data_as(C.POINTER(C.c_ssize_t))
+    args = [n, *[_ptr(a, C.c_int) for a in idx[:3]], _ptr(idx[3], C.c_int) if len(idx) == 4 else None,
+            sx.ctypes.data, sy.ctypes.data, sz.ctypes.data, int(np.dtype(dtype) == np.float64), ext, inner, pp]
+    total = lib().oracle_potential_contact(*args, None, 0)
+    out = np.zeros(max(total, 1), dtype=np.int32)
+    lib().oracle_potential_contact(*args, _ptr(out, C.c_int), total)
+    return ptr, out[:total]

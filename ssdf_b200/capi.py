@@ -127,6 +127,11 @@ for _g in ("ff", "fd", "dd"):
     _QE = [_pd, _vp, _vp, _vp, _pd, _ip, _ip, _ip, _ip, _pd, _vp, _vp, _vp]
     _sig(f"ssdf_b200_closest_within_radius_quads_bvh_{_g}", _QE + [_pd, _vp, _ip] + [_vp] * 4 + [C.c_int])
     _sig(f"ssdf_b200_closest_within_radius_quads_local_bvh_{_g}", _QE + [_pd, _vp, _ip] + [_vp] * 3 + [C.c_int])
+for _g, _gc in (("ff", C.c_float), ("dd", C.c_double)):
+    _PC = [_gc, C.POINTER(C.c_ssize_t), C.POINTER(_ip)]
+    _sig(f"ssdf_b200_potential_contact_triangles_bvh_{_g}", [_pd, _ip, _ip, _ip, _pd, _vp, _vp, _vp] + _PC)
+    _sig(f"ssdf_b200_potential_contact_quads_bvh_{_g}", [_pd, _ip, _ip, _ip, _ip, _pd, _vp, _vp, _vp] + _PC)
+_sig("ssdf_b200_free", [_vp], None)
 _sig("ssdf_points_aabb_signed_distance", [_pd, _vp, _vp, _vp, C.c_int, C.POINTER(C.c_double * 6), C.c_int, _vp,
                                           C.c_int, _vp])
 
@@ -180,7 +185,9 @@ EXPORTED = ["ssdf_status_string", "ssdf_last_error", "ssdf_b200_version", "ssdf_
     [f"ssdf_b200_{k}_{g}{t}" for k in ("compute_aabb", "all_points_aabb_signed_distance") for g in "fd" for t in "fd"] + \
     [f"ssdf_b200_{k}_{g}" for k in ("level_set_triangles", "rebuild_sdf", "refine_field", "round_sdf") for g in ("ff", "dd")] + \
     [f"ssdf_b200_closest_within_radius_{k}_{g}" for k in ("bvh", "local_bvh", "quads_bvh", "quads_local_bvh")
-     for g in ("ff", "fd", "dd")]
+     for g in ("ff", "fd", "dd")] + \
+    [f"ssdf_b200_potential_contact_{k}_bvh_{g}" for k in ("triangles", "quads") for g in ("ff", "dd")] + \
+    ["ssdf_b200_free"]
 
 
 def _status_name(status: int) -> str:
@@ -328,6 +335,27 @@ def closest_within_radius(points, elements, vertices, radius_squared, stride=1, 
                             _p(sz), int(stride), _p(r2), _ipp(outtri), *[_p(a) for a in outs], int(bool(skip_self))),
            fn)
     return (outtri, *outs)
+
+
+def potential_contact(elements, vertices, extrusion, dtype=np.float64):
+    """ssdf::potential_contact_triangles_bvh (three index arrays) / potential_contact_quads_bvh (four)
+    on the GPU: (pc_ptr int64 [n + 1], pc_idx int32 [pc_ptr[n]]), each row in the BVH walk's order."""
+    sx, sy, sz = (_arr(a, dtype) for a in vertices)
+    idx = [_arr(a, np.int32) for a in elements]
+    if len(idx) not in (3, 4):
+        raise ValueError("elements: three (triangles) or four (quads) index arrays")
+    n = len(idx[0])
+    ptr = np.full(n + 1, -7, dtype=np.int64)
+    out = _ip()
+    kind = "quads" if len(idx) == 4 else "triangles"
+    fn = f"ssdf_b200_potential_contact_{kind}_bvh_{_suffix(dtype) * 2}"
+    _check(getattr(lib, fn)(n, *[_ipp(a) for a in idx], len(sx), _p(sx), _p(sy), _p(sz), float(extrusion),
+                            ptr.ctypes.data_as(C.POINTER(C.c_ssize_t)), C.byref(out)), fn)
+    try:
+        pairs = np.ctypeslib.as_array(out, shape=(int(ptr[n]),)).copy() if ptr[n] > 0 else np.zeros(0, np.int32)
+    finally:
+        lib.ssdf_b200_free(C.cast(out, _vp))
+    return ptr, pairs
 
 
 def points_inside_bvh(points, mesh, dtype=np.float64):

@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 #include <float.h>
 #include <stdint.h>
+#include <stdlib.h>
 
 #include <vector>
 
@@ -492,6 +493,262 @@ int within_radius_host(ptrdiff_t npoints, const G *x, const G *y, const G *z, pt
     return SSDF_OK;
 }
 
+
+// ---- candidate contact pairs (serial/bvh/bvh.cpp:834-1196) -----------------------------------------
+//
+// ssdf::potential_contact_triangles_bvh / _quads_bvh: for each element, every other element whose
+// tight box meets its box grown by `extrusion` along its normals and a tenth of that against them,
+// sharing no corner with it; a CSR list whose index array the caller frees with free(). The BVH is
+// built over each element's exact float box (a degenerate triangle from the box's low to its high
+// corner), so a node is entered exactly when a box under it can meet the query box. A row lists its
+// candidates in the order of the element's walk, the same for the same input (the reference's order
+// within a row is that of its threads).
+
+struct PairArgs {
+    int ne, nk;                      // elements, corners per element (3 or 4)
+    const int *e[4];                 // the caller's element indices
+    const float4 *prims;             // [3 * ne] float corners (k_quad_records layout)
+    const float4 *nodes, *boxes;     // BVH over the element boxes: nodes and leaf records
+    float ext, inner;                // extrusion along the normals, and against them
+    int *count;                      // [ne] candidates per element
+    const int *offset;               // [ne] exclusive scan of count (fill pass)
+    int *idx;                        // [total] (fill pass)
+    unsigned long long *total;       // count pass
+};
+
+__device__ __forceinline__ void prim_corners(const float4 *__restrict__ prims, int e, float (&c)[4][3]) {
+    const float4 q0 = __ldg(prims + 3 * e), q1 = __ldg(prims + 3 * e + 1), q2 = __ldg(prims + 3 * e + 2);
+    c[0][0] = q0.x, c[0][1] = q0.y, c[0][2] = q0.z, c[1][0] = q0.w, c[1][1] = q1.x, c[1][2] = q1.y;
+    c[2][0] = q1.z, c[2][1] = q1.w, c[2][2] = q2.x, c[3][0] = q2.y, c[3][1] = q2.z, c[3][2] = q2.w;
+}
+
+__device__ __forceinline__ void cross3(const float (&a)[3], const float (&b)[3], float (&o)[3]) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// v * (1 / sqrt(v . v)) (IEEE division and square root)
+__device__ __forceinline__ void unit3(float (&v)[3]) {
+    const float inv = 1.0f / sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    v[0] = v[0] * inv, v[1] = v[1] * inv, v[2] = v[2] * inv;
+}
+
+// The grown box of element e: its tight box, each corner moved ext along its normal and inner against
+// it. Triangles: the unit normal of (b - a) x (c - a) (cuBQL's Triangle::normal()); quads: one normal
+// per corner from its two edges (serial/bvh/bvh.cpp:1019-1030). min / max ignore NaN.
+__device__ void grown_box(const float (&c)[4][3], int nk, float ext, float inner, float (&lo)[3], float (&hi)[3]) {
+    float n[4][3];
+    if (nk == 3) {
+        const float u[3] = {c[1][0] - c[0][0], c[1][1] - c[0][1], c[1][2] - c[0][2]};
+        const float v[3] = {c[2][0] - c[0][0], c[2][1] - c[0][1], c[2][2] - c[0][2]};
+        cross3(u, v, n[0]);
+        unit3(n[0]);
+        for (int k = 1; k < 3; k++)
+            for (int d = 0; d < 3; d++) n[k][d] = n[0][d];
+    } else {
+        float ab[3], dc[3], ad[3], bc[3];
+        for (int d = 0; d < 3; d++) {
+            ab[d] = c[1][d] - c[0][d], dc[d] = c[2][d] - c[3][d];
+            ad[d] = c[3][d] - c[0][d], bc[d] = c[2][d] - c[1][d];
+        }
+        cross3(ab, ad, n[0]);
+        cross3(ab, bc, n[1]);
+        cross3(dc, bc, n[2]);
+        cross3(dc, ad, n[3]);
+        for (int k = 0; k < 4; k++) unit3(n[k]);
+    }
+    for (int d = 0; d < 3; d++) {
+        lo[d] = c[0][d], hi[d] = c[0][d];
+        for (int k = 1; k < nk; k++) lo[d] = fminf(lo[d], c[k][d]), hi[d] = fmaxf(hi[d], c[k][d]);
+    }
+    for (int k = 0; k < nk; k++)
+        for (int d = 0; d < 3; d++) {
+            const float out = c[k][d] + n[k][d] * ext, in = c[k][d] - n[k][d] * inner;
+            lo[d] = fminf(lo[d], out), hi[d] = fmaxf(hi[d], out);
+            lo[d] = fminf(lo[d], in), hi[d] = fmaxf(hi[d], in);
+        }
+}
+
+// Box vertices of the BVH over the elements: element e is the degenerate triangle (2e, 2e+1, 2e+1)
+// from the low to the high corner of its tight float box.
+__global__ void k_box_vertices(int ne, int nk, const float4 *__restrict__ prims, float *__restrict__ vx,
+                               float *__restrict__ vy, float *__restrict__ vz, int *__restrict__ t0,
+                               int *__restrict__ t1) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    float c[4][3];
+    prim_corners(prims, e, c);
+    float lo[3], hi[3];
+    for (int d = 0; d < 3; d++) {
+        lo[d] = c[0][d], hi[d] = c[0][d];
+        for (int k = 1; k < nk; k++) lo[d] = fminf(lo[d], c[k][d]), hi[d] = fmaxf(hi[d], c[k][d]);
+    }
+    vx[2 * e] = lo[0], vy[2 * e] = lo[1], vz[2 * e] = lo[2];
+    vx[2 * e + 1] = hi[0], vy[2 * e + 1] = hi[1], vz[2 * e + 1] = hi[2];
+    t0[e] = 2 * e;
+    t1[e] = 2 * e + 1;
+}
+
+__device__ __forceinline__ bool meets(const float (&alo)[3], const float (&ahi)[3], float blox, float bhix,
+                                      float bloy, float bhiy, float bloz, float bhiz) {
+    return alo[0] <= bhix && blox <= ahi[0] && alo[1] <= bhiy && bloy <= ahi[1] && alo[2] <= bhiz && bloz <= ahi[2];
+}
+
+// One thread per element. FILL = false counts the candidates, true writes them in the same order.
+template <bool FILL>
+__global__ void __launch_bounds__(128) k_pairs(const PairArgs a) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.ne) return;
+    float c[4][3];
+    prim_corners(a.prims, p, c);
+    float lo[3], hi[3];
+    grown_box(c, a.nk, a.ext, a.inner, lo, hi);
+    int mine[4];
+    for (int k = 0; k < 4; k++) mine[k] = k < a.nk ? __ldg(a.e[k] + p) : -1;
+    int *row = FILL ? a.idx + a.offset[p] : nullptr;
+    const int room = FILL ? a.count[p] : 0;  // the count pass's figure for this row (the walk repeats it)
+    int n = 0;
+    int stack[kStackSize];
+    int sp = 0, node = 0;
+    while (true) {
+        const float4 n0 = __ldg(a.nodes + 4 * node), n1 = __ldg(a.nodes + 4 * node + 1);
+        const float4 n2 = __ldg(a.nodes + 4 * node + 2), n3 = __ldg(a.nodes + 4 * node + 3);
+        const int r[2] = {__float_as_int(n3.x), __float_as_int(n3.y)};
+        const bool w[2] = {r[0] != kEmptyRef && meets(lo, hi, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y),
+                           r[1] != kEmptyRef && meets(lo, hi, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w)};
+        int next = -1;
+        for (int h = 0; h < 2; h++) {
+            if (!w[h]) continue;
+            if (r[h] >= 0) {
+                if (next < 0) next = r[h];
+                else if (sp < kStackSize) stack[sp++] = r[h];
+                continue;
+            }
+            const int first = leaf_first(r[h]), cnt = leaf_count(r[h]);
+            for (int k = first; k < first + cnt; k++) {
+                const float4 b0 = __ldg(a.boxes + 3 * k), b1 = __ldg(a.boxes + 3 * k + 1);
+                const float4 b2 = __ldg(a.boxes + 3 * k + 2);
+                // record: (lo.x, lo.y, lo.z, hi.x), (hi.y, hi.z, hi.x, hi.y), (hi.z, id, ...)
+                if (!meets(lo, hi, b0.x, b0.w, b0.y, b1.x, b0.z, b1.y)) continue;
+                const int t = __float_as_int(b2.y);
+                bool shared = false;
+                for (int j = 0; j < a.nk; j++) {
+                    const int v = __ldg(a.e[j] + t);
+                    for (int i = 0; i < a.nk; i++) shared |= mine[i] == v;
+                }
+                if (shared) continue;
+                if (FILL && n < room) row[n] = t;
+                n++;
+            }
+        }
+        if (next < 0) {
+            if (sp == 0) break;
+            next = stack[--sp];
+        }
+        node = next;
+    }
+    if (!FILL) {
+        a.count[p] = n;
+        atomicAdd(a.total, (unsigned long long)n);
+    }
+}
+
+template <typename G, typename T, bool QUAD>
+int potential_contact_host(ptrdiff_t ne, const int *s0, const int *s1, const int *s2, const int *s3, ptrdiff_t nv,
+                           const G *sx, const G *sy, const G *sz, T extrusion, ptrdiff_t *pc_ptr, int **out_idx) {
+    if (!pc_ptr || !out_idx) return fail(SSDF_ERR_INVALID_ARGUMENT, "null pc_ptr or out_pc_idx");
+    *out_idx = nullptr;
+    if (ne < 0 || nv < 0) return fail(SSDF_ERR_INVALID_ARGUMENT, "negative size");
+    if (ne > 0 && (!s0 || !s1 || !s2 || (QUAD && !s3))) return fail(SSDF_ERR_INVALID_ARGUMENT, "null index array");
+    if (nv > 0 && (!sx || !sy || !sz)) return fail(SSDF_ERR_INVALID_ARGUMENT, "null vertex coordinate array");
+    const int nk = QUAD ? 4 : 3;
+    const int *s[4] = {s0, s1, s2, s3};
+    for (int k = 0; k < nk; k++)
+        for (ptrdiff_t e = 0; e < ne; e++)
+            if (s[k][e] < 0 || s[k][e] >= nv)
+                return fail(SSDF_ERR_INVALID_ARGUMENT, "element " + std::to_string(e) + " has a vertex index outside [0, " +
+                                                           std::to_string(nv) + ")");
+    if (ne > kMaxTriangles) return fail(SSDF_ERR_NOT_SUPPORTED, "too many elements for one BVH");
+    pc_ptr[0] = 0;
+    if (ne == 0) {
+        *out_idx = static_cast<int *>(malloc(sizeof(int)));
+        return *out_idx ? SSDF_OK : fail(SSDF_ERR_OUT_OF_MEMORY, "host index array");
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(SSDF_ERR_CUDA, "no usable CUDA device");
+    cudaStream_t stream = library_stream();
+    if (!stream) return fail(SSDF_ERR_CUDA, "could not create the library stream");
+    Buffers buf(stream);
+    MeshHold mh;
+    mh.stream = stream;
+    PairArgs a{};
+    a.ne = int(ne);
+    a.nk = nk;
+    void *d[4] = {nullptr, nullptr, nullptr, nullptr}, *vx, *vy, *vz;
+    for (int k = 0; k < nk; k++) SSDF_CHECK(buf.upload(&d[k], s[k], sizeof(int) * size_t(ne)));
+    SSDF_CHECK(buf.upload(&vx, sx, sizeof(G) * size_t(nv)));
+    SSDF_CHECK(buf.upload(&vy, sy, sizeof(G) * size_t(nv)));
+    SSDF_CHECK(buf.upload(&vz, sz, sizeof(G) * size_t(nv)));
+    for (int k = 0; k < 4; k++) a.e[k] = static_cast<const int *>(d[k]);
+    void *prims, *bx, *by, *bz, *t0, *t1;
+    SSDF_CHECK(buf.alloc(&prims, sizeof(float4) * 3 * size_t(ne)));
+    const unsigned blocks = unsigned((ne + 127) / 128);
+    k_quad_records<<<unsigned((ne + 255) / 256), 256, 0, stream>>>(int(ne), a.e[0], a.e[1], a.e[2], QUAD ? a.e[3] : a.e[2],
+                                                                  vx, vy, vz, sizeof(G) == 8, (float4 *)prims);
+    SSDF_CUDA(cudaGetLastError());
+    for (void **q : {&bx, &by, &bz}) SSDF_CHECK(buf.alloc(q, sizeof(float) * 2 * size_t(ne)));
+    SSDF_CHECK(buf.alloc(&t0, sizeof(int) * size_t(ne)));
+    SSDF_CHECK(buf.alloc(&t1, sizeof(int) * size_t(ne)));
+    k_box_vertices<<<blocks, 128, 0, stream>>>(int(ne), nk, (const float4 *)prims, (float *)bx, (float *)by,
+                                               (float *)bz, (int *)t0, (int *)t1);
+    SSDF_CUDA(cudaGetLastError());
+    ssdf_build_opts bo;
+    bo.leaf_size = env_int("SSDF_B200_LEAF", 0), bo.keep_fp64 = 0, bo.normals = 0;
+    bo.treelet_opt = env_int("SSDF_B200_TREELET", 1);
+    SSDF_CHECK(ssdf_mesh_create(&mh.mesh, ne, (const int *)t0, (const int *)t1, (const int *)t1, 2 * ne, bx, by, bz,
+                                SSDF_F32, 1, &bo, stream));
+    a.prims = (const float4 *)prims;
+    a.nodes = mh.mesh->m.nodes32;
+    a.boxes = mh.mesh->m.tris32;
+    a.ext = float(extrusion);
+    a.inner = float(T(0.1) * extrusion);
+    void *cnt, *off, *tot;
+    SSDF_CHECK(buf.alloc(&cnt, sizeof(int) * size_t(ne)));
+    SSDF_CHECK(buf.alloc(&off, sizeof(int) * size_t(ne)));
+    SSDF_CHECK(buf.alloc(&tot, sizeof(unsigned long long)));
+    SSDF_CUDA(cudaMemsetAsync(tot, 0, sizeof(unsigned long long), stream));
+    a.count = (int *)cnt;
+    a.total = (unsigned long long *)tot;
+    k_pairs<false><<<blocks, 128, 0, stream>>>(a);
+    SSDF_CUDA(cudaGetLastError());
+    unsigned long long total = 0;
+    SSDF_CUDA(cudaMemcpyAsync(&total, tot, sizeof(total), cudaMemcpyDeviceToHost, stream));
+    SSDF_CUDA(cudaStreamSynchronize(stream));
+    if (total > 0x7fffffffull) return fail(SSDF_ERR_NOT_SUPPORTED, "more than 2^31 - 1 candidate pairs");
+    SSDF_CHECK(exclusive_scan_i32((const int *)cnt, (int *)off, int(ne), stream));
+    void *didx;
+    SSDF_CHECK(buf.alloc(&didx, sizeof(int) * size_t(total)));
+    a.offset = (const int *)off;
+    a.idx = (int *)didx;
+    k_pairs<true><<<blocks, 128, 0, stream>>>(a);
+    SSDF_CUDA(cudaGetLastError());
+    int *host = static_cast<int *>(malloc(sizeof(int) * size_t(total > 0 ? total : 1)));
+    if (!host) return fail(SSDF_ERR_OUT_OF_MEMORY, "host index array");
+    std::vector<int> hoff(size_t(ne) + 1);
+    cudaError_t e = cudaMemcpyAsync(hoff.data(), off, sizeof(int) * size_t(ne), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess && total > 0)
+        e = cudaMemcpyAsync(host, didx, sizeof(int) * size_t(total), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+        free(host);
+        return cuda_fail(e, "contact pair download", __FILE__, __LINE__);
+    }
+    for (ptrdiff_t i = 1; i < ne; i++) pc_ptr[i] = hoff[size_t(i)];
+    pc_ptr[ne] = ptrdiff_t(total);
+    *out_idx = host;
+    return SSDF_OK;
+}
 }  // namespace
 }  // namespace ssdf_b200
 
@@ -536,4 +793,34 @@ extern "C" {
 RADIUS_FUNCS(ff, float, float)
 RADIUS_FUNCS(fd, float, double)
 RADIUS_FUNCS(dd, double, double)
+}
+
+extern "C" {
+int ssdf_b200_potential_contact_triangles_bvh_ff(ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                                 ptrdiff_t nspoints, const float *sx, const float *sy, const float *sz,
+                                                 float extrusion, ptrdiff_t *pc_ptr, int **out_pc_idx) {
+    return ssdf_b200::potential_contact_host<float, float, false>(nselements, s0, s1, s2, nullptr, nspoints, sx, sy, sz,
+                                                                   extrusion, pc_ptr, out_pc_idx);
+}
+int ssdf_b200_potential_contact_triangles_bvh_dd(ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                                 ptrdiff_t nspoints, const double *sx, const double *sy,
+                                                 const double *sz, double extrusion, ptrdiff_t *pc_ptr,
+                                                 int **out_pc_idx) {
+    return ssdf_b200::potential_contact_host<double, double, false>(nselements, s0, s1, s2, nullptr, nspoints, sx, sy,
+                                                                     sz, extrusion, pc_ptr, out_pc_idx);
+}
+int ssdf_b200_potential_contact_quads_bvh_ff(ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                             const int *s3, ptrdiff_t nspoints, const float *sx, const float *sy,
+                                             const float *sz, float extrusion, ptrdiff_t *pc_ptr, int **out_pc_idx) {
+    return ssdf_b200::potential_contact_host<float, float, true>(nselements, s0, s1, s2, s3, nspoints, sx, sy, sz,
+                                                                  extrusion, pc_ptr, out_pc_idx);
+}
+int ssdf_b200_potential_contact_quads_bvh_dd(ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                             const int *s3, ptrdiff_t nspoints, const double *sx, const double *sy,
+                                             const double *sz, double extrusion, ptrdiff_t *pc_ptr,
+                                             int **out_pc_idx) {
+    return ssdf_b200::potential_contact_host<double, double, true>(nselements, s0, s1, s2, s3, nspoints, sx, sy, sz,
+                                                                    extrusion, pc_ptr, out_pc_idx);
+}
+void ssdf_b200_free(void *p) { free(p); }
 }

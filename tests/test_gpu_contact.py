@@ -132,3 +132,57 @@ def test_empty_and_invalid():
     with pytest.raises(S.SsdfError) as e:
         S.closest_within_radius(pts, bad, mesh.coords(), np.ones(50))
     assert e.value.status == S.SSDF_ERR_INVALID_ARGUMENT
+
+
+# ---- candidate contact pairs (potential_contact_triangles_bvh / _quads_bvh) ---------------------
+
+from test_oracle import PC_QUADS, PC_TRIANGLES  # noqa: E402
+
+
+@pytest.mark.parametrize("case", [PC_TRIANGLES, PC_QUADS])
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+def test_potential_contact_known_answers(case, dt):
+    ptr, idx = S.potential_contact(case["e"], (case["x"], case["y"], case["z"]), 0.3, dt)
+    assert list(ptr) == case["ptr"]
+    for e, c in case["contacts"]:
+        assert c in idx[ptr[e]:ptr[e + 1]]
+
+
+def sorted_rows(ptr, idx):
+    return np.concatenate([np.sort(idx[ptr[i]:ptr[i + 1]]) for i in range(len(ptr) - 1)] + [np.zeros(0, idx.dtype)])
+
+
+def small_soup(n, size, seed):
+    rng = np.random.default_rng(seed)
+    v = rng.uniform(0, 1, size=(n, 1, 3)) + rng.uniform(-size, size, size=(n, 3, 3))
+    return W.Mesh(v.reshape(-1, 3), np.arange(3 * n, dtype=np.int32).reshape(-1, 3))
+
+
+def contact_cases():
+    soup = small_soup(3000, 0.03, seed=2)
+    torus = W.torus(nu=64, nv=32, jitter=0.01)
+    q, qv = quad_surface(48, 24, seed=9)
+    return [("soup", soup.indices(), soup.coords(), 0.02), ("torus", torus.indices(), torus.coords(), 0.05),
+            ("quads", q, tuple(qv), 0.03), ("quads-wide", q, tuple(qv), 0.4)]
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+def test_potential_contact_equals_brute_force(dt):
+    for name, elems, verts, ext in contact_cases():
+        ptr, idx = S.potential_contact(elems, verts, ext, dt)
+        wptr, widx = oracle.potential_contact(elems, verts, ext, dt)
+        assert np.array_equal(ptr, wptr), name
+        assert np.array_equal(sorted_rows(ptr, idx), widx), name
+        ptr2, idx2 = S.potential_contact(elems, verts, ext, dt)
+        assert np.array_equal(idx2, idx), name  # the same order on the same input
+        assert ptr[-1] > 0, name  # the cases do have contacts
+
+
+def test_potential_contact_empty_and_invalid():
+    ptr, idx = S.potential_contact([np.zeros(0, np.int32)] * 3, (np.zeros(0),) * 3, 0.1)
+    assert list(ptr) == [0] and len(idx) == 0
+    mesh = W.icosphere(1)
+    bad = [a.copy() for a in mesh.indices()]
+    bad[2][0] = -1
+    with pytest.raises(S.SsdfError):
+        S.potential_contact(bad, mesh.coords(), 0.1)

@@ -72,6 +72,12 @@ def test_cpp_header_compiles_against_c_abi(tmp_path):
         "      fsy, fsz, 1, r2, tri, d2, cx, cy, cz);\n"
         "  (void)ssdf::closest_within_radius_quads_local_bvh<double, double, int>(1, x, y, z, 1, s0, s1, s2, q3, 3, sx,\n"
         "      sy, sz, 1, r2, tri, d2, cx, cy);\n"
+        "  ptrdiff_t pc[2]; int *pci = nullptr;\n"
+        "  (void)ssdf::potential_contact_triangles_bvh<float, float, int, int>(1, s0, s1, s2, 3, fsx, fsy, fsz, 0.1f,\n"
+        "      pc, &pci);\n"
+        "  (void)ssdf::potential_contact_quads_bvh<double, double, int, int>(1, s0, s1, s2, q3, 3, sx, sy, sz, 0.1, pc,\n"
+        "      &pci);\n"
+        "  ssdf_b200_free(pci);\n"
         "  return 0;\n}\n")
     lib = os.path.join(ROOT, "ssdf_b200", "_lib")
     res = subprocess.run(["g++", "-std=c++17", f"-I{ROOT}/include", str(src), "-o", str(tmp_path / "use"),
@@ -115,3 +121,7 @@ def test_radius_queries_validate_on_the_host():
     assert len(out) == 5 and len(out[0]) == 0
     with pytest.raises(ValueError):
         S.closest_within_radius(pts, [np.array([0]), np.array([1]), np.array([2])], verts, np.ones(2))
+    bad = [np.array([0]), np.array([1]), np.array([5])]
+    with pytest.raises(S.SsdfError) as e:
+        S.potential_contact(bad, verts, 0.1)
+    assert e.value.status == S.SSDF_ERR_INVALID_ARGUMENT

@@ -304,3 +304,24 @@ def test_within_radius_oracle_semantics(quads):
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
     if quads:
         assert np.all((b[2] >= 0) & (b[2] <= 1) & (b[3] >= 0) & (b[3] <= 1))
+
+
+# The reference's own known answers for the candidate contact pairs
+# (tests/potential_contact_triangles_bvh_test.cpp:14-78, tests/potential_contact_quads_bvh_test.cpp:21-60).
+PC_TRIANGLES = dict(x=[0, 1, 0, .2, .8, .2, -.5, 3, 4, 3], y=[0, 0, 1, .2, .2, .8, 1.5, 0, 0, 1],
+                    z=[0, 0, 0, .1, .1, .1, 0, 0, 0, 0], e=[[0, 3, 0, 7], [1, 5, 2, 8], [2, 4, 6, 9]],
+                    ptr=[0, 1, 2, 2, 2], contacts=[(0, 1), (1, 0)])
+PC_QUADS = dict(x=[0, 1, 1, 0, 0, 1, 1, 0, 3, 4, 4, 3, 3, 4, 4, 3, 8, 9, 9, 8],
+                y=[0, 0, 1, 1, 0, 0, 1, 1, 0, 0, 1, 1, 0, 0, 1, 1, 0, 0, 1, 1],
+                z=[0, 0, 0, 0, .2, .2, .2, .2, 0, 0, .5, 0, .6, .6, 1.1, .6, 0, 0, 0, 0],
+                e=[[0, 4, 8, 12, 16], [1, 7, 9, 15, 17], [2, 6, 10, 14, 18], [3, 5, 11, 13, 19]],
+                ptr=[0, 1, 2, 3, 4, 4], contacts=[(0, 1), (1, 0), (2, 3), (3, 2)])
+
+
+@pytest.mark.parametrize("case", [PC_TRIANGLES, PC_QUADS])
+def test_potential_contact_known_answers(case):
+    for dt in (np.float32, np.float64):
+        ptr, idx = oracle.potential_contact(case["e"], (case["x"], case["y"], case["z"]), 0.3, dt)
+        assert list(ptr) == case["ptr"]
+        for e, c in case["contacts"]:
+            assert c in idx[ptr[e]:ptr[e + 1]]
