@@ -36,8 +36,8 @@ struct ssdf_batch {
     BatchHeader *h_hdr = nullptr;
     QueryArgs *h_jobs = nullptr;
     long long *h_first = nullptr;
-    // captured graphs, one per (warp, wide) key: a run reuses the graph of its key
-    cudaGraphExec_t exec[4] = {nullptr, nullptr, nullptr, nullptr};
+    // captured graphs, one per (warp, wide, budget) key: a run reuses the graph of its key
+    cudaGraphExec_t exec[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     int sms = 0;
     long long last_total = 0;
 };
@@ -55,6 +55,69 @@ static void batch_free(ssdf_batch *b) {
     cudaFreeHost(b->h_jobs);
     cudaFreeHost(b->h_first);
 }
+
+// The launch sequence of one run with the given traversal and arity: counters reset, then the
+// persistent kernel and the window stage. It reads the job table from device memory only.
+static int enqueue_run(ssdf_batch *b, bool warp, bool wide, bool budget, cudaStream_t s) {
+    BatchLaunch L;
+    L.budget = budget;
+    L.hdr = b->d_hdr;
+    L.jobs = b->d_jobs;
+    L.first_block = b->d_first;
+    L.next_item = b->d_next;
+    L.sms = b->sms;
+    L.warp = warp;
+    L.wide = wide;
+    L.grid = b->sms * batch_blocks_per_sm(b->precision, warp, wide);
+    cudaError_t e = cudaMemsetAsync(b->d_next, 0, sizeof(unsigned long long), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_fbcount, 0, sizeof(int) * b->max_jobs, s);
+    if (e != cudaSuccess) return cuda_fail(e, "batch reset", __FILE__, __LINE__);
+    return launch_batch(L, b->precision, s);
+}
+
+// The packet budget only exists for the fix-up kernel's binary packet walk.
+static bool budget_applies(const ssdf_batch *b, bool warp, bool wide) {
+    return b->precision == SSDF_PREC_F32_FIXUP && warp && !wide;
+}
+
+static int graph_key(bool warp, bool wide, bool budget) { return (warp ? 1 : 0) | (wide ? 2 : 0) | (budget ? 4 : 0); }
+
+// Captures (once) the graph of a (traversal, arity, budget) key on a private stream, thread-local mode.
+static int capture_key(ssdf_batch *b, bool warp, bool wide, bool budget) {
+    const int key = graph_key(warp, wide, budget);
+    if (b->exec[key]) return SSDF_OK;
+    cudaStream_t cap;
+    SSDF_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    int st = SSDF_OK;
+    if (e == cudaSuccess) {
+        st = enqueue_run(b, warp, wide, budget, cap);
+        e = cudaStreamEndCapture(cap, &g);
+    }
+    if (e == cudaSuccess && st == SSDF_OK) e = cudaGraphInstantiate(&b->exec[key], g, 0);
+    if (g) cudaGraphDestroy(g);
+    cudaStreamDestroy(cap);
+    if (st != SSDF_OK) return st;
+    if (e != cudaSuccess) return cuda_fail(e, "batch graph capture", __FILE__, __LINE__);
+    return SSDF_OK;
+}
+
+namespace ssdf_b200 {
+// Captures every graph a run of this batch can use, so that later runs capture nothing. A capture
+// running in one thread while another thread synchronises the device fails; the server calls this
+// before its threads start.
+int batch_capture_graphs(ssdf_batch *b) {
+    for (int warp = 0; warp < 2; warp++)
+        for (int wide = 0; wide < 2; wide++) {
+            if ((b->traversal == 1 && !warp) || (b->traversal == 2 && warp)) continue;
+            if ((b->arity == 2 && wide) || (b->arity == 4 && !wide)) continue;
+            SSDF_CHECK(capture_key(b, warp != 0, wide != 0, false));
+            if (budget_applies(b, warp != 0, wide != 0)) SSDF_CHECK(capture_key(b, warp != 0, wide != 0, true));
+        }
+    return SSDF_OK;
+}
+}  // namespace ssdf_b200
 
 extern "C" {
 
@@ -189,10 +252,12 @@ int ssdf_batch_run(ssdf_batch *b, int use_graph, void *stream_) {
             for (int *q : p) cudaFreeAsync(q, s);
         }
     } orders{{}, stream};
-    long long total = 0;
+    long long total = 0, nq = 0;
+    for (const auto &j : b->jobs) nq += j.is_grid ? j.nx * j.ny * j.nz : j.npoints;
     size_t off = 0;
     for (int k = 0; k < njobs; k++) {
         QueryArgs a = b->jobs[order[k]];
+        a.warp_budget = resolve_warp_budget(a.warp_budget, nq);
         if (sort_points && !a.is_grid && a.npoints >= kSortMinPoints) {
             int *ord = nullptr;
             SSDF_CHECK(morton_point_order(a.npoints, a.x, a.y, a.z, a.coord_f64, a.m.nodes32, &ord, stream));
@@ -222,41 +287,12 @@ int ssdf_batch_run(ssdf_batch *b, int use_graph, void *stream_) {
     SSDF_CUDA(cudaMemcpyAsync(b->d_hdr, b->h_hdr, sizeof(BatchHeader), cudaMemcpyHostToDevice, stream));
     SSDF_CUDA(cudaMemcpyAsync(b->d_jobs, b->h_jobs, sizeof(QueryArgs) * njobs, cudaMemcpyHostToDevice, stream));
     SSDF_CUDA(cudaMemcpyAsync(b->d_first, b->h_first, sizeof(long long) * njobs, cudaMemcpyHostToDevice, stream));
-    BatchLaunch L;
-    L.hdr = b->d_hdr;
-    L.jobs = b->d_jobs;
-    L.first_block = b->d_first;
-    L.next_item = b->d_next;
-    L.sms = b->sms;
-    L.warp = warp;
-    L.wide = wide;
-    L.grid = b->sms * batch_blocks_per_sm(b->precision, warp, wide);
-    const bool count = env_int("SSDF_B200_COUNT", 0) != 0;
-    auto enqueue = [&](cudaStream_t s) -> int {
-        cudaError_t e = cudaMemsetAsync(b->d_next, 0, sizeof(unsigned long long), s);
-        if (e == cudaSuccess) e = cudaMemsetAsync(b->d_fbcount, 0, sizeof(int) * b->max_jobs, s);
-        if (e != cudaSuccess) return cuda_fail(e, "batch reset", __FILE__, __LINE__);
-        return launch_batch(L, b->precision, s);
-    };
-    if (!use_graph || count) return enqueue(stream);
-    const int key = (warp ? 1 : 0) | (wide ? 2 : 0);
-    if (!b->exec[key]) {
-        cudaStream_t cap;
-        SSDF_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
-        cudaGraph_t g = nullptr;
-        cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
-        int st = SSDF_OK;
-        if (e == cudaSuccess) {
-            st = enqueue(cap);
-            e = cudaStreamEndCapture(cap, &g);
-        }
-        if (e == cudaSuccess && st == SSDF_OK) e = cudaGraphInstantiate(&b->exec[key], g, 0);
-        if (g) cudaGraphDestroy(g);
-        cudaStreamDestroy(cap);
-        if (st != SSDF_OK) return st;
-        if (e != cudaSuccess) return cuda_fail(e, "batch graph capture", __FILE__, __LINE__);
-    }
-    SSDF_CUDA(cudaGraphLaunch(b->exec[key], stream));
+    bool budget = false;
+    for (int k = 0; k < njobs; k++) budget |= b->h_jobs[k].warp_budget > 0;
+    budget = budget && budget_applies(b, warp, wide);
+    if (!use_graph || env_int("SSDF_B200_COUNT", 0) != 0) return enqueue_run(b, warp, wide, budget, stream);
+    SSDF_CHECK(capture_key(b, warp, wide, budget));
+    SSDF_CUDA(cudaGraphLaunch(b->exec[graph_key(warp, wide, budget)], stream));
     return SSDF_OK;
 }
 

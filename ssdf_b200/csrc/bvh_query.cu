@@ -29,6 +29,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <type_traits>
 
 #include "device_geom.cuh"
 #include "internal.h"
@@ -358,6 +359,7 @@ template <int Q>
 struct FastPolicy {
     using R = float;
     static constexpr int kQn = Q;
+    static constexpr bool kBudgeted = true;
     const DeviceMesh &m;
     float px[Q], py[Q], pz[Q], best[Q], thr[Q], evicted[Q], wmax[Q];
     float tau_rel;
@@ -375,6 +377,12 @@ struct FastPolicy {
     __device__ __forceinline__ void disable(int q) {
         set(q, 0.f, 0.f, 0.f, finf());
         thr[q] = -1.f;
+    }
+    // the walk stops early: every live query goes to the second stage with its current window
+    __device__ __forceinline__ void abandon() {
+#pragma unroll
+        for (int q = 0; q < Q; q++)
+            if (thr[q] > 0.f) evicted[q] = 0.f;
     }
     __device__ __forceinline__ void boxes(int node, float (&d0)[Q], float (&d1)[Q], int &r0, int &r1) const {
         const Node32 n = load_node32(m.nodes32, node);
@@ -465,16 +473,29 @@ __device__ __forceinline__ float stack_key_lo(double d) { return __double2float_
 __device__ __forceinline__ float stack_key_hi(float t) { return t; }
 __device__ __forceinline__ float stack_key_hi(double t) { return __double2float_ru(t); }
 
+// Policies that can hand their queries to a second stage (P::kBudgeted) stop a packet's walk after a
+// work budget; the others always finish it.
+template <class P, class = void>
+struct HasBudget : std::false_type {};
+template <class P>
+struct HasBudget<P, std::void_t<decltype(P::kBudgeted)>> : std::bool_constant<P::kBudgeted> {};
+template <class P>
+constexpr bool budgeted() {
+    return HasBudget<P>::value;
+}
+
 // Packet walk (a grid warp as one packet): the node ids on the stack are the same in every lane, so
 // the warp keeps one stack in shared memory instead of 32 copies in local memory. An entry keeps
 // the smallest box distance over the warp's lanes (one redux.sync on the float bits, which order
 // like the values for non-negative floats) and is entered on pop while that is below the largest
 // lane threshold: a superset of "some lane's distance below its own threshold", so never a miss.
-template <bool COUNT, class P>
-__device__ __forceinline__ void traverse_packet(P &p, Counters &cnt) {
+template <bool COUNT, bool BUDGET, class P>
+__device__ __forceinline__ void traverse_packet(P &p, Counters &cnt, int budget) {
     using R = typename P::R;
     constexpr int Q = P::kQn;
     constexpr unsigned kAll = 0xffffffffu;
+    int work = 0;  // triangle records the packet has tested (the same in every lane; BUDGET only)
+    if (budget <= 0) budget = 0x7fffffff;
     __shared__ int s_node[kThreads / 32][kStackSize];
     __shared__ float s_dist[kThreads / 32][kStackSize];
     int *snode = s_node[threadIdx.x >> 5];
@@ -510,6 +531,7 @@ __device__ __forceinline__ void traverse_packet(P &p, Counters &cnt) {
             if (!__any_sync(kAll, m != 0u)) continue;
             if (rc < 0) {
                 p.template leaf<COUNT>(leaf_first(rc), leaf_count(rc), m, cnt);
+                if constexpr (BUDGET && budgeted<P>()) work += leaf_count(rc);
             } else if (next < 0) {
                 next = rc;
             } else if (sp < kStackSize) {
@@ -520,6 +542,12 @@ __device__ __forceinline__ void traverse_packet(P &p, Counters &cnt) {
             }
         }
         if (next < 0) {
+            if constexpr (BUDGET && budgeted<P>()) {
+                if (work > budget) {  // warp-uniform; checked where a path ends
+                    p.abandon();
+                    break;
+                }
+            }
             const float tl = live ? stack_key_hi(p.max_thr()) : 0.f;
             const float tmax = __uint_as_float(__reduce_max_sync(kAll, __float_as_uint(tl)));
             while (sp > 0) {
@@ -540,10 +568,10 @@ __device__ __forceinline__ void traverse_packet(P &p, Counters &cnt) {
 // warp walk one path together -- a child is entered if any lane wants it, the nearer child is the
 // one most lanes rank first -- so node and triangle loads are warp-uniform (broadcast) and leaf work
 // does not diverge. Every lane must call it (warp-synchronous when WARP).
-template <bool WARP, bool COUNT, class P>
-__device__ __forceinline__ void traverse(P &p, Counters &cnt) {
+template <bool WARP, bool COUNT, bool BUDGET, class P>
+__device__ __forceinline__ void traverse(P &p, Counters &cnt, int budget) {
     if constexpr (WARP) {
-        traverse_packet<COUNT>(p, cnt);
+        traverse_packet<COUNT, BUDGET>(p, cnt, budget);
         return;
     }
     using R = typename P::R;
@@ -691,12 +719,12 @@ __device__ __forceinline__ void traverse4(P &p, Counters &cnt) {
     }
 }
 
-template <bool WARP, bool WIDE, bool COUNT, class P>
-__device__ __forceinline__ void walk(P &p, Counters &cnt) {
+template <bool WARP, bool WIDE, bool COUNT, bool BUDGET = false, class P>
+__device__ __forceinline__ void walk(P &p, Counters &cnt, int budget = 0) {
     if (WIDE)
         traverse4<WARP, COUNT>(p, cnt);
     else
-        traverse<WARP, COUNT>(p, cnt);
+        traverse<WARP, COUNT, BUDGET>(p, cnt, budget);
 }
 
 // ---- outputs ----------------------------------------------------------------------------------------
@@ -824,7 +852,7 @@ __device__ __forceinline__ void flush_counters(const QueryArgs &a, const Counter
 // One block of 128 lanes x kQ queries. Lanes without a query (the edge of a grid brick, the tail of
 // a point list) take part in warp-mode traversal with a negative threshold, so they never ask for
 // a node.
-template <int PREC, bool WARP, bool WIDE, bool COUNT>
+template <int PREC, bool WARP, bool WIDE, bool COUNT, bool BUDGET>
 __device__ __forceinline__ void query_block(const QueryArgs &a, long long block, Counters &cnt) {
     constexpr int Q = kQ;
     long long qid[Q], gi[Q], gj[Q], gk[Q];
@@ -895,7 +923,7 @@ __device__ __forceinline__ void query_block(const QueryArgs &a, long long block,
                 p.disable(s);
             }
         }
-        if (WARP || any) walk<WARP, WIDE, COUNT>(p, cnt);
+        if (WARP || any) walk<WARP, WIDE, COUNT, BUDGET>(p, cnt, a.warp_budget);
 #pragma unroll
         for (int s = 0; s < Q; s++) {
             if (!valid[s]) continue;
@@ -932,11 +960,13 @@ __device__ __forceinline__ void query_block(const QueryArgs &a, long long block,
     }
 }
 
-template <int PREC, bool WARP, bool WIDE, bool COUNT>
+// BUDGET: the fix-up kernel's packets stop after QueryArgs::warp_budget triangle records (a separate
+// instantiation, so the kernels without it compile as if it did not exist).
+template <int PREC, bool WARP, bool WIDE, bool COUNT, bool BUDGET = false>
 __global__ void __launch_bounds__(kThreads, PREC == SSDF_PREC_F64 ? 1 : SSDF_B200_QUERY_MIN_BLOCKS)
     k_query(const QueryArgs a) {
     Counters cnt;
-    query_block<PREC, WARP, WIDE, COUNT>(a, blockIdx.x, cnt);
+    query_block<PREC, WARP, WIDE, COUNT, BUDGET>(a, blockIdx.x, cnt);
     if (COUNT) flush_counters(a, cnt);
 }
 
@@ -1089,7 +1119,7 @@ __global__ void __launch_bounds__(kThreads) k_window(const QueryArgs a, int cap)
 // re-instantiated: only the table is rewritten before each replay. Blocks pull work items (one
 // 128-query block of one job) from an atomic counter, largest jobs first (the host orders them).
 
-template <int PREC, bool WARP, bool WIDE, bool COUNT>
+template <int PREC, bool WARP, bool WIDE, bool COUNT, bool BUDGET = false>
 __global__ void __launch_bounds__(kThreads, PREC == SSDF_PREC_F64 ? 1 : SSDF_B200_QUERY_MIN_BLOCKS)
     k_query_batch(const BatchHeader *__restrict__ hdr, const QueryArgs *__restrict__ jobs,
                   const long long *__restrict__ first_block, unsigned long long *__restrict__ next_item) {
@@ -1108,7 +1138,7 @@ __global__ void __launch_bounds__(kThreads, PREC == SSDF_PREC_F64 ? 1 : SSDF_B20
             const int mid = (lo + hi + 1) >> 1;
             if (__ldg(first_block + mid) <= it) lo = mid; else hi = mid - 1;
         }
-        query_block<PREC, WARP, WIDE, COUNT>(jobs[lo], it - __ldg(first_block + lo), cnt);
+        query_block<PREC, WARP, WIDE, COUNT, BUDGET>(jobs[lo], it - __ldg(first_block + lo), cnt);
     }
     if (COUNT && njobs > 0) flush_counters(jobs[0], cnt);
 }
@@ -1143,10 +1173,23 @@ int window_stack_cap() {
 
 template <int PREC, bool WARP, bool WIDE>
 cudaError_t launch_batch_main(const BatchLaunch &b, bool count, cudaStream_t stream) {
-    if (count)
-        k_query_batch<PREC, WARP, WIDE, true><<<b.grid, kThreads, 0, stream>>>(b.hdr, b.jobs, b.first_block, b.next_item);
-    else
-        k_query_batch<PREC, WARP, WIDE, false><<<b.grid, kThreads, 0, stream>>>(b.hdr, b.jobs, b.first_block, b.next_item);
+    constexpr bool kCanBudget = PREC == SSDF_PREC_F32_FIXUP && WARP && !WIDE;
+    if constexpr (kCanBudget) {
+        if (b.budget) {
+            if (count)
+                k_query_batch<PREC, WARP, WIDE, true, true><<<b.grid, kThreads, 0, stream>>>(b.hdr, b.jobs, b.first_block,
+                                                                                            b.next_item);
+            else
+                k_query_batch<PREC, WARP, WIDE, false, true><<<b.grid, kThreads, 0, stream>>>(b.hdr, b.jobs, b.first_block,
+                                                                                             b.next_item);
+        }
+    }
+    if (!kCanBudget || !b.budget) {
+        if (count)
+            k_query_batch<PREC, WARP, WIDE, true><<<b.grid, kThreads, 0, stream>>>(b.hdr, b.jobs, b.first_block, b.next_item);
+        else
+            k_query_batch<PREC, WARP, WIDE, false><<<b.grid, kThreads, 0, stream>>>(b.hdr, b.jobs, b.first_block, b.next_item);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || PREC != SSDF_PREC_F32_FIXUP) return e;
     if (count)
@@ -1176,6 +1219,15 @@ thread_local unsigned long long t_last_counts[4] = {0, 0, 0, 0};
 
 template <int PREC, bool WARP, bool WIDE>
 cudaError_t launch_main(const QueryArgs &a, bool count, unsigned nblocks, cudaStream_t stream) {
+    if constexpr (PREC == SSDF_PREC_F32_FIXUP && WARP && !WIDE) {
+        if (a.warp_budget > 0) {
+            if (count)
+                k_query<PREC, WARP, WIDE, true, true><<<nblocks, kThreads, 0, stream>>>(a);
+            else
+                k_query<PREC, WARP, WIDE, false, true><<<nblocks, kThreads, 0, stream>>>(a);
+            return cudaGetLastError();
+        }
+    }
     if (count)
         k_query<PREC, WARP, WIDE, true><<<nblocks, kThreads, 0, stream>>>(a);
     else
@@ -1318,6 +1370,7 @@ int launch_query(const QueryArgs &args_in, int precision, cudaStream_t stream) {
     // plain FP64 kernel: the fix-up filter sees each such triangle through a wide proxy, whose keys
     // crowd the window. Both give the same bits.
     if (precision == SSDF_PREC_F32_FIXUP && sliver_heavy(a.m)) precision = SSDF_PREC_F64;
+    a.warp_budget = resolve_warp_budget(a.warp_budget, n);
     if (a.output == SSDF_OUT_CLOSEST && (!a.m.tris64 || !a.outx || !a.outy || !a.outz || !a.outtri))
         return fail(SSDF_ERR_INVALID_ARGUMENT, "closest-point queries need outx/outy/outz/outtri and double data");
     if (precision == SSDF_PREC_F32 && (a.output == SSDF_OUT_SDF || a.output == SSDF_OUT_CLOSEST))

@@ -668,6 +668,7 @@ static int fill_query(const ssdf_mesh *mesh, const ssdf_query_opts *opts, QueryA
     a->coord_f64 = opts->coord_type == SSDF_F64;
     a->out_f64 = opts->out_type == SSDF_F64;
     a->tau_rel = tau_rel_from_env();
+    a->warp_budget = env_int("SSDF_B200_WARP_BUDGET", -1);
     return SSDF_OK;
 }
 

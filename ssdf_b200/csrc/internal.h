@@ -108,6 +108,10 @@ struct QueryArgs {
     void *outx, *outy, *outz;
     // fix-up window: tau = tau_rel * (coord_scale + d)
     float tau_rel;
+    // fix-up path, warp packets: a packet that has tested more than this many triangle records hands
+    // its queries to the second stage (a warp per query) with their current windows; 0: no limit;
+    // < 0: the default for the launch's size (resolve_warp_budget)
+    int warp_budget;
     // overflow list of the FP32 fix-up kernel (query, final window), finished by k_window
     int *fallback_ids;
     float *fallback_thr;
@@ -137,6 +141,7 @@ struct BatchLaunch {
     int grid;   // persistent blocks (SMs x resident blocks per SM)
     int sms;
     bool warp, wide;
+    bool budget;  // the fix-up packets stop after the jobs' warp_budget (k_query_batch<..., BUDGET>)
 };
 
 // ---- mesh build (mesh_build.cu) ------------------------------------------------------------------
@@ -161,6 +166,7 @@ int launch_query(const QueryArgs &args, int precision, cudaStream_t stream);
 int launch_query_noalloc(const QueryArgs &args, cudaStream_t stream);
 long long noalloc_max_queries();
 int launch_batch(const BatchLaunch &b, int precision, cudaStream_t stream);
+int batch_capture_graphs(ssdf_batch *b);  // batch.cu
 int batch_blocks_per_sm(int precision, bool warp, bool wide);
 bool default_warp(int is_grid);
 bool default_wide();
@@ -214,6 +220,17 @@ int round_device(const GridDesc &gd, const T *d_f, T radius, T band, bool open, 
 
 // ---- small helpers -------------------------------------------------------------------------------
 inline int grid_blocks(long long n, int threads) { return int((n + threads - 1) / threads); }
+// Default of QueryArgs::warp_budget, for launches (single, or a whole batch) of at most
+// kBudgetMaxQueries queries; larger launches run without one. SSDF_B200_WARP_BUDGET sets it for every
+// launch (0 = no limit). Measured on B200: with 2048 the 64^3 icosphere grid runs 1.83 -> 1.31 ms and a
+// 110^3 grid on an 81,920-triangle sphere 22.2 -> 8.5 ms (packets near the centre, where every
+// triangle is almost equidistant, hand their queries to the warp-per-query stage: the launch's tail
+// shortens). A launch that fills the GPU many times over gains nothing from a shorter tail and pays
+// for the repeated work (the 256-mesh batch: 257 -> 275 ms).
+constexpr int kWarpBudget = 2048;
+constexpr long long kBudgetMaxQueries = 1ll << 21;
+// QueryArgs::warp_budget for a launch of n queries when it was left to the default (< 0).
+inline int resolve_warp_budget(int b, long long n) { return b >= 0 ? b : (n <= kBudgetMaxQueries ? kWarpBudget : 0); }
 // Point lists of at least this many queries are visited in Morton order (SSDF_B200_SORT_POINTS=0
 // keeps input order).
 constexpr long long kSortMinPoints = 4096;

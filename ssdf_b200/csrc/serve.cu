@@ -166,7 +166,9 @@ void evict_over_budget(ssdf_server *s, int keep) {
         Resident &v = s->resident[victim];
         if (victim == keep || v.pins > 0) continue;
         s->resident_bytes -= v.bytes;
-        ssdf_mesh_destroy(v.mesh);
+        // no batch holds it, so nothing in flight reads it: a stream-ordered free on the build stream,
+        // without the device-wide wait of ssdf_mesh_destroy (which would stall every slot)
+        ssdf_mesh_destroy_async(v.mesh, s->build_stream);
         li = s->lru.erase(li);
         s->resident.erase(victim);
         s->evictions++;
@@ -378,6 +380,7 @@ int ssdf_server_create(ssdf_server **out, const ssdf_server_opts *opts) {
         if (st == SSDF_OK) st = ssdf_batch_create(&sl.batch, opts->max_batch_jobs, opts->precision, 0, 0);
         // overflow lists sized once: a run that grew them would wait for the other slot's batch
         if (st == SSDF_OK) st = ssdf_batch_reserve(sl.batch, (long long)cap, sl.stream);
+        if (st == SSDF_OK) st = batch_capture_graphs(sl.batch);  // no capture once the threads run
     }
     if (st != SSDF_OK) {
         ssdf_server_destroy(s);

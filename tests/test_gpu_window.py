@@ -150,3 +150,34 @@ def test_sliver_heavy_mesh_is_handed_to_fp64():
         assert (c == 0) if limit is not None else (c > 0)
     dm.close()
     assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("budget", [8, 64, 0])
+def test_packet_budget_hands_queries_to_second_stage(budget):
+    """A warp packet that has tested more triangle records than SSDF_B200_WARP_BUDGET stops and hands
+    its queries, with their current windows, to the warp-per-query stage: the result stays the FP64
+    one at every node (single launch and batch), and small budgets do send queries there."""
+    mesh = W.icosphere(4)
+    lo, hi = mesh.bbox()
+    grid = W.Grid((48, 40, 36), tuple(lo - 0.3), tuple(hi + 0.3))
+    dm = S.DeviceMesh(mesh)
+    ref = torch.empty(grid.size, dtype=torch.float64, device="cuda")
+    rtri = torch.empty(grid.size, dtype=torch.int32, device="cuda")
+    dm.query_grid(grid, ref, rtri, precision=S.PREC_F64)
+    out = torch.empty_like(ref)
+    tri = torch.empty_like(rtri)
+    with env(SSDF_B200_WARP_BUDGET=budget, SSDF_B200_COUNT=1):
+        dm.query_grid(grid, out, tri, precision=S.PREC_F32_FIXUP)
+        torch.cuda.synchronize()
+        fb = S.last_query_counts()["fallback_queries"]
+    assert torch.equal(out, ref) and torch.equal(tri, rtri)
+    assert (fb > grid.size // 10) if budget == 8 else True
+    bout = torch.empty_like(ref)
+    with env(SSDF_B200_WARP_BUDGET=budget):
+        b = S.Batch(4, S.PREC_F32_FIXUP)
+        b.add_grid(dm, grid, bout)
+        b.run(use_graph=False)
+        torch.cuda.synchronize()
+        b.close()
+    assert torch.equal(bout, ref)
+    dm.close()
