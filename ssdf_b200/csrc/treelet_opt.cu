@@ -2,7 +2,8 @@
 // construction of high-quality bounding volume hierarchies", HPG 2013).
 //
 // One bottom-up pass with per-node arrival counters (the second thread to reach a node owns it, so
-// its subtree is final): every node with at least kTreeletLeaves triangles below it roots a treelet,
+// its subtree is final; a warp then works on its lanes' treelets together): every node with at least
+// kTreeletLeaves triangles below it roots a treelet,
 // grown from its two children by opening the largest-area internal member until it has seven
 // members. The binary tree over those members with the lowest surface-area cost,
 //     cost(node) = area(node) + cost(left) + cost(right),   cost(triangle) = area(triangle),
@@ -66,85 +67,106 @@ __device__ __forceinline__ void set_parent(const TreeArrays &t, int ref, int par
         __stcg(t.parent_leaf + (-ref - 1), parent);
 }
 
-// Optimises the treelet rooted at internal node x (its subtree is final).
-__device__ void optimize_treelet(const TreeArrays &t, int x) {
+// A treelet in the making, in shared memory (one per warp): its members and their boxes and costs,
+// the internal nodes it reuses, and the dynamic programme's cost and best split of every subset.
+struct TreeletWork {
+    float mb[kTreeletLeaves][6];
+    float mcost[kTreeletLeaves];
     int member[kTreeletLeaves];
     int inner[kTreeletLeaves - 1];
+    int m, ni;  // members, internal nodes (m < 3: nothing to optimise)
+    float old_cost;
+    float c[kSubsets];
+    unsigned char split[kSubsets];
+};
+
+// One lane: grows the treelet rooted at internal node x (its subtree is final) from its two children
+// by opening the largest-area internal member until it has seven members. A treelet of fewer than
+// three members gets its cost stored here and w.m < 3.
+__device__ void form_treelet(const TreeArrays &t, int x, TreeletWork &w) {
     int m = 2, ni = 1;
-    member[0] = __ldcg(t.child_l + x);
-    member[1] = __ldcg(t.child_r + x);
-    inner[0] = x;
-    float mb[kTreeletLeaves][6];
-    ref_box32(t, member[0], mb[0]);
-    ref_box32(t, member[1], mb[1]);
+    w.member[0] = __ldcg(t.child_l + x);
+    w.member[1] = __ldcg(t.child_r + x);
+    w.inner[0] = x;
+    ref_box32(t, w.member[0], w.mb[0]);
+    ref_box32(t, w.member[1], w.mb[1]);
     while (m < kTreeletLeaves) {
         int pick = -1;
         float best = -1.f;
         for (int k = 0; k < m; k++) {
-            if (member[k] >= 0) {
-                const float a = area6(mb[k]);
+            if (w.member[k] >= 0) {
+                const float a = area6(w.mb[k]);
                 if (a > best) best = a, pick = k;
             }
         }
         if (pick < 0) break;
-        const int y = member[pick];
-        inner[ni++] = y;
-        member[pick] = __ldcg(t.child_l + y);
-        member[m] = __ldcg(t.child_r + y);
-        ref_box32(t, member[pick], mb[pick]);
-        ref_box32(t, member[m], mb[m]);
+        const int y = w.member[pick];
+        w.inner[ni++] = y;
+        w.member[pick] = __ldcg(t.child_l + y);
+        w.member[m] = __ldcg(t.child_r + y);
+        ref_box32(t, w.member[pick], w.mb[pick]);
+        ref_box32(t, w.member[m], w.mb[m]);
         m++;
     }
-    float mcost[kTreeletLeaves];
+    w.m = m, w.ni = ni;
     if (m < 3) {
         float b[6];
         for (int q = 0; q < 6; q++) b[q] = __ldcg(t.nbox32 + 6 * x + q);
-        __stcg(t.cost + x, area6(b) + ref_cost(t, member[0]) + ref_cost(t, member[1]));
+        __stcg(t.cost + x, area6(b) + ref_cost(t, w.member[0]) + ref_cost(t, w.member[1]));
         return;
     }
-    for (int k = 0; k < m; k++) mcost[k] = ref_cost(t, member[k]);
+    for (int k = 0; k < m; k++) w.mcost[k] = ref_cost(t, w.member[k]);
     // current cost of the treelet: the old internal nodes' areas + members' costs
     float old_cost = 0.f;
     for (int k = 0; k < ni; k++) {
         float b[6];
-        for (int q = 0; q < 6; q++) b[q] = __ldcg(t.nbox32 + 6 * inner[k] + q);
+        for (int q = 0; q < 6; q++) b[q] = __ldcg(t.nbox32 + 6 * w.inner[k] + q);
         old_cost += area6(b);
     }
-    for (int k = 0; k < m; k++) old_cost += mcost[k];
-    // dynamic programme over subsets
-    const int full = (1 << m) - 1;
-    float c[kSubsets];
-    unsigned char split[kSubsets];
-    for (int s = 1; s <= full; s++) {
-        float b[6] = {FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX};
-        int nbits = 0, only = 0;
-        for (int k = 0; k < m; k++) {
-            if (!((s >> k) & 1)) continue;
-            nbits++, only = k;
-            for (int q = 0; q < 6; q += 2) b[q] = fminf(b[q], mb[k][q]), b[q + 1] = fmaxf(b[q + 1], mb[k][q + 1]);
+    for (int k = 0; k < m; k++) old_cost += w.mcost[k];
+    w.old_cost = old_cost;
+}
+
+// The whole warp: the best binary tree over the members, by dynamic programming over the member
+// subsets in rounds of growing size (a round reads only smaller subsets), the lanes sharing each
+// round's subsets. Each subset's split search is the sequential one (same order, same ties).
+__device__ void treelet_dp(TreeletWork &w, int lane) {
+    const int m = w.m, full = (1 << m) - 1;
+    for (int s = 1 + lane; s <= full; s += 32)
+        if ((s & (s - 1)) == 0) w.c[s] = w.mcost[__ffs(s) - 1], w.split[s] = 0;
+    __syncwarp();
+    for (int size = 2; size <= m; size++) {
+        for (int s = 1 + lane; s <= full; s += 32) {
+            if (__popc(s) != size) continue;
+            float b[6] = {FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX};
+            for (int k = 0; k < m; k++) {
+                if (!((s >> k) & 1)) continue;
+                for (int q = 0; q < 6; q += 2) b[q] = fminf(b[q], w.mb[k][q]), b[q + 1] = fmaxf(b[q + 1], w.mb[k][q + 1]);
+            }
+            float best = FLT_MAX;
+            int bp = 0;
+            // partitions (p, s \ p) with p holding the lowest member of s: each split once
+            const int low = s & -s;
+            for (int p = (s - 1) & s; p > 0; p = (p - 1) & s) {
+                if (!(p & low)) continue;
+                const float v = w.c[p] + w.c[s ^ p];
+                if (v < best) best = v, bp = p;
+            }
+            w.c[s] = area6(b) + best;
+            w.split[s] = (unsigned char)bp;
         }
-        if (nbits == 1) {
-            c[s] = mcost[only];
-            split[s] = 0;
-            continue;
-        }
-        float best = FLT_MAX;
-        int bp = 0;
-        // partitions (p, s \ p) with p holding the lowest member of s: each split once
-        const int low = s & -s;
-        for (int p = (s - 1) & s; p > 0; p = (p - 1) & s) {
-            if (!(p & low)) continue;
-            const float v = c[p] + c[s ^ p];
-            if (v < best) best = v, bp = p;
-        }
-        c[s] = area6(b) + best;
-        split[s] = (unsigned char)bp;
+        __syncwarp();
     }
-    if (!(c[full] < old_cost * (1.f - 1e-6f))) {
-        __stcg(t.cost + x, old_cost);
+}
+
+// One lane: replaces the treelet's arrangement by the programme's when it is cheaper, reusing the
+// treelet's internal nodes (the root keeps x), then fixes boxes, counts and costs bottom-up.
+__device__ void rebuild_treelet(const TreeArrays &t, int x, const TreeletWork &w) {
+    const int m = w.m, full = (1 << m) - 1;
+    if (!(w.c[full] < w.old_cost * (1.f - 1e-6f))) {
+        __stcg(t.cost + x, w.old_cost);
         return;
     }
-    // rebuild: internal nodes of the new tree take the treelet's internal ids, the root keeps x
     int stack_set[kTreeletLeaves], stack_node[kTreeletLeaves];
     int sp = 0, used = 1;
     stack_set[sp] = full, stack_node[sp] = x, sp++;
@@ -154,14 +176,14 @@ __device__ void optimize_treelet(const TreeArrays &t, int x) {
         sp--;
         const int s = stack_set[sp], node = stack_node[sp];
         order_node[norder] = node, order_set[norder] = s, norder++;
-        const int halves[2] = {split[s], s ^ split[s]};
+        const int halves[2] = {w.split[s], s ^ w.split[s]};
         int refs[2];
         for (int h = 0; h < 2; h++) {
             const int hs = halves[h];
             if ((hs & (hs - 1)) == 0) {
-                refs[h] = member[__ffs(hs) - 1];
+                refs[h] = w.member[__ffs(hs) - 1];
             } else {
-                refs[h] = inner[used++];
+                refs[h] = w.inner[used++];
                 stack_set[sp] = hs, stack_node[sp] = refs[h], sp++;
             }
         }
@@ -186,31 +208,61 @@ __device__ void optimize_treelet(const TreeArrays &t, int x) {
             __stcg(t.nbox64 + 6 * node + q + 1, fmax(dl[q + 1], dr[q + 1]));
         }
         __stcg(t.count + node, ref_count(t, l) + ref_count(t, r));
-        __stcg(t.cost + node, c[order_set[k]] - 0.f);
+        __stcg(t.cost + node, w.c[order_set[k]] - 0.f);
         __threadfence();
     }
 }
 
-__global__ void k_treelets(int n, TreeArrays t, int *arrivals) {
+constexpr int kTreeletThreads = 128;
+
+// One thread per triangle climbs from its leaf; the second thread to reach a node owns it (its
+// subtree is then final). Each round, the warp optimises its lanes' owned treelets one after the
+// other, all 32 lanes sharing each one's dynamic programme. Lanes without work stay in the loop (the
+// warp-wide votes need every lane) until the whole warp has climbed out.
+__global__ void __launch_bounds__(kTreeletThreads) k_treelets(int n, TreeArrays t, int *arrivals) {
+    __shared__ TreeletWork s_work[kTreeletThreads / 32];
+    TreeletWork &w = s_work[threadIdx.x >> 5];
+    constexpr unsigned kAll = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    int node = __ldcg(t.parent_leaf + p);
-    while (node >= 0) {
-        __threadfence();
-        if (atomicAdd(&arrivals[node], 1) == 0) return;
-        __threadfence();
-        const int l = __ldcg(t.child_l + node), r = __ldcg(t.child_r + node);
-        const int cnt = ref_count(t, l) + ref_count(t, r);
-        __stcg(t.count + node, cnt);
-        if (cnt >= kTreeletLeaves) {
-            optimize_treelet(t, node);
-        } else {
-            float b[6];
-            for (int q = 0; q < 6; q++) b[q] = __ldcg(t.nbox32 + 6 * node + q);
-            __stcg(t.cost + node, area6(b) + ref_cost(t, l) + ref_cost(t, r));
+    int node = p < n ? __ldcg(t.parent_leaf + p) : -1;
+    while (__any_sync(kAll, node >= 0)) {
+        bool own = false;
+        if (node >= 0) {
+            __threadfence();
+            if (atomicAdd(&arrivals[node], 1) == 0) {
+                node = -1;  // the first arrival: the other child's thread continues
+            } else {
+                __threadfence();
+                const int l = __ldcg(t.child_l + node), r = __ldcg(t.child_r + node);
+                const int cnt = ref_count(t, l) + ref_count(t, r);
+                __stcg(t.count + node, cnt);
+                if (cnt >= kTreeletLeaves) {
+                    own = true;
+                } else {
+                    float b[6];
+                    for (int q = 0; q < 6; q++) b[q] = __ldcg(t.nbox32 + 6 * node + q);
+                    __stcg(t.cost + node, area6(b) + ref_cost(t, l) + ref_cost(t, r));
+                }
+            }
         }
-        __threadfence();
-        node = __ldcg(t.parent_int + node);
+        unsigned todo = __ballot_sync(kAll, own);
+        while (todo) {
+            const int owner = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const int x = __shfl_sync(kAll, node, owner);
+            if (lane == owner) form_treelet(t, x, w);
+            __syncwarp();
+            if (w.m >= 3) {
+                treelet_dp(w, lane);
+                if (lane == owner) rebuild_treelet(t, x, w);
+            }
+            __syncwarp();
+        }
+        if (node >= 0) {
+            __threadfence();
+            node = __ldcg(t.parent_int + node);
+        }
     }
 }
 
@@ -286,7 +338,7 @@ int treelet_optimize(int n, int *child_l, int *child_r, int *parent_int, int *pa
         TreeArrays t{child_l, child_r, parent_int, parent_leaf, nbox32, nbox64, pbox32, pbox64, sorted_ids, cost, count};
         e = cudaMemsetAsync(arrivals, 0, sizeof(int) * nint, stream);
         if (e == cudaSuccess) {
-            k_treelets<<<grid_blocks(n, 128), 128, 0, stream>>>(n, t, arrivals);
+            k_treelets<<<grid_blocks(n, kTreeletThreads), kTreeletThreads, 0, stream>>>(n, t, arrivals);
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) {
