@@ -576,6 +576,22 @@ class DeviceMesh:
         self.nt = mesh.nt
         self.nv = mesh.nv
 
+    @classmethod
+    def from_device(cls, s0, s1, s2, sx, sy, sz, keep_fp64=True, normals=False, leaf_size=0, treelet=True,
+                    stream=None):
+        """A mesh from device arrays (torch CUDA tensors: int32 indices, one float dtype for the
+        vertices), built without a host round trip."""
+        self = cls.__new__(cls)
+        self._h = C.c_void_p()
+        opts = BuildOpts(int(leaf_size), int(keep_fp64), int(normals), int(treelet))
+        _check(lib.ssdf_mesh_create(C.byref(self._h), s0.numel(), C.cast(C.c_void_p(_dptr(s0)), _ip),
+                                    C.cast(C.c_void_p(_dptr(s1)), _ip), C.cast(C.c_void_p(_dptr(s2)), _ip),
+                                    sx.numel(), _dptr(sx), _dptr(sy), _dptr(sz), _dtype_code(sx), 1, C.byref(opts),
+                                    _stream_handle(stream)), "ssdf_mesh_create")
+        self.nt = s0.numel()
+        self.nv = sx.numel()
+        return self
+
     def close(self):
         if self._h:
             lib.ssdf_mesh_destroy(self._h)
