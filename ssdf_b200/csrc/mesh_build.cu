@@ -773,7 +773,7 @@ static int mesh_build_impl(MeshStorage *s, MeshStorage *tmp, DeviceMesh *m, int 
         k_refit<<<grid_blocks(nt, 256), 256, 0, stream>>>(nt, ids, child_l, child_r, parent_int, parent_leaf, box32,
                                                           box64, nbox32, nbox64, arrivals);
         LAUNCH_CHECK("k_refit");
-        if (opts.treelet_opt) {
+        for (int round = 0; round < opts.treelet_opt && round < 8; round++) {  // treelet_opt: rounds (0 = none)
             SSDF_CHECK(treelet_optimize(nt, child_l, child_r, parent_int, parent_leaf, first_of, nbox32, nbox64,
                                         box32, box64, ids, stream));
         }
