@@ -382,7 +382,7 @@ typedef struct {
     int leaf_size;    /* triangles per BVH leaf, 1..16 (0: 4)                                 */
     int keep_fp64;    /* 1: also keep double triangles and nodes (F64 and fix-up queries)      */
     int normals;      /* 1: build pseudo-normals (signed queries)                             */
-    int treelet_opt;  /* 1: SAH treelet refinement of the LBVH (0: plain LBVH); 1 by default    */
+    int treelet_opt;  /* rounds of SAH treelet refinement of the LBVH (0: plain LBVH; <= 8); 1 by default */
 } ssdf_build_opts;
 
 typedef struct {
