@@ -144,3 +144,25 @@ def test_deterministic():
     a = S.edf_index(pts, mesh)
     b = S.edf_index(pts, mesh)
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_nan_and_infinite_points():
+    """Points with a NaN or infinite coordinate take part like the reference's loops take them: no
+    comparison with NaN succeeds, so such a point keeps its incoming value, the others are exact; every
+    method and precision agrees with the oracle, and the points around them are unaffected (sorted
+    and unsorted lists)."""
+    mesh = W.icosphere(2)
+    rng = np.random.default_rng(9)
+    for n in (300, 5000):
+        pts = rng.uniform(-1.5, 1.5, size=(3, n))
+        pts[0, ::37] = np.nan
+        pts[1, 5::41] = np.inf
+        pts[2, 7::43] = -np.inf
+        init = np.where(np.arange(n) % 5 == 0, 0.3, np.finfo(np.float64).max)
+        want, wtri = oracle.edf(pts, mesh, out=init, with_index=True)
+        for method in ALL_UNSIGNED:
+            got = run_unsigned(method, pts, mesh, out=init)
+            assert np.array_equal(got, want, equal_nan=True), (method, n)
+        with env(SSDF_B200_PRECISION="f64"):
+            g64, t64 = S.edf_index(pts, mesh, out=init)
+        assert np.array_equal(g64, want, equal_nan=True) and np.array_equal(t64, np.where(wtri >= 0, wtri, -1))
