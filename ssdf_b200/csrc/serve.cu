@@ -196,8 +196,8 @@ int admit(ssdf_server *s, int id) {
 }
 
 void finish(ssdf_server *s, Slot &sl, int status) {
-    // copy results to the callers and stamp latencies (caller holds no lock)
-    const auto now = Clock::now();
+    // copy results to the callers, then stamp latencies: a request counts as served once its results
+    // are in the caller's arrays (caller holds no lock)
     for (size_t k = 0; k < sl.reqs.size(); k++) {
         Request &r = *sl.reqs[k];
         const long long n = r.grid ? r.nx * r.ny * r.nz : r.n;
@@ -207,6 +207,7 @@ void finish(ssdf_server *s, Slot &sl, int status) {
         }
         r.status = status;
     }
+    const auto now = Clock::now();
     std::lock_guard<std::mutex> lock(s->mu);
     for (auto &rp : sl.reqs) {
         rp->done = true;
