@@ -213,11 +213,17 @@ __device__ __forceinline__ void boxes4_fast(const DeviceMesh &m, int node, float
 struct Tri32 {
     float ax, ay, az, bx, by, bz, cx, cy, cz;
     int id;
-    float pen;  // fix-up filter records: 0, or +inf for a proxy (never the window's centre)
 };
+
+// The fix-up filter's record of leaf position p (DeviceMesh::filt32, 4 x float4): the precomputed
+// triangle (or proxy); the fourth vector holds the id and the proxy flag.
+__device__ __forceinline__ FiltRec load_filt(const float4 *__restrict__ f, int p) {
+    const float4 u = __ldg(f + 4 * p), v = __ldg(f + 4 * p + 1), w = __ldg(f + 4 * p + 2);
+    return FiltRec{u.x, u.y, u.z, v.x, v.y, v.z, w.x, w.y, w.z, u.w, v.w, w.w};
+}
 __device__ __forceinline__ Tri32 load_tri32(const float4 *__restrict__ t, int p) {
     const float4 u = __ldg(t + 3 * p), v = __ldg(t + 3 * p + 1), w = __ldg(t + 3 * p + 2);
-    return Tri32{u.x, u.y, u.z, u.w, v.x, v.y, v.z, v.w, w.x, __float_as_int(w.y), w.z};
+    return Tri32{u.x, u.y, u.z, u.w, v.x, v.y, v.z, v.w, w.x, __float_as_int(w.y)};
 }
 
 struct Tri64 {
@@ -431,16 +437,16 @@ struct FastPolicy {
     template <bool COUNT>
     __device__ __forceinline__ void leaf(int first, int n, unsigned mask, Counters &cnt) {
         for (int k = 0; k < n; k++) {
-            const Tri32 t = load_tri32(m.filt32, first + k);
+            const FiltRec t = load_filt(m.filt32, first + k);
+            const float pen = __ldg(m.filt32 + 4 * (first + k) + 3).y;
 #pragma unroll
             for (int q = 0; q < Q; q++) {
                 if (!((mask >> q) & 1u)) continue;
-                const float d2 =
-                    tri_dist_sq_fast(px[q], py[q], pz[q], t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
+                const float d2 = tri_dist_sq_filter(px[q], py[q], pz[q], t);
                 if (COUNT) cnt.tri++;
                 if (d2 < thr[q]) {
                     insert(q, d2, first + k);
-                    if (d2 + t.pen < best[q]) {
+                    if (d2 + pen < best[q]) {
                         best[q] = d2;
                         thr[q] = window_thr(best[q], tau_rel, m.coord_scale);
                     }
@@ -998,8 +1004,7 @@ __device__ __forceinline__ void window_leaf(const DeviceMesh &m, int ref, float 
                                             bool count) {
     const int first = leaf_first(ref), n = leaf_count(ref);
     for (int k = 0; k < n; k++) {
-        const Tri32 t = load_tri32(m.filt32, first + k);  // the first stage's key
-        const float f = tri_dist_sq_fast(px, py, pz, t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
+        const float f = tri_dist_sq_filter(px, py, pz, load_filt(m.filt32, first + k));  // the first stage's key
         if (count) cnt.tri++;
         if (f < thr) {
             const Tri64 u = load_tri64(m.tris64, first + k);

@@ -113,49 +113,56 @@ __device__ __forceinline__ void tri_closest_point_exact(const T px, const T py, 
     oz = az + abz * v + acz * w;
 }
 
-// FP32 filter of the fix-up path: the same regions with fused multiply-adds and an approximate
-// reciprocal. Its error against the exact double value is covered by the fix-up window.
-__device__ __forceinline__ float tri_dist_sq_fast(const float px, const float py, const float pz, const float ax,
-                                                  const float ay, const float az, const float bx, const float by,
-                                                  const float bz, const float cx, const float cy, const float cz) {
-    const float abx = bx - ax, aby = by - ay, abz = bz - az;
-    const float acx = cx - ax, acy = cy - ay, acz = cz - az;
-    const float apx = px - ax, apy = py - ay, apz = pz - az;
-    const float d1 = fmaf(abx, apx, fmaf(aby, apy, abz * apz));
-    const float d2 = fmaf(acx, apx, fmaf(acy, apy, acz * apz));
+// FP32 filter of the fix-up path: Ericson's regions (Real-Time Collision Detection, 5.1.5) over a
+// precomputed record -- corner a, edges ab and ac, and the products ab.ab, ac.ac, ab.ac -- so that
+// the dot products with b - p and c - p follow from those with a - p by one subtraction each, with
+// fused multiply-adds and an approximate reciprocal. Its error against the exact double value is
+// covered by the fix-up window.
+struct FiltRec {
+    float ax, ay, az, abx, aby, abz, acx, acy, acz, abab, acac, abac;
+};
+__device__ __forceinline__ float tri_dist_sq_filter(const float px, const float py, const float pz, const FiltRec &r) {
+    const float apx = px - r.ax, apy = py - r.ay, apz = pz - r.az;
+    const float d1 = fmaf(r.abx, apx, fmaf(r.aby, apy, r.abz * apz));
+    const float d2 = fmaf(r.acx, apx, fmaf(r.acy, apy, r.acz * apz));
     if (d1 <= 0.f && d2 <= 0.f) return fmaf(apx, apx, fmaf(apy, apy, apz * apz));
-    const float bpx = px - bx, bpy = py - by, bpz = pz - bz;
-    const float d3 = fmaf(abx, bpx, fmaf(aby, bpy, abz * bpz));
-    const float d4 = fmaf(acx, bpx, fmaf(acy, bpy, acz * bpz));
-    if (d3 >= 0.f && d4 <= d3) return fmaf(bpx, bpx, fmaf(bpy, bpy, bpz * bpz));
+    const float d3 = d1 - r.abab, d4 = d2 - r.abac;  // ab.(p - b), ac.(p - b)
+    if (d3 >= 0.f && d4 <= d3) {
+        const float bx = apx - r.abx, by = apy - r.aby, bz = apz - r.abz;
+        return fmaf(bx, bx, fmaf(by, by, bz * bz));
+    }
     const float vc = fmaf(d1, d4, -d3 * d2);
     if (vc <= 0.f && d1 >= 0.f && d3 <= 0.f) {
         const float v = __fdividef(d1, d1 - d3);
-        const float dx = apx - v * abx, dy = apy - v * aby, dz = apz - v * abz;
+        const float dx = fmaf(-v, r.abx, apx), dy = fmaf(-v, r.aby, apy), dz = fmaf(-v, r.abz, apz);
         return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     }
-    const float cpx = px - cx, cpy = py - cy, cpz = pz - cz;
-    const float d5 = fmaf(abx, cpx, fmaf(aby, cpy, abz * cpz));
-    const float d6 = fmaf(acx, cpx, fmaf(acy, cpy, acz * cpz));
-    if (d6 >= 0.f && d5 <= d6) return fmaf(cpx, cpx, fmaf(cpy, cpy, cpz * cpz));
+    const float d5 = d1 - r.abac, d6 = d2 - r.acac;  // ab.(p - c), ac.(p - c)
+    if (d6 >= 0.f && d5 <= d6) {
+        const float cx = apx - r.acx, cy = apy - r.acy, cz = apz - r.acz;
+        return fmaf(cx, cx, fmaf(cy, cy, cz * cz));
+    }
     const float vb = fmaf(d5, d2, -d1 * d6);
     if (vb <= 0.f && d2 >= 0.f && d6 <= 0.f) {
         const float w = __fdividef(d2, d2 - d6);
-        const float dx = apx - w * acx, dy = apy - w * acy, dz = apz - w * acz;
+        const float dx = fmaf(-w, r.acx, apx), dy = fmaf(-w, r.acy, apy), dz = fmaf(-w, r.acz, apz);
         return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     }
     const float va = fmaf(d3, d6, -d5 * d4);
     if (va <= 0.f && (d4 - d3) >= 0.f && (d5 - d6) >= 0.f) {
         const float w = __fdividef(d4 - d3, (d4 - d3) + (d5 - d6));
-        const float dx = bpx - w * (cx - bx), dy = bpy - w * (cy - by), dz = bpz - w * (cz - bz);
+        // p - (b + w (c - b)) = (p - a) - ab - w (ac - ab)
+        const float dx = fmaf(-w, r.acx - r.abx, apx - r.abx);
+        const float dy = fmaf(-w, r.acy - r.aby, apy - r.aby);
+        const float dz = fmaf(-w, r.acz - r.abz, apz - r.abz);
         return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     }
     const float denom = __frcp_rn(va + vb + vc);
     const float v = vb * denom;
     const float w = vc * denom;
-    const float dx = apx - fmaf(abx, v, acx * w);
-    const float dy = apy - fmaf(aby, v, acy * w);
-    const float dz = apz - fmaf(abz, v, acz * w);
+    const float dx = apx - fmaf(r.abx, v, r.acx * w);
+    const float dy = apy - fmaf(r.aby, v, r.acy * w);
+    const float dz = apz - fmaf(r.abz, v, r.acz * w);
     return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
 }
 

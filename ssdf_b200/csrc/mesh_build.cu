@@ -480,9 +480,20 @@ __device__ bool filter_record(double ax, double ay, double az, double bx, double
         for (int a = 0; a < 3; a++)
             for (int d = 0; d < 3; d++) v[a][d] = pr[a][d];
     }
-    out[0] = make_float4(float(v[0][0]), float(v[0][1]), float(v[0][2]), float(v[1][0]));
-    out[1] = make_float4(float(v[1][1]), float(v[1][2]), float(v[2][0]), float(v[2][1]));
-    out[2] = make_float4(float(v[2][2]), __int_as_float(t), ill ? __int_as_float(0x7f800000) : 0.f, 0.f);
+    // a, ab = b - a, ac = c - a and the products ab.ab, ac.ac, ab.ac, from the rounded corners (so the
+    // record is the triangle the float corners describe), in double and then rounded once
+    float f[3][3];
+    for (int k = 0; k < 3; k++)
+        for (int d = 0; d < 3; d++) f[k][d] = float(v[k][d]);
+    double eb[3], ec[3];
+    for (int d = 0; d < 3; d++) eb[d] = double(f[1][d]) - double(f[0][d]), ec[d] = double(f[2][d]) - double(f[0][d]);
+    const double bb = eb[0] * eb[0] + eb[1] * eb[1] + eb[2] * eb[2];
+    const double cc = ec[0] * ec[0] + ec[1] * ec[1] + ec[2] * ec[2];
+    const double bc = eb[0] * ec[0] + eb[1] * ec[1] + eb[2] * ec[2];
+    out[0] = make_float4(f[0][0], f[0][1], f[0][2], float(bb));
+    out[1] = make_float4(float(eb[0]), float(eb[1]), float(eb[2]), float(cc));
+    out[2] = make_float4(float(ec[0]), float(ec[1]), float(ec[2]), float(bc));
+    out[3] = make_float4(__int_as_float(t), ill ? __int_as_float(0x7f800000) : 0.f, 0.f, 0.f);
     return ill;
 }
 
@@ -499,7 +510,7 @@ __global__ void k_tri_records(int nt, const int *__restrict__ sorted_ids, const 
     t32[3 * p + 0] = make_float4(float(ax), float(ay), float(az), float(bx));
     t32[3 * p + 1] = make_float4(float(by), float(bz), float(cx), float(cy));
     t32[3 * p + 2] = make_float4(float(cz), __int_as_float(t), 0.f, 0.f);
-    if (filt && filter_record(ax, ay, az, bx, by, bz, cx, cy, cz, t, filt + 3 * size_t(p))) atomicAdd(nill, 1);
+    if (filt && filter_record(ax, ay, az, bx, by, bz, cx, cy, cz, t, filt + 4 * size_t(p))) atomicAdd(nill, 1);
     if (t64) {
         t64[5 * p + 0] = make_double2(ax, ay);
         t64[5 * p + 1] = make_double2(az, bx);
@@ -822,7 +833,7 @@ static int mesh_build_impl(MeshStorage *s, MeshStorage *tmp, DeviceMesh *m, int 
     double2 *t64 = nullptr;
     SSDF_CHECK(dalloc(s, &t32, 3 * size_t(nt), stream));
     if (keep64) SSDF_CHECK(dalloc(s, &t64, 5 * size_t(nt), stream));
-    if (keep64) SSDF_CHECK(dalloc(s, &filt, 3 * size_t(nt), stream));  // the fix-up path's filter records
+    if (keep64) SSDF_CHECK(dalloc(s, &filt, 4 * size_t(nt), stream));  // the fix-up path's filter records
     k_tri_records<<<grid_blocks(nt, 256), 256, 0, stream>>>(nt, ids, s0, s1, s2, vx, vy, vz, t32, t64, filt,
                                                             flags + 10);
     LAUNCH_CHECK("k_tri_records");
