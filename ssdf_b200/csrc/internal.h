@@ -44,7 +44,7 @@ int cuda_fail(cudaError_t err, const char *what, const char *file, int line);
 // A reference >= 0 is an internal node; < 0 is a leaf ~((first << 5) | (count - 1)) over the
 // triangle records in leaf order; kEmptyRef is an empty slot (its box is inverted).
 // Triangles in leaf order:
-//   FP32 record (3 x float4): (ax, ay, az, bx), (by, bz, cx, cy), (cz, id bits, pen, -)
+//   FP32 record (3 x float4): (ax, ay, az, bx), (by, bz, cx, cy), (cz, id bits, -, -)
 //   FP64 record (5 x double2): (ax, ay), (az, bx), (by, bz), (cx, cy), (cz, id)
 // where id is the triangle's index in the caller's s0/s1/s2 and a, b, c its vertices s0, s1, s2.
 constexpr int kEmptyRef = -2147483647 - 1;  // INT_MIN
@@ -73,9 +73,10 @@ struct DeviceMesh {
     const double2 *nodes4_64 = nullptr;  // [14 * nnodes4] or null
     const float4 *tris32 = nullptr;    // [3 * nt], leaf order
     const double2 *tris64 = nullptr;   // [5 * nt], leaf order, or null
-    // the fix-up path's FP32 filter records, [3 * nt], leaf order, with the double data or null: the
-    // FP32 record of the triangle (pen 0), or of a well-conditioned proxy containing an
-    // ill-conditioned one (pen +inf; mesh_build.cu, filter_record)
+    // the fix-up path's FP32 filter records, [4 * nt], leaf order, with the double data or null:
+    // (ax, ay, az, ab.ab), (abx, aby, abz, ac.ac), (acx, acy, acz, ab.ac), (id bits, pen, -, -) of the
+    // triangle (pen 0), or of a well-conditioned proxy containing an ill-conditioned one (pen +inf;
+    // mesh_build.cu, filter_record)
     const float4 *filt32 = nullptr;
     // sign data, caller's triangle order
     const int *s0 = nullptr, *s1 = nullptr, *s2 = nullptr;  // [nt]
