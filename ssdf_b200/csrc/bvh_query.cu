@@ -47,12 +47,13 @@ constexpr int kThreads = 128;
 #endif
 constexpr int kCand = SSDF_B200_WINDOW_SLOTS;
 
-// Minimum resident blocks per SM the float query kernels are compiled for: 10 blocks of 128 caps
-// them at 48 registers (the fix-up window lives in shared memory). The traversal is issue-latency
+// Minimum resident blocks per SM the float query kernels are compiled for: 9 blocks of 128 cap
+// them at 56 registers (the fix-up window lives in shared memory). The traversal is issue-latency
 // bound, so the occupancy this buys outweighs the few spills (measured on the torus-knot grid:
-// 24.5 ms against 34 ms uncapped); the double kernel keeps its registers.
+// 17.8 ms against 18.4 ms for 10 blocks at 48 registers, 18.6 ms for 8 at 64, and 34 ms uncapped);
+// the double kernel keeps its registers.
 #ifndef SSDF_B200_QUERY_MIN_BLOCKS
-#define SSDF_B200_QUERY_MIN_BLOCKS 10
+#define SSDF_B200_QUERY_MIN_BLOCKS 9
 #endif
 
 struct Counters {
@@ -345,10 +346,16 @@ struct ExactPolicy {
 };
 
 // F32X: float filter. Per query, the kCand smallest float d^2 inside the window
-// (sqrt(best) + tau)^2 are kept, sorted, in shared memory (slot (q, s) of thread t at
+// (sqrt(best) + tau)^2 are kept, unordered, in shared memory (slot (q, s) of thread t at
 // [(q * kCand + s) * kThreads + t]: consecutive threads, consecutive banks), with the smallest d^2
-// pushed out of the slots. The float filter's error is second order in its error along the
-// triangle's plane, which stays small unless the triangle is ill-conditioned (a needle or a
+// pushed out of the slots. A candidate is appended to the used slots; only when they are full are
+// the entries the shrinking window has left behind dropped (their d^2 is at or above the final
+// window, so dropping them loses nothing), and if every slot is still inside the window the largest
+// of the kCand + 1 is pushed out. The slots hold the same inside-the-window set as a sorted list
+// would, for an append instead of a sorted insertion.
+//
+// The float filter's error is second order in its error along the triangle's plane, which stays
+// small unless the triangle is ill-conditioned (a needle or a
 // sliver: the face-region solve divides by its area). Such a triangle is filtered through a
 // well-conditioned proxy that contains it (DeviceMesh::filt32): a lower bound of its distance,
 // within the float filter's error, which may enter the window but, with its +inf penalty, never
@@ -367,7 +374,8 @@ struct FastPolicy {
     static constexpr int kQn = Q;
     static constexpr bool kBudgeted = true;
     const DeviceMesh &m;
-    float px[Q], py[Q], pz[Q], best[Q], thr[Q], evicted[Q], wmax[Q];
+    float px[Q], py[Q], pz[Q], best[Q], thr[Q], evicted[Q];
+    int used[Q];  // window slots in use
     float tau_rel;
     float *wd;
     int *wp;
@@ -375,10 +383,8 @@ struct FastPolicy {
         : m(mesh), tau_rel(tau), wd(sd + threadIdx.x), wp(sp + threadIdx.x) {}
     __device__ __forceinline__ int slot(int q, int s) const { return (q * kCand + s) * kThreads; }
     __device__ __forceinline__ void set(int q, float x, float y, float z, float init) {
-        px[q] = x, py[q] = y, pz[q] = z, best[q] = init, evicted[q] = finf(), wmax[q] = finf();
+        px[q] = x, py[q] = y, pz[q] = z, best[q] = init, evicted[q] = finf(), used[q] = 0;
         thr[q] = window_thr(init, tau_rel, m.coord_scale);
-#pragma unroll
-        for (int s = 0; s < kCand; s++) wd[slot(q, s)] = finf(), wp[slot(q, s)] = -1;
     }
     __device__ __forceinline__ void disable(int q) {
         set(q, 0.f, 0.f, 0.f, finf());
@@ -416,23 +422,36 @@ struct FastPolicy {
         return t;
     }
     __device__ __forceinline__ void insert(int q, float d, int p) {
-        if (!(d < wmax[q])) {
-            evicted[q] = fminf(evicted[q], d);
+        if (used[q] < kCand) {
+            wd[slot(q, used[q])] = d;
+            wp[slot(q, used[q])] = p;
+            used[q]++;
             return;
         }
-#pragma unroll
+        // full: keep the entries still inside the window, in place
+        int w = 0, imax = 0;
+        float vmax = -1.f;
         for (int s = 0; s < kCand; s++) {
             const float cur = wd[slot(q, s)];
-            if (d < cur) {
+            if (cur < thr[q]) {
                 const int cp = wp[slot(q, s)];
-                wd[slot(q, s)] = d;
-                wp[slot(q, s)] = p;
-                d = cur;
-                p = cp;
+                wd[slot(q, w)] = cur;
+                wp[slot(q, w)] = cp;
+                if (cur > vmax) vmax = cur, imax = w;
+                w++;
             }
         }
-        evicted[q] = fminf(evicted[q], d);
-        wmax[q] = wd[slot(q, kCand - 1)];
+        if (w < kCand) {
+            wd[slot(q, w)] = d;
+            wp[slot(q, w)] = p;
+            used[q] = w + 1;
+        } else if (d < vmax) {  // every slot inside the window: the largest of the kCand + 1 goes
+            evicted[q] = fminf(evicted[q], vmax);
+            wd[slot(q, imax)] = d;
+            wp[slot(q, imax)] = p;
+        } else {
+            evicted[q] = fminf(evicted[q], d);
+        }
     }
     template <bool COUNT>
     __device__ __forceinline__ void leaf(int first, int n, unsigned mask, Counters &cnt) {
@@ -945,8 +964,7 @@ __device__ __forceinline__ void query_block(const QueryArgs &a, long long block,
             query_point(a, q, gi[s], gj[s], gk[s], rx, ry, rz);
             double b = initial_bound(a, q);
             int bid = -1, bpos = -1;
-#pragma unroll
-            for (int c = 0; c < kCand; c++) {
+            for (int c = 0; c < p.used[s]; c++) {
                 const int ix = p.slot(s, c);
                 if (p.wd[ix] < p.thr[s]) {
                     const int pos = p.wp[ix];
