@@ -874,6 +874,23 @@ __device__ __forceinline__ void flush_counters(const QueryArgs &a, const Counter
 
 // ---- kernels ----------------------------------------------------------------------------------------
 
+// Streamed download: the block's results are stored; the last block of its chunk to finish tells the
+// host, which copies the chunk out while the launch goes on. Every thread fences its own stores
+// before the block counts itself, and the last block fences at system scope before the flag.
+__device__ __forceinline__ void signal_chunk(const QueryArgs &a) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned c = blockIdx.x / unsigned(a.chunk_blocks);
+        const unsigned members = min(unsigned(a.chunk_blocks), gridDim.x - c * unsigned(a.chunk_blocks));
+        if (atomicAdd(a.chunk_counts + c, 1) == int(members) - 1) {
+            __threadfence_system();
+            *(volatile int *)(a.chunk_flags + c) = 1;
+        }
+    }
+}
+
 // One block of 128 lanes x kQ queries. Lanes without a query (the edge of a grid brick, the tail of
 // a point list) take part in warp-mode traversal with a negative threshold, so they never ask for
 // a node.
@@ -986,12 +1003,16 @@ __device__ __forceinline__ void query_block(const QueryArgs &a, long long block,
 
 // BUDGET: the fix-up kernel's packets stop after QueryArgs::warp_budget triangle records (a separate
 // instantiation, so the kernels without it compile as if it did not exist).
-template <int PREC, bool WARP, bool WIDE, bool COUNT, bool BUDGET = false>
+// SIGNAL: the streamed grid download's instantiation, whose blocks count themselves done per chunk
+// (a separate instantiation: the dormant signal code cost the fix-up kernel 3 % where it was merely
+// compiled in).
+template <int PREC, bool WARP, bool WIDE, bool COUNT, bool BUDGET = false, bool SIGNAL = false>
 __global__ void __launch_bounds__(kThreads, PREC == SSDF_PREC_F64 ? 1 : SSDF_B200_QUERY_MIN_BLOCKS)
     k_query(const QueryArgs a) {
     Counters cnt;
     query_block<PREC, WARP, WIDE, COUNT, BUDGET>(a, blockIdx.x, cnt);
     if (COUNT) flush_counters(a, cnt);
+    if constexpr (SIGNAL) signal_chunk(a);
 }
 
 // ---- second fix-up stage: one warp per overflowed query --------------------------------------------
@@ -1251,8 +1272,12 @@ cudaError_t launch_main(const QueryArgs &a, bool count, unsigned nblocks, cudaSt
             return cudaGetLastError();
         }
     }
+    // a counting or budgeted launch raises no chunk flags: its streamed download copies every chunk
+    // once the launch has ended
     if (count)
         k_query<PREC, WARP, WIDE, true><<<nblocks, kThreads, 0, stream>>>(a);
+    else if (a.chunk_flags)
+        k_query<PREC, WARP, WIDE, false, false, true><<<nblocks, kThreads, 0, stream>>>(a);
     else
         k_query<PREC, WARP, WIDE, false><<<nblocks, kThreads, 0, stream>>>(a);
     return cudaGetLastError();
@@ -1377,6 +1402,11 @@ unsigned window_grid() {
 }
 
 int launch_query(const QueryArgs &args_in, int precision, cudaStream_t stream) {
+    return launch_query_keep(args_in, precision, stream, nullptr);
+}
+
+int launch_query_keep(const QueryArgs &args_in, int precision, cudaStream_t stream, int **fallback_list) {
+    if (fallback_list) *fallback_list = nullptr;
     retain_pool_memory();
     QueryArgs a = args_in;
     const long long n = a.is_grid ? a.nx * a.ny * a.nz : a.npoints;
@@ -1461,7 +1491,10 @@ int launch_query(const QueryArgs &args_in, int precision, cudaStream_t stream) {
         h[3] = (unsigned long long)nfb;
         memcpy(t_last_counts, h, sizeof(h));
     }
-    if (fb) cudaFreeAsync(fb, stream);
+    if (fb && fallback_list && st == SSDF_OK)
+        *fallback_list = fb;  // [count, ids...]; the caller frees it (stream-ordered)
+    else if (fb)
+        cudaFreeAsync(fb, stream);
     if (counters) cudaFreeAsync(counters, stream);
     return st;
 }

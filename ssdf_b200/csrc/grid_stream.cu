@@ -1,0 +1,224 @@
+// Streamed download of a grid query into page-locked host arrays.
+//
+// The drop-in grid entry points (ssdf::sample_sdf_bvh and the other host-array grid calls,
+// serial/bvh/bvh.cpp) build the BVH, query every node and hand the values back in the caller's
+// arrays. The query kernel and the device-to-host copy of its results would run one after the other;
+// here the copy of each slab chunk starts as soon as the kernel has finished that chunk:
+//
+//   - a grid launch's blocks are slab-major (bricks of 8 x 4 x 4kQ nodes, x fastest, then y, then
+//     z), so the blocks of whole z-slabs cover one contiguous range of the output;
+//   - the last block of a chunk to finish raises the chunk's flag in page-locked host memory
+//     (signal_chunk in bvh_query.cu), and this thread, which would otherwise wait for the launch,
+//     polls the flags and issues one cudaMemcpyAsync per finished chunk on a second stream;
+//   - the fix-up arithmetic finishes a few queries in its second stage, after the chunk that holds
+//     them may have been copied: their final values are gathered on the device once the launch is
+//     done and written into the host arrays after every chunk copy has landed.
+//
+// The host arrays end up with the same bits as a launch followed by one copy.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "internal.h"
+
+namespace ssdf_b200 {
+
+namespace {
+
+constexpr int kMaxChunks = 64;
+constexpr int kTargetChunks = 16;
+// Below this many nodes the copy is short next to the launch overhead it would hide.
+constexpr long long kStreamMinQueries = 1ll << 22;
+
+struct ThreadResources {
+    int device = -1;
+    cudaStream_t copy = nullptr;  // chunk copies
+    int *flags = nullptr;         // [kMaxChunks], page-locked, mapped
+    int *dflags = nullptr;        // the flags' device address
+};
+thread_local ThreadResources t_res;
+
+int thread_resources(ThreadResources **out) {
+    int dev = 0;
+    SSDF_CUDA(cudaGetDevice(&dev));
+    ThreadResources &r = t_res;
+    if (r.device != dev) {  // one set per thread; a thread that changes device gets a new set
+        r = ThreadResources{};
+        SSDF_CUDA(cudaStreamCreateWithFlags(&r.copy, cudaStreamNonBlocking));
+        SSDF_CUDA(cudaHostAlloc((void **)&r.flags, sizeof(int) * kMaxChunks, cudaHostAllocMapped));
+        SSDF_CUDA(cudaHostGetDevicePointer((void **)&r.dflags, r.flags, 0));
+        r.device = dev;
+    }
+    *out = &r;
+    return SSDF_OK;
+}
+
+bool page_locked(const void *p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();  // an unknown pointer is not an error here
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
+// The final values of the second stage's queries, packed for one copy: values (as out's type), then
+// triangle indices.
+__global__ void k_gather_fallback(int count, const int *__restrict__ ids, const void *__restrict__ out, int out_f64,
+                                  const int *__restrict__ tri, void *__restrict__ vals, int *__restrict__ tris) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int q = ids[i];
+    if (out_f64)
+        ((double *)vals)[i] = ((const double *)out)[q];
+    else
+        ((float *)vals)[i] = ((const float *)out)[q];
+    if (tri) tris[i] = tri[q];
+}
+
+// Contiguous element range [lo, hi) of chunk c.
+struct ChunkPlan {
+    long long planes_per_chunk, plane_elems, nz;
+    int nchunks, chunk_blocks;
+    long long lo(int c) const { return std::min(nz, c * planes_per_chunk) * plane_elems; }
+    long long hi(int c) const { return std::min(nz, (c + 1) * planes_per_chunk) * plane_elems; }
+};
+
+ChunkPlan plan_chunks(const QueryArgs &a) {
+    const long long slab = 4 * kQ;  // z-planes of one row of bricks
+    const long long bxn = (a.nx + 7) / 8, byn = (a.ny + 3) / 4;
+    const long long slabs = (a.nz + slab - 1) / slab;
+    const long long per = (slabs + kTargetChunks - 1) / kTargetChunks;
+    ChunkPlan p;
+    p.planes_per_chunk = per * slab;
+    p.plane_elems = a.nx * a.ny;
+    p.nz = a.nz;
+    p.nchunks = int((slabs + per - 1) / per);
+    p.chunk_blocks = int(per * bxn * byn);
+    return p;
+}
+
+}  // namespace
+
+bool streamed_download_applies(long long n, const void *host_out, const int *host_tri) {
+    if (n < kStreamMinQueries || env_int("SSDF_B200_STREAM_DOWNLOAD", 1) == 0) return false;
+    return page_locked(host_out) && (!host_tri || page_locked(host_tri));
+}
+
+int launch_query_streamed(const QueryArgs &args, int precision, void *host_out, int *host_tri, cudaStream_t stream) {
+    QueryArgs a = args;
+    if (!a.is_grid) return fail(SSDF_ERR_INVALID_ARGUMENT, "streamed download serves grids");
+    const long long n = a.nx * a.ny * a.nz;
+    if (n <= 0) return SSDF_OK;
+    const ChunkPlan plan = plan_chunks(a);
+    if (plan.nchunks > kMaxChunks || plan.chunk_blocks <= 0 || query_blocks(a) > 0x7fffffffll)
+        return fail(SSDF_ERR_NOT_SUPPORTED, "grid too large for the streamed download");
+    ThreadResources *r = nullptr;
+    SSDF_CHECK(thread_resources(&r));
+    const size_t esz = a.out_f64 ? sizeof(double) : sizeof(float);
+    int *counts = nullptr;
+    SSDF_CUDA(cudaMallocAsync(&counts, sizeof(int) * kMaxChunks, stream));
+    struct Cleanup {
+        int *counts;
+        int *fb = nullptr;
+        cudaStream_t s;
+        cudaEvent_t done = nullptr;
+        ~Cleanup() {
+            if (fb) cudaFreeAsync(fb, s);
+            cudaFreeAsync(counts, s);
+            if (done) cudaEventDestroy(done);
+        }
+    } cl{counts, nullptr, stream};
+    SSDF_CUDA(cudaMemsetAsync(counts, 0, sizeof(int) * kMaxChunks, stream));
+    // the previous call on this thread has returned, so nothing reads the flags any more
+    memset(r->flags, 0, sizeof(int) * kMaxChunks);
+    a.chunk_counts = counts;
+    a.chunk_flags = r->dflags;
+    a.chunk_blocks = plan.chunk_blocks;
+    SSDF_CUDA(cudaEventCreateWithFlags(&cl.done, cudaEventDisableTiming));
+    SSDF_CHECK(launch_query_keep(a, precision, stream, &cl.fb));
+    SSDF_CUDA(cudaEventRecord(cl.done, stream));
+
+    // copy each chunk once its flag is up, or once the launch has ended (a counting or budgeted launch
+    // raises no flags)
+    const volatile int *flags = r->flags;
+    std::vector<char> sent(size_t(plan.nchunks), 0);
+    int issued = 0, st = SSDF_OK;
+    while (issued < plan.nchunks && st == SSDF_OK) {
+        const cudaError_t q = cudaEventQuery(cl.done);
+        if (q != cudaSuccess && q != cudaErrorNotReady) {
+            st = cuda_fail(q, "streamed grid query", __FILE__, __LINE__);
+            break;
+        }
+        const bool ended = q == cudaSuccess;
+        bool progress = false;
+        for (int c = 0; c < plan.nchunks && st == SSDF_OK; c++) {
+            if (sent[c] || !(ended || flags[c])) continue;
+            const long long lo = plan.lo(c), hi = plan.hi(c);
+            cudaError_t e = cudaMemcpyAsync((char *)host_out + lo * esz, (const char *)a.out + lo * esz,
+                                            size_t(hi - lo) * esz, cudaMemcpyDeviceToHost, r->copy);
+            if (e == cudaSuccess && host_tri)
+                e = cudaMemcpyAsync(host_tri + lo, a.outtri + lo, sizeof(int) * size_t(hi - lo),
+                                    cudaMemcpyDeviceToHost, r->copy);
+            if (e != cudaSuccess) st = cuda_fail(e, "chunk copy", __FILE__, __LINE__);
+            sent[c] = 1;
+            issued++;
+            progress = true;
+        }
+        if (!progress) std::this_thread::yield();
+    }
+    if (st == SSDF_OK) cudaGetLastError();  // a not-ready poll is no error
+    // the second stage's queries: their final values, gathered once the launch is done
+    int nfb = 0;
+    void *vals = nullptr;
+    int *tris = nullptr;
+    std::vector<char> hvals;
+    std::vector<int> hids, htris;
+    if (st == SSDF_OK && cl.fb) {
+        cudaError_t e = cudaMemcpyAsync(&nfb, cl.fb, sizeof(int), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) st = cuda_fail(e, "second-stage count", __FILE__, __LINE__);
+        if (st == SSDF_OK && nfb > 0) {
+            e = cudaMallocAsync(&vals, esz * size_t(nfb), stream);
+            if (e == cudaSuccess && host_tri) e = cudaMallocAsync((void **)&tris, sizeof(int) * size_t(nfb), stream);
+            if (e == cudaSuccess) {
+                k_gather_fallback<<<unsigned((nfb + 255) / 256), 256, 0, stream>>>(nfb, cl.fb + 1, a.out, a.out_f64,
+                                                                                   host_tri ? a.outtri : nullptr,
+                                                                                   vals, tris);
+                e = cudaGetLastError();
+            }
+            hvals.resize(esz * size_t(nfb));
+            hids.resize(size_t(nfb));
+            if (host_tri) htris.resize(size_t(nfb));
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(hids.data(), cl.fb + 1, sizeof(int) * size_t(nfb), cudaMemcpyDeviceToHost, stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(hvals.data(), vals, esz * size_t(nfb), cudaMemcpyDeviceToHost, stream);
+            if (e == cudaSuccess && host_tri)
+                e = cudaMemcpyAsync(htris.data(), tris, sizeof(int) * size_t(nfb), cudaMemcpyDeviceToHost, stream);
+            if (vals) cudaFreeAsync(vals, stream);
+            if (tris) cudaFreeAsync(tris, stream);
+            if (e != cudaSuccess) st = cuda_fail(e, "second-stage gather", __FILE__, __LINE__);
+        }
+    }
+    // every chunk copy has landed before the second stage's values overwrite theirs
+    const cudaError_t ec = cudaStreamSynchronize(r->copy);
+    const cudaError_t es = cudaStreamSynchronize(stream);
+    if (st == SSDF_OK && ec != cudaSuccess) st = cuda_fail(ec, "chunk copies", __FILE__, __LINE__);
+    if (st == SSDF_OK && es != cudaSuccess) st = cuda_fail(es, "streamed grid query", __FILE__, __LINE__);
+    if (st == SSDF_OK) {
+        for (int i = 0; i < nfb; i++) {
+            const size_t q = size_t(hids[size_t(i)]);
+            memcpy((char *)host_out + q * esz, hvals.data() + size_t(i) * esz, esz);
+            if (host_tri) host_tri[q] = htris[size_t(i)];
+        }
+    }
+    return st;
+}
+
+}  // namespace ssdf_b200

@@ -124,6 +124,12 @@ struct QueryArgs {
     int force_arity;
     // point lists: the visiting order (query index per slot, Morton-sorted), or null (input order)
     const int *order;
+    // streamed download of a grid (launch_query_streamed): the blocks of chunk c (blockIdx.x /
+    // chunk_blocks, whole slabs of the grid) count themselves in chunk_counts[c] (device memory), and
+    // the last one raises chunk_flags[c] (page-locked host memory); null: off
+    int *chunk_counts;
+    int *chunk_flags;
+    int chunk_blocks;
 };
 
 // Job table header of a batch (device memory).
@@ -164,6 +170,17 @@ int exclusive_scan_i32(const int *in, int *out, int n, cudaStream_t stream);
 
 // ---- queries (bvh_query.cu) ----------------------------------------------------------------------
 int launch_query(const QueryArgs &args, int precision, cudaStream_t stream);
+// launch_query that, on success with the fix-up arithmetic, hands back the second stage's query list
+// (device ints: count, then the query indices) instead of freeing it; *fallback_list stays null for
+// the other arithmetics. The caller frees it with cudaFreeAsync on `stream`.
+int launch_query_keep(const QueryArgs &args, int precision, cudaStream_t stream, int **fallback_list);
+// A grid query whose results go to page-locked host arrays: args.out / args.outtri are device
+// buffers of the grid's size, and each slab chunk is copied to host_out / host_tri as soon as the
+// kernel has finished it, so the download overlaps the query. Returns when the host arrays hold the
+// results (the same bits as launch_query followed by a copy).
+int launch_query_streamed(const QueryArgs &args, int precision, void *host_out, int *host_tri, cudaStream_t stream);
+// Whether the streamed grid download applies: n queries, outputs in page-locked host memory.
+bool streamed_download_applies(long long n, const void *host_out, const int *host_tri);
 int launch_query_noalloc(const QueryArgs &args, cudaStream_t stream);
 long long noalloc_max_queries();
 int launch_batch(const BatchLaunch &b, int precision, cudaStream_t stream);
