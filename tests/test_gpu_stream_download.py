@@ -119,3 +119,53 @@ def test_streamed_switch_off(mesh, grid, monkeypatch):
     grid_call("ssdf_b200_sample_sdf_bvh_dd", mesh, grid, got, np.float64)
     assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
     assert os.environ["SSDF_B200_STREAM_DOWNLOAD"] == "0"
+
+
+@pytest.mark.parametrize("shape", [(2048, 2049, 1), (33, 31, 4104)])
+def test_streamed_flat_and_tall_grids(mesh, shape):
+    """One slab (a single chunk) and thousands of slabs (many slabs per chunk)."""
+    import torch
+
+    lo, hi = mesh.bbox()
+    grid = W.Grid(shape, tuple(lo - 0.1), tuple(hi + 0.1))
+    assert grid.size >= 1 << 22
+    want = np.zeros(grid.size)
+    grid_call("ssdf_b200_sample_sdf_bvh_dd", mesh, grid, want, np.float64)
+    got = pinned(grid.size, torch.float64)
+    got[:] = np.nan
+    grid_call("ssdf_b200_sample_sdf_bvh_dd", mesh, grid, got, np.float64)
+    assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
+
+
+def test_streamed_calls_from_two_threads(mesh, grid):
+    """Each calling thread polls its own chunk flags: two threads streaming at once both get their
+    own grid's bits."""
+    import threading
+
+    import torch
+
+    lo, hi = mesh.bbox()
+    grids = [grid, W.Grid((161, 170, 158), tuple(lo - 0.3), tuple(hi + 0.3))]
+    wants = []
+    for g in grids:
+        w = np.zeros(g.size)
+        grid_call("ssdf_b200_sample_sdf_bvh_dd", mesh, g, w, np.float64)
+        wants.append(w)
+    outs = [pinned(g.size, torch.float64) for g in grids]
+    errors = []
+
+    def work(i):
+        try:
+            for _ in range(3):
+                outs[i][:] = np.nan
+                grid_call("ssdf_b200_sample_sdf_bvh_dd", mesh, grids[i], outs[i], np.float64)
+                assert np.array_equal(outs[i].view(np.uint64), wants[i].view(np.uint64))
+        except Exception as ex:  # reported on the main thread
+            errors.append(repr(ex))
+
+    threads = [threading.Thread(target=work, args=(i,)) for i in range(2)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
