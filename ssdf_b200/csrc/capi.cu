@@ -145,18 +145,12 @@ float tau_rel_from_env() {
     return t > 0.f ? t : 1.0f / 65536.0f;
 }
 
-// Queries below which a one-call mesh skips the SAH treelet refinement: the refinement is latency
-// bound (about 1.1-1.7 ms whatever the mesh size) and saves 0-15 % of the query, so a call this small
-// loses by it (measured on B200: a 5,120-triangle sphere's 64^3 grid call 3.3 -> 2.1 ms; 20,480
-// triangles, 96^3: 4.5 -> 3.1 ms; the beam lattice's 8e6 points gain 5.4 ms by it).
-constexpr long long kTreeletMinQueries = 1ll << 21;
-
 ssdf_build_opts build_opts_for(int precision, int output, long long nqueries) {
     ssdf_build_opts o;
     o.leaf_size = env_int("SSDF_B200_LEAF", 0);
     o.keep_fp64 = (precision != SSDF_PREC_F32 || output == SSDF_OUT_SDF || output == SSDF_OUT_CLOSEST) ? 1 : 0;
     o.normals = output == SSDF_OUT_SDF ? 1 : 0;
-    o.treelet_opt = env_int("SSDF_B200_TREELET", nqueries >= kTreeletMinQueries ? 1 : 0);
+    o.treelet_opt = call_treelet_rounds(nqueries);
     return o;
 }
 

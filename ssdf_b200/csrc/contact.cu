@@ -426,7 +426,7 @@ int within_radius_host(ptrdiff_t npoints, const G *x, const G *y, const G *z, pt
     if (have_mesh) {
         ssdf_build_opts bo;
         bo.leaf_size = env_int("SSDF_B200_LEAF", 0), bo.keep_fp64 = 0, bo.normals = 0;
-        bo.treelet_opt = env_int("SSDF_B200_TREELET", 1);
+        bo.treelet_opt = call_treelet_rounds(npoints);
         if (QUAD) {  // halves (0, 1, 2) and (0, 2, 3): record 2e + h belongs to quad e
             std::vector<int> h0(size_t(2 * ne)), h1(size_t(2 * ne)), h2(size_t(2 * ne));
             for (ptrdiff_t e = 0; e < ne; e++) {
@@ -705,7 +705,7 @@ int potential_contact_host(ptrdiff_t ne, const int *s0, const int *s1, const int
     SSDF_CUDA(cudaGetLastError());
     ssdf_build_opts bo;
     bo.leaf_size = env_int("SSDF_B200_LEAF", 0), bo.keep_fp64 = 0, bo.normals = 0;
-    bo.treelet_opt = env_int("SSDF_B200_TREELET", 1);
+    bo.treelet_opt = call_treelet_rounds(ne);
     SSDF_CHECK(ssdf_mesh_create(&mh.mesh, ne, (const int *)t0, (const int *)t1, (const int *)t1, 2 * ne, bx, by, bz,
                                 SSDF_F32, 1, &bo, stream));
     a.prims = (const float4 *)prims;

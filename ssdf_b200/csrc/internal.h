@@ -258,6 +258,15 @@ int morton_point_order(long long n, const void *x, const void *y, const void *z,
                        int **order, cudaStream_t stream);
 int env_int(const char *name, int dflt);
 const char *env_str(const char *name);
+// Treelet refinement rounds for a mesh that one host-array call builds and queries once: none below
+// 2^21 queries (SSDF_B200_TREELET overrides). The refinement is latency bound (about 1.1-1.7 ms
+// whatever the mesh size) and saves 0-15 % of a query, so a smaller call loses by it. Measured on
+// B200: a 5,120-triangle sphere's 64^3 grid call 3.3 -> 2.1 ms without it, 131,072-triangle
+// potential_contact 4.0 -> 2.3 ms, 2e6-point closest_within_radius 12.7 -> 11.1 ms; the beam
+// lattice's 8e6 points gain 5.4 ms by it.
+inline int call_treelet_rounds(long long nqueries) {
+    return env_int("SSDF_B200_TREELET", nqueries >= (1ll << 21) ? 1 : 0);
+}
 cudaStream_t library_stream();  // per-thread non-blocking stream for the blocking entry points
 void retain_pool_memory();      // keep freed scratch in the device's default pool (once per device)
 
