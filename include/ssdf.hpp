@@ -102,11 +102,15 @@ int closest_point_bvh(const ptrdiff_t npoints, const G *const SSDF_RESTRICT x, c
     if constexpr (std::is_same<G, float>::value && std::is_same<T, float>::value)
         return ssdf_b200_closest_point_bvh_ff(npoints, x, y, z, nselements, s0, s1, s2, nspoints, sx, sy, sz, outd,
                                               outx, outy, outz, outtri);
+    else if constexpr (std::is_same<G, float>::value && std::is_same<T, double>::value)
+        return ssdf_b200_closest_point_bvh_fd(npoints, x, y, z, nselements, s0, s1, s2, nspoints, sx, sy, sz, outd,
+                                              outx, outy, outz, outtri);
     else if constexpr (std::is_same<G, double>::value && std::is_same<T, double>::value)
         return ssdf_b200_closest_point_bvh_dd(npoints, x, y, z, nselements, s0, s1, s2, nspoints, sx, sy, sz, outd,
                                               outx, outy, outz, outtri);
     else
-        static_assert(detail::always_false<G, T>::value, "closest_point_bvh: <float,float>, <double,double>");
+        static_assert(detail::always_false<G, T>::value,
+                      "closest_point_bvh: <float,float>, <float,double>, <double,double>");
 }
 
 #define SSDF_B200_GRID_SIG(G, T)                                                                                  \

@@ -101,6 +101,12 @@ int ssdf_b200_closest_point_bvh_ff(ptrdiff_t npoints, const float *x, const floa
                                    ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
                                    ptrdiff_t nspoints, const float *sx, const float *sy, const float *sz, float *outd,
                                    float *outx, float *outy, float *outz, int *outtri);
+/* closest_point_bvh<float, double, int> (serial/bvh/bvh.cpp:1162-1179): float points and mesh, double
+ * distance (the FP64 distance of the float-valued inputs), closest point rounded to float. */
+int ssdf_b200_closest_point_bvh_fd(ptrdiff_t npoints, const float *x, const float *y, const float *z,
+                                   ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                   ptrdiff_t nspoints, const float *sx, const float *sy, const float *sz, double *outd,
+                                   float *outx, float *outy, float *outz, int *outtri);
 int ssdf_b200_closest_point_bvh_dd(ptrdiff_t npoints, const double *x, const double *y, const double *z,
                                    ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
                                    ptrdiff_t nspoints, const double *sx, const double *sy, const double *sz,
@@ -405,6 +411,13 @@ int ssdf_mesh_destroy(ssdf_mesh *mesh);
 int ssdf_mesh_destroy_async(ssdf_mesh *mesh, void *stream);
 /* BVH statistics: nodes, leaves, depth, bytes resident on the device. */
 int ssdf_mesh_stats(const ssdf_mesh *mesh, int64_t *nodes, int64_t *leaves, int64_t *depth, int64_t *bytes);
+/* The fix-up path's view of a mesh (no counterpart in the reference): tau_rel, the relative width of
+ * its FP32 window (tau = tau_rel (M + d), M the largest coordinate magnitude, d the distance; at least
+ * 2^-16, wider for meshes of a few large triangles); float_filter, 1 when fix-up requests on it run the
+ * FP32 filter, 0 when they run the FP64 kernel (coordinates beyond 2^28, triangles that rounding to
+ * float collapses or makes smaller than 2^-23, or more than half of its triangles slivers); slivers,
+ * the triangles the filter sees through a proxy. Any pointer may be null. */
+int ssdf_mesh_filter_info(const ssdf_mesh *mesh, float *tau_rel, int *float_filter, int64_t *slivers);
 
 /* Query at device points (x, y, z of coord_type). outx/outy/outz (coord_type) and outtri may be NULL
  * except for SSDF_OUT_CLOSEST. Asynchronous on `stream`. */

@@ -24,7 +24,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libssdf_ref.so")
-REF_SRC = "/root/reference"
+# where the reference's sources are (read only; SSDF_REFERENCE_SRC overrides the default)
+REF_SRC = os.environ.get("SSDF_REFERENCE_SRC", "/root/reference")
 
 _pd = C.c_ssize_t
 _dp = C.POINTER(C.c_double)

@@ -77,7 +77,7 @@ for _n in ("ssdf_edf_f", "ssdf_edf_d", "ssdf_b200_edf_ff", "ssdf_b200_edf_dd", "
     _sig(_n, _EDF)
 for _n in ("ssdf_b200_edf_index_dd", "ssdf_b200_edf_index_ff", "ssdf_b200_sdf_points_dd"):
     _sig(_n, _EDF + [_ip])
-for _n in ("ssdf_b200_closest_point_bvh_ff", "ssdf_b200_closest_point_bvh_dd"):
+for _n in ("ssdf_b200_closest_point_bvh_ff", "ssdf_b200_closest_point_bvh_fd", "ssdf_b200_closest_point_bvh_dd"):
     _sig(_n, _EDF + [_vp, _vp, _vp, _ip])
 _sig("ssdf_b200_sample_sqedf_bvh_ff", _GRID + [C.c_float] * 6 + [_vp])
 _sig("ssdf_b200_sample_sdf_bvh_ff", _GRID + [C.c_float] * 6 + [_vp])
@@ -89,6 +89,7 @@ _sig("ssdf_mesh_create", [C.POINTER(_vp), _pd, _ip, _ip, _ip, _pd, _vp, _vp, _vp
 _sig("ssdf_mesh_destroy", [_vp])
 _sig("ssdf_mesh_destroy_async", [_vp, _vp])
 _sig("ssdf_mesh_stats", [_vp] + [C.POINTER(C.c_int64)] * 4)
+_sig("ssdf_mesh_filter_info", [_vp, C.POINTER(C.c_float), C.POINTER(C.c_int), C.POINTER(C.c_int64)])
 _sig("ssdf_query_points", [_vp, _pd, _vp, _vp, _vp, _vp, _ip, _vp, _vp, _vp, C.POINTER(QueryOpts), _vp])
 _sig("ssdf_query_grid", [_vp, _pd, _pd, _pd, C.POINTER(C.c_double * 3), C.POINTER(C.c_double * 3), _vp, _ip,
                          C.POINTER(QueryOpts), _vp])
@@ -170,10 +171,10 @@ _sig("ssdf_server_reset_stats", [_vp])
 EXPORTED = ["ssdf_status_string", "ssdf_last_error", "ssdf_b200_version", "ssdf_edf_f", "ssdf_edf_d",
             "ssdf_b200_edf_ff", "ssdf_b200_edf_dd", "ssdf_b200_edf_celllist_ff", "ssdf_b200_edf_celllist_dd",
             "ssdf_b200_edf_bvh_ff", "ssdf_b200_edf_bvh_fd", "ssdf_b200_edf_bvh_dd", "ssdf_b200_closest_point_bvh_ff",
-            "ssdf_b200_closest_point_bvh_dd", "ssdf_b200_sample_sqedf_bvh_ff", "ssdf_b200_sample_sqedf_bvh_dd",
+            "ssdf_b200_closest_point_bvh_fd", "ssdf_b200_closest_point_bvh_dd", "ssdf_b200_sample_sqedf_bvh_ff", "ssdf_b200_sample_sqedf_bvh_dd",
             "ssdf_b200_sample_sdf_bvh_ff", "ssdf_b200_sample_sdf_bvh_dd", "ssdf_b200_edf_index_dd",
             "ssdf_b200_edf_index_ff", "ssdf_b200_sdf_points_dd", "ssdf_b200_sample_sdf_index_bvh_dd",
-            "ssdf_mesh_create", "ssdf_mesh_destroy", "ssdf_mesh_stats", "ssdf_query_points", "ssdf_query_grid",
+            "ssdf_mesh_create", "ssdf_mesh_destroy", "ssdf_mesh_stats", "ssdf_mesh_filter_info", "ssdf_query_points", "ssdf_query_grid",
             "ssdf_last_query_counts", "ssdf_b200_fma_peak", "ssdf_batch_create", "ssdf_batch_destroy", "ssdf_batch_clear",
             "ssdf_batch_size", "ssdf_batch_add_grid", "ssdf_batch_add_points", "ssdf_batch_run",
             "ssdf_batch_last_blocks", "ssdf_query_grid_noalloc", "ssdf_query_grid_noalloc_max", "ssdf_server_create",
@@ -297,16 +298,17 @@ def sdf_points(points, mesh):
     return o, tri
 
 
-def closest_point_bvh(points, mesh, outd=None, dtype=np.float64):
-    """ssdf::closest_point_bvh: (outd, outx, outy, outz, outtri), updated where closer than outd."""
+def closest_point_bvh(points, mesh, outd=None, dtype=np.float64, tdtype=None):
+    """ssdf::closest_point_bvh<G, T>: (outd, outx, outy, outz, outtri), updated where closer than outd.
+    dtype is G (points, mesh, closest point), tdtype T (distance; G by default)."""
+    tdtype = dtype if tdtype is None else tdtype
     x, y, z = _points(points, dtype)
     n = len(x)
-    d = _init_out(n, dtype, outd)
+    d = _init_out(n, tdtype, outd)
     ox, oy, oz = np.zeros(n, dtype), np.zeros(n, dtype), np.zeros(n, dtype)
     tri = np.full(n, -1, dtype=np.int32)
-    s = _suffix(dtype)
     hm = _HostMesh(mesh, dtype)
-    fn = f"ssdf_b200_closest_point_bvh_{s}{s}"
+    fn = f"ssdf_b200_closest_point_bvh_{_suffix(dtype)}{_suffix(tdtype)}"
     _check(getattr(lib, fn)(n, _p(x), _p(y), _p(z), *hm.args(), _p(d), _p(ox), _p(oy), _p(oz), _ipp(tri)), fn)
     return d, ox, oy, oz, tri
 
@@ -607,6 +609,13 @@ class DeviceMesh:
         v = [C.c_int64() for _ in range(4)]
         _check(lib.ssdf_mesh_stats(self._h, *[C.byref(a) for a in v]), "ssdf_mesh_stats")
         return dict(nodes=v[0].value, leaves=v[1].value, depth=v[2].value, bytes=v[3].value)
+
+    def filter_info(self):
+        """The fix-up path's view of the mesh: window width tau_rel, whether fix-up requests run the FP32
+        filter (else the FP64 kernel), and how many triangles the filter sees through a proxy."""
+        t, ok, n = C.c_float(), C.c_int(), C.c_int64()
+        _check(lib.ssdf_mesh_filter_info(self._h, C.byref(t), C.byref(ok), C.byref(n)), "ssdf_mesh_filter_info")
+        return dict(tau_rel=t.value, float_filter=bool(ok.value), slivers=n.value)
 
     def query_points(self, x, y, z, out, outtri=None, outx=None, outy=None, outz=None, precision=PREC_F32_FIXUP,
                      output=OUT_EDF, coord_type=F64, out_type=F64, stream=None):

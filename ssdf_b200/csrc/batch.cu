@@ -7,6 +7,11 @@
 // and the fix-up window stage finishes every job's overflowed queries. The table lives in device
 // memory and the kernels read it there, so the captured graph (two memsets + two kernels) replays
 // for any batch composition; only the table is rewritten (from pinned memory) before each replay.
+//
+// A fix-up batch keeps a second table for the jobs whose meshes the FP64 kernel answers faster or
+// alone (made mostly of slivers, or outside the float filter's preconditions: fixup_runs_f64): the
+// persistent FP64 kernel runs those after the fix-up kernels, in the same graph, so every job of the
+// batch gets the arithmetic it would get alone.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -24,20 +29,20 @@ struct ssdf_batch {
     int traversal = 0;  // 0 auto, 1 warp, 2 thread
     int arity = 0;      // 0 auto, 2, 4
     std::vector<QueryArgs> jobs;
-    // device table
-    BatchHeader *d_hdr = nullptr;
-    QueryArgs *d_jobs = nullptr;
-    long long *d_first = nullptr;
-    unsigned long long *d_next = nullptr;
+    // device tables: [0] the batch's own arithmetic, [1] the FP64 jobs of a fix-up batch
+    BatchHeader *d_hdr = nullptr;  // [2]
+    QueryArgs *d_jobs = nullptr, *d_jobs64 = nullptr;
+    long long *d_first = nullptr, *d_first64 = nullptr;
+    unsigned long long *d_next = nullptr;  // [2]
     int *d_fbcount = nullptr;
     int *d_fb = nullptr;
     size_t fb_cap = 0;  // ints
     // pinned staging
-    BatchHeader *h_hdr = nullptr;
-    QueryArgs *h_jobs = nullptr;
-    long long *h_first = nullptr;
-    // captured graphs, one per (warp, wide, budget) key: a run reuses the graph of its key
-    cudaGraphExec_t exec[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    BatchHeader *h_hdr = nullptr;  // [2]
+    QueryArgs *h_jobs = nullptr, *h_jobs64 = nullptr;
+    long long *h_first = nullptr, *h_first64 = nullptr;
+    // captured graphs, one per (warp, wide, budget, FP64 table) key: a run reuses the graph of its key
+    cudaGraphExec_t exec[16] = {};
     int sms = 0;
     long long last_total = 0;
 };
@@ -47,18 +52,23 @@ static void batch_free(ssdf_batch *b) {
         if (g) cudaGraphExecDestroy(g);
     cudaFree(b->d_hdr);
     cudaFree(b->d_jobs);
+    cudaFree(b->d_jobs64);
     cudaFree(b->d_first);
+    cudaFree(b->d_first64);
     cudaFree(b->d_next);
     cudaFree(b->d_fbcount);
     cudaFree(b->d_fb);
     cudaFreeHost(b->h_hdr);
     cudaFreeHost(b->h_jobs);
+    cudaFreeHost(b->h_jobs64);
     cudaFreeHost(b->h_first);
+    cudaFreeHost(b->h_first64);
 }
 
 // The launch sequence of one run with the given traversal and arity: counters reset, then the
-// persistent kernel and the window stage. It reads the job table from device memory only.
-static int enqueue_run(ssdf_batch *b, bool warp, bool wide, bool budget, cudaStream_t s) {
+// persistent kernel and the window stage, then (f64) the persistent FP64 kernel over the second
+// table. It reads the job tables from device memory only.
+static int enqueue_run(ssdf_batch *b, bool warp, bool wide, bool budget, bool f64, cudaStream_t s) {
     BatchLaunch L;
     L.budget = budget;
     L.hdr = b->d_hdr;
@@ -69,10 +79,19 @@ static int enqueue_run(ssdf_batch *b, bool warp, bool wide, bool budget, cudaStr
     L.warp = warp;
     L.wide = wide;
     L.grid = b->sms * batch_blocks_per_sm(b->precision, warp, wide);
-    cudaError_t e = cudaMemsetAsync(b->d_next, 0, sizeof(unsigned long long), s);
+    cudaError_t e = cudaMemsetAsync(b->d_next, 0, 2 * sizeof(unsigned long long), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d_fbcount, 0, sizeof(int) * b->max_jobs, s);
     if (e != cudaSuccess) return cuda_fail(e, "batch reset", __FILE__, __LINE__);
-    return launch_batch(L, b->precision, s);
+    SSDF_CHECK(launch_batch(L, b->precision, s));
+    if (!f64) return SSDF_OK;
+    BatchLaunch D = L;
+    D.budget = false;
+    D.hdr = b->d_hdr + 1;
+    D.jobs = b->d_jobs64;
+    D.first_block = b->d_first64;
+    D.next_item = b->d_next + 1;
+    D.grid = b->sms * batch_blocks_per_sm(SSDF_PREC_F64, warp, wide);
+    return launch_batch(D, SSDF_PREC_F64, s);
 }
 
 // The packet budget only exists for the fix-up kernel's binary packet walk.
@@ -80,11 +99,14 @@ static bool budget_applies(const ssdf_batch *b, bool warp, bool wide) {
     return b->precision == SSDF_PREC_F32_FIXUP && warp && !wide;
 }
 
-static int graph_key(bool warp, bool wide, bool budget) { return (warp ? 1 : 0) | (wide ? 2 : 0) | (budget ? 4 : 0); }
+static int graph_key(bool warp, bool wide, bool budget, bool f64) {
+    return (warp ? 1 : 0) | (wide ? 2 : 0) | (budget ? 4 : 0) | (f64 ? 8 : 0);
+}
 
-// Captures (once) the graph of a (traversal, arity, budget) key on a private stream, thread-local mode.
-static int capture_key(ssdf_batch *b, bool warp, bool wide, bool budget) {
-    const int key = graph_key(warp, wide, budget);
+// Captures (once) the graph of a (traversal, arity, budget, FP64 table) key on a private stream,
+// thread-local mode.
+static int capture_key(ssdf_batch *b, bool warp, bool wide, bool budget, bool f64) {
+    const int key = graph_key(warp, wide, budget, f64);
     if (b->exec[key]) return SSDF_OK;
     cudaStream_t cap;
     SSDF_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
@@ -92,7 +114,7 @@ static int capture_key(ssdf_batch *b, bool warp, bool wide, bool budget) {
     cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
     int st = SSDF_OK;
     if (e == cudaSuccess) {
-        st = enqueue_run(b, warp, wide, budget, cap);
+        st = enqueue_run(b, warp, wide, budget, f64, cap);
         e = cudaStreamEndCapture(cap, &g);
     }
     if (e == cudaSuccess && st == SSDF_OK) e = cudaGraphInstantiate(&b->exec[key], g, 0);
@@ -112,8 +134,11 @@ int batch_capture_graphs(ssdf_batch *b) {
         for (int wide = 0; wide < 2; wide++) {
             if ((b->traversal == 1 && !warp) || (b->traversal == 2 && warp)) continue;
             if ((b->arity == 2 && wide) || (b->arity == 4 && !wide)) continue;
-            SSDF_CHECK(capture_key(b, warp != 0, wide != 0, false));
-            if (budget_applies(b, warp != 0, wide != 0)) SSDF_CHECK(capture_key(b, warp != 0, wide != 0, true));
+            for (int f64 = 0; f64 < (b->precision == SSDF_PREC_F32_FIXUP ? 2 : 1); f64++) {
+                SSDF_CHECK(capture_key(b, warp != 0, wide != 0, false, f64 != 0));
+                if (budget_applies(b, warp != 0, wide != 0))
+                    SSDF_CHECK(capture_key(b, warp != 0, wide != 0, true, f64 != 0));
+            }
         }
     return SSDF_OK;
 }
@@ -134,14 +159,19 @@ int ssdf_batch_create(ssdf_batch **out, int max_jobs, int precision, int travers
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_hdr, sizeof(BatchHeader));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_hdr, 2 * sizeof(BatchHeader));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_jobs, sizeof(QueryArgs) * max_jobs);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_jobs64, sizeof(QueryArgs) * max_jobs);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_first, sizeof(long long) * max_jobs);
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_next, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_first64, sizeof(long long) * max_jobs);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_next, 2 * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_fbcount, sizeof(int) * max_jobs);
-    if (e == cudaSuccess) e = cudaMallocHost(&b->h_hdr, sizeof(BatchHeader));
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_hdr, 2 * sizeof(BatchHeader));
     if (e == cudaSuccess) e = cudaMallocHost(&b->h_jobs, sizeof(QueryArgs) * max_jobs);
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_jobs64, sizeof(QueryArgs) * max_jobs);
     if (e == cudaSuccess) e = cudaMallocHost(&b->h_first, sizeof(long long) * max_jobs);
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_first64, sizeof(long long) * max_jobs);
+    if (e == cudaSuccess) memset(b->h_hdr, 0, 2 * sizeof(BatchHeader));
     if (e != cudaSuccess) {
         batch_free(b);
         delete b;
@@ -233,15 +263,19 @@ int ssdf_batch_run(ssdf_batch *b, int use_graph, void *stream_) {
     }
     const bool warp = b->traversal == 1 ? true : b->traversal == 2 ? false : default_warp(any_grid || any_sorted);
     const bool wide = b->arity == 4 ? true : b->arity == 2 ? false : default_wide();
-    // largest jobs first: the tail of the launch is then made of small items
+    // the FP64 table of a fix-up batch: jobs whose meshes the FP64 kernel answers (fixup_runs_f64)
+    const bool fixup = b->precision == SSDF_PREC_F32_FIXUP;
+    auto to_f64 = [&](const QueryArgs &a) { return fixup && fixup_runs_f64(a.m); };
+    // largest jobs first: the tail of each launch is then made of small items
     std::vector<int> order(njobs);
     for (int i = 0; i < njobs; i++) order[i] = i;
     auto cost = [&](const QueryArgs &a) { return double(query_blocks(a)) * std::log2(2.0 + a.m.nt); };
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost(b->jobs[x]) > cost(b->jobs[y]); });
-    // fix-up overflow lists: one slice of (ids, thresholds) per job
+    // fix-up overflow lists: one slice of (ids, thresholds) per job of the first table
     size_t need = 0;
-    if (b->precision == SSDF_PREC_F32_FIXUP)
-        for (const auto &j : b->jobs) need += 2 * size_t(j.is_grid ? j.nx * j.ny * j.nz : j.npoints);
+    if (fixup)
+        for (const auto &j : b->jobs)
+            if (!to_f64(j)) need += 2 * size_t(j.is_grid ? j.nx * j.ny * j.nz : j.npoints);
     if (need > b->fb_cap) SSDF_CHECK(ssdf_batch_reserve(b, (long long)(need / 2), stream));
     // the staging buffers may still feed the previous run's copies
     SSDF_CUDA(cudaStreamSynchronize(stream));
@@ -252,11 +286,12 @@ int ssdf_batch_run(ssdf_batch *b, int use_graph, void *stream_) {
             for (int *q : p) cudaFreeAsync(q, s);
         }
     } orders{{}, stream};
-    long long total = 0, nq = 0;
+    long long total = 0, total64 = 0, nq = 0;
     for (const auto &j : b->jobs) nq += j.is_grid ? j.nx * j.ny * j.nz : j.npoints;
     size_t off = 0;
-    for (int k = 0; k < njobs; k++) {
-        QueryArgs a = b->jobs[order[k]];
+    int k = 0, k64 = 0;
+    for (int r = 0; r < njobs; r++) {
+        QueryArgs a = b->jobs[order[r]];
         a.warp_budget = resolve_warp_budget(a.warp_budget, nq);
         if (sort_points && !a.is_grid && a.npoints >= kSortMinPoints) {
             int *ord = nullptr;
@@ -264,7 +299,18 @@ int ssdf_batch_run(ssdf_batch *b, int use_graph, void *stream_) {
             orders.p.push_back(ord);
             a.order = ord;
         }
-        if (b->precision == SSDF_PREC_F32_FIXUP) {
+        a.counters = nullptr;
+        if (to_f64(a)) {
+            a.fallback_count = nullptr;
+            a.fallback_ids = nullptr;
+            a.fallback_thr = nullptr;
+            a.warp_budget = 0;
+            b->h_jobs64[k64] = a;
+            b->h_first64[k64++] = total64;
+            total64 += query_blocks(a);
+            continue;
+        }
+        if (fixup) {
             const size_t n = size_t(a.is_grid ? a.nx * a.ny * a.nz : a.npoints);
             a.fallback_count = b->d_fbcount + k;
             a.fallback_ids = b->d_fb + off;
@@ -275,24 +321,30 @@ int ssdf_batch_run(ssdf_batch *b, int use_graph, void *stream_) {
             a.fallback_ids = nullptr;
             a.fallback_thr = nullptr;
         }
-        a.counters = nullptr;
         b->h_jobs[k] = a;
-        b->h_first[k] = total;
+        b->h_first[k++] = total;
         total += query_blocks(a);
     }
-    b->h_hdr->njobs = njobs;
-    b->h_hdr->pad = 0;
-    b->h_hdr->total_blocks = total;
-    b->last_total = total;
-    SSDF_CUDA(cudaMemcpyAsync(b->d_hdr, b->h_hdr, sizeof(BatchHeader), cudaMemcpyHostToDevice, stream));
-    SSDF_CUDA(cudaMemcpyAsync(b->d_jobs, b->h_jobs, sizeof(QueryArgs) * njobs, cudaMemcpyHostToDevice, stream));
-    SSDF_CUDA(cudaMemcpyAsync(b->d_first, b->h_first, sizeof(long long) * njobs, cudaMemcpyHostToDevice, stream));
+    b->h_hdr[0] = BatchHeader{k, 0, total};
+    b->h_hdr[1] = BatchHeader{k64, 0, total64};
+    b->last_total = total + total64;
+    SSDF_CUDA(cudaMemcpyAsync(b->d_hdr, b->h_hdr, 2 * sizeof(BatchHeader), cudaMemcpyHostToDevice, stream));
+    if (k > 0) {
+        SSDF_CUDA(cudaMemcpyAsync(b->d_jobs, b->h_jobs, sizeof(QueryArgs) * k, cudaMemcpyHostToDevice, stream));
+        SSDF_CUDA(cudaMemcpyAsync(b->d_first, b->h_first, sizeof(long long) * k, cudaMemcpyHostToDevice, stream));
+    }
+    if (k64 > 0) {
+        SSDF_CUDA(cudaMemcpyAsync(b->d_jobs64, b->h_jobs64, sizeof(QueryArgs) * k64, cudaMemcpyHostToDevice, stream));
+        SSDF_CUDA(
+            cudaMemcpyAsync(b->d_first64, b->h_first64, sizeof(long long) * k64, cudaMemcpyHostToDevice, stream));
+    }
     bool budget = false;
-    for (int k = 0; k < njobs; k++) budget |= b->h_jobs[k].warp_budget > 0;
+    for (int j = 0; j < k; j++) budget |= b->h_jobs[j].warp_budget > 0;
     budget = budget && budget_applies(b, warp, wide);
-    if (!use_graph || env_int("SSDF_B200_COUNT", 0) != 0) return enqueue_run(b, warp, wide, budget, stream);
-    SSDF_CHECK(capture_key(b, warp, wide, budget));
-    SSDF_CUDA(cudaGraphLaunch(b->exec[graph_key(warp, wide, budget)], stream));
+    const bool f64 = k64 > 0;
+    if (!use_graph) return enqueue_run(b, warp, wide, budget, f64, stream);
+    SSDF_CHECK(capture_key(b, warp, wide, budget, f64));
+    SSDF_CUDA(cudaGraphLaunch(b->exec[graph_key(warp, wide, budget, f64)], stream));
     return SSDF_OK;
 }
 

@@ -953,14 +953,22 @@ __device__ __forceinline__ void query_block(const QueryArgs &a, long long block,
         __shared__ float s_wd[kQ * kCand * kThreads];
         __shared__ int s_wp[kQ * kCand * kThreads];
         FastPolicy<Q> p(a.m, a.tau_rel, s_wd, s_wp);
+        bool exact[Q];  // a finite point beyond the float filter's range: the second stage, exactly
 #pragma unroll
         for (int s = 0; s < Q; s++) {
+            exact[s] = false;
             if (valid[s]) {
                 double x, y, z;
                 query_point(a, qid[s], gi[s], gj[s], gk[s], x, y, z);
+                const double ax = fabs(x), ay = fabs(y), az = fabs(z);
+                exact[s] = (ax > kFilterMaxCoord || ay > kFilterMaxCoord || az > kFilterMaxCoord) &&
+                           ax < dinf() && ay < dinf() && az < dinf();
                 const double init = initial_bound(a, qid[s]);
                 // float start bound rounded up, so no triangle closer in double is cut off
-                p.set(s, float(x), float(y), float(z), init < dinf() ? __double2float_ru(init) : finf());
+                if (exact[s])
+                    p.disable(s);
+                else
+                    p.set(s, float(x), float(y), float(z), init < dinf() ? __double2float_ru(init) : finf());
             } else {
                 p.disable(s);
             }
@@ -970,10 +978,10 @@ __device__ __forceinline__ void query_block(const QueryArgs &a, long long block,
         for (int s = 0; s < Q; s++) {
             if (!valid[s]) continue;
             const long long q = qid[s];
-            if (p.evicted[s] < p.thr[s]) {
+            if (exact[s] || p.evicted[s] < p.thr[s]) {
                 const int slot = atomicAdd(a.fallback_count, 1);
                 a.fallback_ids[slot] = int(q);  // q < 2^31 is checked on the host
-                a.fallback_thr[slot] = p.thr[s];
+                a.fallback_thr[slot] = exact[s] ? finf() : p.thr[s];
                 continue;
             }
             // the double point and bound are recomputed here rather than kept live through the walk
@@ -1038,6 +1046,10 @@ struct WindowBest {
     int id, pos;
 };
 
+// A window of +inf takes every node and triangle, whatever its float key (a query point beyond the
+// float filter's range, whose keys may have overflowed, is answered this way: exactly, in double).
+__device__ __forceinline__ bool in_window(float key, float thr) { return key < thr || thr == finf(); }
+
 __device__ __forceinline__ void window_leaf(const DeviceMesh &m, int ref, float px, float py, float pz, float thr,
                                             double qx, double qy, double qz, WindowBest &b, Counters &cnt,
                                             bool count) {
@@ -1045,7 +1057,7 @@ __device__ __forceinline__ void window_leaf(const DeviceMesh &m, int ref, float 
     for (int k = 0; k < n; k++) {
         const float f = tri_dist_sq_filter(px, py, pz, load_filt(m.filt32, first + k));  // the first stage's key
         if (count) cnt.tri++;
-        if (f < thr) {
+        if (in_window(f, thr)) {
             const Tri64 u = load_tri64(m.tris64, first + k);
             const double e2 =
                 tri_dist_sq_exact<double>(qx, qy, qz, u.ax, u.ay, u.az, u.bx, u.by, u.bz, u.cx, u.cy, u.cz);
@@ -1072,7 +1084,7 @@ __device__ __noinline__ void window_subtree(const DeviceMesh &m, int root, float
 #pragma unroll
         for (int h = 0; h < 2; h++) {
             const int c = h ? n.r1 : n.r0;
-            if (c == kEmptyRef || !((h ? d1 : d0) < thr)) continue;
+            if (c == kEmptyRef || !in_window(h ? d1 : d0, thr)) continue;
             if (c < 0)
                 window_leaf(m, c, px, py, pz, thr, qx, qy, qz, b, cnt, count);
             else if (sp < kStackSize)
@@ -1111,8 +1123,8 @@ __device__ void window_warp(const QueryArgs &a, int idx, int *__restrict__ stack
             const float d1 = box_dist_sq_fast(px, py, pz, n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w);
             if (COUNT) cnt.box += 2;
             c0 = n.r0, c1 = n.r1;
-            w0 = c0 != kEmptyRef && d0 < thr;
-            w1 = c1 != kEmptyRef && d1 < thr;
+            w0 = c0 != kEmptyRef && in_window(d0, thr);
+            w1 = c1 != kEmptyRef && in_window(d1, thr);
             if (w0 && c0 < 0) {
                 window_leaf(m, c0, px, py, pz, thr, qx, qy, qz, b, cnt, COUNT);
                 w0 = false;
@@ -1363,6 +1375,11 @@ bool sliver_heavy(const DeviceMesh &m) {
     return m.nt > 0 && double(m.nill) > f * double(m.nt);
 }
 
+// A fix-up request on this mesh runs the FP64 kernel (the same bits): a mesh made mostly of slivers,
+// or one outside the float filter's preconditions (coordinates beyond 2^28, a record that rounding to
+// float made degenerate or too small, or a window wider than 2^-8).
+bool fixup_runs_f64(const DeviceMesh &m) { return sliver_heavy(m) || !m.filter_ok; }
+
 
 int morton_point_order(long long n, const void *x, const void *y, const void *z, int f64, const float4 *nodes32,
                        int **order, cudaStream_t stream) {
@@ -1422,7 +1439,7 @@ int launch_query_keep(const QueryArgs &args_in, int precision, cudaStream_t stre
     // A mesh made mostly of ill-conditioned triangles (needles, slivers) is answered faster by the
     // plain FP64 kernel: the fix-up filter sees each such triangle through a wide proxy, whose keys
     // crowd the window. Both give the same bits.
-    if (precision == SSDF_PREC_F32_FIXUP && sliver_heavy(a.m)) precision = SSDF_PREC_F64;
+    if (precision == SSDF_PREC_F32_FIXUP && fixup_runs_f64(a.m)) precision = SSDF_PREC_F64;
     a.warp_budget = resolve_warp_budget(a.warp_budget, n);
     if (a.output == SSDF_OUT_CLOSEST && (!a.m.tris64 || !a.outx || !a.outy || !a.outz || !a.outtri))
         return fail(SSDF_ERR_INVALID_ARGUMENT, "closest-point queries need outx/outy/outz/outtri and double data");
@@ -1514,9 +1531,11 @@ int batch_blocks_per_sm(int precision, bool warp, bool wide) {
 }
 
 // Enqueues the persistent batch kernel (and the fix-up window stage) on `stream`; the job table and
-// counters in `b` must already be in device memory. Capturable in a CUDA graph.
+// counters in `b` must already be in device memory. Capturable in a CUDA graph. Batch jobs carry no
+// counter buffer (QueryArgs::counters is null), so batch launches never take the counting
+// instantiations, whatever SSDF_B200_COUNT says.
 int launch_batch(const BatchLaunch &b, int precision, cudaStream_t stream) {
-    const bool count = env_int("SSDF_B200_COUNT", 0) != 0;
+    const bool count = false;
     cudaError_t e;
     if (precision == SSDF_PREC_F64)
         e = launch_batch_prec<SSDF_PREC_F64>(b, count, stream);
@@ -1553,7 +1572,8 @@ static std::mutex g_noalloc_mutex;
 static int *g_noalloc_ptr[256];
 
 // Device address of g_noalloc_scratch on the current device, looked up once per device (the host
-// symbol is only a stand-in for it).
+// symbol is only a stand-in for it). The address belongs to the device's context: a process that calls
+// cudaDeviceReset on a device must not use the allocation-free query on that device afterwards.
 static int noalloc_scratch(int **ptr) {
     int dev = 0;
     SSDF_CUDA(cudaGetDevice(&dev));
@@ -1571,7 +1591,9 @@ static int noalloc_scratch(int **ptr) {
 
 long long noalloc_max_queries() { return kNoAllocMaxQueries; }
 
-// The fix-up query of `args` with its overflow list in g_noalloc_scratch: no allocation.
+// The fix-up query of `args` with its overflow list in g_noalloc_scratch: no allocation. It takes the
+// same launch decisions as launch_query_keep: the packet work budget of a launch this size, and the
+// FP64 kernel (which needs no scratch) for a mesh made mostly of ill-conditioned triangles.
 int launch_query_noalloc(const QueryArgs &args_in, cudaStream_t stream) {
     QueryArgs a = args_in;
     const long long n = a.is_grid ? a.nx * a.ny * a.nz : a.npoints;
@@ -1584,14 +1606,20 @@ int launch_query_noalloc(const QueryArgs &args_in, cudaStream_t stream) {
         return fail(SSDF_ERR_INVALID_ARGUMENT, "fix-up queries need the double triangles and BVH (keep_fp64=1)");
     if (a.output == SSDF_OUT_SDF && !a.m.face_n)
         return fail(SSDF_ERR_INVALID_ARGUMENT, "signed queries need a mesh built with normals=1");
+    a.counters = nullptr;
+    const bool warp = use_warp(a), wide = use_wide(a);
+    const long long nblocks = query_blocks(a);
+    if (fixup_runs_f64(a.m)) {  // the same bits from the FP64 kernel, which has no overflow list
+        const cudaError_t e = launch_prec<SSDF_PREC_F64>(a, warp, wide, false, unsigned(nblocks), stream);
+        if (e != cudaSuccess) return cuda_fail(e, "allocation-free query launch", __FILE__, __LINE__);
+        return SSDF_OK;
+    }
+    a.warp_budget = resolve_warp_budget(a.warp_budget, n);
     int *scratch = nullptr;
     SSDF_CHECK(noalloc_scratch(&scratch));
-    a.counters = nullptr;
     a.fallback_count = scratch;
     a.fallback_ids = scratch + 1;
     a.fallback_thr = reinterpret_cast<float *>(scratch + 1 + n);
-    const bool warp = use_warp(a), wide = use_wide(a);
-    const long long nblocks = query_blocks(a);
     cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(int), stream);  // the count starts at zero
     if (e == cudaSuccess) e = launch_prec<SSDF_PREC_F32_FIXUP>(a, warp, wide, false, unsigned(nblocks), stream);
     if (e == cudaSuccess) {

@@ -139,6 +139,7 @@ int precision_from_env(int dflt) {
     return dflt;
 }
 
+// SSDF_B200_TAU: a wider fix-up window than the mesh's own minimum (never a narrower one).
 float tau_rel_from_env() {
     const char *v = env_str("SSDF_B200_TAU");
     const float t = v ? float(atof(v)) : 0.f;
@@ -443,6 +444,17 @@ int ssdf_b200_closest_point_bvh_ff(ptrdiff_t npoints, const float *x, const floa
     return bvh_points_host<float, float>(npoints, x, y, z, nselements, s0, s1, s2, nspoints, sx, sy, sz, outd, outtri,
                                          outx, outy, outz, SSDF_OUT_CLOSEST, precision_from_env(SSDF_PREC_F32_FIXUP));
 }
+// float coordinates, double distance: the double distance of the float-valued mesh and points, the
+// closest point rounded to float, written where the double distance is below the incoming outd
+int ssdf_b200_closest_point_bvh_fd(ptrdiff_t npoints, const float *x, const float *y, const float *z,
+                                   ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                   ptrdiff_t nspoints, const float *sx, const float *sy, const float *sz, double *outd,
+                                   float *outx, float *outy, float *outz, int *outtri) {
+    if (npoints > 0 && nselements > 0 && (!outx || !outy || !outz || !outtri))
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "null closest-point output array");
+    return bvh_points_host<float, double>(npoints, x, y, z, nselements, s0, s1, s2, nspoints, sx, sy, sz, outd, outtri,
+                                          outx, outy, outz, SSDF_OUT_CLOSEST, precision_from_env(SSDF_PREC_F32_FIXUP));
+}
 int ssdf_b200_closest_point_bvh_dd(ptrdiff_t npoints, const double *x, const double *y, const double *z,
                                    ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
                                    ptrdiff_t nspoints, const double *sx, const double *sy, const double *sz,
@@ -649,6 +661,14 @@ int ssdf_mesh_destroy_async(ssdf_mesh *mesh, void *stream) {
     return SSDF_OK;
 }
 
+int ssdf_mesh_filter_info(const ssdf_mesh *mesh, float *tau_rel, int *float_filter, int64_t *slivers) {
+    if (!mesh) return fail(SSDF_ERR_INVALID_ARGUMENT, "null mesh");
+    if (tau_rel) *tau_rel = mesh->m.tau_rel_min;
+    if (float_filter) *float_filter = mesh->m.filt32 && !fixup_runs_f64(mesh->m) ? 1 : 0;
+    if (slivers) *slivers = mesh->m.nill;
+    return SSDF_OK;
+}
+
 int ssdf_mesh_stats(const ssdf_mesh *mesh, int64_t *nodes, int64_t *leaves, int64_t *depth, int64_t *bytes) {
     if (!mesh) return fail(SSDF_ERR_INVALID_ARGUMENT, "null mesh");
     if (nodes) *nodes = mesh->m.nnodes;
@@ -673,7 +693,8 @@ static int fill_query(const ssdf_mesh *mesh, const ssdf_query_opts *opts, QueryA
     a->output = opts->output;
     a->coord_f64 = opts->coord_type == SSDF_F64;
     a->out_f64 = opts->out_type == SSDF_F64;
-    a->tau_rel = tau_rel_from_env();
+    // the mesh's own minimum (wider for meshes of a few large triangles); the environment may only widen it
+    a->tau_rel = std::max(tau_rel_from_env(), mesh->m.tau_rel_min);
     a->warp_budget = env_int("SSDF_B200_WARP_BUDGET", -1);
     return SSDF_OK;
 }

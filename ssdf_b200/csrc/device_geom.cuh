@@ -116,8 +116,14 @@ __device__ __forceinline__ void tri_closest_point_exact(const T px, const T py, 
 // FP32 filter of the fix-up path: Ericson's regions (Real-Time Collision Detection, 5.1.5) over a
 // precomputed record -- corner a, edges ab and ac, and the products ab.ab, ac.ac, ab.ac -- so that
 // the dot products with b - p and c - p follow from those with a - p by one subtraction each, with
-// fused multiply-adds and an approximate reciprocal. Its error against the exact double value is
-// covered by the fix-up window.
+// fused multiply-adds and an approximate quotient on the edges. In the face region the key is the
+// squared distance to the plane, (n.ap)^2 / n.n with n = ab x ac, rather than the distance to the
+// point the barycentric solve gives: its rounding error does not grow with the square of the
+// triangle's aspect ratio. The error against the exact distance (input rounding, every fmaf, the
+// quotient and reciprocal, the region decisions) is bounded by
+//   u (8 R + 7.7 alpha L) + min(D, 2 D^2 / d),  D = 90 u alpha R,  u = 2^-24,
+// R the largest distance from p to a corner, L the longest edge, alpha = L / (smallest altitude),
+// d the distance; the fix-up window is sized per mesh to twice that (mesh_build.cu, filter_bound).
 struct FiltRec {
     float ax, ay, az, abx, aby, abz, acx, acy, acz, abab, acac, abac;
 };
@@ -157,13 +163,13 @@ __device__ __forceinline__ float tri_dist_sq_filter(const float px, const float 
         const float dz = fmaf(-w, r.acz - r.abz, apz - r.abz);
         return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     }
-    const float denom = __frcp_rn(va + vb + vc);
-    const float v = vb * denom;
-    const float w = vc * denom;
-    const float dx = apx - fmaf(r.abx, v, r.acx * w);
-    const float dy = apy - fmaf(r.aby, v, r.acy * w);
-    const float dz = apz - fmaf(r.abz, v, r.acz * w);
-    return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    // inside: the plane's distance, n = ab x ac
+    const float nx = fmaf(r.aby, r.acz, -r.abz * r.acy);
+    const float ny = fmaf(r.abz, r.acx, -r.abx * r.acz);
+    const float nz = fmaf(r.abx, r.acy, -r.aby * r.acx);
+    const float nq = fmaf(nx, apx, fmaf(ny, apy, nz * apz));
+    const float nn = fmaf(nx, nx, fmaf(ny, ny, nz * nz));
+    return nq * (nq * __frcp_rn(nn));  // this order keeps every intermediate finite for |coordinates| <= 2^28
 }
 
 // Point-box squared distance (serial/edf/edf.hpp:55-69 computes the same quantity); used only to

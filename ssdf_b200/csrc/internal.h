@@ -87,7 +87,21 @@ struct DeviceMesh {
     float coord_scale = 0.f;
     // triangles the fix-up filter sees through a proxy (ill-conditioned; 0 without the double data)
     int nill = 0;
+    // the fix-up window's smallest relative width for this mesh (at least 2^-16; wider when its
+    // records are large against coord_scale), and whether the float filter can serve it at all
+    // (coordinates within 2^28, no record that float rounding made degenerate, needle-like or
+    // too small); see set_filter_window
+    float tau_rel_min = 1.0f / 65536.0f;
+    int filter_ok = 0;
 };
+
+// Largest coordinate magnitude of a mesh, or of a query point, that the fix-up path's float filter
+// takes: every product it forms then stays finite (|p - a| < 2^30, dot products < 2^60, their
+// products < 2^120). Points beyond it are answered exactly by the second stage.
+constexpr float kFilterMaxCoord = 268435456.0f;  // 2^28
+// Sets DeviceMesh::tau_rel_min and ::filter_ok from the largest bound term of the mesh's filter
+// records (mesh_build.cu, filter_bound) and whether every record is safe.
+void set_filter_window(DeviceMesh *m, float largest_term, bool records_safe);
 
 // Everything a query launch needs; built by the host entry points.
 struct QueryArgs {
@@ -184,6 +198,8 @@ bool streamed_download_applies(long long n, const void *host_out, const int *hos
 int launch_query_noalloc(const QueryArgs &args, cudaStream_t stream);
 long long noalloc_max_queries();
 int launch_batch(const BatchLaunch &b, int precision, cudaStream_t stream);
+// Whether a fix-up request on this mesh runs the FP64 kernel instead (bvh_query.cu).
+bool fixup_runs_f64(const DeviceMesh &m);
 int batch_capture_graphs(ssdf_batch *b);  // batch.cu
 int batch_blocks_per_sm(int precision, bool warp, bool wide);
 bool default_warp(int is_grid);

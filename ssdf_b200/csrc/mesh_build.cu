@@ -497,6 +497,63 @@ __device__ bool filter_record(double ax, double ay, double az, double bx, double
     return ill;
 }
 
+// The fix-up window's bound term of one filter record (the triangle the float corners describe, or its
+// proxy): the FP32 filter's error at a query p is at most u (8 R + 7.7 alpha L) + min(D, 2 D^2 / d) with
+// D = 90 u alpha R (device_geom.cuh, tri_dist_sq_filter; the derivation is in the design notes), u =
+// 2^-24, L the record's longest edge, alpha = L^2 / |ab x ac| and R the largest distance from p to a
+// corner. That is at most u (17 d + (16 + 188 alpha) L) at any distance d (near the record R <= 2L; far
+// from it the D^2 term is below u d); with the input rounding of p and of the corners it stays below
+// u (18.1 d + 2 sqrt(3) M) + u (20 + 188 alpha) L, M the largest coordinate magnitude. This returns the
+// record's term (20 + 188 alpha) L, and false when the record is not safe
+// for the float filter: an edge shorter than 2^-23 (its products underflow), a record that rounding
+// to float made degenerate or needle-like (alpha > 16), or a non-finite value.
+__device__ bool filter_bound(const float4 *__restrict__ rec, float *term) {
+    const double e1[3] = {rec[1].x, rec[1].y, rec[1].z}, e2[3] = {rec[2].x, rec[2].y, rec[2].z};
+    const double e3[3] = {e2[0] - e1[0], e2[1] - e1[1], e2[2] - e1[2]};
+    const double l1 = e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2];
+    const double l2 = e2[0] * e2[0] + e2[1] * e2[1] + e2[2] * e2[2];
+    const double l3 = e3[0] * e3[0] + e3[1] * e3[1] + e3[2] * e3[2];
+    const double ll = fmax(fmax(l1, l2), l3);
+    *term = 0.f;
+    if (ll == 0.0) return true;  // all corners equal: only the corner test runs, exactly
+    const double nx = e1[1] * e2[2] - e1[2] * e2[1], ny = e1[2] * e2[0] - e1[0] * e2[2];
+    const double nz = e1[0] * e2[1] - e1[1] * e2[0];
+    const double n = sqrt(nx * nx + ny * ny + nz * nz);
+    const double shortest = fmin(fmin(l1, l2), l3);
+    const double alpha = ll / n;
+    if (!(shortest >= 0x1p-46) || !(alpha <= 16.0) || !(ll < 0x1p120)) return false;
+    *term = __double2float_ru((20.0 + 188.0 * alpha) * sqrt(ll));
+    return true;
+}
+
+}  // namespace
+
+// The window (sqrt(best) + tau)^2 (1 + 2^-16), tau = tau_rel (M + sqrt(best)), keeps the double
+// winner whenever tau exceeds the sum of its key's error above its distance and the error below of
+// the key that set best. With the bound above both are at most u (18.1 d + 2 sqrt(3) M + term), so
+// tau_rel >= u (6.93 + 2 term / M) and tau_rel >= 36.2 u suffice (2^-9 added for best lying below
+// the winner's distance; the (1 + 2^-16) factor covers the rounding of the window itself). The
+// default 2^-16 = 256 u holds them
+// whenever term / M <= 124: for the torus-knot tube the term is about 0.1 M, for a 5,120-triangle
+// sphere 0.2 M; a mesh of a few large triangles gets a wider window. A mesh whose window would pass
+// 2^-8, or with a record the float filter cannot take, is answered by the FP64 kernel.
+void set_filter_window(DeviceMesh *m, float largest_term, bool records_safe) {
+    const double u = 0x1p-24, M = double(m->coord_scale);
+    double tau = 1.0 / 65536.0;
+    if (largest_term > 0.f) {
+        if (!(M > 0.0)) {
+            m->tau_rel_min = 1.0f;
+            m->filter_ok = 0;
+            return;
+        }
+        tau = fmax(tau, u * (6.93 + 2.0 * double(largest_term) / M) * (1.0 + 0x1p-9));
+    }
+    m->tau_rel_min = float(tau) < tau ? nextafterf(float(tau), INFINITY) : float(tau);
+    m->filter_ok = records_safe && M <= double(kFilterMaxCoord) && tau <= 0x1p-8 ? 1 : 0;
+}
+
+namespace {
+
 __global__ void k_tri_records(int nt, const int *__restrict__ sorted_ids, const int *__restrict__ s0,
                               const int *__restrict__ s1, const int *__restrict__ s2, const double *__restrict__ vx,
                               const double *__restrict__ vy, const double *__restrict__ vz, float4 *__restrict__ t32,
@@ -510,7 +567,14 @@ __global__ void k_tri_records(int nt, const int *__restrict__ sorted_ids, const 
     t32[3 * p + 0] = make_float4(float(ax), float(ay), float(az), float(bx));
     t32[3 * p + 1] = make_float4(float(by), float(bz), float(cx), float(cy));
     t32[3 * p + 2] = make_float4(float(cz), __int_as_float(t), 0.f, 0.f);
-    if (filt && filter_record(ax, ay, az, bx, by, bz, cx, cy, cz, t, filt + 4 * size_t(p))) atomicAdd(nill, 1);
+    if (filt) {
+        if (filter_record(ax, ay, az, bx, by, bz, cx, cy, cz, t, filt + 4 * size_t(p))) atomicAdd(nill, 1);
+        float term;
+        if (filter_bound(filt + 4 * size_t(p), &term))
+            atomicMax(nill + 1, __float_as_int(term));  // non-negative floats order like their bits
+        else
+            atomicAdd(nill + 2, 1);
+    }
     if (t64) {
         t64[5 * p + 0] = make_double2(ax, ay);
         t64[5 * p + 1] = make_double2(az, bx);
@@ -709,7 +773,9 @@ static int mesh_build_impl(MeshStorage *s, MeshStorage *tmp, DeviceMesh *m, int 
                                                                  (const float *)gz, vx, vy, vz);
     LAUNCH_CHECK("k_widen");
     // validation + per-triangle boxes
-    int *flags;  // [0] first bad triangle, [1..6] scene, [7] scale, [8..9] depth / leaves, [10] ill
+    // [0] first bad triangle, [1..6] scene, [7] scale, [8..9] depth / leaves, [10] ill, [11] largest
+    // filter bound term (float bits), [12] records unsafe for the float filter
+    int *flags;
     SSDF_CHECK(dalloc(tmp, &flags, 16, stream));
     {
         // ordered-int encodings (f2o) of +FLT_MAX and -FLT_MAX seed the scene min / max
@@ -837,15 +903,20 @@ static int mesh_build_impl(MeshStorage *s, MeshStorage *tmp, DeviceMesh *m, int 
     k_tri_records<<<grid_blocks(nt, 256), 256, 0, stream>>>(nt, ids, s0, s1, s2, vx, vy, vz, t32, t64, filt,
                                                             flags + 10);
     LAUNCH_CHECK("k_tri_records");
-    int scale_bits = 0, nill = 0;
+    int scale_bits = 0, filt_info[3] = {0, 0, 0};
     SSDF_CUDA(cudaMemcpyAsync(&scale_bits, flags + 7, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    SSDF_CUDA(cudaMemcpyAsync(&nill, flags + 10, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    SSDF_CUDA(cudaMemcpyAsync(filt_info, flags + 10, sizeof(filt_info), cudaMemcpyDeviceToHost, stream));
     if (opts.normals) SSDF_CHECK(build_normals(s, m, s0, s1, s2, vx, vy, vz, stream));
     SSDF_CUDA(cudaStreamSynchronize(stream));
     float scale;
     memcpy(&scale, &scale_bits, sizeof(float));
     m->coord_scale = scale;
-    m->nill = nill;
+    m->nill = filt_info[0];
+    if (keep64) {
+        float term;
+        memcpy(&term, &filt_info[1], sizeof(float));
+        set_filter_window(m, term, filt_info[2] == 0);
+    }
     m->depth = depth_leaves[0];
     m->nleaves = depth_leaves[1];
     m->nodes32 = nodes32;

@@ -32,96 +32,112 @@ namespace {
 
 constexpr int kThreadsR = 128;
 
-// The six tetrahedra of a cell about its diagonal from corner 0 to corner 7; corner c sits at
-// (c & 1, (c >> 1) & 1, (c >> 2) & 1) in cell units.
-__constant__ int c_tets[6][4] = {{0, 1, 3, 7}, {0, 1, 5, 7}, {0, 2, 3, 7}, {0, 2, 6, 7}, {0, 4, 5, 7}, {0, 4, 6, 7}};
+// ---- marching tetrahedra ------------------------------------------------------------------------
+//
+// A cell's corners are numbered c = x + 2 y + 4 z for its offsets x, y, z in {0, 1}. Within a cell a
+// corner's grid index grows with its number (the grid's strides are 1 < nx < nx ny whenever the grid
+// has cells), so the corner of lower grid index on an edge is its lower-numbered corner: an edge is
+// named by its code (lo << 3) | hi, and its crossing is interpolated from lo.
+//
+// The cell is cut into the six tetrahedra about its 0-7 diagonal (the order of this list is the order
+// of the output). For each tetrahedron and each 4-bit pattern p of its corners above the level (bit s
+// for its corner s), the table below lists the crossing edges of the triangles to emit, in emission
+// order:
+//   - a corner alone on its side of the level: one triangle on that corner's three edges, the other
+//     corners taken in the tetrahedron's order;
+//   - two corners on each side (u0, u1 above, d0, d1 not, each pair in the tetrahedron's order): the
+//     quadrilateral u0d0, u0d1, u1d1, u1d0, emitted as its triangles (0, 1, 2) and (0, 2, 3).
+// An entry packs the triangle count in bits 0-1 and six 6-bit edge codes from bit 2 on.
+constexpr int kTetCorner[6][4] = {{0, 1, 3, 7}, {0, 1, 5, 7}, {0, 2, 3, 7}, {0, 2, 6, 7}, {0, 4, 5, 7}, {0, 4, 6, 7}};
 
-struct CellValues {
-    long long g[8];    // grid index of each corner
-    double v[8];       // value less the level
-    double p[8][3];    // position
+struct TetTable {
+    unsigned long long entry[6][16];
+    int corner[6][4];
 };
 
-template <typename T>
-__device__ bool load_corners(const GridDesc &gd, const T *__restrict__ f, double level, long long i, long long j,
-                             long long k, CellValues &c) {
-    const long long sy = gd.n[0], sz = gd.n[0] * gd.n[1];
-    int above = 0;
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-        const long long ci = i + (q & 1), cj = j + ((q >> 1) & 1), ck = k + ((q >> 2) & 1);
-        c.g[q] = ci + cj * sy + ck * sz;
-        c.v[q] = double(f[c.g[q]]) - level;
-        above += c.v[q] > 0 ? 1 : 0;
-    }
-    if (above == 0 || above == 8) return false;
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-        const long long ijk[3] = {i + (q & 1), j + ((q >> 1) & 1), k + ((q >> 2) & 1)};
-#pragma unroll
-        for (int d = 0; d < 3; d++) c.p[q][d] = gd.o[d] + double(ijk[d]) * gd.h[d];
-    }
-    return true;
-}
+constexpr unsigned edge_code(int a, int b) { return a < b ? unsigned((a << 3) | b) : unsigned((b << 3) | a); }
 
-// The level crossing on the edge between corners a and b, interpolated from the corner of lower grid
-// index.
-__device__ void edge_crossing(const CellValues &c, int a, int b, double q[3]) {
-    if (c.g[b] < c.g[a]) {
-        const int s = a;
-        a = b;
-        b = s;
-    }
-    const double t = c.v[a] / (c.v[a] - c.v[b]);
-#pragma unroll
-    for (int d = 0; d < 3; d++) q[d] = c.p[a][d] + t * (c.p[b][d] - c.p[a][d]);
-}
-
-// The 0, 1 or 2 triangles of tetrahedron tet, degenerate ones (two vertices equal in G) dropped.
-template <typename G>
-__device__ int tet_triangles(const CellValues &c, int tet, double tri[2][3][3]) {
-    int up[4], down[4], nu = 0, nd = 0;
-    for (int a = 0; a < 4; a++) {
-        const int q = c_tets[tet][a];
-        if (c.v[q] > 0)
-            up[nu++] = q;
-        else
-            down[nd++] = q;
-    }
-    if (nu == 0 || nd == 0) return 0;
-    int m;
-    if (nu == 1 || nd == 1) {
-        // one corner apart: the triangle on its three edges
-        const int lone = nu == 1 ? up[0] : down[0];
-        const int *others = nu == 1 ? down : up;
-        for (int a = 0; a < 3; a++) edge_crossing(c, lone, others[a], tri[0][a]);
-        m = 1;
-    } else {
-        // two and two: the quadrilateral on the four edges between them, as triangles (0,1,2), (0,2,3)
-        double q[4][3];
-        edge_crossing(c, up[0], down[0], q[0]);
-        edge_crossing(c, up[0], down[1], q[1]);
-        edge_crossing(c, up[1], down[1], q[2]);
-        edge_crossing(c, up[1], down[0], q[3]);
-        const int quad[2][3] = {{0, 1, 2}, {0, 2, 3}};
-        for (int s = 0; s < 2; s++)
-            for (int a = 0; a < 3; a++)
-                for (int d = 0; d < 3; d++) tri[s][a][d] = q[quad[s][a]][d];
-        m = 2;
-    }
-    int kept = 0;
-    for (int s = 0; s < m; s++) {
-        bool degenerate = false;
-        for (int a = 0; a < 3; a++) {
-            const int b = (a + 1) % 3;
-            degenerate |= G(tri[s][a][0]) == G(tri[s][b][0]) && G(tri[s][a][1]) == G(tri[s][b][1]) &&
-                          G(tri[s][a][2]) == G(tri[s][b][2]);
+constexpr TetTable make_tet_table() {
+    TetTable tab{};
+    for (int tet = 0; tet < 6; tet++) {
+        for (int pat = 0; pat < 16; pat++) {
+            int hi[4] = {0, 0, 0, 0}, lo[4] = {0, 0, 0, 0}, nh = 0, nl = 0;
+            for (int s = 0; s < 4; s++) {
+                if ((pat >> s) & 1)
+                    hi[nh++] = kTetCorner[tet][s];
+                else
+                    lo[nl++] = kTetCorner[tet][s];
+            }
+            unsigned edges[6] = {0, 0, 0, 0, 0, 0};
+            int ntri = 0;
+            if (nh == 1 || nl == 1) {
+                const int alone = nh == 1 ? hi[0] : lo[0];
+                const int *rest = nh == 1 ? lo : hi;
+                for (int v = 0; v < 3; v++) edges[v] = edge_code(alone, rest[v]);
+                ntri = 1;
+            } else if (nh == 2) {
+                const unsigned quad[4] = {edge_code(hi[0], lo[0]), edge_code(hi[0], lo[1]), edge_code(hi[1], lo[1]),
+                                          edge_code(hi[1], lo[0])};
+                const int split[6] = {0, 1, 2, 0, 2, 3};
+                for (int v = 0; v < 6; v++) edges[v] = quad[split[v]];
+                ntri = 2;
+            }
+            unsigned long long e = (unsigned long long)ntri;
+            for (int v = 0; v < 3 * ntri; v++) e |= (unsigned long long)edges[v] << (2 + 6 * v);
+            tab.entry[tet][pat] = e;
         }
-        if (degenerate) continue;
-        if (kept != s)
-            for (int a = 0; a < 3; a++)
-                for (int d = 0; d < 3; d++) tri[kept][a][d] = tri[s][a][d];
-        kept++;
+        for (int s = 0; s < 4; s++) tab.corner[tet][s] = kTetCorner[tet][s];
+    }
+    return tab;
+}
+
+__constant__ TetTable c_tet = make_tet_table();
+
+// One cell (its lowest corner at grid (i, j, k)): corner values less the level and the pattern of the
+// corners above it.
+struct MtCell {
+    double val[8];
+    unsigned above;
+    long long base[3];
+};
+
+// The crossing of edge `code` (corner positions o + index * h, then the interpolation from the lower
+// corner, in the reference's expression order; the library is built without contraction).
+__device__ __forceinline__ void mt_crossing(const GridDesc &gd, const MtCell &c, unsigned code, double q[3]) {
+    const int a = int(code >> 3), b = int(code & 7);
+    const double t = c.val[a] / (c.val[a] - c.val[b]);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const double pa = gd.o[d] + double(c.base[d] + ((a >> d) & 1)) * gd.h[d];
+        const double pb = gd.o[d] + double(c.base[d] + ((b >> d) & 1)) * gd.h[d];
+        q[d] = pa + t * (pb - pa);
+    }
+}
+
+// Visits the cell's triangles in output order, each as its three vertices rounded to G, skipping those
+// with two vertices equal in G (a corner on the level makes crossings coincide); returns how many.
+template <typename G, class Emit>
+__device__ int mt_cell_triangles(const GridDesc &gd, const MtCell &c, Emit emit) {
+    int kept = 0;
+    for (int tet = 0; tet < 6; tet++) {
+        unsigned pat = 0;
+#pragma unroll
+        for (int s = 0; s < 4; s++) pat |= ((c.above >> c_tet.corner[tet][s]) & 1u) << s;
+        const unsigned long long e = c_tet.entry[tet][pat];
+        const int ntri = int(e & 3ull);
+        for (int t = 0; t < ntri; t++) {
+            G v[3][3];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                double q[3];
+                mt_crossing(gd, c, unsigned((e >> (2 + 6 * (3 * t + k))) & 63ull), q);
+                v[k][0] = G(q[0]), v[k][1] = G(q[1]), v[k][2] = G(q[2]);
+            }
+            auto same = [&](int a, int b) { return v[a][0] == v[b][0] && v[a][1] == v[b][1] && v[a][2] == v[b][2]; };
+            if (same(0, 1) || same(1, 2) || same(2, 0)) continue;
+            emit(kept, v);
+            kept++;
+        }
     }
     return kept;
 }
@@ -135,28 +151,32 @@ __global__ void __launch_bounds__(kThreadsR) k_marching(GridDesc gd, const T *__
     const long long cell = blockIdx.x * (long long)kThreadsR + threadIdx.x;
     if (cell >= ncells) return;
     const long long cx = gd.n[0] - 1, cy = gd.n[1] - 1;
-    const long long i = cell % cx, r = cell / cx, j = r % cy, k = r / cy;
-    CellValues c;
-    if (!load_corners(gd, f, level, i, j, k, c)) {
+    MtCell c;
+    c.base[0] = cell % cx;
+    c.base[1] = (cell / cx) % cy;
+    c.base[2] = cell / (cx * cy);
+    const long long sy = gd.n[0], sz = gd.n[0] * gd.n[1];
+    const long long g0 = c.base[0] + c.base[1] * sy + c.base[2] * sz;
+    c.above = 0;
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        c.val[q] = double(f[g0 + (q & 1) + ((q >> 1) & 1) * sy + ((q >> 2) & 1) * sz]) - level;
+        c.above |= (c.val[q] > 0 ? 1u : 0u) << q;
+    }
+    if (c.above == 0u || c.above == 0xffu) {  // the level does not cross this cell
         if (!EMIT) count[cell] = 0;
         return;
     }
-    long long next = EMIT ? offset[cell] : 0;
-    int total = 0;
-    for (int t = 0; t < 6; t++) {
-        double tri[2][3][3];
-        const int m = tet_triangles<G>(c, t, tri);
-        if (EMIT) {
-            for (int s = 0; s < m; s++, next++)
-                for (int a = 0; a < 3; a++) {
-                    x[3 * next + a] = G(tri[s][a][0]);
-                    y[3 * next + a] = G(tri[s][a][1]);
-                    z[3 * next + a] = G(tri[s][a][2]);
-                }
-        }
-        total += m;
+    if (EMIT) {
+        const long long first = offset[cell];
+        mt_cell_triangles<G>(gd, c, [&](int t, const G (&v)[3][3]) {
+            const long long o = 3 * (first + t);
+#pragma unroll
+            for (int k = 0; k < 3; k++) x[o + k] = v[k][0], y[o + k] = v[k][1], z[o + k] = v[k][2];
+        });
+    } else {
+        count[cell] = mt_cell_triangles<G>(gd, c, [](int, const G (&)[3][3]) {});
     }
-    if (!EMIT) count[cell] = total;
 }
 
 __global__ void k_soup_indices(long long n, int *__restrict__ s0, int *__restrict__ s1, int *__restrict__ s2) {
@@ -196,33 +216,59 @@ __global__ void k_shift(long long n, T *__restrict__ v, T s) {
     if (p < n) v[p] += s;
 }
 
-// refine_field: coarse samples to multiples of factor, then per axis the cubic through the four
-// nearest samples (the end samples repeated), weights w[4 m + q] for t = m / factor.
-template <typename T>
-__global__ void k_refine_place(GridDesc gd, long long factor, long long fx, long long fxy, const T *__restrict__ f,
-                               T *__restrict__ fine) {
-    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const long long n = gd.n[0] * gd.n[1] * gd.n[2];
-    if (p >= n) return;
-    const long long i = p % gd.n[0], r = p / gd.n[0], j = r % gd.n[1], k = r / gd.n[1];
-    fine[i * factor + fx * (j * factor) + fxy * (k * factor)] = f[p];
+// refine_field (serial/bvh/sdf_rebuild.hpp:40-55). The fine grid's samples at multiples of factor
+// along all three axes are the coarse ones; every other sample is the cubic through the four nearest
+// samples along one axis (the end samples repeated), axis by axis -- x, then y, then z -- each value
+// rounded to T before a later axis reads it. Pass `axis` here computes every fine sample whose index is
+// a multiple of factor along the axes after `axis` and not along `axis` (for x: along any x), one
+// thread per sample, gathering its four inputs from the previous pass's samples on its line (for x:
+// straight from the coarse field, which also places the coarse samples).
+__device__ __forceinline__ void cubic_weights(long long m, long long factor, double w[4]) {
+    const double t = double(m) / double(factor);
+    w[0] = -t * (t - 1) * (t - 2) / 6;
+    w[1] = (t + 1) * (t - 1) * (t - 2) / 2;
+    w[2] = -(t + 1) * t * (t - 2) / 2;
+    w[3] = (t + 1) * t * (t - 1) / 6;
 }
 
-template <typename T>
-__global__ void k_refine_axis(long long n1, long long n2, long long n, long long factor, long long stride,
-                              long long step1, long long step2, const double *__restrict__ w, T *__restrict__ fine) {
-    const long long item = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const long long per_line = (n - 1) * (factor - 1);
-    if (item >= n1 * n2 * per_line) return;
-    const long long line_id = item / per_line, rest = item % per_line;
-    const long long q1 = line_id % n1, q2 = line_id / n1;
-    const long long c = rest / (factor - 1), m = rest % (factor - 1) + 1;
-    T *const line = fine + q1 * step1 + q2 * step2;
-    const long long cm = c > 0 ? c - 1 : 0, cp = c + 2 < n - 1 ? c + 2 : n - 1;
-    const T v0 = line[cm * factor * stride], v1 = line[c * factor * stride], v2 = line[(c + 1) * factor * stride],
-            v3 = line[cp * factor * stride];
-    const double *wm = w + 4 * m;
-    line[(c * factor + m) * stride] = T(wm[0] * v0 + wm[1] * v1 + wm[2] * v2 + wm[3] * v3);
+struct RefineDims {
+    long long coarse[3], fine[3];  // samples per axis
+    long long factor;
+};
+
+template <typename T, int AXIS>
+__global__ void k_refine_pass(RefineDims d, const T *__restrict__ f, T *__restrict__ fine) {
+    // outputs of this pass: fine indices along the axes up to AXIS, coarse ones after it
+    long long ext[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) ext[a] = a <= AXIS ? d.fine[a] : d.coarse[a];
+    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p >= ext[0] * ext[1] * ext[2]) return;
+    long long idx[3] = {p % ext[0], (p / ext[0]) % ext[1], p / (ext[0] * ext[1])};
+    const long long m = idx[AXIS] % d.factor, c = idx[AXIS] / d.factor;
+    if (AXIS > 0 && m == 0) return;  // a multiple of factor along AXIS: an earlier pass wrote it
+    // fine position of the output (indices after AXIS are coarse, so scaled)
+    long long fpos[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) fpos[a] = a <= AXIS ? idx[a] : idx[a] * d.factor;
+    const long long sy = d.fine[0], sz = d.fine[0] * d.fine[1];
+    const long long out = fpos[0] + fpos[1] * sy + fpos[2] * sz;
+    // the line's samples along AXIS at coarse position q: the coarse field (x) or the earlier passes
+    auto line = [&](long long q) -> T {
+        if (AXIS == 0) return f[q + d.coarse[0] * (idx[1] + d.coarse[1] * idx[2])];
+        long long at[3] = {fpos[0], fpos[1], fpos[2]};
+        at[AXIS] = q * d.factor;
+        return fine[at[0] + at[1] * sy + at[2] * sz];
+    };
+    if (m == 0) {  // x pass only: the coarse sample itself
+        fine[out] = line(c);
+        return;
+    }
+    const long long n = d.coarse[AXIS];
+    const T v0 = line(c > 0 ? c - 1 : 0), v1 = line(c), v2 = line(c + 1), v3 = line(c + 2 < n - 1 ? c + 2 : n - 1);
+    double w[4];
+    cubic_weights(m, d.factor, w);
+    fine[out] = T(w[0] * v0 + w[1] * v1 + w[2] * v2 + w[3] * v3);
 }
 
 inline unsigned blocks_for(long long n, int t) { return unsigned((n + t - 1) / t); }
@@ -361,42 +407,20 @@ template <typename G, typename T>
 int refine_device(const GridDesc &gd, const T *d_f, long long factor, T *d_fine, cudaStream_t stream) {
     if (factor < 1) return fail(SSDF_ERR_INVALID_ARGUMENT, "refine_field: factor must be >= 1");
     const GridDesc rg = grid_refined(gd, factor, sizeof(G) == 8);
-    const long long n = gd.n[0] * gd.n[1] * gd.n[2];
-    if (n <= 0) return SSDF_OK;
-    const long long fx = rg.n[0], fxy = rg.n[0] * rg.n[1];
-    k_refine_place<T><<<blocks_for(n, 256), 256, 0, stream>>>(gd, factor, fx, fxy, d_f, d_fine);
+    if (gd.n[0] * gd.n[1] * gd.n[2] <= 0) return SSDF_OK;
+    RefineDims d;
+    for (int a = 0; a < 3; a++) d.coarse[a] = gd.n[a], d.fine[a] = rg.n[a];
+    d.factor = factor;
+    // pass a covers fine extents up to a and coarse ones after it
+    const long long n0 = d.fine[0] * d.coarse[1] * d.coarse[2], n1 = d.fine[0] * d.fine[1] * d.coarse[2],
+                    n2 = d.fine[0] * d.fine[1] * d.fine[2];
+    k_refine_pass<T, 0><<<blocks_for(n0, 256), 256, 0, stream>>>(d, d_f, d_fine);
     SSDF_CUDA(cudaGetLastError());
     if (factor == 1) return SSDF_OK;
-    // weights of the cubic through samples -1, 0, 1, 2 at t = m / factor
-    std::vector<double> w(4 * size_t(factor));
-    for (long long m = 0; m < factor; m++) {
-        const double t = double(m) / double(factor);
-        w[4 * m + 0] = -t * (t - 1) * (t - 2) / 6;
-        w[4 * m + 1] = (t + 1) * (t - 1) * (t - 2) / 2;
-        w[4 * m + 2] = -(t + 1) * t * (t - 2) / 2;
-        w[4 * m + 3] = (t + 1) * t * (t - 1) / 6;
-    }
-    double *dw = nullptr;
-    SSDF_CUDA(cudaMallocAsync(&dw, sizeof(double) * w.size(), stream));
-    SSDF_CUDA(cudaMemcpyAsync(dw, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice, stream));
-    for (int axis = 0; axis < 3; axis++) {
-        const long long stride = axis == 0 ? 1 : (axis == 1 ? fx : fxy);
-        const long long na = gd.n[axis];
-        const int a1 = (axis + 1) % 3, a2 = (axis + 2) % 3;
-        const long long s1 = a1 == 0 ? 1 : (a1 == 1 ? fx : fxy), s2 = a2 == 0 ? 1 : (a2 == 1 ? fx : fxy);
-        const long long c1 = a1 < axis ? 1 : factor, c2 = a2 < axis ? 1 : factor;
-        const long long n1 = a1 < axis ? rg.n[a1] : gd.n[a1], n2 = a2 < axis ? rg.n[a2] : gd.n[a2];
-        const long long items = n1 * n2 * (na - 1) * (factor - 1);
-        if (items <= 0) continue;
-        k_refine_axis<T><<<blocks_for(items, 256), 256, 0, stream>>>(n1, n2, na, factor, stride, c1 * s1, c2 * s2, dw,
-                                                                     d_fine);
-        const cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) {
-            cudaFreeAsync(dw, stream);
-            return cuda_fail(e, "refine_field", __FILE__, __LINE__);
-        }
-    }
-    cudaFreeAsync(dw, stream);
+    k_refine_pass<T, 1><<<blocks_for(n1, 256), 256, 0, stream>>>(d, d_f, d_fine);
+    SSDF_CUDA(cudaGetLastError());
+    k_refine_pass<T, 2><<<blocks_for(n2, 256), 256, 0, stream>>>(d, d_f, d_fine);
+    SSDF_CUDA(cudaGetLastError());
     return SSDF_OK;
 }
 

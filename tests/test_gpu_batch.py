@@ -181,3 +181,54 @@ def test_sorted_point_jobs_in_a_batch(jobs):
             assert np.array_equal(out.cpu().numpy(), want) and np.array_equal(tri.cpu().numpy(), wtri)
         assert np.array_equal(gout.cpu().numpy(), jobs[3]["alone"])
         b.close()
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_sliver_mesh_in_a_fixup_batch(use_graph):
+    """The beam lattice (64 % slivers) beside tori in one fix-up batch: its jobs run in the batch's
+    FP64 table (the arithmetic it gets alone), every job equals the same query alone, bitwise, and
+    the batch's FP64 part costs about what the beam job costs alone."""
+    import torch
+
+    beams = W.beam_lattice(nbeams=4000, seed=7)
+    dmb = S.DeviceMesh(beams)
+    assert not dmb.filter_info()["float_filter"]  # a fix-up request on it runs the FP64 kernel
+    items = [(dmb, W.Grid.padded_nodes(beams, 40, 0.1)), (dmb, W.Grid((23, 31, 17), (0.1, 0.2, 0.0), (0.9, 0.7, 1.0)))]
+    tori = []
+    for k in range(5):
+        m = W.torus(0.6, 0.2, nu=24 + 16 * k, nv=12 + 4 * k, jitter=0.01, seed=30 + k, center=(k, 0.0, -k))
+        dm = S.DeviceMesh(m)
+        assert dm.filter_info()["float_filter"]
+        tori.append(dm)
+        items.append((dm, W.Grid.padded_nodes(m, 24 + 4 * k, 0.1)))
+    alone = []
+    for dm, g in items:
+        out = torch.empty(g.size, dtype=torch.float64, device="cuda")
+        tri = torch.empty(g.size, dtype=torch.int32, device="cuda")
+        dm.query_grid(g, out, tri, precision=S.PREC_F32_FIXUP)
+        torch.cuda.synchronize()
+        alone.append((out.cpu().numpy(), tri.cpu().numpy()))
+    b = S.Batch(len(items), S.PREC_F32_FIXUP)
+    outs = []
+    for run in range(2):
+        b.clear()
+        outs = []
+        for dm, g in (items if run == 0 else items[::-1]):
+            o = torch.full((g.size,), -1.0, dtype=torch.float64, device="cuda")
+            t = torch.full((g.size,), -1, dtype=torch.int32, device="cuda")
+            b.add_grid(dm, g, o, t)
+            outs.append((o, t))
+        b.run(use_graph=use_graph)
+        torch.cuda.synchronize()
+        order = items if run == 0 else items[::-1]
+        want = alone if run == 0 else alone[::-1]
+        for (o, t), (wd, wt), (_, g) in zip(outs, want, order):
+            assert np.array_equal(o.cpu().numpy(), wd) and np.array_equal(t.cpu().numpy(), wt), g.n
+    # the beam grid's nodes match the oracle on a sample
+    g = items[0][1]
+    ids = np.arange(0, g.size, 97)
+    want, wtri = oracle.sdf_points(oracle.grid_points(g)[:, ids], beams)
+    assert np.array_equal(alone[0][0][ids], want) and np.array_equal(alone[0][1][ids], wtri)
+    b.close()
+    for dm in [dmb] + tori:
+        dm.close()

@@ -143,6 +143,25 @@ def test_closest_point_bvh():
         assert np.array_equal(w, g), name
 
 
+def test_closest_point_bvh_float_coords_double_distance():
+    """closest_point_bvh<float, double, int> (serial/bvh/bvh.cpp:1162-1179): float points and mesh,
+    the double distance of those float values, the closest point rounded to float."""
+    mesh = W.torus(nu=80, nv=40, jitter=0.01)
+    meshf = W.Mesh(mesh.vertices.astype(np.float32).astype(np.float64), mesh.triangles)
+    lo, hi = mesh.bbox()
+    pts = W.uniform_points(20000, lo - 0.2, hi + 0.2, seed=6).astype(np.float32)
+    init = np.where(np.arange(20000) % 4 == 0, 0.05, np.finfo(np.float64).max)
+    wd, wx, wy, wz, wt = oracle.closest_point(pts.astype(np.float64), meshf, outd=init)
+    gd, gx, gy, gz, gt = S.closest_point_bvh(pts, mesh, outd=init, dtype=np.float32, tdtype=np.float64)
+    assert gd.dtype == np.float64 and gx.dtype == np.float32
+    assert np.array_equal(gd, wd)
+    assert np.array_equal(gt, wt)
+    upd = wt >= 0
+    for w, g in ((wx, gx), (wy, gy), (wz, gz)):
+        assert np.array_equal(g[upd], w[upd].astype(np.float32))
+        assert np.all(g[~upd] == 0)  # not written where the incoming distance was already smaller
+
+
 def test_sqedf_incoming_values():
     mesh = W.icosphere(3)
     grid = W.Grid((17, 9, 13), (-1.3, -1.2, -1.1), (1.2, 1.3, 1.1))

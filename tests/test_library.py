@@ -50,6 +50,12 @@ def test_cpp_header_compiles_against_c_abi(tmp_path):
         "  (void)ssdf::edf_celllist<float, float, int>;\n"
         "  (void)ssdf::edf_bvh<float, double, int>;\n"
         "  (void)ssdf::closest_point_bvh<double, double, int>;\n"
+        "  (void)ssdf::closest_point_bvh<float, double, int>;\n"
+        "  (void)ssdf::closest_point_bvh<float, float, int>;\n"
+        "  (void)ssdf::edf_bvh<float, float, int>;\n"
+        "  (void)ssdf::edf_bvh<double, double, int>;\n"
+        "  (void)ssdf::sample_sdf_bvh<double, double, int>;\n"
+        "  (void)ssdf::sample_sqedf_bvh<float, float, int>;\n"
         "  (void)ssdf::sample_sdf_bvh<float, float, int>;\n"
         "  (void)ssdf::sample_sqedf_bvh<double, double, int>;\n"
         "  (void)ssdf::compute_aabb<float, double>;\n"
@@ -78,6 +84,22 @@ def test_cpp_header_compiles_against_c_abi(tmp_path):
         "  (void)ssdf::potential_contact_quads_bvh<double, double, int, int>(1, s0, s1, s2, q3, 3, sx, sy, sz, 0.1, pc,\n"
         "      &pci);\n"
         "  ssdf_b200_free(pci);\n"
+        "  // every explicit instantiation of serial/bvh/bvh.cpp:1162-1981\n"
+        "  (void)&ssdf::points_inside_bvh<float, int>;\n"
+        "  (void)&ssdf::sample_inside_bvh<float, int>;\n"
+        "  (void)&ssdf::sample_inside_bvh<double, int>;\n"
+        "  (void)&ssdf::closest_within_radius_bvh<float, double, int>;\n"
+        "  (void)&ssdf::closest_within_radius_bvh<float, float, int>;\n"
+        "  (void)&ssdf::closest_within_radius_local_bvh<float, float, int>;\n"
+        "  (void)&ssdf::closest_within_radius_local_bvh<double, double, int>;\n"
+        "  (void)&ssdf::closest_within_radius_quads_bvh<float, float, int>;\n"
+        "  (void)&ssdf::closest_within_radius_quads_bvh<double, double, int>;\n"
+        "  (void)&ssdf::closest_within_radius_quads_local_bvh<float, float, int>;\n"
+        "  (void)&ssdf::closest_within_radius_quads_local_bvh<float, double, int>;\n"
+        "  (void)&ssdf::potential_contact_triangles_bvh<double, double, int, int>;\n"
+        "  (void)&ssdf::potential_contact_quads_bvh<float, float, int, int>;\n"
+        "  (void)&ssdf::sample_sdf_bvh<double, double, int>;\n"
+        "  (void)&ssdf::sample_sqedf_bvh<float, float, int>;\n"
         "  return 0;\n}\n")
     lib = os.path.join(ROOT, "ssdf_b200", "_lib")
     res = subprocess.run(["g++", "-std=c++17", f"-I{ROOT}/include", str(src), "-o", str(tmp_path / "use"),
