@@ -533,10 +533,10 @@ __device__ bool filter_bound(const float4 *__restrict__ rec, float *term) {
 // the key that set best. With the bound above both are at most u (18.1 d + 2 sqrt(3) M + term), so
 // tau_rel >= u (6.93 + 2 term / M) and tau_rel >= 36.2 u suffice (2^-9 added for best lying below
 // the winner's distance; the (1 + 2^-16) factor covers the rounding of the window itself). The
-// default 2^-16 = 256 u holds them
-// whenever term / M <= 124: for the torus-knot tube the term is about 0.1 M, for a 5,120-triangle
-// sphere 0.2 M; a mesh of a few large triangles gets a wider window. A mesh whose window would pass
-// 2^-8, or with a record the float filter cannot take, is answered by the FP64 kernel.
+// default 2^-16 = 256 u holds them whenever term / M <= 124: the torus-knot tube's largest term is 27.7 M (a triangle of aspect 7.2),
+// a 320-triangle sphere's 94 M; a mesh of a few large triangles gets a wider window. A mesh whose
+// window would pass 2^-8, or with a record the float filter cannot take, is answered by the FP64
+// kernel.
 void set_filter_window(DeviceMesh *m, float largest_term, bool records_safe) {
     const double u = 0x1p-24, M = double(m->coord_scale);
     double tau = 1.0 / 65536.0;
