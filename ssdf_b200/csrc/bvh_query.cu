@@ -56,6 +56,10 @@ constexpr int kCand = SSDF_B200_WINDOW_SLOTS;
 #define SSDF_B200_QUERY_MIN_BLOCKS 9
 #endif
 
+// The double kernel keeps 5 resident blocks per SM (at most 102 registers), its occupancy before the
+// seeded column walk added a few live values.
+constexpr int kF64MinBlocks = 5;
+
 struct Counters {
     unsigned long long tri = 0, box = 0, fix = 0;
 };
@@ -65,24 +69,25 @@ __device__ __forceinline__ float finf() { return __int_as_float(0x7f800000); }
 
 // ---- query mapping ------------------------------------------------------------------------------
 
-// Each lane answers kQ queries. Grid: a block covers 8 (x) x 4 (y) x 4 kQ (z) nodes and a warp
-// 4 x 4 x 2 kQ; lane (lx, ly, lz) takes kQ consecutive z nodes. Point lists: query
+// Each lane answers kQ queries. Grid: a block covers an 8 (x) x 8 (y) column of nodes and, at step
+// `step`, the 2 kQ z-planes from (column * kGridSteps + step) * 2 kQ on; a warp takes a 4 x 4 x 2kQ
+// brick of it, lane (lx, ly, lz) kQ consecutive z nodes. Point lists: query
 // (block * kQ + s) * 128 + thread, so each of a lane's queries is a coalesced load.
-__device__ __forceinline__ bool map_query(const QueryArgs &a, long long b, int s, long long &q, long long &i,
-                                          long long &j, long long &k) {
+__device__ __forceinline__ bool map_query(const QueryArgs &a, long long b, int step, int s, long long &q,
+                                          long long &i, long long &j, long long &k) {
     if (!a.is_grid) {
         const long long slot = (b * kQ + s) * kThreads + threadIdx.x;
         if (slot >= a.npoints) return false;
         q = a.order ? (long long)__ldg(a.order + slot) : slot;
         return true;
     }
-    const long long bxn = (a.nx + 7) >> 3, byn = (a.ny + 3) >> 2;
+    const long long bxn = grid_blocks_x(a.nx), byn = grid_blocks_y(a.ny);
     const long long bx = b % bxn, r = b / bxn;
     const long long by = r % byn, bz = r / byn;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     i = bx * 8 + (warp & 1) * 4 + (lane & 3);
-    j = by * 4 + ((lane >> 2) & 3);
-    k = (bz * 4 + (warp >> 1) * 2 + (lane >> 4)) * kQ + s;
+    j = by * 8 + (warp >> 1) * 4 + ((lane >> 2) & 3);
+    k = ((bz * kGridSteps + step) * 2 + (lane >> 4)) * kQ + s;
     q = i + a.nx * (j + a.ny * k);
     return i < a.nx && j < a.ny && k < a.nz;
 }
@@ -302,6 +307,18 @@ struct ExactPolicy {
         px[q] = py[q] = pz[q] = T(0), best[q] = T(0), bid[q] = -1, bpos[q] = -1;
         thr[q] = T(-1);
     }
+    // Starts query q from the triangle at leaf position pos, as if the walk had tested it first (it
+    // replaces the incoming bound only when strictly closer; the walk meets it again without effect).
+    __device__ __forceinline__ void seed(int q, int pos) {
+        const auto t = ExactData<T>::tri(m, pos);
+        const T d2 = tri_dist_sq_exact<T>(px[q], py[q], pz[q], t.ax, t.ay, t.az, t.bx, t.by, t.bz, t.cx, t.cy, t.cz);
+        if (d2 < best[q]) {
+            best[q] = d2;
+            bid[q] = t.id;
+            bpos[q] = pos;
+            thr[q] = best[q] * ExactData<T>::rel + margin;
+        }
+    }
     __device__ __forceinline__ void boxes(int node, T (&d0)[Q], T (&d1)[Q], int &r0, int &r1) const {
         const auto n = ExactData<T>::node(m, node);
 #pragma unroll
@@ -389,6 +406,18 @@ struct FastPolicy {
     __device__ __forceinline__ void disable(int q) {
         set(q, 0.f, 0.f, 0.f, finf());
         thr[q] = -1.f;
+    }
+    // Starts query q's window from the key of the triangle at leaf position pos (not a proxy), as the
+    // walk would on meeting it: best is then still the key of a tested triangle, and the walk inserts
+    // the triangle when it meets it.
+    __device__ __forceinline__ void seed(int q, int pos) {
+        const FiltRec t = load_filt(m.filt32, pos);
+        const float pen = __ldg(m.filt32 + 4 * pos + 3).y;
+        const float d2 = tri_dist_sq_filter(px[q], py[q], pz[q], t);
+        if (pen == 0.f && d2 < best[q]) {
+            best[q] = d2;
+            thr[q] = window_thr(best[q], tau_rel, m.coord_scale);
+        }
     }
     // the walk stops early: every live query goes to the second stage with its current window
     __device__ __forceinline__ void abandon() {
@@ -891,21 +920,17 @@ __device__ __forceinline__ void signal_chunk(const QueryArgs &a) {
     }
 }
 
-// One block of 128 lanes x kQ queries. Lanes without a query (the edge of a grid brick, the tail of
-// a point list) take part in warp-mode traversal with a negative threshold, so they never ask for
-// a node.
+// One block of 128 lanes x kQ queries: a point-list block, or one step of a grid block's column.
+// Lanes without a query (the edge of a grid brick, the tail of a point list) take part in warp-mode
+// traversal with a negative threshold, so they never ask for a node. seed[s] is the leaf position of
+// the closest triangle the lane's query s found one step below (-1: none); it is updated here.
 template <int PREC, bool WARP, bool WIDE, bool COUNT, bool BUDGET>
-__device__ __forceinline__ void query_block(const QueryArgs &a, long long block, Counters &cnt) {
+__device__ __forceinline__ void query_step(const QueryArgs &a, int step, const bool (&valid)[kQ],
+                                           const long long (&qid)[kQ], const long long (&gi)[kQ],
+                                           const long long (&gj)[kQ], const long long (&gk)[kQ], bool any,
+                                           int (&seed)[kQ], Counters &cnt) {
     constexpr int Q = kQ;
-    long long qid[Q], gi[Q], gj[Q], gk[Q];
-    bool valid[Q];
-    bool any = false;
-#pragma unroll
-    for (int s = 0; s < Q; s++) {
-        gi[s] = gj[s] = gk[s] = 0;
-        valid[s] = map_query(a, block, s, qid[s], gi[s], gj[s], gk[s]);
-        any |= valid[s];
-    }
+    const bool seeded = a.seed != 0 && step > 0;
     if (PREC == SSDF_PREC_F64) {
         ExactPolicy<double, Q> p(a.m);
 #pragma unroll
@@ -914,14 +939,18 @@ __device__ __forceinline__ void query_block(const QueryArgs &a, long long block,
                 double x, y, z;
                 query_point(a, qid[s], gi[s], gj[s], gk[s], x, y, z);
                 p.set(s, x, y, z, initial_bound(a, qid[s]));
+                if (seeded && seed[s] >= 0) p.seed(s, seed[s]);
             } else {
                 p.disable(s);
             }
         }
         if (WARP || any) walk<WARP, WIDE, COUNT>(p, cnt);
 #pragma unroll
-        for (int s = 0; s < Q; s++)
-            if (valid[s]) write_result(a, qid[s], p.px[s], p.py[s], p.pz[s], p.best[s], p.bid[s], p.bpos[s]);
+        for (int s = 0; s < Q; s++) {
+            if (!valid[s]) continue;
+            write_result(a, qid[s], p.px[s], p.py[s], p.pz[s], p.best[s], p.bid[s], p.bpos[s]);
+            if (p.bpos[s] >= 0) seed[s] = p.bpos[s];
+        }
     } else if (PREC == SSDF_PREC_F32) {
         // the reference's float arithmetic end to end (edf<float>'s value); edf and sqedf outputs
         ExactPolicy<float, Q> p(a.m);
@@ -933,6 +962,7 @@ __device__ __forceinline__ void query_block(const QueryArgs &a, long long block,
                 const long long q = qid[s];
                 const float o = a.out_f64 ? float(((const double *)a.out)[q]) : ((const float *)a.out)[q];
                 p.set(s, float(x), float(y), float(z), a.output == SSDF_OUT_SQEDF ? o : o * o);
+                if (seeded && seed[s] >= 0) p.seed(s, seed[s]);
             } else {
                 p.disable(s);
             }
@@ -948,6 +978,7 @@ __device__ __forceinline__ void query_block(const QueryArgs &a, long long block,
                 store_out(a, q, double(sqrtf(p.best[s])));
                 if (a.outtri && p.bid[s] >= 0) a.outtri[q] = p.bid[s];
             }
+            if (p.bpos[s] >= 0) seed[s] = p.bpos[s];
         }
     } else {
         __shared__ float s_wd[kQ * kCand * kThreads];
@@ -965,10 +996,12 @@ __device__ __forceinline__ void query_block(const QueryArgs &a, long long block,
                            ax < dinf() && ay < dinf() && az < dinf();
                 const double init = initial_bound(a, qid[s]);
                 // float start bound rounded up, so no triangle closer in double is cut off
-                if (exact[s])
+                if (exact[s]) {
                     p.disable(s);
-                else
+                } else {
                     p.set(s, float(x), float(y), float(z), init < dinf() ? __double2float_ru(init) : finf());
+                    if (seeded && seed[s] >= 0) p.seed(s, seed[s]);
+                }
             } else {
                 p.disable(s);
             }
@@ -1005,7 +1038,32 @@ __device__ __forceinline__ void query_block(const QueryArgs &a, long long block,
                 }
             }
             write_result(a, q, rx, ry, rz, b, bid, bpos);
+            if (bpos >= 0) seed[s] = bpos;
         }
+    }
+}
+
+// A point-list block, or a grid block's column step by step (each step seeded from the one below).
+template <int PREC, bool WARP, bool WIDE, bool COUNT, bool BUDGET>
+__device__ __forceinline__ void query_block(const QueryArgs &a, long long block, Counters &cnt) {
+    constexpr int Q = kQ;
+    int seed[Q];
+#pragma unroll
+    for (int s = 0; s < Q; s++) seed[s] = -1;
+    const int steps = a.is_grid ? kGridSteps : 1;
+    for (int step = 0; step < steps; step++) {
+        long long qid[Q], gi[Q], gj[Q], gk[Q];
+        bool valid[Q];
+        bool any = false;
+#pragma unroll
+        for (int s = 0; s < Q; s++) {
+            gi[s] = gj[s] = gk[s] = 0;
+            valid[s] = map_query(a, block, step, s, qid[s], gi[s], gj[s], gk[s]);
+            any |= valid[s];
+        }
+        // the column has left the grid (block-uniform: higher steps have no node either)
+        if (step > 0 && !__syncthreads_or(any)) break;
+        query_step<PREC, WARP, WIDE, COUNT, BUDGET>(a, step, valid, qid, gi, gj, gk, any, seed, cnt);
     }
 }
 
@@ -1015,7 +1073,7 @@ __device__ __forceinline__ void query_block(const QueryArgs &a, long long block,
 // (a separate instantiation: the dormant signal code cost the fix-up kernel 3 % where it was merely
 // compiled in).
 template <int PREC, bool WARP, bool WIDE, bool COUNT, bool BUDGET = false, bool SIGNAL = false>
-__global__ void __launch_bounds__(kThreads, PREC == SSDF_PREC_F64 ? 1 : SSDF_B200_QUERY_MIN_BLOCKS)
+__global__ void __launch_bounds__(kThreads, PREC == SSDF_PREC_F64 ? kF64MinBlocks : SSDF_B200_QUERY_MIN_BLOCKS)
     k_query(const QueryArgs a) {
     Counters cnt;
     query_block<PREC, WARP, WIDE, COUNT, BUDGET>(a, blockIdx.x, cnt);
@@ -1176,7 +1234,7 @@ __global__ void __launch_bounds__(kThreads) k_window(const QueryArgs a, int cap)
 // 128-query block of one job) from an atomic counter, largest jobs first (the host orders them).
 
 template <int PREC, bool WARP, bool WIDE, bool COUNT, bool BUDGET = false>
-__global__ void __launch_bounds__(kThreads, PREC == SSDF_PREC_F64 ? 1 : SSDF_B200_QUERY_MIN_BLOCKS)
+__global__ void __launch_bounds__(kThreads, PREC == SSDF_PREC_F64 ? kF64MinBlocks : SSDF_B200_QUERY_MIN_BLOCKS)
     k_query_batch(const BatchHeader *__restrict__ hdr, const QueryArgs *__restrict__ jobs,
                   const long long *__restrict__ first_block, unsigned long long *__restrict__ next_item) {
     __shared__ long long s_item;

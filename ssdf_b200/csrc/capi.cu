@@ -696,6 +696,7 @@ static int fill_query(const ssdf_mesh *mesh, const ssdf_query_opts *opts, QueryA
     // the mesh's own minimum (wider for meshes of a few large triangles); the environment may only widen it
     a->tau_rel = std::max(tau_rel_from_env(), mesh->m.tau_rel_min);
     a->warp_budget = env_int("SSDF_B200_WARP_BUDGET", -1);
+    a->seed = env_int("SSDF_B200_SEED", 1) != 0 ? 1 : 0;
     return SSDF_OK;
 }
 

@@ -144,6 +144,8 @@ struct QueryArgs {
     int *chunk_counts;
     int *chunk_flags;
     int chunk_blocks;
+    // grid launches: start each step of a block's column from the triangles found one step below
+    int seed;
 };
 
 // Job table header of a batch (device memory).
@@ -209,10 +211,22 @@ bool default_wide();
 #define SSDF_B200_QUERIES_PER_LANE 1
 #endif
 constexpr int kQ = SSDF_B200_QUERIES_PER_LANE;
-// Blocks of 128 lanes x kQ queries one job needs (grid bricks of 8 x 4 x 4kQ nodes, or 128 kQ
+// Grid launches: a block of 128 lanes covers an 8 x 8 column of nodes and walks it upwards in
+// kGridSteps steps of 2 kQ z-planes (each warp a 4 x 4 x 2kQ brick per step). A lane starts each
+// step from the closest triangle it found one step below, 2 kQ nodes away: a tight upper bound
+// (SSDF_B200_SEED=0 starts from the incoming bound alone).
+#ifndef SSDF_B200_GRID_STEPS
+#define SSDF_B200_GRID_STEPS 4
+#endif
+constexpr int kGridSteps = SSDF_B200_GRID_STEPS;
+constexpr long long kGridBlockPlanes = 2ll * kQ * kGridSteps;  // z-planes of one grid block
+__host__ __device__ inline long long grid_blocks_x(long long nx) { return (nx + 7) / 8; }
+__host__ __device__ inline long long grid_blocks_y(long long ny) { return (ny + 7) / 8; }
+__host__ __device__ inline long long grid_blocks_z(long long nz) { return (nz + kGridBlockPlanes - 1) / kGridBlockPlanes; }
+// Blocks of 128 lanes one job needs (grid columns as above, x fastest, then y, then z; or 128 kQ
 // consecutive points).
 inline long long query_blocks(const QueryArgs &a) {
-    if (a.is_grid) return ((a.nx + 7) / 8) * ((a.ny + 3) / 4) * ((a.nz + 4 * kQ - 1) / (4 * kQ));
+    if (a.is_grid) return grid_blocks_x(a.nx) * grid_blocks_y(a.ny) * grid_blocks_z(a.nz);
     return (a.npoints + 128 * kQ - 1) / (128 * kQ);
 }
 
