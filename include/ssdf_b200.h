@@ -423,6 +423,13 @@ int ssdf_mesh_filter_info(const ssdf_mesh *mesh, float *tau_rel, int *float_filt
  * except for SSDF_OUT_CLOSEST. Asynchronous on `stream`. */
 int ssdf_query_points(ssdf_mesh *mesh, ptrdiff_t npoints, const void *x, const void *y, const void *z, void *out,
                       int *outtri, void *outx, void *outy, void *outz, const ssdf_query_opts *opts, void *stream);
+/* ssdf::edf / ssdf::edf_celllist (serial/ssdf.hpp:447-619, 642-963) on device arrays: method 0 the
+ * brute force (edf), 1 the cell list (edf_celllist); points, vertices and out all of coord_type
+ * (G == T, as the reference instantiates them), out in/out; outtri (the closest triangle) may be
+ * NULL. Enqueued on `stream`; returns when the query has finished (it reads back a validation flag). */
+int ssdf_edf_device(int method, ptrdiff_t npoints, const void *x, const void *y, const void *z, ptrdiff_t nselements,
+                    const int *s0, const int *s1, const int *s2, ptrdiff_t nspoints, const void *sx, const void *sy,
+                    const void *sz, int coord_type, void *out, int *outtri, void *stream);
 /* Query at the node grid nx*ny*nz over [lo, hi] (ssdf's convention, G = coord_type precision). */
 int ssdf_query_grid(ssdf_mesh *mesh, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, const double lo[3],
                     const double hi[3], void *out, int *outtri, const ssdf_query_opts *opts, void *stream);

@@ -90,6 +90,7 @@ _sig("ssdf_mesh_destroy", [_vp])
 _sig("ssdf_mesh_destroy_async", [_vp, _vp])
 _sig("ssdf_mesh_stats", [_vp] + [C.POINTER(C.c_int64)] * 4)
 _sig("ssdf_mesh_filter_info", [_vp, C.POINTER(C.c_float), C.POINTER(C.c_int), C.POINTER(C.c_int64)])
+_sig("ssdf_edf_device", [C.c_int, _pd, _vp, _vp, _vp, _pd, _vp, _vp, _vp, _pd, _vp, _vp, _vp, C.c_int, _vp, _vp, _vp])
 _sig("ssdf_query_points", [_vp, _pd, _vp, _vp, _vp, _vp, _ip, _vp, _vp, _vp, C.POINTER(QueryOpts), _vp])
 _sig("ssdf_query_grid", [_vp, _pd, _pd, _pd, C.POINTER(C.c_double * 3), C.POINTER(C.c_double * 3), _vp, _ip,
                          C.POINTER(QueryOpts), _vp])
@@ -174,7 +175,7 @@ EXPORTED = ["ssdf_status_string", "ssdf_last_error", "ssdf_b200_version", "ssdf_
             "ssdf_b200_closest_point_bvh_fd", "ssdf_b200_closest_point_bvh_dd", "ssdf_b200_sample_sqedf_bvh_ff", "ssdf_b200_sample_sqedf_bvh_dd",
             "ssdf_b200_sample_sdf_bvh_ff", "ssdf_b200_sample_sdf_bvh_dd", "ssdf_b200_edf_index_dd",
             "ssdf_b200_edf_index_ff", "ssdf_b200_sdf_points_dd", "ssdf_b200_sample_sdf_index_bvh_dd",
-            "ssdf_mesh_create", "ssdf_mesh_destroy", "ssdf_mesh_stats", "ssdf_mesh_filter_info", "ssdf_query_points", "ssdf_query_grid",
+            "ssdf_mesh_create", "ssdf_mesh_destroy", "ssdf_mesh_stats", "ssdf_mesh_filter_info", "ssdf_edf_device", "ssdf_query_points", "ssdf_query_grid",
             "ssdf_last_query_counts", "ssdf_b200_fma_peak", "ssdf_batch_create", "ssdf_batch_destroy", "ssdf_batch_clear",
             "ssdf_batch_size", "ssdf_batch_add_grid", "ssdf_batch_add_points", "ssdf_batch_run",
             "ssdf_batch_last_blocks", "ssdf_query_grid_noalloc", "ssdf_query_grid_noalloc_max", "ssdf_server_create",
@@ -272,6 +273,18 @@ def edf_celllist(points, mesh, out=None, dtype=np.float64):
     """ssdf::edf_celllist<G, G, int>: GPU cell list, bitwise the reference's value."""
     s = _suffix(dtype)
     return _edf_call(f"ssdf_b200_edf_celllist_{s}{s}", points, mesh, out, dtype, dtype)
+
+
+def edf_device(method, x, y, z, s0, s1, s2, sx, sy, sz, out, outtri=None, stream=None):
+    """ssdf_edf_device: edf (method 0, brute force) or edf_celllist (1) on torch CUDA tensors; points,
+    vertices and out of one float type, out in/out; returns when the query is done."""
+    import torch
+
+    ct = F64 if out.dtype == torch.float64 else F32
+    _check(lib.ssdf_edf_device(int(method), x.numel(), _dptr(x), _dptr(y), _dptr(z), s0.numel(), _dptr(s0), _dptr(s1),
+                               _dptr(s2), sx.numel(), _dptr(sx), _dptr(sy), _dptr(sz), ct, _dptr(out),
+                               _dptr(outtri) if outtri is not None else None, _stream_handle(stream)),
+           "ssdf_edf_device")
 
 
 def edf_bvh(points, mesh, out=None, gdtype=np.float64, tdtype=None):

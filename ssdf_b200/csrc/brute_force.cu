@@ -76,13 +76,16 @@ __device__ __forceinline__ float abs_margin<float>(float scale) {
 }
 
 // One thread per point; triangle tiles of TILE records double-buffered in shared memory.
-template <typename T, int TILE>
+// COUNT: the counting instantiation (box and Ericson tests into counters[0..1]).
+template <typename T, int TILE, bool COUNT>
 __global__ void __launch_bounds__(kBruteThreads) k_brute_tile(int npoints, const T *__restrict__ x,
                                                               const T *__restrict__ y, const T *__restrict__ z,
                                                               int nt, const T *__restrict__ rec, T *__restrict__ out,
                                                               int *__restrict__ outtri,
                                                               const int *__restrict__ scale_bits,
-                                                              int *__restrict__ err) {
+                                                              int *__restrict__ err,
+                                                              unsigned long long *__restrict__ counters) {
+    unsigned long long n_tri = 0, n_box = 0;
     // The kernel has no static shared memory, so the dynamic window starts at the CTA's shared
     // base: two mbarriers in its first 16 bytes, tile buffers from byte 128 (TMA needs 16).
     extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -132,8 +135,10 @@ __global__ void __launch_bounds__(kBruteThreads) k_brute_tile(int npoints, const
             const T *r = tile + kRec * k;
             const T db = box_dist_sq<T>(px, py, pz, r[9], r[10], r[11], r[12], r[13], r[14]);
             const bool want = valid && db < thr;
+            if (COUNT) n_box += valid ? 1 : 0;
             if (!__any_sync(0xffffffffu, want)) continue;
             if (want) {
+                if (COUNT) n_tri++;
                 const T d2 = tri_dist_sq_exact<T>(px, py, pz, r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7], r[8]);
                 if (d2 < best) {
                     best = d2;
@@ -158,15 +163,18 @@ __global__ void __launch_bounds__(kBruteThreads) k_brute_tile(int npoints, const
         out[p] = sqrt(best);
         if (outtri && bid >= 0) outtri[p] = bid;
     }
+    if (COUNT) flush_pair_counts(counters, n_tri, n_box);
 }
 
 // One warp per point: lanes take triangles lane, lane + 32, ...; shuffle-reduced lexicographic min.
-template <typename T>
+template <typename T, bool COUNT>
 __global__ void __launch_bounds__(kBruteThreads) k_brute_warp(int npoints, const T *__restrict__ x,
                                                               const T *__restrict__ y, const T *__restrict__ z,
                                                               int nt, const T *__restrict__ rec, T *__restrict__ out,
                                                               int *__restrict__ outtri,
-                                                              const int *__restrict__ scale_bits) {
+                                                              const int *__restrict__ scale_bits,
+                                                              unsigned long long *__restrict__ counters) {
+    unsigned long long n_tri = 0, n_box = 0;
     const int warp = (blockIdx.x * kBruteThreads + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= npoints) return;
@@ -181,7 +189,9 @@ __global__ void __launch_bounds__(kBruteThreads) k_brute_warp(int npoints, const
         const T *r = rec + size_t(kRec) * t;
         const T db = box_dist_sq<T>(px, py, pz, __ldg(r + 9), __ldg(r + 10), __ldg(r + 11), __ldg(r + 12),
                                     __ldg(r + 13), __ldg(r + 14));
+        if (COUNT) n_box++;
         if (!(db < thr)) continue;
+        if (COUNT) n_tri++;
         const T d2 = tri_dist_sq_exact<T>(px, py, pz, __ldg(r), __ldg(r + 1), __ldg(r + 2), __ldg(r + 3),
                                           __ldg(r + 4), __ldg(r + 5), __ldg(r + 6), __ldg(r + 7), __ldg(r + 8));
         if (d2 < best) {
@@ -203,6 +213,7 @@ __global__ void __launch_bounds__(kBruteThreads) k_brute_warp(int npoints, const
         out[warp] = sqrt(best);
         if (outtri && bid >= 0) outtri[warp] = bid;
     }
+    if (COUNT) flush_pair_counts(counters, n_tri, n_box);
 }
 
 template <typename T>
@@ -227,23 +238,39 @@ int brute_impl(ptrdiff_t npoints, const T *x, const T *y, const T *z, ptrdiff_t 
                                                                      flags, flags + 2);
         e = cudaGetLastError();
     }
+    const bool count = env_int("SSDF_B200_COUNT", 0) != 0;
+    unsigned long long *counters = nullptr, hc[2] = {0, 0};
+    if (e == cudaSuccess && count) {
+        e = cudaMallocAsync(&counters, 2 * sizeof(unsigned long long), stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), stream);
+    }
     if (e == cudaSuccess) {
         if (npoints < 148 * 64) {
             const long long threads = (long long)npoints * 32;
-            k_brute_warp<T><<<grid_blocks(threads, kBruteThreads), kBruteThreads, 0, stream>>>(
-                int(npoints), x, y, z, int(nt), rec, out, outtri, flags + 2);
+            if (count)
+                k_brute_warp<T, true><<<grid_blocks(threads, kBruteThreads), kBruteThreads, 0, stream>>>(
+                    int(npoints), x, y, z, int(nt), rec, out, outtri, flags + 2, counters);
+            else
+                k_brute_warp<T, false><<<grid_blocks(threads, kBruteThreads), kBruteThreads, 0, stream>>>(
+                    int(npoints), x, y, z, int(nt), rec, out, outtri, flags + 2, counters);
         } else {
             const size_t smem = 128 + 2 * size_t(TILE) * kRec * sizeof(T);
-            e = cudaFuncSetAttribute(k_brute_tile<T, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            auto kern = count ? k_brute_tile<T, TILE, true> : k_brute_tile<T, TILE, false>;
+            e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
             if (e == cudaSuccess)
-                k_brute_tile<T, TILE><<<grid_blocks(npoints, kBruteThreads), kBruteThreads, smem, stream>>>(
-                    int(npoints), x, y, z, int(nt), rec, out, outtri, flags + 2, flags);
+                kern<<<grid_blocks(npoints, kBruteThreads), kBruteThreads, smem, stream>>>(
+                    int(npoints), x, y, z, int(nt), rec, out, outtri, flags + 2, flags, counters);
         }
         if (e == cudaSuccess) e = cudaGetLastError();
     }
     int h[4] = {0x7fffffff, 0, 0, 0};
     if (e == cudaSuccess) e = cudaMemcpyAsync(h, flags, sizeof(h), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess && counters) e = cudaMemcpyAsync(hc, counters, sizeof(hc), cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (counters) {
+        cudaFreeAsync(counters, stream);
+        if (e == cudaSuccess) set_last_counts(hc[0], hc[1], 0, 0);
+    }
     if (e != cudaSuccess) st = cuda_fail(e, "brute-force edf", __FILE__, __LINE__);
     else if (h[0] != 0x7fffffff)
         st = fail(SSDF_ERR_INVALID_ARGUMENT, "triangle " + std::to_string(h[0]) + " has a vertex index out of range");

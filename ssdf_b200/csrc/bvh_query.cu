@@ -1364,6 +1364,11 @@ cudaError_t launch_prec(const QueryArgs &a, bool warp, bool wide, bool count, un
 
 }  // namespace
 
+void set_last_counts(unsigned long long tri, unsigned long long box, unsigned long long fix,
+                     unsigned long long fallback) {
+    t_last_counts[0] = tri, t_last_counts[1] = box, t_last_counts[2] = fix, t_last_counts[3] = fallback;
+}
+
 int query_counts(int64_t *tri, int64_t *box, int64_t *fix, int64_t *fallback) {
     if (tri) *tri = (int64_t)t_last_counts[0];
     if (box) *box = (int64_t)t_last_counts[1];

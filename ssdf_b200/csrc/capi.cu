@@ -740,6 +740,21 @@ int fill_grid_args(ssdf_mesh *mesh, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, co
 
 extern "C" {
 
+int ssdf_edf_device(int method, ptrdiff_t npoints, const void *x, const void *y, const void *z, ptrdiff_t nselements,
+                    const int *s0, const int *s1, const int *s2, ptrdiff_t nspoints, const void *sx, const void *sy,
+                    const void *sz, int coord_type, void *out, int *outtri, void *stream) {
+    if (method != 0 && method != 1) return fail(SSDF_ERR_INVALID_ARGUMENT, "ssdf_edf_device: method 0 (edf) or 1 (celllist)");
+    if (coord_type != SSDF_F32 && coord_type != SSDF_F64) return fail(SSDF_ERR_INVALID_ARGUMENT, "bad coord_type");
+    if (npoints < 0 || nselements < 0 || nspoints < 0) return fail(SSDF_ERR_INVALID_ARGUMENT, "negative size");
+    if (npoints == 0 || nselements == 0 || nspoints == 0) return SSDF_OK;
+    if (!x || !y || !z || !out || !s0 || !s1 || !s2 || !sx || !sy || !sz)
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "null array");
+    const int f64 = coord_type == SSDF_F64;
+    const cudaStream_t st = (cudaStream_t)stream;
+    return method == 0 ? brute_force_edf(f64, npoints, x, y, z, nselements, s0, s1, s2, nspoints, sx, sy, sz, out, outtri, st)
+                       : celllist_edf(f64, npoints, x, y, z, nselements, s0, s1, s2, nspoints, sx, sy, sz, out, outtri, st);
+}
+
 int ssdf_query_points(ssdf_mesh *mesh, ptrdiff_t npoints, const void *x, const void *y, const void *z, void *out,
                       int *outtri, void *outx, void *outy, void *outz, const ssdf_query_opts *opts, void *stream) {
     QueryArgs a;

@@ -170,15 +170,19 @@ __device__ __forceinline__ float cl_abs_margin<float>(float scale) {
     return s * s;
 }
 
-template <typename T>
+// COUNT: the counting instantiation (Ericson tests, and box tests of cells and triangles, into
+// counters[0..1]).
+template <typename T, bool COUNT>
 __global__ void __launch_bounds__(128) k_cl_query(int npoints, const T *__restrict__ x, const T *__restrict__ y,
                                                   const T *__restrict__ z, CellGrid g, float scale,
                                                   const int *__restrict__ cell_start, const int *__restrict__ cell_end,
                                                   const T *__restrict__ cbox, const T *__restrict__ rec,
                                                   const int *__restrict__ rid, const float *__restrict__ smin, const float *__restrict__ smax,
-                                                  T *__restrict__ out, int *__restrict__ outtri) {
+                                                  T *__restrict__ out, int *__restrict__ outtri,
+                                                  unsigned long long *__restrict__ counters) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= npoints) return;
+    unsigned long long n_tri = 0, n_box = 0;
     const T px = x[q], py = y[q], pz = z[q];
     const T o = out[q];
     T best = o * o;
@@ -219,6 +223,7 @@ __global__ void __launch_bounds__(128) k_cl_query(int npoints, const T *__restri
             const int b = __ldg(cell_start + c), e = __ldg(cell_end + c);
             if (e <= b) continue;
             const T *cb = cbox + 6 * c;
+            if (COUNT) n_box++;
             if (!(box_dist_sq<T>(px, py, pz, __ldg(cb), __ldg(cb + 1), __ldg(cb + 2), __ldg(cb + 3), __ldg(cb + 4),
                                  __ldg(cb + 5)) < thr))
                 continue;
@@ -230,9 +235,11 @@ __global__ void __launch_bounds__(128) k_cl_query(int npoints, const T *__restri
             }
             auto eval = [&](int p) {
                 const T *rr = rec + size_t(kRec) * p;
+                if (COUNT) n_box++;
                 if (!(box_dist_sq<T>(px, py, pz, __ldg(rr + 9), __ldg(rr + 10), __ldg(rr + 11), __ldg(rr + 12),
                                      __ldg(rr + 13), __ldg(rr + 14)) < thr))
                     return;
+                if (COUNT) n_tri++;
                 const T d2 = tri_dist_sq_exact<T>(px, py, pz, __ldg(rr), __ldg(rr + 1), __ldg(rr + 2), __ldg(rr + 3),
                                                   __ldg(rr + 4), __ldg(rr + 5), __ldg(rr + 6), __ldg(rr + 7),
                                                   __ldg(rr + 8));
@@ -257,6 +264,10 @@ __global__ void __launch_bounds__(128) k_cl_query(int npoints, const T *__restri
     }
     out[q] = sqrt(best);
     if (outtri && bid >= 0) outtri[q] = bid;
+    if (COUNT) {  // untimed: one atomic per thread (the last warp may be partial)
+        atomicAdd(counters, n_tri);
+        atomicAdd(counters + 1, n_box);
+    }
 }
 
 int bits_for(unsigned long long v) {
@@ -301,6 +312,7 @@ int celllist_impl(ptrdiff_t npoints, const T *x, const T *y, const T *z, ptrdiff
     hred[6] = enc(0.0);
     hred[7] = 0;
     const int herr[4] = {0x7fffffff, 0, 0, 0};
+    unsigned long long *counters = nullptr;  // the counting instantiation's (SSDF_B200_COUNT)
     cudaError_t e = cudaMemcpyAsync(red, hred, sizeof(hred), cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(err, herr, sizeof(herr), cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) {
@@ -374,11 +386,31 @@ int celllist_impl(ptrdiff_t npoints, const T *x, const T *y, const T *z, ptrdiff
         k_cl_cells<T><<<grid_blocks(ncells, 128), 128, 0, stream>>>(int(ncells), cstart, cend, rec, smax, cbox);
         const double scale = std::max({std::fabs(gmin[0]), std::fabs(gmin[1]), std::fabs(gmin[2]),
                                        std::fabs(gmax[0]), std::fabs(gmax[1]), std::fabs(gmax[2])});
-        k_cl_query<T><<<grid_blocks(npoints, 128), 128, 0, stream>>>(int(npoints), x, y, z, g, float(scale), cstart,
-                                                                    cend, cbox, rec, rid, smin, smax, out, outtri);
-        e = cudaGetLastError();
+        const bool count = env_int("SSDF_B200_COUNT", 0) != 0;
+        if (count) {
+            e = cudaMallocAsync(&counters, 2 * sizeof(unsigned long long), stream);
+            if (e == cudaSuccess) e = cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), stream);
+        }
+        if (e == cudaSuccess) {
+            if (count)
+                k_cl_query<T, true><<<grid_blocks(npoints, 128), 128, 0, stream>>>(
+                    int(npoints), x, y, z, g, float(scale), cstart, cend, cbox, rec, rid, smin, smax, out, outtri,
+                    counters);
+            else
+                k_cl_query<T, false><<<grid_blocks(npoints, 128), 128, 0, stream>>>(
+                    int(npoints), x, y, z, g, float(scale), cstart, cend, cbox, rec, rid, smin, smax, out, outtri,
+                    counters);
+            e = cudaGetLastError();
+        }
     }
+    unsigned long long hc[2] = {0, 0};
+    if (e == cudaSuccess && st == SSDF_OK && counters)
+        e = cudaMemcpyAsync(hc, counters, sizeof(hc), cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess && st == SSDF_OK) e = cudaStreamSynchronize(stream);
+    if (counters) {
+        cudaFreeAsync(counters, stream);
+        if (e == cudaSuccess && st == SSDF_OK) set_last_counts(hc[0], hc[1], 0, 0);
+    }
     if (e != cudaSuccess && st == SSDF_OK) st = cuda_fail(e, "cell list edf", __FILE__, __LINE__);
     release();
     return st;

@@ -230,7 +230,26 @@ inline long long query_blocks(const QueryArgs &a) {
     return (a.npoints + 128 * kQ - 1) / (128 * kQ);
 }
 
+// The counts ssdf_last_query_counts reports for this thread's last counting launch (bvh_query.cu).
+void set_last_counts(unsigned long long tri, unsigned long long box, unsigned long long fix,
+                     unsigned long long fallback);
+// Warp-summed, one 64-bit atomic per warp: counts of a counting launch (c[0] triangle tests, c[1]
+// box tests). Every lane of the warp must call it.
+__device__ __forceinline__ void flush_pair_counts(unsigned long long *c, unsigned long long tri,
+                                                  unsigned long long box) {
+    for (int o = 16; o > 0; o >>= 1) {
+        tri += __shfl_xor_sync(0xffffffffu, tri, o);
+        box += __shfl_xor_sync(0xffffffffu, box, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(c, tri);
+        atomicAdd(c + 1, box);
+    }
+}
+
 // ---- brute force and cell list (brute_force.cu, celllist.cu) -------------------------------------
+// With SSDF_B200_COUNT set, both run a counting instantiation and leave their triangle (Ericson)
+// and box tests in ssdf_last_query_counts.
 int brute_force_edf(int f64, ptrdiff_t npoints, const void *x, const void *y, const void *z, ptrdiff_t nt,
                     const int *s0, const int *s1, const int *s2, ptrdiff_t nv, const void *sx, const void *sy,
                     const void *sz, void *out, int *outtri, cudaStream_t stream);

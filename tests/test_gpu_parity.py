@@ -206,3 +206,41 @@ def test_traversal_modes(mode, arity, knot):
             assert np.array_equal(gsd[knot["ids"]], knot["sd"]), prec
             assert np.array_equal(gtri[knot["ids"]], knot["stri"]), prec
     assert np.array_equal(sd, knot["sd"]) and np.array_equal(tri, knot["stri"])
+
+
+@pytest.mark.parametrize("method", [0, 1])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_edf_device_arrays(method, dtype):
+    """ssdf_edf_device (edf / edf_celllist on device arrays) equals the host-array entry points bit for
+    bit, closest triangle included; its counting launch reports its box and Ericson tests."""
+    import os
+
+    import torch
+
+    mesh = W.icosphere(3)
+    lo, hi = mesh.bbox()
+    pts = W.uniform_points(30011, lo - 0.3, hi + 0.3, seed=41).astype(dtype)
+    tdt = torch.float64 if dtype == np.float64 else torch.float32
+    want = (S.edf if method == 0 else S.edf_celllist)(pts, mesh, dtype=dtype)
+    x, y, z = (torch.tensor(np.ascontiguousarray(a), device="cuda") for a in pts)
+    sx, sy, sz = (torch.tensor(np.ascontiguousarray(a, dtype=dtype), device="cuda") for a in mesh.coords())
+    s0, s1, s2 = (torch.tensor(np.ascontiguousarray(a, dtype=np.int32), device="cuda") for a in mesh.indices())
+    out = torch.full((len(x),), float(np.finfo(dtype).max), dtype=tdt, device="cuda")
+    tri = torch.full((len(x),), -1, dtype=torch.int32, device="cuda")
+    os.environ["SSDF_B200_COUNT"] = "1"
+    try:
+        S.edf_device(method, x, y, z, s0, s1, s2, sx, sy, sz, out, tri)
+        counts = S.last_query_counts()
+    finally:
+        del os.environ["SSDF_B200_COUNT"]
+    assert np.array_equal(out.cpu().numpy(), want)
+    wtri = oracle.edf(pts[:, ::97].astype(np.float64), W.Mesh(mesh.vertices.astype(dtype).astype(np.float64),
+                                                                mesh.triangles), with_index=True)[1]
+    if dtype == np.float64:
+        assert np.array_equal(tri.cpu().numpy()[::97], wtri)
+    assert counts["triangle_tests"] >= len(x) and counts["box_tests"] >= counts["triangle_tests"]
+    if method == 0:
+        assert counts["box_tests"] == len(x) * mesh.nt  # the brute force box-tests every pair
+    out2 = torch.full((len(x),), float(np.finfo(dtype).max), dtype=tdt, device="cuda")
+    S.edf_device(method, x, y, z, s0, s1, s2, sx, sy, sz, out2)
+    assert torch.equal(out, out2)
