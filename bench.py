@@ -15,7 +15,14 @@ computed with the FP32 traversal + FP64 fix-up kernel. Synthetic, seeded inputs 
 * ``roofline``: the query kernel against the measured FP32 FMA peak of this GPU (the path is
   FP32-pipe bound; its HBM traffic is the output stream), flops counted by an instrumented launch;
 * ``cpu_baseline``: the reference's own OpenMP ``edf_celllist<double>`` (compiled from its sources
-  into oracle/_ref) on a seeded sample of the same grid nodes, all host threads.
+  into oracle/_ref) on a seeded sample of the same grid nodes, all host threads;
+* ``error``: the fix-up result against the plain FP64 one at every node (distance bits and closest
+  triangle), and, in the cpu_baseline leg, max / RMS error against the reference's FP64 distance on its
+  sample and value / sign / index mismatches against the oracle's signed distance on part of it;
+* ``e2e_pageable``: ``e2e`` into ordinary (pageable) host memory, as the reference's drivers allocate;
+* ``dense`` (``--workload icosphere``): the GPU ``edf`` and ``edf_celllist`` over device arrays with
+  their counted work against the measured FP64 peak (the reference's ``edf`` is timed beside
+  ``edf_celllist`` in cpu_baseline).
 
 ``--impl reference`` times that reference CPU code alone. With torchrun (N > 1) every rank runs
 an independent replica (the path does not shard across GPUs here: "replicas only"), the step time
@@ -59,6 +66,7 @@ def parse_args():
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-batch", action="store_true", help="skip the 256-mesh batched leg")
+    p.add_argument("--no-dense", action="store_true", help="skip the edf / edf_celllist leg (icosphere workload)")
     p.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     p.add_argument("--batch-meshes", type=int, default=256)
     p.add_argument("--serve-meshes", type=int, default=512)
@@ -160,11 +168,30 @@ def cpu_reference_rate(mesh, grid, nsample, seed=17, steps=1):
     ids = np.sort(rng.choice(grid.size, size=min(nsample, grid.size), replace=False))
     q = oracle.grid_points(grid)[:, ids].copy()
     times = []
+    vals = None
     for _ in range(steps):
         t0 = time.perf_counter()
-        oracle.ref_edf(q, mesh, which="celllist")
+        vals = oracle.ref_edf(q, mesh, which="celllist")
         times.append(time.perf_counter() - t0)
-    return len(ids), times
+    return len(ids), times, ids, vals
+
+
+def error_stats(got, want, diag):
+    """Max / RMS absolute error of got against want and the max relative to the bbox diagonal."""
+    err = np.abs(np.asarray(got, dtype=np.float64) - np.asarray(want, dtype=np.float64))
+    return {"max_abs": float(err.max()) if err.size else 0.0, "rms": float(np.sqrt(np.mean(err ** 2))) if err.size else 0.0,
+            "max_rel_to_bbox_diagonal": float(err.max() / diag) if err.size else 0.0}
+
+
+def signed_check(S, oracle, grid, mesh, ids, gd, gt, diag):
+    """Signed distances and closest triangles against the oracle at grid nodes ids (its double restatement
+    of ssdf's signed sampler): value, sign and index mismatches."""
+    want, wtri = oracle.sdf_points(oracle.grid_points(grid)[:, ids], mesh)
+    res = error_stats(gd, want, diag)
+    res.update({"nodes": int(len(ids)), "value_mismatches": int(np.sum(gd != want)),
+                "sign_mismatches": int(np.sum(np.signbit(gd) != np.signbit(want))),
+                "index_mismatches": int(np.sum(gt != wtri))})
+    return res
 
 
 def beams_workload(n=512, npoints=8_000_000):
@@ -186,16 +213,18 @@ def cpu_reference_points(mesh, pts_grid, nsample, dtype, seed=17, steps=1):
     pts, grid = pts_grid
     rng = np.random.default_rng(seed)
     half = nsample // 2
-    a = pts[:, np.sort(rng.choice(pts.shape[1], size=half, replace=False))]
+    pt_ids = np.sort(rng.choice(pts.shape[1], size=half, replace=False))
+    a = pts[:, pt_ids]
     ids = np.sort(rng.choice(grid.size, size=nsample - half, replace=False))
     b = oracle.grid_points(grid)[:, ids].astype(dtype)
     q = np.concatenate([a, b], axis=1).astype(dtype)
     times = []
+    vals = None
     for _ in range(steps):
         t0 = time.perf_counter()
-        oracle.ref_edf(q, mesh, dtype=dtype, which="celllist")
+        vals = oracle.ref_edf(q, mesh, dtype=dtype, which="celllist")
         times.append(time.perf_counter() - t0)
-    return q.shape[1], times
+    return q.shape[1], times, (pt_ids, ids, q, vals)
 
 
 def run_beams(S, args, rank, world, dist):
@@ -249,6 +278,7 @@ def run_beams(S, args, rank, world, dist):
     c2 = S.last_query_counts()
     del os.environ["SSDF_B200_COUNT"]
     counts = {k: c1[k] + c2[k] for k in c1}
+    out_keep = out.cpu().numpy()
     flops = 79.0 * counts["triangle_tests"] + 8.0 * counts["box_tests"]
     step_s = statistics.median(ms) * 1e-3
     peak = S.fma_peak_tflops(False)
@@ -298,11 +328,22 @@ def run_beams(S, args, rank, world, dist):
                        "api": "ssdf_b200_edf_index_ff on the 8e6 points (page-locked host arrays, blocking; wall clock)"}
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            n, times = cpu_reference_points(mesh, (pts, grid), min(args.cpu_sample, REF_SAMPLE), np.float32)
+            n, times, (pt_ids, g_ids, q, ref_f) = cpu_reference_points(mesh, (pts, grid),
+                                                                       min(args.cpu_sample, REF_SAMPLE), np.float32)
             line["cpu_baseline"] = {"value": n / times[0], "unit": "queries/s", "cores": os.cpu_count(),
                                     "kind": "reference",
                                     "sample": f"{n} seeded queries (half points, half grid nodes), "
                                               f"ssdf::edf_celllist<float>, oracle/_ref built from the reference's sources"}
+            # error of this line's float arithmetic (the reference's own, bitwise) against double
+            import oracle
+
+            got = np.concatenate([out_keep[:npts][pt_ids], out_keep[npts:][g_ids]])
+            ref_d = oracle.ref_edf(q.astype(np.float64), mesh, which="celllist")
+            lo, hi = mesh.bbox()
+            err = error_stats(got, ref_d, float(np.linalg.norm(hi - lo)))
+            err.update({"vs": "the reference's edf_celllist<double> at the same float queries (FP64)",
+                        "sample": int(n), "mismatches_vs_reference_float": int(np.sum(got != ref_f))})
+            line["error"] = err
         except Exception as ex:
             line["cpu_baseline"] = {"error": repr(ex)}
     dm.close()
@@ -319,11 +360,11 @@ def run_reference(args, rank, world):
     cores = os.cpu_count()
     if args.workload == "beams":
         mesh, pts = beams_workload(args.grid)
-        n, times = cpu_reference_points(mesh, pts, REF_SAMPLE, np.float32, steps=args.warmup + args.steps)
+        n, times, _ = cpu_reference_points(mesh, pts, REF_SAMPLE, np.float32, steps=args.warmup + args.steps)
         sample = f"{n} seeded queries of the beam-lattice set per step, ssdf::edf_celllist<float,float,int>"
     else:
         mesh, grid = workload(args.grid, args.workload)
-        n, times = cpu_reference_rate(mesh, grid, REF_SAMPLE, steps=args.warmup + args.steps)
+        n, times, _, _ = cpu_reference_rate(mesh, grid, REF_SAMPLE, steps=args.warmup + args.steps)
         sample = (f"{n} seeded nodes of the {args.grid}^3 grid per step, ssdf::edf_celllist<double,double,int> "
                   f"(unsigned; the reference has no CPU signed grid sampler without cuBQL)")
     timed = times[args.warmup:]
@@ -414,6 +455,16 @@ def main():
     peak = S.fma_peak_tflops(False)
     stats = dm.stats()
     alg_bytes = nq * 8 + stats["bytes"]
+    # untimed: the fix-up result against the plain FP64 one at every node (distance bits, triangle)
+    tri_x = torch.empty(nq, dtype=torch.int32, device="cuda")
+    out_64 = torch.empty(nq, dtype=torch.float64, device="cuda")
+    tri_64 = torch.empty(nq, dtype=torch.int32, device="cuda")
+    dm.query_grid(grid, out, tri_x, precision=S.PREC_F32_FIXUP, output=S.OUT_SDF, stream=stream)
+    dm.query_grid(grid, out_64, tri_64, precision=S.PREC_F64, output=S.OUT_SDF, stream=stream)
+    torch.cuda.synchronize()
+    vs_fp64 = {"nodes": nq, "distance_mismatches": int((out.view(torch.int64) != out_64.view(torch.int64)).sum()),
+               "index_mismatches": int((tri_x != tri_64).sum())}
+    del out_64, tri_64
     line = {
         "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_x / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -431,9 +482,15 @@ def main():
                              "peak_gbs": _hbm_peak()}},
         "clocks": clk,
         "mesh": stats,
+        "error": {"fixup_vs_fp64_every_node": vs_fp64},
     }
     if args.workload == "knot":
         _attach_traffic(line)
+    if args.workload == "icosphere" and not args.no_dense:
+        try:
+            line["dense"] = dense_leg(S, mesh, grid, args)
+        except Exception as ex:  # pragma: no cover - reported, not fatal
+            line["dense"] = {"error": repr(ex)}
 
     if args.workload != "knot":
         args.no_batch = args.no_serve = True
@@ -450,15 +507,35 @@ def main():
     if not args.no_e2e:
         try:
             line["e2e"] = e2e(S, mesh, grid, args)
+            line["e2e_pageable"] = e2e(S, mesh, grid, args, pageable=True)
         except Exception as ex:  # pragma: no cover - reported, not fatal
             line["e2e"] = {"error": repr(ex)}
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            n, times = cpu_reference_rate(mesh, grid, args.cpu_sample)
+            n, times, ids, ref_d = cpu_reference_rate(mesh, grid, args.cpu_sample)
             line["cpu_baseline"] = {"value": n / times[0], "unit": "queries/s", "cores": os.cpu_count(),
                                     "kind": "reference",
                                     "sample": f"{n} seeded grid nodes, ssdf::edf_celllist<double> (unsigned), "
                                               f"oracle/_ref built from the reference's sources"}
+            # this line's error: |distance| against the reference's own edf_celllist<double> on that
+            # sample, and signs, values and triangles against the oracle on part of it
+            import oracle
+
+            gd = out.cpu().numpy()
+            gt = tri_x.cpu().numpy()
+            diag = mesh.diagonal()
+            err = error_stats(np.abs(gd[ids]), ref_d, diag)
+            err.update({"vs": "the reference's edf_celllist<double> (unsigned) at the sampled nodes", "sample": int(n),
+                        "mismatches_vs_reference": int(np.sum(np.abs(gd[ids]) != ref_d))})
+            sub = ids[:: max(1, len(ids) // 4096)]
+            err["signed_vs_oracle"] = signed_check(S, oracle, grid, mesh, sub, gd[sub], gt[sub], diag)
+            line["error"].update(err)
+            if args.workload == "icosphere":  # config 1 names the reference's edf beside edf_celllist
+                q = oracle.grid_points(grid)[:, ids].copy()
+                t0 = time.perf_counter()
+                oracle.ref_edf(q, mesh, which="edf")
+                line["cpu_baseline"]["edf"] = {"value": len(ids) / (time.perf_counter() - t0), "unit": "queries/s",
+                                               "sample": f"the same {len(ids)} nodes, ssdf::edf<double,double,int>"}
         except Exception as ex:
             line["cpu_baseline"] = {"error": repr(ex)}
     dm.close()
@@ -574,12 +651,13 @@ def serving_leg(S, args):
     return out
 
 
-def e2e(S, mesh, grid, args):
-    """Through the drop-in C ABI from host arrays: upload, build, query, download (pinned)."""
+def e2e(S, mesh, grid, args, pageable=False):
+    """Through the drop-in C ABI from host arrays: upload, build, query, download (into page-locked
+    memory, or ordinary pageable numpy memory as the reference's drivers allocate)."""
     import torch
 
     nq = grid.size
-    host_out = torch.empty(nq, dtype=torch.float64, pin_memory=True).numpy()
+    host_out = np.empty(nq) if pageable else torch.empty(nq, dtype=torch.float64, pin_memory=True).numpy()
     hm = S.capi._HostMesh(mesh, np.float64)
     nx, ny, nz = grid.n
     import ctypes as C
@@ -600,7 +678,55 @@ def e2e(S, mesh, grid, args):
     dt = (time.perf_counter() - t0) / k
     h2d = sum(a.nbytes for a in (hm.sx, hm.sy, hm.sz, hm.s0, hm.s1, hm.s2))
     return {"value": nq / dt, "unit": "queries/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": nq * 8,
-            "ms_per_call": dt * 1e3, "api": "ssdf_b200_sample_sdf_bvh_dd (host arrays, blocking; wall clock)"}
+            "ms_per_call": dt * 1e3, "api": "ssdf_b200_sample_sdf_bvh_dd (host arrays, blocking; wall clock)",
+            "output_memory": "pageable" if pageable else "page-locked"}
+
+
+def dense_leg(S, mesh, grid, args):
+    """Config 1's plain methods on the GPU: ssdf::edf (brute force) and ssdf::edf_celllist over device
+    arrays at the grid's nodes (ssdf_edf_device, FP64), timed with CUDA events, each with its counted
+    work against the measured FP64 FMA peak; the reference's own edf and edf_celllist<double> on the
+    host cores are timed on a sample in the cpu_baseline leg."""
+    import torch
+
+    nx, ny, nz = grid.n
+    h = [(grid.hi[d] - grid.lo[d]) / (grid.n[d] - 1) for d in range(3)]
+    ii, jj, kk = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    pts = [grid.lo[d] + (ii, jj, kk)[d].transpose(2, 1, 0).ravel() * h[d] for d in range(3)]
+    x, y, z = (torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda") for a in pts)
+    sx, sy, sz = (torch.tensor(np.ascontiguousarray(a, dtype=np.float64), device="cuda") for a in mesh.coords())
+    s0, s1, s2 = (torch.tensor(np.ascontiguousarray(a, dtype=np.int32), device="cuda") for a in mesh.indices())
+    n = x.numel()
+    out = torch.empty(n, dtype=torch.float64, device="cuda")
+    big = float(np.finfo(np.float64).max)
+    stream = torch.cuda.current_stream()
+    peak64 = S.fma_peak_tflops(True)
+    res = {"points": n, "triangles": mesh.nt, "dtype": "f64"}
+    for method, name in ((0, "edf"), (1, "edf_celllist")):
+        ms = []
+        for rep in range(3 + args.steps):
+            out.fill_(big)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            S.edf_device(method, x, y, z, s0, s1, s2, sx, sy, sz, out, stream=stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if rep >= 3:
+                ms.append(e0.elapsed_time(e1))
+        os.environ["SSDF_B200_COUNT"] = "1"
+        out.fill_(big)
+        S.edf_device(method, x, y, z, s0, s1, s2, sx, sy, sz, out, stream=stream)
+        counts = S.last_query_counts()
+        del os.environ["SSDF_B200_COUNT"]
+        t = statistics.median(ms) * 1e-3
+        flops = 79.0 * counts["triangle_tests"] + 8.0 * counts["box_tests"]
+        res[name] = {"queries_per_s": n / t, "ms": t * 1e3, "triangle_tests": counts["triangle_tests"],
+                     "box_tests": counts["box_tests"],
+                     "roofline": {"bound": "fp64", "achieved": flops / t / 1e12, "peak": peak64, "unit": "TFLOP/s",
+                                  "frac": flops / t / 1e12 / peak64,
+                                  "peak_source": "measured FP64 FMA microbenchmark on this GPU (ssdf_b200_fma_peak)",
+                                  "note": "the whole call (record build, launch, flag read-back) in the time"}}
+    return res
 
 
 def _hbm_peak():
