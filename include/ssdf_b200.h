@@ -37,6 +37,7 @@ extern "C" {
 #define SSDF_ERR_CUDA 3             /* a CUDA runtime call or kernel launch failed            */
 #define SSDF_ERR_NOT_SUPPORTED 4    /* a size or option beyond what this build handles        */
 #define SSDF_ERR_INTERNAL 5         /* a device-side check fired (bounded wait, stack depth)  */
+#define SSDF_ERR_BUSY 6             /* the server's queue is over its admission limit: retry  */
 
 /* Human-readable name of a status code. */
 const char *ssdf_status_string(int status);
@@ -466,6 +467,13 @@ int ssdf_batch_add_grid(ssdf_batch *batch, ssdf_mesh *mesh, ptrdiff_t nx, ptrdif
                         const double lo[3], const double hi[3], void *out, int *outtri, const ssdf_query_opts *opts);
 int ssdf_batch_add_points(ssdf_batch *batch, ssdf_mesh *mesh, ptrdiff_t npoints, const void *x, const void *y,
                           const void *z, void *out, int *outtri, const ssdf_query_opts *opts);
+/* Adds the z-planes z0 .. z0 + nz_slab - 1 of the node grid nx*ny*nz over [lo, hi] as one job: the
+ * nodes keep the whole grid's coordinates (origin and spacing from the whole grid), so the slab's
+ * results are bit for bit those of the same planes in a whole-grid job; out / outtri hold the slab's
+ * nx*ny*nz_slab values. Lets a large grid be split into jobs that share batches with others. */
+int ssdf_batch_add_grid_slab(ssdf_batch *batch, ssdf_mesh *mesh, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz,
+                             const double lo[3], const double hi[3], ptrdiff_t z0, ptrdiff_t nz_slab, void *out,
+                             int *outtri, const ssdf_query_opts *opts);
 /* Runs every job in one persistent launch (plus the fix-up window stage) on `stream`, asynchronously.
  * use_graph = 1: the launch sequence is captured into a CUDA graph on the first run and replayed
  * afterwards for any composition of jobs (the job table is device-resident). */
@@ -502,6 +510,11 @@ typedef struct {
     int precision;         /* SSDF_PREC_F32_FIXUP or SSDF_PREC_F64                             */
     int leaf_size;         /* BVH leaf size of resident meshes (0: default)                    */
     int slots;             /* batches in flight at once, 1..16 (0: 4); each holds its buffers  */
+    long long max_queued_queries; /* admission limit: a request that would bring the queries waiting
+                                     to be packed above it is refused with SSDF_ERR_BUSY (0: none) */
+    int split_queries;     /* requests larger than this are answered as parts (z-slabs of a grid,
+                              runs of a point list) packed round-robin with the other waiting
+                              requests (0: 262144; must not exceed max_batch_queries)              */
 } ssdf_server_opts;
 
 typedef struct {
@@ -510,6 +523,7 @@ typedef struct {
     long long queries, batches, evictions, builds;
     long long resident_bytes, resident_meshes;
     double seconds;                       /* first submit -> last completion                   */
+    long long rejected;                   /* requests refused by the admission limit           */
 } ssdf_server_report;
 
 /* A scheduler thread packs waiting requests into one persistent batch launch per free slot (several
@@ -521,7 +535,8 @@ int ssdf_server_destroy(ssdf_server *server);
 /* Registers a mesh (host arrays, copied); it is built on the device when first queried. */
 int ssdf_server_add_mesh(ssdf_server *server, ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
                          ptrdiff_t nspoints, const double *sx, const double *sy, const double *sz, int *mesh_id);
-/* Asynchronous requests; the host arrays must stay valid until ssdf_server_wait returns. */
+/* Asynchronous requests; the host arrays must stay valid until ssdf_server_wait returns. A request
+ * over the admission limit returns SSDF_ERR_BUSY at once (nothing is queued). */
 int ssdf_server_submit_points(ssdf_server *server, int mesh_id, ptrdiff_t npoints, const double *x, const double *y,
                               const double *z, double *out, int *outtri, long long *ticket);
 int ssdf_server_submit_grid(ssdf_server *server, int mesh_id, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz,

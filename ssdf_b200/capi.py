@@ -26,6 +26,7 @@ LIB_PATH = os.environ.get("SSDF_B200_LIBRARY") or os.path.join(HERE, "_lib", "li
 
 SSDF_OK = 0
 SSDF_ERR_INVALID_ARGUMENT, SSDF_ERR_OUT_OF_MEMORY, SSDF_ERR_CUDA, SSDF_ERR_NOT_SUPPORTED, SSDF_ERR_INTERNAL = 1, 2, 3, 4, 5
+SSDF_ERR_BUSY = 6
 F32, F64 = 0, 1
 PREC_F32, PREC_F64, PREC_F32_FIXUP = 0, 1, 2
 OUT_EDF, OUT_SQEDF, OUT_SDF, OUT_CLOSEST = 0, 1, 2, 3
@@ -103,6 +104,8 @@ _sig("ssdf_batch_clear", [_vp])
 _sig("ssdf_batch_size", [_vp])
 _sig("ssdf_batch_add_grid", [_vp, _vp, _pd, _pd, _pd, C.POINTER(C.c_double * 3), C.POINTER(C.c_double * 3), _vp, _ip,
                              C.POINTER(QueryOpts)])
+_sig("ssdf_batch_add_grid_slab", [_vp, _vp, _pd, _pd, _pd, C.POINTER(C.c_double * 3), C.POINTER(C.c_double * 3), _pd,
+                                  _pd, _vp, _ip, C.POINTER(QueryOpts)])
 _sig("ssdf_batch_add_points", [_vp, _vp, _pd, _vp, _vp, _vp, _vp, _ip, C.POINTER(QueryOpts)])
 _sig("ssdf_batch_run", [_vp, C.c_int, _vp])
 _sig("ssdf_batch_last_blocks", [_vp], C.c_longlong)
@@ -140,14 +143,15 @@ _sig("ssdf_points_aabb_signed_distance", [_pd, _vp, _vp, _vp, C.c_int, C.POINTER
 
 class ServerOpts(C.Structure):
     _fields_ = [("memory_budget", C.c_size_t), ("max_batch_queries", C.c_int), ("max_batch_jobs", C.c_int),
-                ("precision", C.c_int), ("leaf_size", C.c_int), ("slots", C.c_int)]
+                ("precision", C.c_int), ("leaf_size", C.c_int), ("slots", C.c_int),
+                ("max_queued_queries", C.c_longlong), ("split_queries", C.c_int)]
 
 
 class ServerStats(C.Structure):
     _fields_ = [("completed", C.c_longlong), ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double),
                 ("queries", C.c_longlong), ("batches", C.c_longlong), ("evictions", C.c_longlong),
                 ("builds", C.c_longlong), ("resident_bytes", C.c_longlong), ("resident_meshes", C.c_longlong),
-                ("seconds", C.c_double)]
+                ("seconds", C.c_double), ("rejected", C.c_longlong)]
 
 
 _dp_ = C.POINTER(C.c_double)
@@ -177,7 +181,7 @@ EXPORTED = ["ssdf_status_string", "ssdf_last_error", "ssdf_b200_version", "ssdf_
             "ssdf_b200_edf_index_ff", "ssdf_b200_sdf_points_dd", "ssdf_b200_sample_sdf_index_bvh_dd",
             "ssdf_mesh_create", "ssdf_mesh_destroy", "ssdf_mesh_stats", "ssdf_mesh_filter_info", "ssdf_edf_device", "ssdf_query_points", "ssdf_query_grid",
             "ssdf_last_query_counts", "ssdf_b200_fma_peak", "ssdf_batch_create", "ssdf_batch_destroy", "ssdf_batch_clear",
-            "ssdf_batch_size", "ssdf_batch_add_grid", "ssdf_batch_add_points", "ssdf_batch_run",
+            "ssdf_batch_size", "ssdf_batch_add_grid", "ssdf_batch_add_grid_slab", "ssdf_batch_add_points", "ssdf_batch_run",
             "ssdf_batch_last_blocks", "ssdf_query_grid_noalloc", "ssdf_query_grid_noalloc_max", "ssdf_server_create",
             "ssdf_server_destroy", "ssdf_server_add_mesh", "ssdf_server_submit_points", "ssdf_server_submit_grid",
             "ssdf_server_wait", "ssdf_server_stats", "ssdf_server_reset_stats", "ssdf_autotune_grid",
@@ -691,6 +695,18 @@ class Batch:
                                        C.byref(o)), "ssdf_batch_add_grid")
         self._keep.append((mesh, out, outtri))
 
+    def add_grid_slab(self, mesh: "DeviceMesh", grid, z0, nz, out, outtri=None, output=OUT_SDF, coord_type=F64,
+                      out_type=F64):
+        """The z-planes z0 .. z0 + nz - 1 of grid as one job, with the whole grid's node coordinates."""
+        o = QueryOpts(self.precision, output, coord_type, out_type)
+        lo = (C.c_double * 3)(*grid.lo)
+        hi = (C.c_double * 3)(*grid.hi)
+        tri = C.cast(C.c_void_p(_dptr(outtri)), _ip) if outtri is not None else None
+        gx, gy, gz = (int(v) for v in grid.n)
+        _check(lib.ssdf_batch_add_grid_slab(self._h, mesh._h, gx, gy, gz, C.byref(lo), C.byref(hi), int(z0), int(nz),
+                                            _dptr(out), tri, C.byref(o)), "ssdf_batch_add_grid_slab")
+        self._keep.append((mesh, out, outtri))
+
     def add_points(self, mesh: "DeviceMesh", x, y, z, out, outtri=None, output=OUT_SDF, coord_type=F64, out_type=F64):
         o = QueryOpts(self.precision, output, coord_type, out_type)
         tri = C.cast(C.c_void_p(_dptr(outtri)), _ip) if outtri is not None else None
@@ -709,10 +725,10 @@ class Server:
     """Continuous-batching request loop over resident meshes (host arrays in and out)."""
 
     def __init__(self, memory_budget=120 << 30, max_batch_queries=1 << 22, max_batch_jobs=64,
-                 precision=PREC_F32_FIXUP, leaf_size=0, slots=0):
+                 precision=PREC_F32_FIXUP, leaf_size=0, slots=0, max_queued_queries=0, split_queries=0):
         self._h = C.c_void_p()
         o = ServerOpts(int(memory_budget), int(max_batch_queries), int(max_batch_jobs), int(precision),
-                       int(leaf_size), int(slots))
+                       int(leaf_size), int(slots), int(max_queued_queries), int(split_queries))
         _check(lib.ssdf_server_create(C.byref(self._h), C.byref(o)), "ssdf_server_create")
         self._inflight = {}
 

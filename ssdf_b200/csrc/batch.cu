@@ -223,6 +223,19 @@ int ssdf_batch_add_grid(ssdf_batch *b, ssdf_mesh *mesh, ptrdiff_t nx, ptrdiff_t 
     return batch_add(b, a, opts);
 }
 
+int ssdf_batch_add_grid_slab(ssdf_batch *b, ssdf_mesh *mesh, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz,
+                             const double lo[3], const double hi[3], ptrdiff_t z0, ptrdiff_t nz_slab, void *out,
+                             int *outtri, const ssdf_query_opts *opts) {
+    if (!b || !opts) return fail(SSDF_ERR_INVALID_ARGUMENT, "null batch or options");
+    if (z0 < 0 || nz_slab < 0 || z0 + nz_slab > nz)
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "ssdf_batch_add_grid_slab: planes outside the grid");
+    QueryArgs a;
+    SSDF_CHECK(fill_grid_args(mesh, nx, ny, nz, lo, hi, out, outtri, opts, &a));
+    a.nz = nz_slab;  // the grid's origin and spacing stay those of the whole grid
+    a.z0 = z0;
+    return batch_add(b, a, opts);
+}
+
 int ssdf_batch_add_points(ssdf_batch *b, ssdf_mesh *mesh, ptrdiff_t npoints, const void *x, const void *y,
                           const void *z, void *out, int *outtri, const ssdf_query_opts *opts) {
     if (!b || !opts) return fail(SSDF_ERR_INVALID_ARGUMENT, "null batch or options");

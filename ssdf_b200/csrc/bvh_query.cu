@@ -105,11 +105,11 @@ __device__ __forceinline__ void query_point(const QueryArgs &a, long long q, lon
         if (a.coord_f64) {
             x = grid_coord<double>(a.lo64[0], a.h64[0], i);
             y = grid_coord<double>(a.lo64[1], a.h64[1], j);
-            z = grid_coord<double>(a.lo64[2], a.h64[2], k);
+            z = grid_coord<double>(a.lo64[2], a.h64[2], k + a.z0);
         } else {
             x = grid_coord<float>(a.lo32[0], a.h32[0], i);
             y = grid_coord<float>(a.lo32[1], a.h32[1], j);
-            z = grid_coord<float>(a.lo32[2], a.h32[2], k);
+            z = grid_coord<float>(a.lo32[2], a.h32[2], k + a.z0);
         }
     } else if (a.coord_f64) {
         x = __ldg((const double *)a.x + q);

@@ -385,6 +385,7 @@ const char *ssdf_status_string(int status) {
         case SSDF_ERR_CUDA: return "SSDF_ERR_CUDA";
         case SSDF_ERR_NOT_SUPPORTED: return "SSDF_ERR_NOT_SUPPORTED";
         case SSDF_ERR_INTERNAL: return "SSDF_ERR_INTERNAL";
+        case SSDF_ERR_BUSY: return "SSDF_ERR_BUSY";
         default: return "SSDF_ERR_UNKNOWN";
     }
 }

@@ -146,6 +146,9 @@ struct QueryArgs {
     int chunk_blocks;
     // grid launches: start each step of a block's column from the triangles found one step below
     int seed;
+    // grid jobs: the z-planes nz of this job are planes z0 .. z0 + nz - 1 of a larger grid with the
+    // same origin and spacing (node coordinates use the global plane; outputs are the job's own)
+    long long z0;
 };
 
 // Job table header of a batch (device memory).

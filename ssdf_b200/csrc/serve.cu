@@ -5,6 +5,13 @@
 //   * admission: a mesh is built on the device when a request first needs it and stays resident
 //     while the resident bytes fit the memory budget; beyond it the least recently used meshes that
 //     no in-flight batch holds are evicted (and rebuilt if asked for again);
+//   * admission: with a queued-query limit, a request that would bring the queries waiting to be
+//     packed above it is refused at once with SSDF_ERR_BUSY (counted), so the queue, and with it the
+//     latency of accepted requests, stays bounded under overload;
+//   * parts: a request larger than split_queries is answered as parts -- z-slabs of a grid (keeping
+//     the whole grid's node coordinates, so each value is the one a whole-grid query gives) or runs
+//     of a point list; the scheduler takes one part of each waiting request in turn, so a small
+//     request goes into the next batch beside a large one instead of behind it;
 //   * continuous batching: a scheduler thread packs the requests that are waiting into one batch
 //     (ssdf_batch_* -- one persistent launch, replayed as a CUDA graph) up to a query budget, stages
 //     the point lists through pinned memory, and launches it on a free slot (4 by default), each
@@ -66,6 +73,13 @@ struct Request {
     Clock::time_point submitted;
     int status = SSDF_OK;
     bool done = false;
+    // parts: units are z-planes of a grid or points of a list
+    long long units = 0;       // nz or n
+    long long unit_size = 1;   // queries per unit (nx * ny for a grid)
+    long long part_units = 0;  // units per part
+    long long next = 0;        // first unit not yet packed
+    int parts_out = 0;         // parts packed and not yet delivered
+    long long queries() const { return units * unit_size; }
 };
 
 struct Slot {
@@ -76,8 +90,9 @@ struct Slot {
     int *d_tri = nullptr;
     double *h_pts = nullptr, *h_out = nullptr;
     int *h_tri = nullptr;
-    std::vector<std::shared_ptr<Request>> reqs;
-    std::vector<long long> offsets;
+    std::vector<std::shared_ptr<Request>> reqs;  // one per job (a part of a request)
+    std::vector<long long> offsets;              // the job's first value in the slot's buffers
+    std::vector<long long> part_first, part_units;
     std::vector<int> meshes;
     bool busy = false;      // packed or in flight
     bool inflight = false;  // launched; its completer waits on the event
@@ -96,7 +111,9 @@ struct ssdf_server {
     std::unordered_map<int, Resident> resident;
     std::list<int> lru;  // front = most recent
     size_t resident_bytes = 0;
-    std::deque<std::shared_ptr<Request>> pending;
+    std::deque<std::shared_ptr<Request>> pending;  // requests with parts not yet packed
+    long long queued_queries = 0;                  // queries of those parts
+    long long rejected = 0;
     std::unordered_map<long long, std::shared_ptr<Request>> tickets;
     long long next_ticket = 1;
     std::vector<Slot> slots;
@@ -200,19 +217,21 @@ void finish(ssdf_server *s, Slot &sl, int status) {
     // are in the caller's arrays (caller holds no lock)
     for (size_t k = 0; k < sl.reqs.size(); k++) {
         Request &r = *sl.reqs[k];
-        const long long n = r.grid ? r.nx * r.ny * r.nz : r.n;
+        const long long first = sl.part_first[k] * r.unit_size, n = sl.part_units[k] * r.unit_size;
         if (status == SSDF_OK) {
-            par_memcpy(r.out, sl.h_out + sl.offsets[k], sizeof(double) * size_t(n));
-            if (r.outtri) par_memcpy(r.outtri, sl.h_tri + sl.offsets[k], sizeof(int) * size_t(n));
+            par_memcpy(r.out + first, sl.h_out + sl.offsets[k], sizeof(double) * size_t(n));
+            if (r.outtri) par_memcpy(r.outtri + first, sl.h_tri + sl.offsets[k], sizeof(int) * size_t(n));
         }
-        r.status = status;
     }
     const auto now = Clock::now();
     std::lock_guard<std::mutex> lock(s->mu);
     for (auto &rp : sl.reqs) {
-        rp->done = true;
+        if (status != SSDF_OK) rp->status = status;
+        rp->parts_out--;
+        if (rp->parts_out > 0 || rp->next < rp->units || rp->done) continue;
+        rp->done = true;  // its last part: the request's results are all in the caller's arrays
         s->latencies_ms.push_back(std::chrono::duration<double, std::milli>(now - rp->submitted).count());
-        s->queries_done += rp->grid ? rp->nx * rp->ny * rp->nz : rp->n;
+        s->queries_done += rp->queries();
     }
     for (int id : sl.meshes) {
         auto it = s->resident.find(id);
@@ -231,6 +250,8 @@ void finish(ssdf_server *s, Slot &sl, int status) {
     s->last_done = now;
     sl.reqs.clear();
     sl.offsets.clear();
+    sl.part_first.clear();
+    sl.part_units.clear();
     sl.meshes.clear();
     sl.busy = false;
     sl.inflight = false;
@@ -253,27 +274,48 @@ void scheduler_loop(ssdf_server *s) {
         if (s->stop) return;
         Slot &sl = *free_slot();
         sl.t_pack = Clock::now();
-        // pack waiting requests (FIFO) up to the query and job budgets
+        // pack waiting requests' parts up to the query and job budgets, one part of each request in
+        // turn (oldest first), until nothing more fits
         long long used = 0, used_pts = 0;
-        while (!s->pending.empty() && int(sl.reqs.size()) < s->opts.max_batch_jobs) {
-            auto &r = s->pending.front();
-            const long long n = r->grid ? r->nx * r->ny * r->nz : r->n;
-            if (used + n > cap) break;
-            int st = admit(s, r->mesh_id);
-            if (st != SSDF_OK) {
-                r->status = st;
-                r->done = true;
-                s->pending.pop_front();
-                s->cv_done.notify_all();
-                continue;
+        bool progress = true;
+        while (progress && int(sl.reqs.size()) < s->opts.max_batch_jobs) {
+            progress = false;
+            for (auto it = s->pending.begin();
+                 it != s->pending.end() && int(sl.reqs.size()) < s->opts.max_batch_jobs;) {
+                auto r = *it;
+                const long long units = std::min(r->part_units, r->units - r->next);
+                const long long n = units * r->unit_size;
+                if (used + n > cap) {
+                    ++it;
+                    continue;
+                }
+                const int st = admit(s, r->mesh_id);
+                if (st != SSDF_OK) {  // this and its remaining parts fail; parts in flight finish
+                    r->status = st;
+                    s->queued_queries -= (r->units - r->next) * r->unit_size;
+                    r->next = r->units;
+                    if (r->parts_out == 0) r->done = true;
+                    it = s->pending.erase(it);
+                    s->cv_done.notify_all();
+                    continue;
+                }
+                s->resident[r->mesh_id].pins++;
+                sl.meshes.push_back(r->mesh_id);
+                sl.offsets.push_back(used);
+                sl.part_first.push_back(r->next);
+                sl.part_units.push_back(units);
+                sl.reqs.push_back(r);
+                r->next += units;
+                r->parts_out++;
+                s->queued_queries -= n;
+                used += n;
+                if (!r->grid) used_pts += n;
+                progress = true;
+                if (r->next == r->units)
+                    it = s->pending.erase(it);
+                else
+                    ++it;
             }
-            s->resident[r->mesh_id].pins++;
-            sl.meshes.push_back(r->mesh_id);
-            sl.offsets.push_back(used);
-            sl.reqs.push_back(r);
-            used += n;
-            if (!r->grid) used_pts += n;
-            s->pending.pop_front();
         }
         if (sl.reqs.empty()) continue;
         sl.busy = true;
@@ -294,16 +336,18 @@ void scheduler_loop(ssdf_server *s) {
             Request &r = *sl.reqs[k];
             double *out = sl.d_out + sl.offsets[k];
             int *tri = sl.d_tri + sl.offsets[k];
+            const long long first = sl.part_first[k], units = sl.part_units[k];
             if (r.grid) {
-                st = ssdf_batch_add_grid(sl.batch, ms[k], r.nx, r.ny, r.nz, r.lo, r.hi, out, tri, &qo);
+                st = ssdf_batch_add_grid_slab(sl.batch, ms[k], r.nx, r.ny, r.nz, r.lo, r.hi, first, units, out, tri,
+                                              &qo);
             } else {
                 double *hx = sl.h_pts + 3 * poff;
-                par_memcpy(hx, r.x, sizeof(double) * size_t(r.n));
-                par_memcpy(hx + r.n, r.y, sizeof(double) * size_t(r.n));
-                par_memcpy(hx + 2 * r.n, r.z, sizeof(double) * size_t(r.n));
+                par_memcpy(hx, r.x + first, sizeof(double) * size_t(units));
+                par_memcpy(hx + units, r.y + first, sizeof(double) * size_t(units));
+                par_memcpy(hx + 2 * units, r.z + first, sizeof(double) * size_t(units));
                 double *dx = sl.d_pts + 3 * poff;
-                st = ssdf_batch_add_points(sl.batch, ms[k], r.n, dx, dx + r.n, dx + 2 * r.n, out, tri, &qo);
-                poff += r.n;
+                st = ssdf_batch_add_points(sl.batch, ms[k], units, dx, dx + units, dx + 2 * units, out, tri, &qo);
+                poff += units;
             }
         }
         cudaError_t e = cudaSuccess;
@@ -362,6 +406,12 @@ int ssdf_server_create(ssdf_server **out, const ssdf_server_opts *opts) {
     if (opts->slots < 0 || opts->slots > 16) {
         delete s;
         return fail(SSDF_ERR_INVALID_ARGUMENT, "ssdf_server_create: slots must be 0 (default 4) or 1..16");
+    }
+    if (s->opts.split_queries == 0) s->opts.split_queries = std::min(1 << 18, opts->max_batch_queries);
+    if (s->opts.split_queries < 0 || s->opts.split_queries > opts->max_batch_queries || opts->max_queued_queries < 0) {
+        delete s;
+        return fail(SSDF_ERR_INVALID_ARGUMENT,
+                    "ssdf_server_create: split_queries must be 0..max_batch_queries, max_queued_queries >= 0");
     }
     s->slots = std::vector<Slot>(opts->slots ? opts->slots : 4);
     int st = SSDF_OK;
@@ -446,12 +496,25 @@ int ssdf_server_add_mesh(ssdf_server *s, ptrdiff_t nselements, const int *s0, co
 }
 
 static int submit(ssdf_server *s, std::shared_ptr<Request> r, long long *ticket) {
-    const long long n = r->grid ? r->nx * r->ny * r->nz : r->n;
-    if (n <= 0 || n > s->opts.max_batch_queries)
-        return fail(SSDF_ERR_INVALID_ARGUMENT, "request size must be 1.." + std::to_string(s->opts.max_batch_queries));
+    r->units = r->grid ? r->nz : r->n;
+    r->unit_size = r->grid ? r->nx * r->ny : 1;
+    const long long n = r->queries();
+    if (r->units <= 0 || r->unit_size <= 0 || n >= 0x7fffffffll)
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "request size must be 1 .. 2^31 - 1 queries");
+    if (r->unit_size > s->opts.max_batch_queries)
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "one z-plane of the grid exceeds max_batch_queries (" +
+                                                   std::to_string(s->opts.max_batch_queries) + ")");
+    r->part_units = std::max(1ll, (long long)s->opts.split_queries / r->unit_size);
     std::lock_guard<std::mutex> lock(s->mu);
     if (r->mesh_id < 0 || r->mesh_id >= int(s->meshes.size()))
         return fail(SSDF_ERR_INVALID_ARGUMENT, "unknown mesh id");
+    if (s->opts.max_queued_queries > 0 && s->queued_queries > 0 &&
+        s->queued_queries + n > s->opts.max_queued_queries) {
+        s->rejected++;
+        return fail(SSDF_ERR_BUSY, "server queue over its admission limit (" +
+                                       std::to_string(s->opts.max_queued_queries) + " queued queries)");
+    }
+    s->queued_queries += n;
     r->ticket = s->next_ticket++;
     r->submitted = Clock::now();
     if (!s->any_submit) s->first_submit = r->submitted, s->any_submit = true;
@@ -518,6 +581,7 @@ int ssdf_server_stats(ssdf_server *s, ssdf_server_report *st) {
     st->builds = s->builds;
     st->resident_bytes = (long long)s->resident_bytes;
     st->resident_meshes = (long long)s->resident.size();
+    st->rejected = s->rejected;
     if (s->any_submit)
         st->seconds = std::chrono::duration<double>(s->last_done - s->first_submit).count();
     return SSDF_OK;
@@ -527,7 +591,7 @@ int ssdf_server_reset_stats(ssdf_server *s) {
     if (!s) return fail(SSDF_ERR_INVALID_ARGUMENT, "null server");
     std::lock_guard<std::mutex> lock(s->mu);
     s->latencies_ms.clear();
-    s->queries_done = s->batches = s->evictions = s->builds = 0;
+    s->queries_done = s->batches = s->evictions = s->builds = s->rejected = 0;
     s->any_submit = false;
     return SSDF_OK;
 }

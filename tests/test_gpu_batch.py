@@ -232,3 +232,29 @@ def test_sliver_mesh_in_a_fixup_batch(use_graph):
     b.close()
     for dm in [dmb] + tori:
         dm.close()
+
+
+def test_grid_slabs_equal_the_whole_grid():
+    """ssdf_batch_add_grid_slab: z-slabs of a grid, each a job of its own, keep the whole grid's node
+    coordinates, so together they equal the whole-grid query bit for bit (float grids too)."""
+    import torch
+
+    mesh = W.torus(0.8, 0.25, nu=64, nv=24, jitter=0.01, seed=9)
+    dm = S.DeviceMesh(mesh)
+    grid = W.Grid((37, 29, 41), (-1.2, -1.17, -0.4), (1.13, 1.2, 0.43))
+    for prec, ct in ((S.PREC_F32_FIXUP, S.F64), (S.PREC_F64, S.F64), (S.PREC_F32_FIXUP, S.F32)):
+        whole = torch.empty(grid.size, dtype=torch.float64, device="cuda")
+        wtri = torch.empty(grid.size, dtype=torch.int32, device="cuda")
+        dm.query_grid(grid, whole, wtri, precision=prec, coord_type=ct)
+        out = torch.full((grid.size,), -1.0, dtype=torch.float64, device="cuda")
+        tri = torch.full((grid.size,), -1, dtype=torch.int32, device="cuda")
+        b = S.Batch(8, prec)
+        plane = grid.n[0] * grid.n[1]
+        for z0, nz in ((0, 7), (7, 1), (8, 20), (28, 13)):
+            b.add_grid_slab(dm, grid, z0, nz, out[z0 * plane:(z0 + nz) * plane], tri[z0 * plane:(z0 + nz) * plane],
+                            coord_type=ct)
+        b.run(use_graph=False)
+        torch.cuda.synchronize()
+        assert torch.equal(out, whole) and torch.equal(tri, wtri)
+        b.close()
+    dm.close()

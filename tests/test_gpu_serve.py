@@ -129,3 +129,52 @@ def test_slot_counts_give_the_same_results(slots):
         assert np.array_equal(d, wd) and np.array_equal(tri, wtri)
     assert srv.stats()["completed"] == len(reqs)
     srv.close()
+
+
+def test_split_requests_equal_unsplit():
+    """Requests larger than split_queries are answered in parts (z-slabs of a grid, runs of a point
+    list) packed round-robin with other requests; every value equals the request alone, bit for bit."""
+    ms = meshes()
+    reqs = requests(ms, seed=4)
+    big_grid = ("grid", 1, W.Grid.padded_nodes(ms[1], 53, 0.1))  # 148,877 nodes: 19 slabs of 2809 x 3 planes
+    big_pts = ("points", 3, W.uniform_points(70001, *(np.array(ms[3].bbox()) + [[-0.1], [0.1]]), seed=77))
+    reqs = [big_grid] + reqs[:10] + [big_pts] + reqs[10:20]
+    want = [alone(ms, r) for r in reqs]
+    srv = S.Server(memory_budget=1 << 30, max_batch_queries=1 << 17, max_batch_jobs=32, split_queries=9000, slots=3)
+    ids = [srv.add_mesh(m) for m in ms]
+    tickets = [srv.submit_grid(ids[mid], q) if kind == "grid" else srv.submit_points(ids[mid], q)
+               for kind, mid, q in reqs]
+    for t, (wd, wt) in zip(tickets, want):
+        d, tri = srv.wait(t)
+        assert np.array_equal(d, wd) and np.array_equal(tri, wt)
+    st = srv.stats()
+    assert st["completed"] == len(reqs) and st["rejected"] == 0
+    srv.close()
+
+
+def test_admission_limit_refuses_with_busy():
+    """Past the queued-query limit a submit returns SSDF_ERR_BUSY at once; the accepted requests are
+    answered exactly, and the refusals are counted."""
+    ms = meshes()
+    srv = S.Server(memory_budget=1 << 30, max_batch_queries=1 << 16, max_batch_jobs=8, slots=1,
+                   max_queued_queries=60000)
+    ids = [srv.add_mesh(m) for m in ms]
+    grid = W.Grid.padded_nodes(ms[0], 30, 0.1)  # 27,000 queries
+    want = alone(ms, ("grid", 0, grid))
+    accepted, busy = [], 0
+    for _ in range(40):
+        try:
+            accepted.append(srv.submit_grid(ids[0], grid))
+        except S.SsdfError as e:
+            assert e.status == S.SSDF_ERR_BUSY
+            busy += 1
+    assert busy > 0 and accepted
+    for t in accepted:
+        d, tri = srv.wait(t)
+        assert np.array_equal(d, want[0]) and np.array_equal(tri, want[1])
+    st = srv.stats()
+    assert st["rejected"] == busy and st["completed"] == len(accepted)
+    # once the queue has drained, requests are accepted again
+    t = srv.submit_grid(ids[0], grid)
+    srv.wait(t)
+    srv.close()
