@@ -233,6 +233,7 @@ int ssdf_batch_add_grid_slab(ssdf_batch *b, ssdf_mesh *mesh, ptrdiff_t nx, ptrdi
     SSDF_CHECK(fill_grid_args(mesh, nx, ny, nz, lo, hi, out, outtri, opts, &a));
     a.nz = nz_slab;  // the grid's origin and spacing stay those of the whole grid
     a.z0 = z0;
+    set_grid_steps(&a);
     return batch_add(b, a, opts);
 }
 
@@ -299,13 +300,21 @@ int ssdf_batch_run(ssdf_batch *b, int use_graph, void *stream_) {
             for (int *q : p) cudaFreeAsync(q, s);
         }
     } orders{{}, stream};
-    long long total = 0, total64 = 0, nq = 0;
-    for (const auto &j : b->jobs) nq += j.is_grid ? j.nx * j.ny * j.nz : j.npoints;
+    long long total = 0, total64 = 0, nq = 0, one_step = 0;
+    for (auto &j : b->jobs) {
+        nq += j.is_grid ? j.nx * j.ny * j.nz : j.npoints;
+        if (j.is_grid) j.grid_steps = 1;
+        one_step += query_blocks(j);
+    }
+    // the batch fills the GPU as a whole: its grid jobs walk columns of as many steps as its total
+    // work leaves four waves of blocks for
+    const int steps = grid_steps_for(one_step);
     size_t off = 0;
     int k = 0, k64 = 0;
     for (int r = 0; r < njobs; r++) {
         QueryArgs a = b->jobs[order[r]];
         a.warp_budget = resolve_warp_budget(a.warp_budget, nq);
+        if (a.is_grid) a.grid_steps = steps;
         if (sort_points && !a.is_grid && a.npoints >= kSortMinPoints) {
             int *ord = nullptr;
             SSDF_CHECK(morton_point_order(a.npoints, a.x, a.y, a.z, a.coord_f64, a.m.nodes32, &ord, stream));

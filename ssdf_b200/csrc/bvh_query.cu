@@ -70,7 +70,7 @@ __device__ __forceinline__ float finf() { return __int_as_float(0x7f800000); }
 // ---- query mapping ------------------------------------------------------------------------------
 
 // Each lane answers kQ queries. Grid: a block covers an 8 (x) x 8 (y) column of nodes and, at step
-// `step`, the 2 kQ z-planes from (column * kGridSteps + step) * 2 kQ on; a warp takes a 4 x 4 x 2kQ
+// `step`, the 2 kQ z-planes from (column * grid_steps + step) * 2 kQ on; a warp takes a 4 x 4 x 2kQ
 // brick of it, lane (lx, ly, lz) kQ consecutive z nodes. Point lists: query
 // (block * kQ + s) * 128 + thread, so each of a lane's queries is a coalesced load.
 __device__ __forceinline__ bool map_query(const QueryArgs &a, long long b, int step, int s, long long &q,
@@ -87,7 +87,7 @@ __device__ __forceinline__ bool map_query(const QueryArgs &a, long long b, int s
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     i = bx * 8 + (warp & 1) * 4 + (lane & 3);
     j = by * 8 + (warp >> 1) * 4 + ((lane >> 2) & 3);
-    k = ((bz * kGridSteps + step) * 2 + (lane >> 4)) * kQ + s;
+    k = ((bz * a.grid_steps + step) * 2 + (lane >> 4)) * kQ + s;
     q = i + a.nx * (j + a.ny * k);
     return i < a.nx && j < a.ny && k < a.nz;
 }
@@ -1050,7 +1050,7 @@ __device__ __forceinline__ void query_block(const QueryArgs &a, long long block,
     int seed[Q];
 #pragma unroll
     for (int s = 0; s < Q; s++) seed[s] = -1;
-    const int steps = a.is_grid ? kGridSteps : 1;
+    const int steps = a.is_grid ? a.grid_steps : 1;
     for (int step = 0; step < steps; step++) {
         long long qid[Q], gi[Q], gj[Q], gk[Q];
         bool valid[Q];
@@ -1424,6 +1424,28 @@ __global__ void k_point_keys(long long n, const void *__restrict__ x, const void
     }
     keys[i] = key;
     vals[i] = int(i);
+}
+
+int grid_steps_for(long long one_step_blocks) {
+    const int forced = env_int("SSDF_B200_GRID_STEPS", 0);
+    if (forced > 0) return forced < kMaxGridSteps ? forced : kMaxGridSteps;
+    static int slots[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int &r = slots[dev & 63];
+    if (r == 0) {
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        r = std::max(1, sms) * SSDF_B200_QUERY_MIN_BLOCKS;
+    }
+    int steps = kMaxGridSteps;
+    while (steps > 1 && one_step_blocks / steps < 4ll * r) steps >>= 1;
+    return steps;
+}
+
+void set_grid_steps(QueryArgs *a) {
+    if (!a->is_grid) return;
+    a->grid_steps = grid_steps_for(grid_blocks_x(a->nx) * grid_blocks_y(a->ny) * grid_blocks_z(a->nz, 1));
 }
 
 // Measured on B200: the torus knot with 29 % of its triangles slivers still runs 1.4x faster on the

@@ -734,6 +734,7 @@ int fill_grid_args(ssdf_mesh *mesh, ptrdiff_t nx, ptrdiff_t ny, ptrdiff_t nz, co
     }
     a->out = out;
     a->outtri = outtri;
+    set_grid_steps(a);
     return SSDF_OK;
 }
 

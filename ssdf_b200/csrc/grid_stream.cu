@@ -5,7 +5,7 @@
 // arrays. The query kernel and the device-to-host copy of its results would run one after the other;
 // here the copy of each slab chunk starts as soon as the kernel has finished that chunk:
 //
-//   - a grid launch's blocks are slab-major (columns of 8 x 8 x kGridBlockPlanes nodes, x fastest,
+//   - a grid launch's blocks are slab-major (columns of 8 x 8 x grid_block_planes nodes, x fastest,
 //     then y, then z), so the blocks of whole z-slabs cover one contiguous range of the output;
 //   - the last block of a chunk to finish raises the chunk's flag in page-locked host memory
 //     (signal_chunk in bvh_query.cu), and this thread, which would otherwise wait for the launch,
@@ -90,9 +90,9 @@ struct ChunkPlan {
 };
 
 ChunkPlan plan_chunks(const QueryArgs &a) {
-    const long long slab = kGridBlockPlanes;  // z-planes of one row of grid blocks
+    const long long slab = grid_block_planes(a.grid_steps);  // z-planes of one row of grid blocks
     const long long bxn = grid_blocks_x(a.nx), byn = grid_blocks_y(a.ny);
-    const long long slabs = grid_blocks_z(a.nz);
+    const long long slabs = grid_blocks_z(a.nz, a.grid_steps);
     const long long per = (slabs + kTargetChunks - 1) / kTargetChunks;
     ChunkPlan p;
     p.planes_per_chunk = per * slab;

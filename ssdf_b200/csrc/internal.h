@@ -146,6 +146,8 @@ struct QueryArgs {
     int chunk_blocks;
     // grid launches: start each step of a block's column from the triangles found one step below
     int seed;
+    // grid launches: z-steps of 2 kQ planes each block walks (1 .. kMaxGridSteps)
+    int grid_steps;
     // grid jobs: the z-planes nz of this job are planes z0 .. z0 + nz - 1 of a larger grid with the
     // same origin and spacing (node coordinates use the global plane; outputs are the job's own)
     long long z0;
@@ -215,23 +217,29 @@ bool default_wide();
 #endif
 constexpr int kQ = SSDF_B200_QUERIES_PER_LANE;
 // Grid launches: a block of 128 lanes covers an 8 x 8 column of nodes and walks it upwards in
-// kGridSteps steps of 2 kQ z-planes (each warp a 4 x 4 x 2kQ brick per step). A lane starts each
-// step from the closest triangle it found one step below, 2 kQ nodes away: a tight upper bound
-// (SSDF_B200_SEED=0 starts from the incoming bound alone).
-#ifndef SSDF_B200_GRID_STEPS
-#define SSDF_B200_GRID_STEPS 4
-#endif
-constexpr int kGridSteps = SSDF_B200_GRID_STEPS;
-constexpr long long kGridBlockPlanes = 2ll * kQ * kGridSteps;  // z-planes of one grid block
+// QueryArgs::grid_steps steps (1 .. kMaxGridSteps) of 2 kQ z-planes (each warp a 4 x 4 x 2kQ brick per
+// step). A lane starts each step from the closest triangle it found one step below, 2 kQ nodes away:
+// a tight upper bound (SSDF_B200_SEED=0 starts from the incoming bound alone). Large grids take
+// kMaxGridSteps; a grid too small to fill the GPU with such columns takes fewer (grid_steps_for).
+constexpr int kMaxGridSteps = 4;
 __host__ __device__ inline long long grid_blocks_x(long long nx) { return (nx + 7) / 8; }
 __host__ __device__ inline long long grid_blocks_y(long long ny) { return (ny + 7) / 8; }
-__host__ __device__ inline long long grid_blocks_z(long long nz) { return (nz + kGridBlockPlanes - 1) / kGridBlockPlanes; }
+__host__ __device__ inline long long grid_block_planes(int steps) { return 2ll * kQ * steps; }
+__host__ __device__ inline long long grid_blocks_z(long long nz, int steps) {
+    return (nz + grid_block_planes(steps) - 1) / grid_block_planes(steps);
+}
 // Blocks of 128 lanes one job needs (grid columns as above, x fastest, then y, then z; or 128 kQ
 // consecutive points).
 inline long long query_blocks(const QueryArgs &a) {
-    if (a.is_grid) return grid_blocks_x(a.nx) * grid_blocks_y(a.ny) * grid_blocks_z(a.nz);
+    if (a.is_grid) return grid_blocks_x(a.nx) * grid_blocks_y(a.ny) * grid_blocks_z(a.nz, a.grid_steps);
     return (a.npoints + 128 * kQ - 1) / (128 * kQ);
 }
+// Steps per grid block for a launch whose work, at one step per block, is `one_step_blocks` blocks:
+// the most steps (up to kMaxGridSteps) that still leave four waves of resident blocks on this
+// device (SSDF_B200_GRID_STEPS overrides). bvh_query.cu.
+int grid_steps_for(long long one_step_blocks);
+// Sets QueryArgs::grid_steps of a grid job from its own size (no-op for point lists).
+void set_grid_steps(QueryArgs *a);
 
 // The counts ssdf_last_query_counts reports for this thread's last counting launch (bvh_query.cu).
 void set_last_counts(unsigned long long tri, unsigned long long box, unsigned long long fix,
