@@ -499,6 +499,22 @@ int ssdf_autotune_grid(ptrdiff_t nselements, const int *s0, const int *s1, const
                        const double lo[3], const double hi[3], int precision, const char *cache_path,
                        ssdf_tuning *best);
 
+/* ---- pedf_update's selection steps on the device (distributed/psdf.hpp:327-470) -------------- */
+/* The box of npoints device points grown by their distances out: box6 (device, coord_type) =
+ * min(x - r), min(y - r), min(z - r), max(x + r), max(y + r), max(z + r), r = out in coord_type
+ * (psdf.hpp:327-361); (max, max, max, lowest, lowest, lowest) for no points. Asynchronous. */
+int ssdf_grown_box(ptrdiff_t npoints, const void *x, const void *y, const void *z, const void *out, int coord_type,
+                   int out_type, void *box6, void *stream);
+/* For each of nboxes boxes (device, 6 values of coord_type each, in ssdf_grown_box's order), the
+ * triangles whose corner box meets it (closed intervals, psdf.hpp:378-452), in triangle order: their
+ * corners (x0 y0 z0 x1 y1 z1 x2 y2 z2) into the device array corners, box after box, and their count
+ * per box into the HOST array counts[nboxes]. With corners NULL only the counts are computed; a
+ * total above capacity (triangles) is an error. Returns when done. */
+int ssdf_triangles_meeting_boxes(ptrdiff_t nselements, const int *s0, const int *s1, const int *s2,
+                                 ptrdiff_t nspoints, const void *sx, const void *sy, const void *sz, int coord_type,
+                                 int nboxes, const void *boxes, void *corners, long long capacity, long long *counts,
+                                 void *stream);
+
 /* ---- serving loop: continuous batching over resident meshes (no reference counterpart) ------- */
 
 typedef struct ssdf_server ssdf_server;

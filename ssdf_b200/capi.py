@@ -91,6 +91,9 @@ _sig("ssdf_mesh_destroy", [_vp])
 _sig("ssdf_mesh_destroy_async", [_vp, _vp])
 _sig("ssdf_mesh_stats", [_vp] + [C.POINTER(C.c_int64)] * 4)
 _sig("ssdf_mesh_filter_info", [_vp, C.POINTER(C.c_float), C.POINTER(C.c_int), C.POINTER(C.c_int64)])
+_sig("ssdf_grown_box", [_pd, _vp, _vp, _vp, _vp, C.c_int, C.c_int, _vp, _vp])
+_sig("ssdf_triangles_meeting_boxes", [_pd, _vp, _vp, _vp, _pd, _vp, _vp, _vp, C.c_int, C.c_int, _vp, _vp,
+                                      C.c_longlong, C.POINTER(C.c_longlong), _vp])
 _sig("ssdf_edf_device", [C.c_int, _pd, _vp, _vp, _vp, _pd, _vp, _vp, _vp, _pd, _vp, _vp, _vp, C.c_int, _vp, _vp, _vp])
 _sig("ssdf_query_points", [_vp, _pd, _vp, _vp, _vp, _vp, _ip, _vp, _vp, _vp, C.POINTER(QueryOpts), _vp])
 _sig("ssdf_query_grid", [_vp, _pd, _pd, _pd, C.POINTER(C.c_double * 3), C.POINTER(C.c_double * 3), _vp, _ip,
@@ -179,7 +182,7 @@ EXPORTED = ["ssdf_status_string", "ssdf_last_error", "ssdf_b200_version", "ssdf_
             "ssdf_b200_closest_point_bvh_fd", "ssdf_b200_closest_point_bvh_dd", "ssdf_b200_sample_sqedf_bvh_ff", "ssdf_b200_sample_sqedf_bvh_dd",
             "ssdf_b200_sample_sdf_bvh_ff", "ssdf_b200_sample_sdf_bvh_dd", "ssdf_b200_edf_index_dd",
             "ssdf_b200_edf_index_ff", "ssdf_b200_sdf_points_dd", "ssdf_b200_sample_sdf_index_bvh_dd",
-            "ssdf_mesh_create", "ssdf_mesh_destroy", "ssdf_mesh_stats", "ssdf_mesh_filter_info", "ssdf_edf_device", "ssdf_query_points", "ssdf_query_grid",
+            "ssdf_mesh_create", "ssdf_mesh_destroy", "ssdf_mesh_stats", "ssdf_mesh_filter_info", "ssdf_edf_device", "ssdf_grown_box", "ssdf_triangles_meeting_boxes", "ssdf_query_points", "ssdf_query_grid",
             "ssdf_last_query_counts", "ssdf_b200_fma_peak", "ssdf_batch_create", "ssdf_batch_destroy", "ssdf_batch_clear",
             "ssdf_batch_size", "ssdf_batch_add_grid", "ssdf_batch_add_grid_slab", "ssdf_batch_add_points", "ssdf_batch_run",
             "ssdf_batch_last_blocks", "ssdf_query_grid_noalloc", "ssdf_query_grid_noalloc_max", "ssdf_server_create",
@@ -289,6 +292,39 @@ def edf_device(method, x, y, z, s0, s1, s2, sx, sy, sz, out, outtri=None, stream
                                _dptr(s2), sx.numel(), _dptr(sx), _dptr(sy), _dptr(sz), ct, _dptr(out),
                                _dptr(outtri) if outtri is not None else None, _stream_handle(stream)),
            "ssdf_edf_device")
+
+
+def grown_box(x, y, z, out, stream=None):
+    """ssdf_grown_box on torch CUDA tensors: [min(p - r) x3, max(p + r) x3] in the coordinates' type."""
+    import torch
+
+    box = torch.empty(6, dtype=x.dtype, device=x.device)
+    ct = F64 if x.dtype == torch.float64 else F32
+    ot = F64 if out.dtype == torch.float64 else F32
+    _check(lib.ssdf_grown_box(x.numel(), _dptr(x), _dptr(y), _dptr(z), _dptr(out), ct, ot, _dptr(box),
+                              _stream_handle(stream)), "ssdf_grown_box")
+    return box
+
+
+def triangles_meeting_boxes(s0, s1, s2, sx, sy, sz, boxes, stream=None):
+    """ssdf_triangles_meeting_boxes on torch CUDA tensors: (corners [m, 9], counts per box) for the
+    boxes [k, 6], each box's triangles in triangle order, box after box."""
+    import torch
+
+    k = boxes.shape[0]
+    boxes = boxes.contiguous()
+    counts = (C.c_longlong * max(k, 1))()
+    ct = F64 if sx.dtype == torch.float64 else F32
+    args = (s0.numel(), _dptr(s0), _dptr(s1), _dptr(s2), sx.numel(), _dptr(sx), _dptr(sy), _dptr(sz), ct, k,
+            _dptr(boxes))
+    _check(lib.ssdf_triangles_meeting_boxes(*args, None, 0, counts, _stream_handle(stream)),
+           "ssdf_triangles_meeting_boxes")
+    total = sum(counts[i] for i in range(k))
+    corners = torch.empty((total, 9), dtype=sx.dtype, device=sx.device)
+    if total:
+        _check(lib.ssdf_triangles_meeting_boxes(*args, _dptr(corners), total, counts, _stream_handle(stream)),
+               "ssdf_triangles_meeting_boxes")
+    return corners, [int(counts[i]) for i in range(k)]
 
 
 def edf_bvh(points, mesh, out=None, gdtype=np.float64, tdtype=None):

@@ -173,47 +173,29 @@ def pedf(x, y, z, s0, s1, s2, sx, sy, sz, out, group=None, use_allgather=None, s
     return out
 
 
-def grown_box(x, y, z, out):
-    """The box of the points grown by their current distances, [min(p - r), max(p + r)] per axis in the
-    coordinates' type (psdf.hpp:323-360); an inverted box (max, lowest) when there are no points."""
-    import torch
-
-    if x.numel() == 0:
-        big = torch.finfo(x.dtype).max
-        return torch.tensor([big, big, big, -big, -big, -big], dtype=x.dtype, device=x.device)
-    r = out.to(x.dtype)
-    lo = torch.stack([(x - r).min(), (y - r).min(), (z - r).min()])
-    hi = torch.stack([(x + r).max(), (y + r).max(), (z + r).max()])
-    return torch.cat([lo, hi])
-
-
-def update_candidates(x, y, z, out, s0, s1, s2, sx, sy, sz, group=None):
+def update_candidates(x, y, z, out, s0, s1, s2, sx, sy, sz, group=None, select=None):
     """The triangles every rank sends this one for pedf_update: each rank's local triangles whose box
-    meets this rank's grown point box (psdf.hpp:362-470), as corner triples [m, 9] (x0 y0 z0 x1 ... z2)
-    in the coordinates' type, in rank order."""
+    meets this rank's grown point box (psdf.hpp:327-470), as corner triples [m, 9] (x0 y0 z0 x1 ... z2)
+    in the coordinates' type, in rank order. The grown box and the selection run on the device
+    (ssdf_grown_box, ssdf_triangles_meeting_boxes); `select` = (grown_box, meeting) replaces them with
+    host functions of the same contract, for exchange tests on CPU process groups."""
     import torch
 
+    from . import capi
+
+    grown, meeting = select if select is not None else (capi.grown_box, capi.triangles_meeting_boxes)
     dist = _dist()
     world, rank = _world(group)
-    box = grown_box(x, y, z, out)
+    box = grown(x, y, z, out)
     boxes = [torch.empty_like(box) for _ in range(world)]
     dist.all_gather(boxes, box, group=group)
-    corners = torch.stack([sx[s0.long()], sy[s0.long()], sz[s0.long()], sx[s1.long()], sy[s1.long()], sz[s1.long()],
-                           sx[s2.long()], sy[s2.long()], sz[s2.long()]], 1) if s0.numel() else \
-        torch.zeros((0, 9), dtype=sx.dtype, device=sx.device)
-    tlo = torch.stack([corners[:, 0::3].min(1).values, corners[:, 1::3].min(1).values, corners[:, 2::3].min(1).values], 1)
-    thi = torch.stack([corners[:, 0::3].max(1).values, corners[:, 1::3].max(1).values, corners[:, 2::3].max(1).values], 1)
-    send = []
-    for b in boxes:
-        # intersects(): !(tmax < bmin || tmin > bmax) on every axis
-        hit = ~((thi < b[:3]) | (tlo > b[3:])).any(1)
-        send.append(corners[hit].contiguous())
-    counts = torch.tensor([t.shape[0] for t in send], dtype=torch.int64, device=sx.device)
+    corners, per_rank = meeting(s0, s1, s2, sx, sy, sz, torch.stack(boxes))
+    counts = torch.tensor(per_rank, dtype=torch.int64, device=sx.device)
     recv = torch.empty_like(counts)
     dist.all_to_all_single(recv, counts, group=group)
     out_sizes, in_sizes = [int(v) for v in recv.tolist()], [int(v) for v in counts.tolist()]
     got = torch.empty((sum(out_sizes), 9), dtype=sx.dtype, device=sx.device)
-    dist.all_to_all_single(got, torch.cat(send), output_split_sizes=out_sizes, input_split_sizes=in_sizes,
+    dist.all_to_all_single(got, corners.contiguous(), output_split_sizes=out_sizes, input_split_sizes=in_sizes,
                            group=group)
     return got
 

@@ -1,7 +1,9 @@
 """The exchange steps of pedf / pedf_update (ssdf_b200/distributed.py) with two and three gloo
 ranks on CPU: the gathered surface (indices shifted by the vertex counts of the ranks before), the
 parts broadcast in rank order, and the candidate triangles each rank receives for pedf_update
-against a brute-force selection of every rank's triangles meeting its grown point box."""
+against a brute-force selection of every rank's triangles meeting its grown point box. The ranks have
+no GPU, so the device selection steps (tests/test_gpu_distributed.py checks them) are replaced by
+host stand-ins of the same contract; what runs here is the exchange."""
 
 import os
 import socket
@@ -30,6 +32,32 @@ def rank_data(rank, seed=5):
     return pts, out, tris, verts
 
 
+def host_grown_box(x, y, z, out):
+    """Stand-in for ssdf_grown_box on CPU tensors (the exchange tests run gloo ranks without a GPU)."""
+    import torch
+
+    if x.numel() == 0:
+        big = torch.finfo(x.dtype).max
+        return torch.tensor([big, big, big, -big, -big, -big], dtype=x.dtype)
+    r = out.to(x.dtype)
+    return torch.stack([(x - r).min(), (y - r).min(), (z - r).min(), (x + r).max(), (y + r).max(), (z + r).max()])
+
+
+def host_meeting(s0, s1, s2, sx, sy, sz, boxes):
+    """Stand-in for ssdf_triangles_meeting_boxes on CPU tensors: corners of the triangles meeting each
+    box, box after box, and the count per box."""
+    import torch
+
+    if s0.numel() == 0:
+        return torch.zeros((0, 9), dtype=sx.dtype), [0] * boxes.shape[0]
+    corners = torch.stack([sx[s0.long()], sy[s0.long()], sz[s0.long()], sx[s1.long()], sy[s1.long()], sz[s1.long()],
+                           sx[s2.long()], sy[s2.long()], sz[s2.long()]], 1)
+    tlo = torch.stack([corners[:, d::3].min(1).values for d in range(3)], 1)
+    thi = torch.stack([corners[:, d::3].max(1).values for d in range(3)], 1)
+    parts = [corners[~((thi < b[:3]) | (tlo > b[3:])).any(1)] for b in boxes]
+    return torch.cat(parts), [p.shape[0] for p in parts]
+
+
 def _rank(rank, world, port, seed, results):
     import torch
     import torch.distributed as dist
@@ -43,7 +71,8 @@ def _rank(rank, world, port, seed, results):
         x, y, z, s0, s1, s2, sx, sy, sz = t
         g = D.gather_surface(s0, s1, s2, sx, sy, sz)
         parts = [(root, *[a.numpy().copy() for a in p]) for root, *p in D.surface_parts(s0, s1, s2, sx, sy, sz)]
-        cand = D.update_candidates(x, y, z, torch.from_numpy(out), s0, s1, s2, sx, sy, sz)
+        cand = D.update_candidates(x, y, z, torch.from_numpy(out), s0, s1, s2, sx, sy, sz,
+                                   select=(host_grown_box, host_meeting))
         results[rank] = ([a.numpy().copy() for a in g], parts, cand.numpy().copy())
     finally:
         dist.destroy_process_group()

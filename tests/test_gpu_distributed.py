@@ -50,3 +50,49 @@ def test_pedf_equals_edf(group, dtype):
     out = dev(np.minimum(init, want * dtype(1.5)))
     D.pedf_update(x, y, z, s0, s1, s2, sx, sy, sz, out)
     assert np.array_equal(out.cpu().numpy(), want)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_selection_steps_on_the_device(dtype):
+    """ssdf_grown_box and ssdf_triangles_meeting_boxes against a brute-force selection: the grown box
+    of points with distances (an empty point set gives the inverted box), and for several boxes the
+    corners of every triangle meeting each, in triangle order, box after box."""
+    import torch
+
+    from ssdf_b200 import capi
+
+    tdt = torch.float64 if dtype == np.float64 else torch.float32
+    rng = np.random.default_rng(3)
+    pts = rng.uniform(-1, 1, size=(3, 5003)).astype(dtype)
+    out = rng.uniform(0.01, 0.3, size=5003)
+    x, y, z = (torch.tensor(a, device="cuda") for a in pts)
+    for odt in (torch.float64, torch.float32):
+        r = torch.tensor(out, dtype=odt, device="cuda")
+        box = capi.grown_box(x, y, z, r).cpu().numpy()
+        rr = out.astype(np.float32 if odt == torch.float32 else np.float64).astype(dtype)
+        want = np.concatenate([(pts - rr).min(1), (pts + rr).max(1)])
+        assert np.array_equal(box, want)
+    empty = torch.empty(0, dtype=tdt, device="cuda")
+    big = np.finfo(dtype).max
+    assert np.array_equal(capi.grown_box(empty, empty, empty, empty.double()).cpu().numpy(),
+                          np.array([big, big, big, -big, -big, -big], dtype=dtype))
+    mesh = W.random_soup(3000, seed=5, scale=1.5)
+    v = mesh.vertices.astype(dtype)
+    s = [torch.tensor(np.ascontiguousarray(a, dtype=np.int32), device="cuda") for a in mesh.indices()]
+    sv = [torch.tensor(np.ascontiguousarray(v[:, d]), device="cuda") for d in range(3)]
+    boxes = np.array([[-0.5, -0.5, -0.5, 0.2, 0.3, 0.1], [0.9, -2, -2, 2, 2, 2], [5, 5, 5, 6, 6, 6],
+                      [-2, -2, -2, 2, 2, 2]], dtype=dtype)
+    corners, counts = capi.triangles_meeting_boxes(*s, *sv, torch.tensor(boxes, device="cuda"))
+    c = v[mesh.triangles]  # [m, 3 corners, 3 axes]
+    tlo, thi = c.min(1), c.max(1)
+    rows, want_counts = [], []
+    for b in boxes:
+        hit = ~((thi < b[:3]) | (tlo > b[3:])).any(1)
+        rows.append(c[hit].reshape(-1, 9))
+        want_counts.append(int(hit.sum()))
+    assert counts == want_counts and counts[2] == 0 and counts[3] == mesh.nt
+    assert np.array_equal(corners.cpu().numpy(), np.concatenate(rows))
+    bad = s[0].clone()
+    bad[7] = mesh.nv + 3
+    with pytest.raises(S.SsdfError):
+        capi.triangles_meeting_boxes(bad, s[1], s[2], *sv, torch.tensor(boxes, device="cuda"))
