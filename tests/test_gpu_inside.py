@@ -38,3 +38,50 @@ def test_sample_inside_knot_and_grid_convention():
     ids = np.random.default_rng(2).choice(grid.size, 2000, replace=False)
     want, _ = oracle.sdf_points(oracle.grid_points(grid)[:, ids], mesh)
     assert np.array_equal(got[ids], (want < 0).astype(np.uint8))
+
+
+def ray_parity(points, mesh, direction):
+    """Inside by the parity of a ray's crossings (the rule of the reference's cuBQL build), brute
+    force in double: Moller-Trumbore against every triangle."""
+    v = mesh.vertices[mesh.triangles]  # [m, 3, 3]
+    a, e1, e2 = v[:, 0], v[:, 1] - v[:, 0], v[:, 2] - v[:, 0]
+    d = np.asarray(direction, dtype=np.float64)
+    h = np.cross(d, e2)
+    det = np.einsum("ij,ij->i", e1, h)
+    ok = np.abs(det) > 1e-14
+    inv = np.where(ok, 1.0 / np.where(ok, det, 1.0), 0.0)
+    flags = []
+    for p in points.T:
+        s = p - a
+        u = inv * np.einsum("ij,ij->i", s, h)
+        q = np.cross(s, e1)
+        w = inv * (q @ d)
+        t = inv * np.einsum("ij,ij->i", e2, q)
+        hit = ok & (u >= 0) & (w >= 0) & (u + w <= 1) & (t > 0)
+        flags.append(int(hit.sum()) % 2)
+    return np.array(flags, dtype=np.uint8)
+
+
+def test_inside_on_an_open_mesh():
+    """An open mesh (a sphere with its top cap removed): the flags are the sign of the signed
+    distance -- the side of the nearest surface its pseudo-normals face -- which needs no closed
+    surface. The reference's ray parity is defined only for closed surfaces: on this open cup it depends
+    on the ray's direction. On a closed sphere both rules agree away from the surface."""
+    full = W.icosphere(3, radius=1.0, displacement=0.0)
+    cen = full.vertices[full.triangles].mean(1)
+    cup = W.Mesh(full.vertices, full.triangles[cen[:, 2] < 0.6])
+    rng = np.random.default_rng(8)
+    p = rng.uniform(-1.2, 1.2, size=(3, 3000))
+    got = S.points_inside_bvh(p, cup)
+    sd, _ = oracle.sdf_points(p, cup)
+    assert np.array_equal(got, (sd < 0).astype(np.uint8))  # what this library returns, everywhere
+    # a point in the cup below the opening, near its axis: inside by the pseudo-normal rule; the ray
+    # parity says inside along -z (one crossing) and outside along +z (it leaves through the opening)
+    q = np.array([[0.0], [0.0], [0.5]])
+    assert S.points_inside_bvh(q, cup)[0] == 1
+    assert ray_parity(q, cup, (0, 0, -1))[0] == 1 and ray_parity(q, cup, (0, 0, 1))[0] == 0
+    # closed sphere: the two rules agree away from the surface
+    r = np.linalg.norm(p, axis=0)
+    far = np.abs(r - 1.0) > 0.05
+    sub = p[:, far][:, :400]
+    assert np.array_equal(S.points_inside_bvh(sub, full), ray_parity(sub, full, (0.3, 0.5, 0.81)))
