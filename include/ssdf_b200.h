@@ -515,6 +515,24 @@ int ssdf_triangles_meeting_boxes(ptrdiff_t nselements, const int *s0, const int 
                                  int nboxes, const void *boxes, void *corners, long long capacity, long long *counts,
                                  void *stream);
 
+/* ---- ssdf::pedf / ssdf::pedf_update (distributed/psdf.hpp:149-302, 304-482) over NCCL --------
+ * One process per GPU, every rank of the communicator calls it (collective). comm is an ncclComm_t;
+ * this rank's points (x, y, z), its part of the surface (s0, s1, s2 over its own nspoints vertices)
+ * and out are DEVICE arrays; the exchanges run on `stream` and the call returns when out holds
+ * min(out, distance to the union of every rank's part) -- bitwise what the single-process edf_bvh
+ * gives on the whole surface. coord_type / out_type: <F64, F64>, <F32, F64> or <F32, F32>.
+ * ssdf_pedf_nccl gathers the whole surface (SSDF_USE_ALLGATHER=1, default) or broadcasts the parts one
+ * after the other (0), as the reference; ssdf_pedf_update_nccl exchanges only the triangles meeting
+ * each rank's points' box grown by their current out (which must hold upper bounds). NCCL is opened
+ * at the first call (libnccl.so.2); without it these return SSDF_ERR_NOT_SUPPORTED. */
+int ssdf_pedf_nccl(void *comm, ptrdiff_t npoints, const void *x, const void *y, const void *z, ptrdiff_t nselements,
+                   const int *s0, const int *s1, const int *s2, ptrdiff_t nspoints, const void *sx, const void *sy,
+                   const void *sz, int coord_type, int out_type, void *out, void *stream);
+int ssdf_pedf_update_nccl(void *comm, ptrdiff_t npoints, const void *x, const void *y, const void *z,
+                          ptrdiff_t nselements, const int *s0, const int *s1, const int *s2, ptrdiff_t nspoints,
+                          const void *sx, const void *sy, const void *sz, int coord_type, int out_type, void *out,
+                          void *stream);
+
 /* ---- serving loop: continuous batching over resident meshes (no reference counterpart) ------- */
 
 typedef struct ssdf_server ssdf_server;

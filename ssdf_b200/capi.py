@@ -94,6 +94,8 @@ _sig("ssdf_mesh_filter_info", [_vp, C.POINTER(C.c_float), C.POINTER(C.c_int), C.
 _sig("ssdf_grown_box", [_pd, _vp, _vp, _vp, _vp, C.c_int, C.c_int, _vp, _vp])
 _sig("ssdf_triangles_meeting_boxes", [_pd, _vp, _vp, _vp, _pd, _vp, _vp, _vp, C.c_int, C.c_int, _vp, _vp,
                                       C.c_longlong, C.POINTER(C.c_longlong), _vp])
+for _n in ("ssdf_pedf_nccl", "ssdf_pedf_update_nccl"):
+    _sig(_n, [_vp, _pd, _vp, _vp, _vp, _pd, _vp, _vp, _vp, _pd, _vp, _vp, _vp, C.c_int, C.c_int, _vp, _vp])
 _sig("ssdf_edf_device", [C.c_int, _pd, _vp, _vp, _vp, _pd, _vp, _vp, _vp, _pd, _vp, _vp, _vp, C.c_int, _vp, _vp, _vp])
 _sig("ssdf_query_points", [_vp, _pd, _vp, _vp, _vp, _vp, _ip, _vp, _vp, _vp, C.POINTER(QueryOpts), _vp])
 _sig("ssdf_query_grid", [_vp, _pd, _pd, _pd, C.POINTER(C.c_double * 3), C.POINTER(C.c_double * 3), _vp, _ip,
@@ -182,7 +184,7 @@ EXPORTED = ["ssdf_status_string", "ssdf_last_error", "ssdf_b200_version", "ssdf_
             "ssdf_b200_closest_point_bvh_fd", "ssdf_b200_closest_point_bvh_dd", "ssdf_b200_sample_sqedf_bvh_ff", "ssdf_b200_sample_sqedf_bvh_dd",
             "ssdf_b200_sample_sdf_bvh_ff", "ssdf_b200_sample_sdf_bvh_dd", "ssdf_b200_edf_index_dd",
             "ssdf_b200_edf_index_ff", "ssdf_b200_sdf_points_dd", "ssdf_b200_sample_sdf_index_bvh_dd",
-            "ssdf_mesh_create", "ssdf_mesh_destroy", "ssdf_mesh_stats", "ssdf_mesh_filter_info", "ssdf_edf_device", "ssdf_grown_box", "ssdf_triangles_meeting_boxes", "ssdf_query_points", "ssdf_query_grid",
+            "ssdf_mesh_create", "ssdf_mesh_destroy", "ssdf_mesh_stats", "ssdf_mesh_filter_info", "ssdf_edf_device", "ssdf_grown_box", "ssdf_triangles_meeting_boxes", "ssdf_pedf_nccl", "ssdf_pedf_update_nccl", "ssdf_query_points", "ssdf_query_grid",
             "ssdf_last_query_counts", "ssdf_b200_fma_peak", "ssdf_batch_create", "ssdf_batch_destroy", "ssdf_batch_clear",
             "ssdf_batch_size", "ssdf_batch_add_grid", "ssdf_batch_add_grid_slab", "ssdf_batch_add_points", "ssdf_batch_run",
             "ssdf_batch_last_blocks", "ssdf_query_grid_noalloc", "ssdf_query_grid_noalloc_max", "ssdf_server_create",

@@ -96,3 +96,61 @@ def test_selection_steps_on_the_device(dtype):
     bad[7] = mesh.nv + 3
     with pytest.raises(S.SsdfError):
         capi.triangles_meeting_boxes(bad, s[1], s[2], *sv, torch.tensor(boxes, device="cuda"))
+
+
+def one_rank_comm():
+    """A one-rank NCCL communicator on the current device (this machine gives one GPU)."""
+    import ctypes as C
+
+    import torch
+
+    torch.cuda.init()
+    nccl = C.CDLL("libnccl.so.2")
+
+    class UniqueId(C.Structure):
+        _fields_ = [("internal", C.c_char * 128)]
+
+    uid = UniqueId()
+    assert nccl.ncclGetUniqueId(C.byref(uid)) == 0
+    comm = C.c_void_p()
+    assert nccl.ncclCommInitRank(C.byref(comm), 1, uid, 0) == 0
+    return nccl, comm
+
+
+@pytest.mark.parametrize("gt", [(np.float64, np.float64), (np.float32, np.float64), (np.float32, np.float32)])
+@pytest.mark.parametrize("allgather", ["1", "0"])
+def test_pedf_over_nccl_c_abi(gt, allgather, monkeypatch):
+    """ssdf_pedf_nccl / ssdf_pedf_update_nccl (the C ABI under include/ssdf_distributed.hpp) on one rank:
+    pedf equals the drop-in edf_bvh on the whole surface bit for bit, in both modes and every type pair,
+    the incoming out kept where smaller; pedf_update from upper bounds gives the same values."""
+    import ctypes as C
+
+    import torch
+
+    gdt, tdt = gt
+    monkeypatch.setenv("SSDF_USE_ALLGATHER", allgather)
+    mesh = W.torus(0.7, 0.25, nu=60, nv=30, jitter=0.01, seed=2)
+    lo, hi = mesh.bbox()
+    pts = W.uniform_points(7001, lo - 0.3, hi + 0.3, seed=12).astype(gdt)
+    init = np.where(np.arange(7001) % 5 == 0, 0.02, np.finfo(tdt).max).astype(tdt)
+    want = S.edf_bvh(pts, mesh, out=init, gdtype=gdt, tdtype=tdt)
+    td = {np.float64: torch.float64, np.float32: torch.float32}
+    x, y, z = (torch.tensor(np.ascontiguousarray(a), device="cuda") for a in pts)
+    s0, s1, s2 = (torch.tensor(np.ascontiguousarray(a, dtype=np.int32), device="cuda") for a in mesh.indices())
+    sx, sy, sz = (torch.tensor(np.ascontiguousarray(a, dtype=gdt), device="cuda") for a in mesh.coords())
+    ct = S.F64 if gdt == np.float64 else S.F32
+    ot = S.F64 if tdt == np.float64 else S.F32
+    nccl, comm = one_rank_comm()
+    stream = torch.cuda.current_stream().cuda_stream
+    try:
+        for fn, start in (("ssdf_pedf_nccl", init), ("ssdf_pedf_update_nccl", (want * 1.5).astype(tdt))):
+            expect = S.edf_bvh(pts, mesh, out=start, gdtype=gdt, tdtype=tdt)
+            out = torch.tensor(start, dtype=td[tdt], device="cuda")
+            st = getattr(S.lib, fn)(comm, x.numel(), x.data_ptr(), y.data_ptr(), z.data_ptr(), s0.numel(),
+                                    s0.data_ptr(), s1.data_ptr(), s2.data_ptr(), sx.numel(), sx.data_ptr(),
+                                    sy.data_ptr(), sz.data_ptr(), ct, ot, out.data_ptr(), C.c_void_p(stream))
+            assert st == S.SSDF_OK, S.last_error()
+            # pedf_update from bounds 1.5x the answer: every triangle that can improve them is exchanged
+            assert np.array_equal(out.cpu().numpy(), expect), fn
+    finally:
+        nccl.ncclCommDestroy(comm)

@@ -107,6 +107,26 @@ def test_cpp_header_compiles_against_c_abi(tmp_path):
     assert res.returncode == 0, res.stderr
 
 
+def test_distributed_header_compiles_against_c_abi(tmp_path):
+    """include/ssdf_distributed.hpp (pedf / pedf_update over an NCCL communicator) compiles and links."""
+    import subprocess
+
+    src = tmp_path / "dist.cpp"
+    src.write_text(
+        '#include "ssdf_distributed.hpp"\n'
+        "int main() {\n"
+        "  (void)&ssdf::pedf<double, double, int>;\n"
+        "  (void)&ssdf::pedf<float, double, int>;\n"
+        "  (void)&ssdf::pedf_update<float, float, int>;\n"
+        "  (void)&ssdf::pedf_update<double, double, int>;\n"
+        "  return 0;\n}\n")
+    lib = os.path.join(ROOT, "ssdf_b200", "_lib")
+    res = subprocess.run(["g++", "-std=c++17", f"-I{ROOT}/include", "-I/usr/local/cuda/include", str(src), "-o",
+                          str(tmp_path / "dist"), f"-L{lib}", "-lssdf_b200", f"-Wl,-rpath,{lib}"],
+                         capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr
+
+
 def test_build_imports_without_the_library():
     """``from ssdf_b200 import build`` (the first step of a fresh build) must not load the CUDA
     binding, which needs the library it is about to build."""
