@@ -626,7 +626,10 @@ def serving_leg(S, args):
             lo, hi = m.bbox()
             pad = 0.1 * m.diagonal()
             payloads.append(("points", mid, W.uniform_points(n, lo - pad, hi + pad, seed=k), n))
-    srv = S.Server(memory_budget=120 << 30, max_batch_queries=1 << 22, max_batch_jobs=64)
+    # admission limit: at most 8M queries waiting to be packed (about two batches' worth); past it a
+    # submit is refused (SSDF_ERR_BUSY) and counted, so overload shows as rejections, not as latency
+    srv = S.Server(memory_budget=120 << 30, max_batch_queries=1 << 22, max_batch_jobs=64,
+                   max_queued_queries=8 << 20)
     ids = [srv.add_mesh(m) for m, _ in sets]
     # admit every mesh once (building is not part of the latency being measured)
     for mid in range(len(sets)):
@@ -637,16 +640,22 @@ def serving_leg(S, args):
         tickets = []
         t_end = time.perf_counter() + args.serve_seconds
         arrivals = np.random.default_rng(int(lam))
+        offered = 0
         while time.perf_counter() < t_end:
             kind, mid, q, n = payloads[int(arrivals.integers(len(payloads)))]
-            tickets.append(srv.submit_grid(ids[mid], q) if kind == "grid" else srv.submit_points(ids[mid], q))
+            offered += 1
+            try:
+                tickets.append(srv.submit_grid(ids[mid], q) if kind == "grid" else srv.submit_points(ids[mid], q))
+            except S.SsdfError as ex:
+                if ex.status != S.SSDF_ERR_BUSY:
+                    raise
             time.sleep(float(arrivals.exponential(1.0 / lam)))
         for t in tickets:
             srv.wait(t, timeout=300)
         st = srv.stats()
-        out["rates"].append({"lambda_per_s": lam, "requests": st["completed"], "p50_ms": st["p50_ms"],
-                             "p99_ms": st["p99_ms"], "queries_per_s": st["queries"] / max(st["seconds"], 1e-9),
-                             "batches": st["batches"]})
+        out["rates"].append({"lambda_per_s": lam, "offered": offered, "requests": st["completed"],
+                             "rejected": st["rejected"], "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+                             "queries_per_s": st["queries"] / max(st["seconds"], 1e-9), "batches": st["batches"]})
     srv.close()
     return out
 
