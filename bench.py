@@ -602,7 +602,56 @@ def batched_leg(S, args):
     res["speedup_fixup_vs_fp64"] = res["fixup"]["queries_per_s"] / res["fp64"]["queries_per_s"]
     for dm in dms:
         dm.close()
+    res["mixed_arithmetic"] = mixed_batch(S)
     return res
+
+
+def mixed_batch(S):
+    """A sliver-heavy mesh (the beam lattice, 160^3 grid) in a fix-up batch with 16 tori: its job runs in
+    the batch's FP64 table. Reports the mixed batch's time against the tori's fix-up batch alone plus
+    the beam job alone in FP64 (the arithmetic it gets alone)."""
+    import torch
+
+    from ssdf_b200 import workloads as W
+
+    beams = W.beam_lattice()
+    jobs = [(S.DeviceMesh(beams), W.Grid((160, 160, 160), (-0.1, -0.1, -0.1), (1.1, 1.1, 1.1)))]
+    for k in range(16):
+        m = W.torus(0.6, 0.2, nu=64 + 32 * k, nv=24 + 8 * k, jitter=0.01, seed=50 + k, center=(2.0 * k, 0.0, 0.0))
+        jobs.append((S.DeviceMesh(m), W.Grid.padded_nodes(m, 96, 0.1)))
+    outs = [torch.empty(g.size, dtype=torch.float64, device="cuda") for _, g in jobs]
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, reps=4):
+        ms = []
+        for r in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if r:
+                ms.append(e0.elapsed_time(e1))
+        return statistics.median(ms)
+
+    def batch_of(sel):
+        b = S.Batch(len(sel), S.PREC_F32_FIXUP)
+        for i in sel:
+            b.add_grid(jobs[i][0], jobs[i][1], outs[i])
+        return b
+
+    mixed = batch_of(range(len(jobs)))
+    tori = batch_of(range(1, len(jobs)))
+    t_mixed = timed(lambda: mixed.run(use_graph=True, stream=stream))
+    t_tori = timed(lambda: tori.run(use_graph=True, stream=stream))
+    t_beam = timed(lambda: jobs[0][0].query_grid(jobs[0][1], outs[0], None, precision=S.PREC_F64, output=S.OUT_SDF,
+                                                 stream=stream))
+    for b in (mixed, tori):
+        b.close()
+    for dm, _ in jobs:
+        dm.close()
+    return {"beam_lattice_grid": 160 ** 3, "tori": 16, "mixed_ms": t_mixed, "tori_fixup_alone_ms": t_tori,
+            "beam_fp64_alone_ms": t_beam, "beam_share_in_mix_over_alone": (t_mixed - t_tori) / t_beam}
 
 
 def serving_leg(S, args):
