@@ -216,7 +216,7 @@ def cpu_reference_points(mesh, pts_grid, nsample, dtype, seed=17, steps=1):
     pt_ids = np.sort(rng.choice(pts.shape[1], size=half, replace=False))
     a = pts[:, pt_ids]
     ids = np.sort(rng.choice(grid.size, size=nsample - half, replace=False))
-    b = oracle.grid_points(grid)[:, ids].astype(dtype)
+    b = oracle.grid_points(grid, dtype=dtype)[:, ids]  # the nodes in G's arithmetic, as the GPU grid
     q = np.concatenate([a, b], axis=1).astype(dtype)
     times = []
     vals = None

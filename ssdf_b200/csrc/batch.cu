@@ -313,7 +313,7 @@ int ssdf_batch_run(ssdf_batch *b, int use_graph, void *stream_) {
     int k = 0, k64 = 0;
     for (int r = 0; r < njobs; r++) {
         QueryArgs a = b->jobs[order[r]];
-        a.warp_budget = resolve_warp_budget(a.warp_budget, nq);
+        a.warp_budget = resolve_warp_budget(a.warp_budget, nq, a.m.nt);
         if (a.is_grid) a.grid_steps = steps;
         if (sort_points && !a.is_grid && a.npoints >= kSortMinPoints) {
             int *ord = nullptr;
