@@ -71,6 +71,10 @@ def parse_args():
     p.add_argument("--batch-meshes", type=int, default=256)
     p.add_argument("--serve-meshes", type=int, default=512)
     p.add_argument("--serve-seconds", type=float, default=3.0)
+    p.add_argument("--serve-batch-queries", type=int, default=1 << 22, help="serving: queries per batch")
+    p.add_argument("--serve-split", type=int, default=0, help="serving: parts of larger requests (0: default)")
+    p.add_argument("--serve-queue", type=int, default=8 << 20, help="serving: admission limit, queued queries")
+    p.add_argument("--serve-slots", type=int, default=0, help="serving: batches in flight (0: default)")
     a = p.parse_args()
     if a.grid is None:
         a.grid = DEFAULT_GRID[a.workload]
@@ -677,13 +681,15 @@ def serving_leg(S, args):
             payloads.append(("points", mid, W.uniform_points(n, lo - pad, hi + pad, seed=k), n))
     # admission limit: at most 8M queries waiting to be packed (about two batches' worth); past it a
     # submit is refused (SSDF_ERR_BUSY) and counted, so overload shows as rejections, not as latency
-    srv = S.Server(memory_budget=120 << 30, max_batch_queries=1 << 22, max_batch_jobs=64,
-                   max_queued_queries=8 << 20)
+    srv = S.Server(memory_budget=120 << 30, max_batch_queries=args.serve_batch_queries, max_batch_jobs=64,
+                   max_queued_queries=args.serve_queue, split_queries=args.serve_split, slots=args.serve_slots)
     ids = [srv.add_mesh(m) for m, _ in sets]
     # admit every mesh once (building is not part of the latency being measured)
     for mid in range(len(sets)):
         srv.wait(srv.submit_points(ids[mid], np.zeros((3, 1))))
-    out = {"meshes": len(sets), "payloads": len(payloads), "seconds_per_rate": args.serve_seconds, "rates": []}
+    out = {"meshes": len(sets), "payloads": len(payloads), "seconds_per_rate": args.serve_seconds, "rates": [],
+           "server": {"max_batch_queries": args.serve_batch_queries, "split_queries": args.serve_split or "default",
+                      "max_queued_queries": args.serve_queue, "slots": args.serve_slots or "default"}}
     for lam in (50.0, 200.0, 800.0, 3200.0):
         srv.reset_stats()
         tickets = []
