@@ -1440,7 +1440,7 @@ int grid_steps_for(long long one_step_blocks) {
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         r = std::max(1, sms) * SSDF_B200_QUERY_MIN_BLOCKS;
     }
-    int steps = kMaxGridSteps;
+    int steps = kDefaultGridSteps;
     while (steps > 1 && one_step_blocks / steps < 4ll * r) steps >>= 1;
     return steps;
 }

@@ -221,7 +221,8 @@ constexpr int kQ = SSDF_B200_QUERIES_PER_LANE;
 // step). A lane starts each step from the closest triangle it found one step below, 2 kQ nodes away:
 // a tight upper bound (SSDF_B200_SEED=0 starts from the incoming bound alone). Large grids take
 // kMaxGridSteps; a grid too small to fill the GPU with such columns takes fewer (grid_steps_for).
-constexpr int kMaxGridSteps = 4;
+constexpr int kMaxGridSteps = 8;      // the most SSDF_B200_GRID_STEPS may ask for
+constexpr int kDefaultGridSteps = 4;   // the most the launch rule picks
 __host__ __device__ inline long long grid_blocks_x(long long nx) { return (nx + 7) / 8; }
 __host__ __device__ inline long long grid_blocks_y(long long ny) { return (ny + 7) / 8; }
 __host__ __device__ inline long long grid_block_planes(int steps) { return 2ll * kQ * steps; }
