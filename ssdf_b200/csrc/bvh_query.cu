@@ -69,9 +69,9 @@ __device__ __forceinline__ float finf() { return __int_as_float(0x7f800000); }
 
 // ---- query mapping ------------------------------------------------------------------------------
 
-// Each lane answers kQ queries. Grid: a block covers an 8 (x) x 8 (y) column of nodes and, at step
-// `step`, the 2 kQ z-planes from (column * grid_steps + step) * 2 kQ on; a warp takes a 4 x 4 x 2kQ
-// brick of it, lane (lx, ly, lz) kQ consecutive z nodes. Point lists: query
+// Each lane answers kQ queries. Grid: a block covers an 8 (x) x 4 (y) column of nodes and, at step
+// `step`, the 4 kQ z-planes from (column * grid_steps + step) * 4 kQ on; a warp takes a 4 x 4 x 2kQ
+// brick of them, lane (lx, ly, lz) kQ consecutive z nodes. Point lists: query
 // (block * kQ + s) * 128 + thread, so each of a lane's queries is a coalesced load.
 __device__ __forceinline__ bool map_query(const QueryArgs &a, long long b, int step, int s, long long &q,
                                           long long &i, long long &j, long long &k) {
@@ -86,8 +86,8 @@ __device__ __forceinline__ bool map_query(const QueryArgs &a, long long b, int s
     const long long by = r % byn, bz = r / byn;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     i = bx * 8 + (warp & 1) * 4 + (lane & 3);
-    j = by * 8 + (warp >> 1) * 4 + ((lane >> 2) & 3);
-    k = ((bz * a.grid_steps + step) * 2 + (lane >> 4)) * kQ + s;
+    j = by * 4 + ((lane >> 2) & 3);
+    k = (((bz * a.grid_steps + step) * 4 + (warp >> 1) * 2) + (lane >> 4)) * kQ + s;
     q = i + a.nx * (j + a.ny * k);
     return i < a.nx && j < a.ny && k < a.nz;
 }

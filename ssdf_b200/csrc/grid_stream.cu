@@ -5,7 +5,7 @@
 // arrays. The query kernel and the device-to-host copy of its results would run one after the other;
 // here the copy of each slab chunk starts as soon as the kernel has finished that chunk:
 //
-//   - a grid launch's blocks are slab-major (columns of 8 x 8 x grid_block_planes nodes, x fastest,
+//   - a grid launch's blocks are slab-major (columns of 8 x 4 x grid_block_planes nodes, x fastest,
 //     then y, then z), so the blocks of whole z-slabs cover one contiguous range of the output;
 //   - the last block of a chunk to finish raises the chunk's flag in page-locked host memory
 //     (signal_chunk in bvh_query.cu), and this thread, which would otherwise wait for the launch,

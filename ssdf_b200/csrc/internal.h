@@ -216,16 +216,17 @@ bool default_wide();
 #define SSDF_B200_QUERIES_PER_LANE 1
 #endif
 constexpr int kQ = SSDF_B200_QUERIES_PER_LANE;
-// Grid launches: a block of 128 lanes covers an 8 x 8 column of nodes and walks it upwards in
-// QueryArgs::grid_steps steps (1 .. kMaxGridSteps) of 2 kQ z-planes (each warp a 4 x 4 x 2kQ brick per
-// step). A lane starts each step from the closest triangle it found one step below, 2 kQ nodes away:
-// a tight upper bound (SSDF_B200_SEED=0 starts from the incoming bound alone). Large grids take
-// kMaxGridSteps; a grid too small to fill the GPU with such columns takes fewer (grid_steps_for).
+// Grid launches: a block of 128 lanes covers an 8 x 4 column of nodes and walks it upwards in
+// QueryArgs::grid_steps steps (1 .. kMaxGridSteps) of 4 kQ z-planes, each step an 8 x 4 x 4kQ brick
+// of nodes (each warp a 4 x 4 x 2kQ part of it). A lane starts each step from the closest triangle it
+// found one step below, 4 kQ nodes away: a tight upper bound (SSDF_B200_SEED=0 starts from the
+// incoming bound alone). Large grids take kDefaultGridSteps; a grid too small to fill the GPU with
+// such columns takes fewer (grid_steps_for).
 constexpr int kMaxGridSteps = 8;      // the most SSDF_B200_GRID_STEPS may ask for
 constexpr int kDefaultGridSteps = 4;   // the most the launch rule picks
 __host__ __device__ inline long long grid_blocks_x(long long nx) { return (nx + 7) / 8; }
-__host__ __device__ inline long long grid_blocks_y(long long ny) { return (ny + 7) / 8; }
-__host__ __device__ inline long long grid_block_planes(int steps) { return 2ll * kQ * steps; }
+__host__ __device__ inline long long grid_blocks_y(long long ny) { return (ny + 3) / 4; }
+__host__ __device__ inline long long grid_block_planes(int steps) { return 4ll * kQ * steps; }
 __host__ __device__ inline long long grid_blocks_z(long long nz, int steps) {
     return (nz + grid_block_planes(steps) - 1) / grid_block_planes(steps);
 }

@@ -104,10 +104,17 @@ def test_results_same_alone_and_in_the_mix():
 
 
 def test_rejects_oversized_and_unknown():
+    """A grid whose z-plane alone exceeds a batch cannot be split into slabs and is refused; larger
+    requests are otherwise answered in parts (8,000 nodes through 1,000-query batches here)."""
+    mesh = W.icosphere(1)
     srv = S.Server(max_batch_queries=1000, max_batch_jobs=4)
-    mid = srv.add_mesh(W.icosphere(1))
+    mid = srv.add_mesh(mesh)
     with pytest.raises(S.SsdfError):
-        srv.submit_grid(mid, W.Grid((20, 20, 20), (0, 0, 0), (1, 1, 1)))
+        srv.submit_grid(mid, W.Grid((40, 40, 3), (0, 0, 0), (1, 1, 1)))  # 1,600 nodes a plane
+    g = W.Grid((20, 20, 20), (-1, -1, -1), (1, 1, 1))
+    d, tri = srv.wait(srv.submit_grid(mid, g))
+    wd, wt = S.sample_sdf_bvh(mesh, g, with_index=True)
+    assert np.array_equal(d, wd) and np.array_equal(tri, wt)
     with pytest.raises(S.SsdfError):
         srv.submit_points(mid + 5, np.zeros((3, 10)))
     srv.close()
