@@ -221,11 +221,12 @@ struct Tri32 {
     int id;
 };
 
-// The fix-up filter's record of leaf position p (DeviceMesh::filt32, 4 x float4): the precomputed
-// triangle (or proxy); the fourth vector holds the id and the proxy flag.
+// The fix-up filter's record of leaf position p (DeviceMesh::filt32, 3 x float4): the precomputed
+// triangle (or proxy, the sign bit of its ab.ab set).
 __device__ __forceinline__ FiltRec load_filt(const float4 *__restrict__ f, int p) {
-    const float4 u = __ldg(f + 4 * p), v = __ldg(f + 4 * p + 1), w = __ldg(f + 4 * p + 2);
-    return FiltRec{u.x, u.y, u.z, v.x, v.y, v.z, w.x, w.y, w.z, u.w, v.w, w.w};
+    const float4 u = __ldg(f + 3 * p), v = __ldg(f + 3 * p + 1), w = __ldg(f + 3 * p + 2);
+    const float pen = (__float_as_uint(u.w) >> 31) ? __int_as_float(0x7f800000) : 0.f;
+    return FiltRec{u.x, u.y, u.z, v.x, v.y, v.z, w.x, w.y, w.z, fabsf(u.w), v.w, w.w, pen};
 }
 __device__ __forceinline__ Tri32 load_tri32(const float4 *__restrict__ t, int p) {
     const float4 u = __ldg(t + 3 * p), v = __ldg(t + 3 * p + 1), w = __ldg(t + 3 * p + 2);
@@ -412,9 +413,8 @@ struct FastPolicy {
     // the triangle when it meets it.
     __device__ __forceinline__ void seed(int q, int pos) {
         const FiltRec t = load_filt(m.filt32, pos);
-        const float pen = __ldg(m.filt32 + 4 * pos + 3).y;
         const float d2 = tri_dist_sq_filter(px[q], py[q], pz[q], t);
-        if (pen == 0.f && d2 < best[q]) {
+        if (t.pen == 0.f && d2 < best[q]) {
             best[q] = d2;
             thr[q] = window_thr(best[q], tau_rel, m.coord_scale);
         }
@@ -486,7 +486,7 @@ struct FastPolicy {
     __device__ __forceinline__ void leaf(int first, int n, unsigned mask, Counters &cnt) {
         for (int k = 0; k < n; k++) {
             const FiltRec t = load_filt(m.filt32, first + k);
-            const float pen = __ldg(m.filt32 + 4 * (first + k) + 3).y;
+            const float pen = t.pen;
 #pragma unroll
             for (int q = 0; q < Q; q++) {
                 if (!((mask >> q) & 1u)) continue;

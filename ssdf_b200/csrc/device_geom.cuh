@@ -126,6 +126,7 @@ __device__ __forceinline__ void tri_closest_point_exact(const T px, const T py, 
 // d the distance; the fix-up window is sized per mesh to twice that (mesh_build.cu, filter_bound).
 struct FiltRec {
     float ax, ay, az, abx, aby, abz, acx, acy, acz, abab, acac, abac;
+    float pen;  // 0, or +inf for a proxy (a lower bound that may enter the window, never its centre)
 };
 __device__ __forceinline__ float tri_dist_sq_filter(const float px, const float py, const float pz, const FiltRec &r) {
     const float apx = px - r.ax, apy = py - r.ay, apz = pz - r.az;

@@ -73,10 +73,10 @@ struct DeviceMesh {
     const double2 *nodes4_64 = nullptr;  // [14 * nnodes4] or null
     const float4 *tris32 = nullptr;    // [3 * nt], leaf order
     const double2 *tris64 = nullptr;   // [5 * nt], leaf order, or null
-    // the fix-up path's FP32 filter records, [4 * nt], leaf order, with the double data or null:
-    // (ax, ay, az, ab.ab), (abx, aby, abz, ac.ac), (acx, acy, acz, ab.ac), (id bits, pen, -, -) of the
-    // triangle (pen 0), or of a well-conditioned proxy containing an ill-conditioned one (pen +inf;
-    // mesh_build.cu, filter_record)
+    // the fix-up path's FP32 filter records, [3 * nt], leaf order, with the double data or null:
+    // (ax, ay, az, ab.ab), (abx, aby, abz, ac.ac), (acx, acy, acz, ab.ac) of the triangle, or of a
+    // well-conditioned proxy containing an ill-conditioned one, marked by the sign bit of ab.ab
+    // (mesh_build.cu, filter_record)
     const float4 *filt32 = nullptr;
     // sign data, caller's triangle order
     const int *s0 = nullptr, *s1 = nullptr, *s2 = nullptr;  // [nt]

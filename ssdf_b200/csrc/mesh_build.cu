@@ -439,8 +439,8 @@ __global__ void k_depth(int n, int L, const int *__restrict__ count, const int *
 // contains it: PQ widened by L/4 at both ends (L = |PQ|) and an apex L/2 off its middle, towards R in
 // the triangle's plane. R projects inside PQ (PQ is the longest edge) at height below L/8, and the
 // proxy is at least L/6 high over all of PQ, so it contains P, Q and R; its distance is a lower
-// bound of the triangle's, and its height (1/3 of its base) keeps the float test accurate. The
-// record's w.z is 0, or +inf for a proxy (whose key may enter the window but never move its centre).
+// bound of the triangle's, and its height (1/3 of its base) keeps the float test accurate. A proxy's
+// record has the sign bit of its ab.ab set: its key may enter the window but never moves its centre.
 __device__ bool filter_record(double ax, double ay, double az, double bx, double by, double bz, double cx,
                               double cy, double cz, int t, float4 *__restrict__ out) {
     const double abx = bx - ax, aby = by - ay, abz = bz - az, acx = cx - ax, acy = cy - ay, acz = cz - az;
@@ -490,10 +490,12 @@ __device__ bool filter_record(double ax, double ay, double az, double bx, double
     const double bb = eb[0] * eb[0] + eb[1] * eb[1] + eb[2] * eb[2];
     const double cc = ec[0] * ec[0] + ec[1] * ec[1] + ec[2] * ec[2];
     const double bc = eb[0] * ec[0] + eb[1] * ec[1] + eb[2] * ec[2];
-    out[0] = make_float4(f[0][0], f[0][1], f[0][2], float(bb));
+    // a proxy is marked by the sign bit of ab.ab (never negative otherwise)
+    const float fbb = float(bb);
+    out[0] = make_float4(f[0][0], f[0][1], f[0][2], ill ? __int_as_float(__float_as_int(fbb) | 0x80000000) : fbb);
     out[1] = make_float4(float(eb[0]), float(eb[1]), float(eb[2]), float(cc));
     out[2] = make_float4(float(ec[0]), float(ec[1]), float(ec[2]), float(bc));
-    out[3] = make_float4(__int_as_float(t), ill ? __int_as_float(0x7f800000) : 0.f, 0.f, 0.f);
+    (void)t;
     return ill;
 }
 
@@ -568,9 +570,9 @@ __global__ void k_tri_records(int nt, const int *__restrict__ sorted_ids, const 
     t32[3 * p + 1] = make_float4(float(by), float(bz), float(cx), float(cy));
     t32[3 * p + 2] = make_float4(float(cz), __int_as_float(t), 0.f, 0.f);
     if (filt) {
-        if (filter_record(ax, ay, az, bx, by, bz, cx, cy, cz, t, filt + 4 * size_t(p))) atomicAdd(nill, 1);
+        if (filter_record(ax, ay, az, bx, by, bz, cx, cy, cz, t, filt + 3 * size_t(p))) atomicAdd(nill, 1);
         float term;
-        if (filter_bound(filt + 4 * size_t(p), &term))
+        if (filter_bound(filt + 3 * size_t(p), &term))
             atomicMax(nill + 1, __float_as_int(term));  // non-negative floats order like their bits
         else
             atomicAdd(nill + 2, 1);
@@ -899,7 +901,7 @@ static int mesh_build_impl(MeshStorage *s, MeshStorage *tmp, DeviceMesh *m, int 
     double2 *t64 = nullptr;
     SSDF_CHECK(dalloc(s, &t32, 3 * size_t(nt), stream));
     if (keep64) SSDF_CHECK(dalloc(s, &t64, 5 * size_t(nt), stream));
-    if (keep64) SSDF_CHECK(dalloc(s, &filt, 4 * size_t(nt), stream));  // the fix-up path's filter records
+    if (keep64) SSDF_CHECK(dalloc(s, &filt, 3 * size_t(nt), stream));  // the fix-up path's filter records
     k_tri_records<<<grid_blocks(nt, 256), 256, 0, stream>>>(nt, ids, s0, s1, s2, vx, vy, vz, t32, t64, filt,
                                                             flags + 10);
     LAUNCH_CHECK("k_tri_records");
