@@ -74,7 +74,7 @@ def parse_args():
     p.add_argument("--serve-batch-queries", type=int, default=1 << 22, help="serving: queries per batch")
     p.add_argument("--serve-split", type=int, default=0, help="serving: parts of larger requests (0: default)")
     p.add_argument("--serve-queue", type=int, default=8 << 20, help="serving: admission limit, queued queries")
-    p.add_argument("--serve-slots", type=int, default=0, help="serving: batches in flight (0: default)")
+    p.add_argument("--serve-slots", type=int, default=16, help="serving: batches in flight (0: the library default, 8)")
     a = p.parse_args()
     if a.grid is None:
         a.grid = DEFAULT_GRID[a.workload]
@@ -690,6 +690,20 @@ def serving_leg(S, args):
     out = {"meshes": len(sets), "payloads": len(payloads), "seconds_per_rate": args.serve_seconds, "rates": [],
            "server": {"max_batch_queries": args.serve_batch_queries, "split_queries": args.serve_split or "default",
                       "max_queued_queries": args.serve_queue, "slots": args.serve_slots or "default"}}
+    # the latency floor: every payload submitted alone (the median of three), and the p50 / p99 of
+    # those over the uniform draw the arrivals make -- what a request costs with no queue in front
+    alone = []
+    for kind, mid, q, n in payloads:
+        t = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            srv.wait(srv.submit_grid(ids[mid], q) if kind == "grid" else srv.submit_points(ids[mid], q))
+            t.append((time.perf_counter() - t0) * 1e3)
+        alone.append(sorted(t)[1])
+    heavy = int(np.argmax(alone))
+    out["alone"] = {"p50_ms": float(np.percentile(alone, 50)), "p99_ms": float(np.percentile(alone, 99)),
+                    "max_ms": alone[heavy], "heaviest": {"kind": payloads[heavy][0], "queries": payloads[heavy][3],
+                                                         "triangles": int(sets[payloads[heavy][1]][0].nt)}}
     for lam in (50.0, 200.0, 800.0, 3200.0):
         srv.reset_stats()
         tickets = []

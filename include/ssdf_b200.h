@@ -543,7 +543,7 @@ typedef struct {
     int max_batch_jobs;    /* requests packed into one batch                                   */
     int precision;         /* SSDF_PREC_F32_FIXUP or SSDF_PREC_F64                             */
     int leaf_size;         /* BVH leaf size of resident meshes (0: default)                    */
-    int slots;             /* batches in flight at once, 1..16 (0: 4); each holds its buffers  */
+    int slots;             /* batches in flight at once, 1..16 (0: 8); each holds its buffers  */
     long long max_queued_queries; /* admission limit: a request that would bring the queries waiting
                                      to be packed above it is refused with SSDF_ERR_BUSY (0: none) */
     int split_queries;     /* requests larger than this are answered as parts (z-slabs of a grid,

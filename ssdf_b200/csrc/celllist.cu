@@ -172,10 +172,12 @@ __device__ __forceinline__ float cl_abs_margin<float>(float scale) {
 
 // COUNT: the counting instantiation (Ericson tests, and box tests of cells and triangles, into
 // counters[0..1]).
-// Bounded to 8 resident blocks per SM (64 registers): the kernel is latency bound with its loads
-// served by L1 (96 % hits, ncu), and at its natural 94 registers only 5 blocks fit.
+// Bounded to 5 resident blocks per SM (94 registers in double). The kernel is latency bound with its
+// loads served by L1 (96 % hits, ncu), but trading registers for occupancy loses: on the 64^3
+// icosphere grid 3.47 ms at 5 blocks, 3.48 unbounded (102 registers), 3.63 at 6 (80), 3.97 at 7
+// (72, spills) and 3.80 at 8 (64, spills).
 #ifndef SSDF_B200_CL_MIN_BLOCKS
-#define SSDF_B200_CL_MIN_BLOCKS 8
+#define SSDF_B200_CL_MIN_BLOCKS 5
 #endif
 template <typename T, bool COUNT>
 __global__ void __launch_bounds__(128, SSDF_B200_CL_MIN_BLOCKS) k_cl_query(int npoints, const T *__restrict__ x, const T *__restrict__ y,

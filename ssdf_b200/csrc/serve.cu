@@ -405,7 +405,7 @@ int ssdf_server_create(ssdf_server **out, const ssdf_server_opts *opts) {
     const size_t cap = size_t(opts->max_batch_queries);
     if (opts->slots < 0 || opts->slots > 16) {
         delete s;
-        return fail(SSDF_ERR_INVALID_ARGUMENT, "ssdf_server_create: slots must be 0 (default 4) or 1..16");
+        return fail(SSDF_ERR_INVALID_ARGUMENT, "ssdf_server_create: slots must be 0 (default 8) or 1..16");
     }
     if (s->opts.split_queries == 0) s->opts.split_queries = std::min(1 << 18, opts->max_batch_queries);
     if (s->opts.split_queries < 0 || s->opts.split_queries > opts->max_batch_queries || opts->max_queued_queries < 0) {
@@ -413,7 +413,7 @@ int ssdf_server_create(ssdf_server **out, const ssdf_server_opts *opts) {
         return fail(SSDF_ERR_INVALID_ARGUMENT,
                     "ssdf_server_create: split_queries must be 0..max_batch_queries, max_queued_queries >= 0");
     }
-    s->slots = std::vector<Slot>(opts->slots ? opts->slots : 4);
+    s->slots = std::vector<Slot>(opts->slots ? opts->slots : 8);
     int st = SSDF_OK;
     if (cudaStreamCreateWithFlags(&s->build_stream, cudaStreamNonBlocking) != cudaSuccess)
         st = fail(SSDF_ERR_CUDA, "ssdf_server_create: build stream");
