@@ -47,13 +47,13 @@ constexpr int kThreads = 128;
 #endif
 constexpr int kCand = SSDF_B200_WINDOW_SLOTS;
 
-// Minimum resident blocks per SM the float query kernels are compiled for: 9 blocks of 128 cap
-// them at 56 registers (the fix-up window lives in shared memory). The traversal is issue-latency
-// bound, so the occupancy this buys outweighs the few spills (measured on the torus-knot grid:
-// 17.8 ms against 18.4 ms for 10 blocks at 48 registers, 18.6 ms for 8 at 64, and 34 ms uncapped);
-// the double kernel keeps its registers.
+// Minimum resident blocks per SM the float query kernels are compiled for: 10 blocks of 128 cap
+// them at 48 registers (the fix-up window lives in shared memory). The traversal is issue-latency
+// bound, so the occupancy this buys outweighs the spills (measured on the torus-knot grid with the
+// packed box test: 16.79 ms against 17.22 ms for 9 blocks at 56 registers, 17.72 ms for 8 at 64 and
+// 16.77 ms for 11 at 40); the double kernel keeps its registers.
 #ifndef SSDF_B200_QUERY_MIN_BLOCKS
-#define SSDF_B200_QUERY_MIN_BLOCKS 9
+#define SSDF_B200_QUERY_MIN_BLOCKS 10
 #endif
 
 // The double kernel keeps 5 resident blocks per SM (at most 102 registers), its occupancy before the
@@ -214,6 +214,20 @@ __device__ __forceinline__ void boxes4_fast(const DeviceMesh &m, int node, float
     d[2] = box_dist_sq_fast(px, py, pz, lx.z, hx.z, ly.z, hy.z, lz.z, hz.z);
     d[3] = box_dist_sq_fast(px, py, pz, lx.w, hx.w, ly.w, hy.w, lz.w, hz.w);
     r[0] = __float_as_int(rr.x), r[1] = __float_as_int(rr.y), r[2] = __float_as_int(rr.z), r[3] = __float_as_int(rr.w);
+}
+
+// box_dist_sq_fast of both children of a node at once, bit for bit: the clamps per child, the
+// differences and the squared norms as packed FP32 pairs (child 0, child 1) of sm_100's
+// two-wide FP32 instructions (__fadd2_rn, __fmul2_rn and __ffma2_rn round each half as the scalar
+// operation does). One node visit issues 18 instructions for the two boxes instead of 24.
+__device__ __forceinline__ float2 box_dist_sq_pair(const float px, const float py, const float pz, const Node32 &n) {
+    const float2 dx = __fadd2_rn(make_float2(px, px), make_float2(-fminf(fmaxf(px, n.a.x), n.a.y),
+                                                                  -fminf(fmaxf(px, n.b.x), n.b.y)));
+    const float2 dy = __fadd2_rn(make_float2(py, py), make_float2(-fminf(fmaxf(py, n.a.z), n.a.w),
+                                                                  -fminf(fmaxf(py, n.b.z), n.b.w)));
+    const float2 dz = __fadd2_rn(make_float2(pz, pz), make_float2(-fminf(fmaxf(pz, n.c.x), n.c.y),
+                                                                  -fminf(fmaxf(pz, n.c.z), n.c.w)));
+    return __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
 }
 
 struct Tri32 {
@@ -429,8 +443,9 @@ struct FastPolicy {
         const Node32 n = load_node32(m.nodes32, node);
 #pragma unroll
         for (int q = 0; q < Q; q++) {
-            d0[q] = box_dist_sq_fast(px[q], py[q], pz[q], n.a.x, n.a.y, n.a.z, n.a.w, n.c.x, n.c.y);
-            d1[q] = box_dist_sq_fast(px[q], py[q], pz[q], n.b.x, n.b.y, n.b.z, n.b.w, n.c.z, n.c.w);
+            const float2 d = box_dist_sq_pair(px[q], py[q], pz[q], n);
+            d0[q] = d.x;
+            d1[q] = d.y;
         }
         r0 = n.r0;
         r1 = n.r1;

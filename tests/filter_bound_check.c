@@ -1,7 +1,8 @@
 /*
  * Test support (not part of the library): checks the FP32 filter of the fix-up path against the error
  * bound its window is sized from. The filter (ssdf_b200/csrc/device_geom.cuh, tri_dist_sq_filter) is
- * restated here in C with fmaf, an IEEE reciprocal for __frcp_rn and, for __fdividef, the exact
+ * restated here in C, in its region order (corners A, B, C, then the edges, then the face), with
+ * fmaf, an IEEE reciprocal for __frcp_rn and, for __fdividef, the exact
  * quotient rounded and then moved by -2, 0 and +2 ulp (its documented worst case), the largest error
  * of the three taken. The record is built as mesh_build.cu's filter_record builds a well-conditioned
  * triangle's (float corners, edges rounded once, products in double rounded once).
@@ -41,16 +42,16 @@ static float filter(float px, float py, float pz, const Rec *r) {
         const float bx = apx - r->abx, by = apy - r->aby, bz = apz - r->abz;
         return fmaf(bx, bx, fmaf(by, by, bz * bz));
     }
+    const float d5 = d1 - r->abac, d6 = d2 - r->acac;
+    if (d6 >= 0.f && d5 <= d6) {
+        const float cx = apx - r->acx, cy = apy - r->acy, cz = apz - r->acz;
+        return fmaf(cx, cx, fmaf(cy, cy, cz * cz));
+    }
     const float vc = fmaf(d1, d4, -d3 * d2);
     if (vc <= 0.f && d1 >= 0.f && d3 <= 0.f) {
         const float v = quot(d1, d1 - d3);
         const float dx = fmaf(-v, r->abx, apx), dy = fmaf(-v, r->aby, apy), dz = fmaf(-v, r->abz, apz);
         return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    }
-    const float d5 = d1 - r->abac, d6 = d2 - r->acac;
-    if (d6 >= 0.f && d5 <= d6) {
-        const float cx = apx - r->acx, cy = apy - r->acy, cz = apz - r->acz;
-        return fmaf(cx, cx, fmaf(cy, cy, cz * cz));
     }
     const float vb = fmaf(d5, d2, -d1 * d6);
     if (vb <= 0.f && d2 >= 0.f && d6 <= 0.f) {
