@@ -94,9 +94,10 @@ static int enqueue_run(ssdf_batch *b, bool warp, bool wide, bool budget, bool f6
     return launch_batch(D, SSDF_PREC_F64, s);
 }
 
-// The packet budget only exists for the fix-up kernel's binary packet walk.
+// The packet budget exists for the fix-up kernel's packet walks (binary and 4-wide).
 static bool budget_applies(const ssdf_batch *b, bool warp, bool wide) {
-    return b->precision == SSDF_PREC_F32_FIXUP && warp && !wide;
+    (void)wide;
+    return b->precision == SSDF_PREC_F32_FIXUP && warp;
 }
 
 static int graph_key(bool warp, bool wide, bool budget, bool f64) {

@@ -230,6 +230,25 @@ __device__ __forceinline__ float2 box_dist_sq_pair(const float px, const float p
     return __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
 }
 
+// boxes4_fast's distances, bit for bit, with children (0, 1) and (2, 3) as packed FP32 pairs.
+__device__ __forceinline__ void boxes4_pair(const DeviceMesh &m, int node, float px, float py, float pz,
+                                            float (&d)[4], int (&r)[4]) {
+    const float4 *p = m.nodes4_32 + 8 * node;
+    const float4 lx = __ldg(p), hx = __ldg(p + 1), ly = __ldg(p + 2), hy = __ldg(p + 3), lz = __ldg(p + 4),
+                 hz = __ldg(p + 5), rr = __ldg(p + 6);
+    const float2 x2 = make_float2(px, px), y2 = make_float2(py, py), z2 = make_float2(pz, pz);
+    const float2 dx01 = __fadd2_rn(x2, make_float2(-fminf(fmaxf(px, lx.x), hx.x), -fminf(fmaxf(px, lx.y), hx.y)));
+    const float2 dy01 = __fadd2_rn(y2, make_float2(-fminf(fmaxf(py, ly.x), hy.x), -fminf(fmaxf(py, ly.y), hy.y)));
+    const float2 dz01 = __fadd2_rn(z2, make_float2(-fminf(fmaxf(pz, lz.x), hz.x), -fminf(fmaxf(pz, lz.y), hz.y)));
+    const float2 dx23 = __fadd2_rn(x2, make_float2(-fminf(fmaxf(px, lx.z), hx.z), -fminf(fmaxf(px, lx.w), hx.w)));
+    const float2 dy23 = __fadd2_rn(y2, make_float2(-fminf(fmaxf(py, ly.z), hy.z), -fminf(fmaxf(py, ly.w), hy.w)));
+    const float2 dz23 = __fadd2_rn(z2, make_float2(-fminf(fmaxf(pz, lz.z), hz.z), -fminf(fmaxf(pz, lz.w), hz.w)));
+    const float2 s01 = __ffma2_rn(dx01, dx01, __ffma2_rn(dy01, dy01, __fmul2_rn(dz01, dz01)));
+    const float2 s23 = __ffma2_rn(dx23, dx23, __ffma2_rn(dy23, dy23, __fmul2_rn(dz23, dz23)));
+    d[0] = s01.x, d[1] = s01.y, d[2] = s23.x, d[3] = s23.y;
+    r[0] = __float_as_int(rr.x), r[1] = __float_as_int(rr.y), r[2] = __float_as_int(rr.z), r[3] = __float_as_int(rr.w);
+}
+
 struct Tri32 {
     float ax, ay, az, bx, by, bz, cx, cy, cz;
     int id;
@@ -454,7 +473,7 @@ struct FastPolicy {
 #pragma unroll
         for (int q = 0; q < Q; q++) {
             float dq[4];
-            boxes4_fast(m, node, px[q], py[q], pz[q], dq, r);
+            boxes4_pair(m, node, px[q], py[q], pz[q], dq, r);
 #pragma unroll
             for (int c = 0; c < 4; c++) d[c][q] = dq[c];
         }
@@ -788,9 +807,88 @@ __device__ __forceinline__ void traverse4(P &p, Counters &cnt) {
     }
 }
 
+// Packet walk of the 4-wide BVH, the binary packet walk's rules over four children: a child is
+// wanted when any lane wants it; wanted leaves are tested at once; of the wanted internal children
+// the one nearest the brick's centre lane is entered and the others go on the warp's shared stack
+// with the warp's smallest box distance, entered on pop while that is below the largest lane
+// threshold. At most 3 entries a level: the build keeps 3 x (4-wide depth) below kStackSize.
+template <bool COUNT, bool BUDGET, class P>
+__device__ __forceinline__ void traverse4_packet(P &p, Counters &cnt, int budget) {
+    using R = typename P::R;
+    constexpr int Q = P::kQn;
+    constexpr unsigned kAll = 0xffffffffu;
+    int work = 0;
+    if (budget <= 0) budget = 0x7fffffff;
+    __shared__ int s_node[kThreads / 32][kStackSize];
+    __shared__ float s_dist[kThreads / 32][kStackSize];
+    int *snode = s_node[threadIdx.x >> 5];
+    float *sdist = s_dist[threadIdx.x >> 5];
+    const bool live = p.max_thr() >= R(0);
+    int sp = 0;
+    int node = 0;
+    while (true) {
+        R d[4][Q];
+        int r[4];
+        p.boxes4(node, d, r);
+        if (COUNT) cnt.box += 4 * Q;
+        int next = -1;
+        float next_rank = 0.f, next_key = 0.f;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int rc = r[c];
+            const unsigned m = rc == kEmptyRef ? 0u : want_mask(p, d[c]);
+            if (!__any_sync(kAll, m != 0u)) continue;
+            if (rc < 0) {
+                p.template leaf<COUNT>(leaf_first(rc), leaf_count(rc), m, cnt);
+                if constexpr (BUDGET && budgeted<P>()) work += leaf_count(rc);
+                continue;
+            }
+            const R own = min_of<R, Q>(d[c]);
+            const float key =
+                __uint_as_float(__reduce_min_sync(kAll, __float_as_uint(live ? stack_key_lo(own) : finf())));
+            const float rank = __shfl_sync(kAll, float(own), kRepLane);
+            int push = rc;
+            float push_key = key;
+            if (next < 0 || rank < next_rank) {
+                push = next;
+                push_key = next_key;
+                next = rc;
+                next_rank = rank;
+                next_key = key;
+            }
+            if (push >= 0 && sp < kStackSize) {
+                snode[sp] = push;  // every lane stores the same values
+                sdist[sp] = push_key;
+                sp++;
+            }
+        }
+        if (next < 0) {
+            if constexpr (BUDGET && budgeted<P>()) {
+                if (work > budget) {
+                    p.abandon();
+                    break;
+                }
+            }
+            const float tl = live ? stack_key_hi(p.max_thr()) : 0.f;
+            const float tmax = __uint_as_float(__reduce_max_sync(kAll, __float_as_uint(tl)));
+            while (sp > 0) {
+                sp--;
+                if (sdist[sp] < tmax) {
+                    next = snode[sp];
+                    break;
+                }
+            }
+            if (next < 0) break;
+        }
+        node = next;
+    }
+}
+
 template <bool WARP, bool WIDE, bool COUNT, bool BUDGET = false, class P>
 __device__ __forceinline__ void walk(P &p, Counters &cnt, int budget = 0) {
-    if (WIDE)
+    if constexpr (WIDE && WARP)
+        traverse4_packet<COUNT, BUDGET>(p, cnt, budget);
+    else if constexpr (WIDE)
         traverse4<WARP, COUNT>(p, cnt);
     else
         traverse<WARP, COUNT, BUDGET>(p, cnt, budget);
@@ -1304,7 +1402,7 @@ int window_stack_cap() {
 
 template <int PREC, bool WARP, bool WIDE>
 cudaError_t launch_batch_main(const BatchLaunch &b, bool count, cudaStream_t stream) {
-    constexpr bool kCanBudget = PREC == SSDF_PREC_F32_FIXUP && WARP && !WIDE;
+    constexpr bool kCanBudget = PREC == SSDF_PREC_F32_FIXUP && WARP;
     if constexpr (kCanBudget) {
         if (b.budget) {
             if (count)
@@ -1350,7 +1448,7 @@ thread_local unsigned long long t_last_counts[4] = {0, 0, 0, 0};
 
 template <int PREC, bool WARP, bool WIDE>
 cudaError_t launch_main(const QueryArgs &a, bool count, unsigned nblocks, cudaStream_t stream) {
-    if constexpr (PREC == SSDF_PREC_F32_FIXUP && WARP && !WIDE) {
+    if constexpr (PREC == SSDF_PREC_F32_FIXUP && WARP) {
         if (a.warp_budget > 0) {
             if (count)
                 k_query<PREC, WARP, WIDE, true, true><<<nblocks, kThreads, 0, stream>>>(a);

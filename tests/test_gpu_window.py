@@ -152,11 +152,13 @@ def test_sliver_heavy_mesh_is_handed_to_fp64():
     assert np.array_equal(outs[0], outs[1])
 
 
+@pytest.mark.parametrize("arity", [2, 4])
 @pytest.mark.parametrize("budget", [8, 64, 0])
-def test_packet_budget_hands_queries_to_second_stage(budget):
+def test_packet_budget_hands_queries_to_second_stage(budget, arity):
     """A warp packet that has tested more triangle records than SSDF_B200_WARP_BUDGET stops and hands
     its queries, with their current windows, to the warp-per-query stage: the result stays the FP64
-    one at every node (single launch and batch), and small budgets do send queries there."""
+    one at every node (single launch and batch), and small budgets do send queries there. Both the
+    binary and the 4-wide packet walks."""
     mesh = W.icosphere(4)
     lo, hi = mesh.bbox()
     grid = W.Grid((48, 40, 36), tuple(lo - 0.3), tuple(hi + 0.3))
@@ -166,14 +168,14 @@ def test_packet_budget_hands_queries_to_second_stage(budget):
     dm.query_grid(grid, ref, rtri, precision=S.PREC_F64)
     out = torch.empty_like(ref)
     tri = torch.empty_like(rtri)
-    with env(SSDF_B200_WARP_BUDGET=budget, SSDF_B200_COUNT=1):
+    with env(SSDF_B200_WARP_BUDGET=budget, SSDF_B200_COUNT=1, SSDF_B200_ARITY=arity):
         dm.query_grid(grid, out, tri, precision=S.PREC_F32_FIXUP)
         torch.cuda.synchronize()
         fb = S.last_query_counts()["fallback_queries"]
     assert torch.equal(out, ref) and torch.equal(tri, rtri)
     assert (fb > grid.size // 10) if budget == 8 else True
     bout = torch.empty_like(ref)
-    with env(SSDF_B200_WARP_BUDGET=budget):
+    with env(SSDF_B200_WARP_BUDGET=budget, SSDF_B200_ARITY=arity):
         b = S.Batch(4, S.PREC_F32_FIXUP)
         b.add_grid(dm, grid, bout)
         b.run(use_graph=False)
