@@ -241,7 +241,7 @@ int bvh_grid_host(ptrdiff_t nt, const int *s0, const int *s1, const int *s2, ptr
     qo.out_type = sizeof(T) == 8 ? SSDF_F64 : SSDF_F32;
     const double lo[3] = {double(xmin), double(ymin), double(zmin)}, hi[3] = {double(xmax), double(ymax), double(zmax)};
     if (streamed_download_applies(n, out, outtri)) {
-        // page-locked outputs: each slab chunk is copied out while the query goes on
+        // each slab chunk is copied out while the query goes on (pageable arrays through staging)
         QueryArgs a;
         SSDF_CHECK(fill_grid_args(mg.mesh, nx, ny, nz, lo, hi, dout, (int *)dtri, &qo, &a));
         return launch_query_streamed(a, qo.precision, out, outtri, stream);

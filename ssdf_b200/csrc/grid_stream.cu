@@ -1,4 +1,4 @@
-// Streamed download of a grid query into page-locked host arrays.
+// Streamed download of a grid query into host arrays.
 //
 // The drop-in grid entry points (ssdf::sample_sdf_bvh and the other host-array grid calls,
 // serial/bvh/bvh.cpp) build the BVH, query every node and hand the values back in the caller's
@@ -10,6 +10,10 @@
 //   - the last block of a chunk to finish raises the chunk's flag in page-locked host memory
 //     (signal_chunk in bvh_query.cu), and this thread, which would otherwise wait for the launch,
 //     polls the flags and issues one cudaMemcpyAsync per finished chunk on a second stream;
+//   - a page-locked output array receives that copy directly; an ordinary (pageable) one, as the
+//     reference's callers pass (std::vector, numpy), receives it through one of a few page-locked
+//     staging slots that this thread copies into the array once the slot's copy has landed, while
+//     the launch and the next copies go on;
 //   - the fix-up arithmetic finishes a few queries in its second stage, after the chunk that holds
 //     them may have been copied: their final values are gathered on the device once the launch is
 //     done and written into the host arrays after every chunk copy has landed.
@@ -35,11 +39,19 @@ constexpr int kTargetChunks = 16;
 // Below this many nodes the copy is short next to the launch overhead it would hide.
 constexpr long long kStreamMinQueries = 1ll << 22;
 
+// Pageable outputs go through this many page-locked staging slots of one chunk each: a chunk's DMA
+// lands in a free slot, and the calling thread copies the slot into the caller's array while the
+// launch and the next DMAs go on.
+constexpr int kStageSlots = 4;
+
 struct ThreadResources {
     int device = -1;
     cudaStream_t copy = nullptr;  // chunk copies
     int *flags = nullptr;         // [kMaxChunks], page-locked, mapped
     int *dflags = nullptr;        // the flags' device address
+    char *stage = nullptr;        // kStageSlots staging slots, page-locked (grown on demand)
+    size_t stage_bytes = 0;
+    cudaEvent_t landed[kStageSlots] = {};  // a slot's DMA has completed
 };
 thread_local ThreadResources t_res;
 
@@ -52,9 +64,23 @@ int thread_resources(ThreadResources **out) {
         SSDF_CUDA(cudaStreamCreateWithFlags(&r.copy, cudaStreamNonBlocking));
         SSDF_CUDA(cudaHostAlloc((void **)&r.flags, sizeof(int) * kMaxChunks, cudaHostAllocMapped));
         SSDF_CUDA(cudaHostGetDevicePointer((void **)&r.dflags, r.flags, 0));
+        for (int i = 0; i < kStageSlots; i++)
+            SSDF_CUDA(cudaEventCreateWithFlags(&r.landed[i], cudaEventDisableTiming));
         r.device = dev;
     }
     *out = &r;
+    return SSDF_OK;
+}
+
+// Staging slots of at least `slot` bytes each (kept for the thread's later calls).
+int stage_reserve(ThreadResources *r, size_t slot) {
+    const size_t need = slot * kStageSlots;
+    if (r->stage_bytes >= need) return SSDF_OK;
+    if (r->stage) SSDF_CUDA(cudaFreeHost(r->stage));
+    r->stage = nullptr;
+    r->stage_bytes = 0;
+    SSDF_CUDA(cudaHostAlloc((void **)&r->stage, need, cudaHostAllocDefault));
+    r->stage_bytes = need;
     return SSDF_OK;
 }
 
@@ -106,8 +132,9 @@ ChunkPlan plan_chunks(const QueryArgs &a) {
 }  // namespace
 
 bool streamed_download_applies(long long n, const void *host_out, const int *host_tri) {
-    if (n < kStreamMinQueries || env_int("SSDF_B200_STREAM_DOWNLOAD", 1) == 0) return false;
-    return page_locked(host_out) && (!host_tri || page_locked(host_tri));
+    (void)host_out;
+    (void)host_tri;
+    return n >= kStreamMinQueries && env_int("SSDF_B200_STREAM_DOWNLOAD", 1) != 0;
 }
 
 int launch_query_streamed(const QueryArgs &args, int precision, void *host_out, int *host_tri, cudaStream_t stream) {
@@ -121,6 +148,15 @@ int launch_query_streamed(const QueryArgs &args, int precision, void *host_out, 
     ThreadResources *r = nullptr;
     SSDF_CHECK(thread_resources(&r));
     const size_t esz = a.out_f64 ? sizeof(double) : sizeof(float);
+    // A page-locked array takes its chunks' DMA directly; an ordinary (pageable) one through a staging
+    // slot that this thread copies out once the slot's DMA has landed.
+    const bool out_direct = page_locked(host_out);
+    const bool tri_direct = !host_tri || page_locked(host_tri);
+    const bool staged = !out_direct || !tri_direct;
+    const size_t chunk_elems = size_t(plan.planes_per_chunk * plan.plane_elems);
+    const size_t out_part = out_direct ? 0 : chunk_elems * esz;
+    const size_t slot_bytes = out_part + (tri_direct ? 0 : chunk_elems * sizeof(int));
+    if (staged) SSDF_CHECK(stage_reserve(r, slot_bytes));  // before the launch: growing it may block
     int *counts = nullptr;
     SSDF_CUDA(cudaMallocAsync(&counts, sizeof(int) * kMaxChunks, stream));
     struct Cleanup {
@@ -148,8 +184,10 @@ int launch_query_streamed(const QueryArgs &args, int precision, void *host_out, 
     // raises no flags)
     const volatile int *flags = r->flags;
     std::vector<char> sent(size_t(plan.nchunks), 0);
-    int issued = 0, st = SSDF_OK;
-    while (issued < plan.nchunks && st == SSDF_OK) {
+    int slot_chunk[kStageSlots];
+    for (int i = 0; i < kStageSlots; i++) slot_chunk[i] = -1;
+    int issued = 0, delivered = 0, st = SSDF_OK;
+    while (delivered < plan.nchunks && st == SSDF_OK) {
         const cudaError_t q = cudaEventQuery(cl.done);
         if (q != cudaSuccess && q != cudaErrorNotReady) {
             st = cuda_fail(q, "streamed grid query", __FILE__, __LINE__);
@@ -157,17 +195,51 @@ int launch_query_streamed(const QueryArgs &args, int precision, void *host_out, 
         }
         const bool ended = q == cudaSuccess;
         bool progress = false;
-        for (int c = 0; c < plan.nchunks && st == SSDF_OK; c++) {
+        for (int c = 0; c < plan.nchunks && issued < plan.nchunks && st == SSDF_OK; c++) {
             if (sent[c] || !(ended || flags[c])) continue;
+            int slot = -1;
+            if (staged) {
+                for (int i = 0; i < kStageSlots && slot < 0; i++)
+                    if (slot_chunk[i] < 0) slot = i;
+                if (slot < 0) break;  // every slot in use: copy some out first
+            }
             const long long lo = plan.lo(c), hi = plan.hi(c);
-            cudaError_t e = cudaMemcpyAsync((char *)host_out + lo * esz, (const char *)a.out + lo * esz,
-                                            size_t(hi - lo) * esz, cudaMemcpyDeviceToHost, r->copy);
-            if (e == cudaSuccess && host_tri)
-                e = cudaMemcpyAsync(host_tri + lo, a.outtri + lo, sizeof(int) * size_t(hi - lo),
-                                    cudaMemcpyDeviceToHost, r->copy);
+            const size_t cnt = size_t(hi - lo);
+            char *stage = staged ? r->stage + size_t(slot) * slot_bytes : nullptr;
+            void *to_out = out_direct ? (void *)((char *)host_out + lo * esz) : (void *)stage;
+            cudaError_t e = cudaMemcpyAsync(to_out, (const char *)a.out + lo * esz, cnt * esz, cudaMemcpyDeviceToHost,
+                                            r->copy);
+            if (e == cudaSuccess && host_tri) {
+                void *to_tri = tri_direct ? (void *)(host_tri + lo) : (void *)(stage + out_part);
+                e = cudaMemcpyAsync(to_tri, a.outtri + lo, sizeof(int) * cnt, cudaMemcpyDeviceToHost, r->copy);
+            }
+            if (e == cudaSuccess && staged) e = cudaEventRecord(r->landed[slot], r->copy);
             if (e != cudaSuccess) st = cuda_fail(e, "chunk copy", __FILE__, __LINE__);
             sent[c] = 1;
             issued++;
+            progress = true;
+            if (staged)
+                slot_chunk[slot] = c;
+            else
+                delivered++;
+        }
+        // staged chunks whose DMA has landed: into the caller's arrays
+        for (int i = 0; i < kStageSlots && st == SSDF_OK; i++) {
+            if (slot_chunk[i] < 0) continue;
+            const cudaError_t e = cudaEventQuery(r->landed[i]);
+            if (e == cudaErrorNotReady) continue;
+            if (e != cudaSuccess) {
+                st = cuda_fail(e, "chunk copy", __FILE__, __LINE__);
+                break;
+            }
+            const int c = slot_chunk[i];
+            const long long lo = plan.lo(c);
+            const size_t cnt = size_t(plan.hi(c) - lo);
+            const char *stage = r->stage + size_t(i) * slot_bytes;
+            if (!out_direct) memcpy((char *)host_out + lo * esz, stage, cnt * esz);
+            if (!tri_direct) memcpy(host_tri + lo, stage + out_part, sizeof(int) * cnt);
+            slot_chunk[i] = -1;
+            delivered++;
             progress = true;
         }
         if (!progress) std::this_thread::yield();

@@ -195,12 +195,13 @@ int launch_query(const QueryArgs &args, int precision, cudaStream_t stream);
 // (device ints: count, then the query indices) instead of freeing it; *fallback_list stays null for
 // the other arithmetics. The caller frees it with cudaFreeAsync on `stream`.
 int launch_query_keep(const QueryArgs &args, int precision, cudaStream_t stream, int **fallback_list);
-// A grid query whose results go to page-locked host arrays: args.out / args.outtri are device
-// buffers of the grid's size, and each slab chunk is copied to host_out / host_tri as soon as the
-// kernel has finished it, so the download overlaps the query. Returns when the host arrays hold the
-// results (the same bits as launch_query followed by a copy).
+// A grid query whose results go to host arrays: args.out / args.outtri are device buffers of the
+// grid's size, and each slab chunk is copied to host_out / host_tri as soon as the kernel has
+// finished it (through page-locked staging where an array is pageable), so the download overlaps the
+// query. Returns when the host arrays hold the results (the same bits as launch_query followed by a
+// copy).
 int launch_query_streamed(const QueryArgs &args, int precision, void *host_out, int *host_tri, cudaStream_t stream);
-// Whether the streamed grid download applies: n queries, outputs in page-locked host memory.
+// Whether the streamed grid download applies: n queries (at least 2^22) and the switch on.
 bool streamed_download_applies(long long n, const void *host_out, const int *host_tri);
 int launch_query_noalloc(const QueryArgs &args, cudaStream_t stream);
 long long noalloc_max_queries();

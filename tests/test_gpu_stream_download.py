@@ -1,11 +1,11 @@
-"""GPU: the drop-in grid calls with page-locked host outputs, whose slab chunks are copied out while
-the query runs (grids of at least 2^22 nodes).
+"""GPU: the drop-in grid calls whose slab chunks are copied out while the query runs (grids of at
+least 2^22 nodes): straight into page-locked output arrays, through page-locked staging slots into
+ordinary pageable ones.
 
-Each case calls the same C-ABI entry point twice: once into page-locked arrays (streamed download)
-and once into ordinary pageable arrays (query, then one copy), and requires the same bits. The
-grids have ragged sizes, so the last brick row, column and slab are partial; a tiny packet budget
-sends many queries to the fix-up's second stage, whose values are patched in after the chunk
-copies.
+Each case calls the same C-ABI entry point twice: once streamed, and once with the streamed download
+switched off (query, then one copy), and requires the same bits. The grids have ragged sizes, so the
+last brick row, column and slab are partial; a tiny packet budget sends many queries to the fix-up's
+second stage, whose values are patched in after the chunk copies.
 """
 
 import ctypes as C
@@ -39,6 +39,19 @@ def grid_call(fn, mesh, grid, out, dtype, tri=None):
     assert st == 0, S.last_error()
 
 
+def plain_call(fn, mesh, grid, out, dtype, tri=None):
+    """The same call with the streamed download off: the query, then one copy."""
+    old = os.environ.get("SSDF_B200_STREAM_DOWNLOAD")
+    os.environ["SSDF_B200_STREAM_DOWNLOAD"] = "0"
+    try:
+        grid_call(fn, mesh, grid, out, dtype, tri)
+    finally:
+        if old is None:
+            os.environ.pop("SSDF_B200_STREAM_DOWNLOAD", None)
+        else:
+            os.environ["SSDF_B200_STREAM_DOWNLOAD"] = old
+
+
 @pytest.fixture(scope="module")
 def mesh():
     return W.torus_knot_tube(nu=512, nv=32)
@@ -59,7 +72,7 @@ def test_streamed_sdf_matches_plain_download(mesh, grid, budget, monkeypatch):
     if budget:
         monkeypatch.setenv("SSDF_B200_WARP_BUDGET", budget)
     want = np.full(grid.size, np.nan)
-    grid_call("ssdf_b200_sample_sdf_bvh_dd", mesh, grid, want, np.float64)
+    plain_call("ssdf_b200_sample_sdf_bvh_dd", mesh, grid, want, np.float64)
     for _ in range(2):
         got = pinned(grid.size, torch.float64)
         got[:] = np.nan
@@ -78,7 +91,7 @@ def test_streamed_index_and_float_outputs(mesh, grid, monkeypatch):
 
     monkeypatch.setenv("SSDF_B200_WARP_BUDGET", "16")
     want, wtri = np.zeros(grid.size), np.full(grid.size, -7, dtype=np.int32)
-    grid_call("ssdf_b200_sample_sdf_index_bvh_dd", mesh, grid, want, np.float64, wtri)
+    plain_call("ssdf_b200_sample_sdf_index_bvh_dd", mesh, grid, want, np.float64, wtri)
     got, gtri = pinned(grid.size, torch.float64), pinned(grid.size, torch.int32)
     got[:] = 0
     gtri[:] = -7
@@ -87,7 +100,7 @@ def test_streamed_index_and_float_outputs(mesh, grid, monkeypatch):
     assert np.array_equal(gtri, wtri)
     # float grid, FP32 arithmetic
     wf = np.zeros(grid.size, dtype=np.float32)
-    grid_call("ssdf_b200_sample_sqedf_bvh_ff", mesh, grid, wf, np.float32)
+    plain_call("ssdf_b200_sample_sqedf_bvh_ff", mesh, grid, wf, np.float32)
     gf = pinned(grid.size, torch.float32)
     gf[:] = 0
     grid_call("ssdf_b200_sample_sqedf_bvh_ff", mesh, grid, gf, np.float32)
@@ -101,7 +114,7 @@ def test_streamed_squared_distance_keeps_incoming_bound(mesh, grid):
 
     init = np.where(np.arange(grid.size) % 3 == 0, 1e-14, np.inf)
     want = init.copy()
-    grid_call("ssdf_b200_sample_sqedf_bvh_dd", mesh, grid, want, np.float64)
+    plain_call("ssdf_b200_sample_sqedf_bvh_dd", mesh, grid, want, np.float64)
     got = pinned(grid.size, torch.float64)
     got[:] = init
     grid_call("ssdf_b200_sample_sqedf_bvh_dd", mesh, grid, got, np.float64)
@@ -130,7 +143,7 @@ def test_streamed_flat_and_tall_grids(mesh, shape):
     grid = W.Grid(shape, tuple(lo - 0.1), tuple(hi + 0.1))
     assert grid.size >= 1 << 22
     want = np.zeros(grid.size)
-    grid_call("ssdf_b200_sample_sdf_bvh_dd", mesh, grid, want, np.float64)
+    plain_call("ssdf_b200_sample_sdf_bvh_dd", mesh, grid, want, np.float64)
     got = pinned(grid.size, torch.float64)
     got[:] = np.nan
     grid_call("ssdf_b200_sample_sdf_bvh_dd", mesh, grid, got, np.float64)
@@ -149,7 +162,7 @@ def test_streamed_calls_from_two_threads(mesh, grid):
     wants = []
     for g in grids:
         w = np.zeros(g.size)
-        grid_call("ssdf_b200_sample_sdf_bvh_dd", mesh, g, w, np.float64)
+        plain_call("ssdf_b200_sample_sdf_bvh_dd", mesh, g, w, np.float64)
         wants.append(w)
     outs = [pinned(g.size, torch.float64) for g in grids]
     errors = []
@@ -169,3 +182,53 @@ def test_streamed_calls_from_two_threads(mesh, grid):
     for t in threads:
         t.join()
     assert not errors, errors
+
+
+@pytest.mark.parametrize("budget", [None, "16"])
+def test_streamed_into_pageable_arrays(mesh, grid, budget, monkeypatch):
+    """Ordinary numpy arrays (pageable, as the reference's callers pass std::vector memory) take the
+    streamed download through the staging slots: the same bits as the plain call, twice in a row, with
+    second-stage values patched in when the tiny budget sends thousands of queries there."""
+    if budget:
+        monkeypatch.setenv("SSDF_B200_WARP_BUDGET", budget)
+    want, wtri = np.full(grid.size, np.nan), np.full(grid.size, -7, dtype=np.int32)
+    plain_call("ssdf_b200_sample_sdf_index_bvh_dd", mesh, grid, want, np.float64, wtri)
+    for _ in range(2):
+        got, gtri = np.full(grid.size, np.nan), np.full(grid.size, -7, dtype=np.int32)
+        grid_call("ssdf_b200_sample_sdf_index_bvh_dd", mesh, grid, got, np.float64, gtri)
+        assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
+        assert np.array_equal(gtri, wtri)
+
+
+def test_streamed_mixed_page_locked_and_pageable(mesh, grid):
+    """A page-locked distance array with a pageable index array, and the other way round."""
+    import torch
+
+    want, wtri = np.zeros(grid.size), np.zeros(grid.size, dtype=np.int32)
+    plain_call("ssdf_b200_sample_sdf_index_bvh_dd", mesh, grid, want, np.float64, wtri)
+    for out_pinned in (True, False):
+        got = pinned(grid.size, torch.float64) if out_pinned else np.empty(grid.size)
+        gtri = np.empty(grid.size, dtype=np.int32) if out_pinned else pinned(grid.size, torch.int32)
+        got[:] = np.nan
+        gtri[:] = -7
+        grid_call("ssdf_b200_sample_sdf_index_bvh_dd", mesh, grid, got, np.float64, gtri)
+        assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
+        assert np.array_equal(gtri, wtri)
+
+
+def test_streamed_pageable_float_grid_and_small_grids(mesh, grid):
+    """A float grid (4-byte values) through the staging slots, then a larger grid on the same thread
+    (the slots grow) and a grid below 2^22 nodes (the plain path)."""
+    wf = np.zeros(grid.size, dtype=np.float32)
+    plain_call("ssdf_b200_sample_sqedf_bvh_ff", mesh, grid, wf, np.float32)
+    gf = np.zeros(grid.size, dtype=np.float32)
+    grid_call("ssdf_b200_sample_sqedf_bvh_ff", mesh, grid, gf, np.float32)
+    assert np.array_equal(gf.view(np.uint32), wf.view(np.uint32))
+    lo, hi = mesh.bbox()
+    for shape in [(200, 190, 180), (90, 80, 70)]:
+        g = W.Grid(shape, tuple(lo - 0.2), tuple(hi + 0.2))
+        want = np.zeros(g.size)
+        plain_call("ssdf_b200_sample_sdf_bvh_dd", mesh, g, want, np.float64)
+        got = np.full(g.size, np.nan)
+        grid_call("ssdf_b200_sample_sdf_bvh_dd", mesh, g, got, np.float64)
+        assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
