@@ -572,6 +572,8 @@ constexpr bool budgeted() {
     return HasBudget<P>::value;
 }
 
+constexpr int kRepLane = 21;  // (1, 1, 1) of the 4 x 4 x 2 brick
+
 // Packet walk (a grid warp as one packet): the node ids on the stack are the same in every lane, so
 // the warp keeps one stack in shared memory instead of 32 copies in local memory. An entry keeps
 // the smallest box distance over the warp's lanes (one redux.sync on the float bits, which order
@@ -597,7 +599,7 @@ __device__ __forceinline__ void traverse_packet(P &p, Counters &cnt, int budget)
         p.boxes(node, d0, d1, r0, r1);
         if (COUNT) cnt.box += 2 * Q;
         R k0 = min_of<R, Q>(d0), k1 = min_of<R, Q>(d1);
-        if (__popc(__ballot_sync(kAll, k1 < k0)) > 16) {
+        if (__shfl_sync(kAll, k1 < k0, kRepLane)) {  // the nearer child for the brick's centre lane
 #pragma unroll
             for (int q = 0; q < Q; q++) {
                 const R t = d0[q];
@@ -654,8 +656,9 @@ __device__ __forceinline__ void traverse_packet(P &p, Counters &cnt, int budget)
 // Nearest-child-first traversal with a per-lane stack of (node, smallest box distance), culled on
 // pop. WARP = false: every thread walks its own queries. WARP = true (packet): the 32 lanes of a
 // warp walk one path together -- a child is entered if any lane wants it, the nearer child is the
-// one most lanes rank first -- so node and triangle loads are warp-uniform (broadcast) and leaf work
-// does not diverge. Every lane must call it (warp-synchronous when WARP).
+// one the brick's centre lane ranks first (traverse_packet) -- so node and triangle loads are
+// warp-uniform (broadcast) and leaf work does not diverge. Every lane must call it
+// (warp-synchronous when WARP).
 template <bool WARP, bool COUNT, bool BUDGET, class P>
 __device__ __forceinline__ void traverse(P &p, Counters &cnt, int budget) {
     if constexpr (WARP) {
@@ -725,7 +728,6 @@ __device__ __forceinline__ void traverse(P &p, Counters &cnt, int budget) {
 // smallest in thread mode, a representative lane's (the brick centre) in warp mode -- leaves first
 // in that order, then the nearest wanted internal child is entered and the others pushed
 // farthest-first.
-constexpr int kRepLane = 21;  // (1, 1, 1) of the 4 x 4 x 2 brick
 
 template <typename R, int Q>
 __device__ __forceinline__ void cswap4(float (&k)[4], R (&d)[4][Q], int (&r)[4], int i, int j) {

@@ -314,7 +314,8 @@ __device__ __forceinline__ float box_area(const float *b) {
     return dx * dy + dy * dz + dz * dx;
 }
 
-__global__ void k_collapse4(int n_in, const int2 *__restrict__ qin, int2 *__restrict__ qout, int *__restrict__ n_out,
+__global__ void k_collapse4(const int *__restrict__ n_in_ptr, const int2 *__restrict__ qin, int2 *__restrict__ qout,
+                            int *__restrict__ n_out,
                             int *__restrict__ slots, int L, const int *__restrict__ child_l,
                             const int *__restrict__ child_r, const int *__restrict__ first_of,
                             const int *__restrict__ count, const int *__restrict__ sorted_ids,
@@ -322,7 +323,7 @@ __global__ void k_collapse4(int n_in, const int2 *__restrict__ qin, int2 *__rest
                             const float *__restrict__ nbox32, const double *__restrict__ nbox64,
                             float4 *__restrict__ n32, double2 *__restrict__ n64) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n_in) return;
+    if (i >= *n_in_ptr) return;  // the level's size, written by the level above
     const int b = qin[i].x, slot = qin[i].y;
     int c[4] = {child_l[b], child_r[b], 0, 0};
     int nc = 2;
@@ -387,6 +388,25 @@ __global__ void k_collapse4(int n_in, const int2 *__restrict__ qin, int2 *__rest
                          __longlong_as_double((long long)(unsigned(ref[2])) | ((long long)(unsigned(ref[3])) << 32)));
         n64[14 * slot + 13] = make_double2(0.0, 0.0);
     }
+}
+
+// Start of the 4-wide collapse: level 0 is the root (binary node 0 into slot 0), one slot used.
+__global__ void k_collapse4_init(int2 *__restrict__ q0, int *__restrict__ level_sizes, int *__restrict__ slots) {
+    q0[0] = make_int2(0, 0);
+    level_sizes[0] = 1;
+    *slots = 1;
+}
+
+// The flag words of the build: [0] the first bad triangle (none: INT_MAX), [1..6] the scene's box as
+// ordered ints (min seeded with +FLT_MAX, max with -FLT_MAX), the rest zero.
+__global__ void k_init_flags(int *__restrict__ flags) {
+    const int k = threadIdx.x;
+    if (k >= 16) return;
+    int v = 0;
+    if (k == 0) v = 0x7fffffff;
+    if (k >= 1 && k <= 3) v = 0x7f7fffff;
+    if (k >= 4 && k <= 6) v = int(0xff7fffffu ^ 0x7fffffffu);
+    flags[k] = v;
 }
 
 // The 4-wide root of a mesh of <= L triangles: one leaf, three empty slots.
@@ -733,6 +753,20 @@ void mesh_free_async(MeshStorage *storage, cudaStream_t stream) {
 
 size_t mesh_bytes(const MeshStorage *storage) { return storage ? storage->bytes : 0; }
 
+// Deepest 4-wide level the collapse writes: a tree that reaches it is refused (3 x depth4 must stay
+// below kStackSize), so one more level than an accepted tree can have.
+constexpr int kMaxLevels4 = kStackSize / 3 + 1;
+
+// Page-locked words for the build's read-backs (one set per calling thread, kept until exit), so the
+// copies stay asynchronous and the build waits once, at its end.
+constexpr int kReadbackWords = 64;
+static int readback_words(int **out) {
+    static thread_local int *w = nullptr;
+    if (!w) SSDF_CUDA(cudaHostAlloc((void **)&w, sizeof(int) * kReadbackWords, cudaHostAllocPortable));
+    *out = w;
+    return SSDF_OK;
+}
+
 static int mesh_build_impl(MeshStorage *s, MeshStorage *tmp, DeviceMesh *m, int nt, const int *s0_in,
                            const int *s1_in, const int *s2_in, int nv, const void *sx, const void *sy, const void *sz,
                            int coord_f64, int device_ptrs, const ssdf_build_opts &opts, cudaStream_t stream) {
@@ -779,22 +813,20 @@ static int mesh_build_impl(MeshStorage *s, MeshStorage *tmp, DeviceMesh *m, int 
     // filter bound term (float bits), [12] records unsafe for the float filter
     int *flags;
     SSDF_CHECK(dalloc(tmp, &flags, 16, stream));
-    {
-        // ordered-int encodings (f2o) of +FLT_MAX and -FLT_MAX seed the scene min / max
-        int h[16] = {0};
-        h[0] = 0x7fffffff;
-        for (int d = 0; d < 3; d++) h[1 + d] = 0x7f7fffff, h[4 + d] = int(0xff7fffffu ^ 0x7fffffffu);
-        SSDF_CUDA(cudaMemcpyAsync(flags, h, sizeof(h), cudaMemcpyHostToDevice, stream));
-        SSDF_CUDA(cudaStreamSynchronize(stream));  // h lives on this stack frame
+    k_init_flags<<<1, 32, 0, stream>>>(flags);
+    LAUNCH_CHECK("k_init_flags");
+    if (device_ptrs) {
+        // host arrays were checked on the host (check_mesh_host); device arrays are checked here,
+        // before any kernel indexes the vertices with them
+        k_validate<<<grid_blocks(nt, 256), 256, 0, stream>>>(nt, nv, s0, s1, s2, flags);
+        LAUNCH_CHECK("k_validate");
+        int bad = 0;
+        SSDF_CUDA(cudaMemcpyAsync(&bad, flags, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        SSDF_CUDA(cudaStreamSynchronize(stream));
+        if (bad != 0x7fffffff)
+            return fail(SSDF_ERR_INVALID_ARGUMENT, "triangle " + std::to_string(bad) +
+                                                       " has a vertex index outside [0, " + std::to_string(nv) + ")");
     }
-    k_validate<<<grid_blocks(nt, 256), 256, 0, stream>>>(nt, nv, s0, s1, s2, flags);
-    LAUNCH_CHECK("k_validate");
-    int bad = 0;
-    SSDF_CUDA(cudaMemcpyAsync(&bad, flags, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    SSDF_CUDA(cudaStreamSynchronize(stream));
-    if (bad != 0x7fffffff)
-        return fail(SSDF_ERR_INVALID_ARGUMENT, "triangle " + std::to_string(bad) + " has a vertex index outside [0, " +
-                                                   std::to_string(nv) + ")");
     float *box32, *cen;
     double *box64;
     SSDF_CHECK(dalloc(tmp, &box32, 6 * size_t(nt), stream));
@@ -823,8 +855,16 @@ static int mesh_build_impl(MeshStorage *s, MeshStorage *tmp, DeviceMesh *m, int 
     double2 *nodes4_64 = nullptr;
     SSDF_CHECK(dalloc(s, &nodes4_32, 8 * size_t(m->nnodes), stream));
     if (keep64) SSDF_CHECK(dalloc(s, &nodes4_64, 14 * size_t(m->nnodes), stream));
-    int depth_leaves[2] = {1, 1};
+    // read-backs: [0..1] depth and leaves, [2..2 + kMaxLevels4] 4-wide level sizes, then the slots
+    // used, then the coordinate scale and the three filter words
+    static_assert(2 + kMaxLevels4 + 2 + 4 <= kReadbackWords, "read-back words");
+    int *rb = nullptr;
+    SSDF_CHECK(readback_words(&rb));
+    int *const depth_leaves = rb, *const level_hist = rb + 2;
+    int *const scale_word = rb + 2 + kMaxLevels4 + 2, *const filt_info = scale_word + 1;
+    depth_leaves[0] = depth_leaves[1] = 1;
     int nnodes4 = 1, depth4 = 1;
+    bool collapsed = false;
     if (nt <= L) {
         // one leaf over everything (its triangle order is the Morton order)
         k_write_small_root<<<1, 1, 0, stream>>>(nt, box32, box64, nodes32, nodes64);
@@ -866,35 +906,34 @@ static int mesh_build_impl(MeshStorage *s, MeshStorage *tmp, DeviceMesh *m, int 
         k_depth<<<grid_blocks(nint, 256), 256, 0, stream>>>(nt, L, count, parent_int, child_l, child_r, flags + 8);
         LAUNCH_CHECK("k_depth");
         SSDF_CUDA(cudaMemcpyAsync(depth_leaves, flags + 8, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
-        // 4-wide collapse, one level per launch
+        // 4-wide collapse, one level per launch. Each level's kernel reads its size from the level
+        // above, so the host launches kMaxLevels4 levels without waiting between them (a grid of at
+        // most min(4^k, nint) threads at level k); the sizes come back with the build's last sync.
+        // A tree with a level at kMaxLevels4 is too deep for the traversal stack (3 x depth4 <
+        // kStackSize) and is refused below.
         int2 *qa, *qb;
-        int *qcount;  // [0] next-level size, [1] slots used
+        int *level_sizes;  // [kMaxLevels4 + 1] queue sizes per level, then the slots used
         SSDF_CHECK(dalloc(tmp, &qa, nint, stream));
         SSDF_CHECK(dalloc(tmp, &qb, nint, stream));
-        SSDF_CHECK(dalloc(tmp, &qcount, 2, stream));
-        const int2 root = make_int2(0, 0);
-        const int hq[2] = {0, 1};
-        SSDF_CUDA(cudaMemcpyAsync(qa, &root, sizeof(root), cudaMemcpyHostToDevice, stream));
-        SSDF_CUDA(cudaMemcpyAsync(qcount, hq, sizeof(hq), cudaMemcpyHostToDevice, stream));
-        int level_n = 1;
-        depth4 = 0;
-        while (level_n > 0) {
-            depth4++;
-            SSDF_CUDA(cudaMemsetAsync(qcount, 0, sizeof(int), stream));
-            k_collapse4<<<grid_blocks(level_n, 128), 128, 0, stream>>>(level_n, qa, qb, qcount, qcount + 1, L,
-                                                                       child_l, child_r, first_of, count, ids, box32,
-                                                                       box64, nbox32, nbox64, nodes4_32, nodes4_64);
+        SSDF_CHECK(dalloc(tmp, &level_sizes, kMaxLevels4 + 2, stream));
+        SSDF_CUDA(cudaMemsetAsync(level_sizes, 0, sizeof(int) * (kMaxLevels4 + 2), stream));
+        k_collapse4_init<<<1, 1, 0, stream>>>(qa, level_sizes, level_sizes + kMaxLevels4 + 1);
+        LAUNCH_CHECK("k_collapse4_init");
+        long long bound = 1;
+        for (int k = 0; k < kMaxLevels4; k++) {
+            const int n_k = int(std::min<long long>(bound, nint));
+            k_collapse4<<<grid_blocks(n_k, 128), 128, 0, stream>>>(
+                level_sizes + k, qa, qb, level_sizes + k + 1, level_sizes + kMaxLevels4 + 1, L, child_l, child_r,
+                first_of, count, ids, box32, box64, nbox32, nbox64, nodes4_32, nodes4_64);
             LAUNCH_CHECK("k_collapse4");
-            int hc[2];
-            SSDF_CUDA(cudaMemcpyAsync(hc, qcount, sizeof(hc), cudaMemcpyDeviceToHost, stream));
-            SSDF_CUDA(cudaStreamSynchronize(stream));
-            level_n = hc[0];
-            nnodes4 = hc[1];
+            bound *= 4;
             int2 *t = qa;
             qa = qb;
             qb = t;
-            if (depth4 > 4 * kStackSize) return fail(SSDF_ERR_INTERNAL, "4-wide collapse did not terminate");
         }
+        SSDF_CUDA(cudaMemcpyAsync(level_hist, level_sizes, sizeof(int) * (kMaxLevels4 + 2), cudaMemcpyDeviceToHost,
+                                  stream));  // page-locked: no wait here
+        collapsed = true;
     }
     // triangle records in leaf order
     float4 *t32, *filt = nullptr;
@@ -905,19 +944,23 @@ static int mesh_build_impl(MeshStorage *s, MeshStorage *tmp, DeviceMesh *m, int 
     k_tri_records<<<grid_blocks(nt, 256), 256, 0, stream>>>(nt, ids, s0, s1, s2, vx, vy, vz, t32, t64, filt,
                                                             flags + 10);
     LAUNCH_CHECK("k_tri_records");
-    int scale_bits = 0, filt_info[3] = {0, 0, 0};
-    SSDF_CUDA(cudaMemcpyAsync(&scale_bits, flags + 7, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    SSDF_CUDA(cudaMemcpyAsync(filt_info, flags + 10, sizeof(filt_info), cudaMemcpyDeviceToHost, stream));
+    SSDF_CUDA(cudaMemcpyAsync(scale_word, flags + 7, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    SSDF_CUDA(cudaMemcpyAsync(filt_info, flags + 10, 3 * sizeof(int), cudaMemcpyDeviceToHost, stream));
     if (opts.normals) SSDF_CHECK(build_normals(s, m, s0, s1, s2, vx, vy, vz, stream));
-    SSDF_CUDA(cudaStreamSynchronize(stream));
+    SSDF_CUDA(cudaStreamSynchronize(stream));  // the build's one wait: every read-back has landed
     float scale;
-    memcpy(&scale, &scale_bits, sizeof(float));
+    memcpy(&scale, scale_word, sizeof(float));
     m->coord_scale = scale;
     m->nill = filt_info[0];
     if (keep64) {
         float term;
         memcpy(&term, &filt_info[1], sizeof(float));
         set_filter_window(m, term, filt_info[2] == 0);
+    }
+    if (collapsed) {
+        depth4 = 0;
+        while (depth4 <= kMaxLevels4 && level_hist[depth4] > 0) depth4++;
+        nnodes4 = level_hist[kMaxLevels4 + 1];
     }
     m->depth = depth_leaves[0];
     m->nleaves = depth_leaves[1];
