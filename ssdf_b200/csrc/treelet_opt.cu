@@ -70,14 +70,19 @@ __device__ __forceinline__ void set_parent(const TreeArrays &t, int ref, int par
 // A treelet in the making, in shared memory (one per warp): its members and their boxes and costs,
 // the internal nodes it reuses, and the dynamic programme's cost and best split of every subset.
 struct TreeletWork {
+    double mb64[kTreeletLeaves][6];
     float mb[kTreeletLeaves][6];
     float mcost[kTreeletLeaves];
+    int mcount[kTreeletLeaves];
     int member[kTreeletLeaves];
     int inner[kTreeletLeaves - 1];
     int m, ni;  // members, internal nodes (m < 3: nothing to optimise)
     float old_cost;
     float c[kSubsets];
     unsigned char split[kSubsets];
+    // the rebuilt arrangement: internal node onode[k] now covers the members of subset oset[k]
+    int onode[kTreeletLeaves - 1], oset[kTreeletLeaves - 1];
+    int norder;
 };
 
 // One lane: grows the treelet rooted at internal node x (its subtree is final) from its two children
@@ -115,7 +120,11 @@ __device__ void form_treelet(const TreeArrays &t, int x, TreeletWork &w) {
         __stcg(t.cost + x, area6(b) + ref_cost(t, w.member[0]) + ref_cost(t, w.member[1]));
         return;
     }
-    for (int k = 0; k < m; k++) w.mcost[k] = ref_cost(t, w.member[k]);
+    for (int k = 0; k < m; k++) {
+        w.mcost[k] = ref_cost(t, w.member[k]);
+        w.mcount[k] = ref_count(t, w.member[k]);
+        ref_box64(t, w.member[k], w.mb64[k]);
+    }
     // current cost of the treelet: the old internal nodes' areas + members' costs
     float old_cost = 0.f;
     for (int k = 0; k < ni; k++) {
@@ -160,22 +169,23 @@ __device__ void treelet_dp(TreeletWork &w, int lane) {
 }
 
 // One lane: replaces the treelet's arrangement by the programme's when it is cheaper, reusing the
-// treelet's internal nodes (the root keeps x), then fixes boxes, counts and costs bottom-up.
-__device__ void rebuild_treelet(const TreeArrays &t, int x, const TreeletWork &w) {
+// treelet's internal nodes (the root keeps x): child and parent links top-down, and in w.onode /
+// w.oset which members each reused node now covers (w.norder of them; 0 when the old arrangement
+// stays, whose cost is stored here).
+__device__ void rebuild_plan(const TreeArrays &t, int x, TreeletWork &w) {
     const int m = w.m, full = (1 << m) - 1;
+    w.norder = 0;
     if (!(w.c[full] < w.old_cost * (1.f - 1e-6f))) {
         __stcg(t.cost + x, w.old_cost);
         return;
     }
     int stack_set[kTreeletLeaves], stack_node[kTreeletLeaves];
-    int sp = 0, used = 1;
+    int sp = 0, used = 1, norder = 0;
     stack_set[sp] = full, stack_node[sp] = x, sp++;
-    // build top-down, then fix boxes and costs bottom-up in reverse creation order
-    int order_node[kTreeletLeaves - 1], order_set[kTreeletLeaves - 1], norder = 0;
     while (sp > 0) {
         sp--;
         const int s = stack_set[sp], node = stack_node[sp];
-        order_node[norder] = node, order_set[norder] = s, norder++;
+        w.onode[norder] = node, w.oset[norder] = s, norder++;
         const int halves[2] = {w.split[s], s ^ w.split[s]};
         int refs[2];
         for (int h = 0; h < 2; h++) {
@@ -192,25 +202,37 @@ __device__ void rebuild_treelet(const TreeArrays &t, int x, const TreeletWork &w
         set_parent(t, refs[0], node);
         set_parent(t, refs[1], node);
     }
-    for (int k = norder - 1; k >= 0; k--) {
-        const int node = order_node[k];
-        const int l = __ldcg(t.child_l + node), r = __ldcg(t.child_r + node);
-        float bl[6], br[6];
-        double dl[6], dr[6];
-        ref_box32(t, l, bl);
-        ref_box32(t, r, br);
-        ref_box64(t, l, dl);
-        ref_box64(t, r, dr);
+    w.norder = norder;
+}
+
+// The whole warp, after rebuild_plan: lane k writes reused node w.onode[k]'s boxes (float and double),
+// triangle count and cost. A node's box is the union of its members' boxes -- the same values the
+// union of its two children's boxes gives, min and max being exact -- so no lane waits for another.
+__device__ void rebuild_write(const TreeArrays &t, const TreeletWork &w, int lane) {
+    if (lane >= w.norder) return;
+    const int node = w.onode[lane], s = w.oset[lane];
+    float b[6];
+    double d[6];
+    int cnt = 0;
+    bool first = true;
+    for (int j = 0; j < w.m; j++) {
+        if (!((s >> j) & 1)) continue;
         for (int q = 0; q < 6; q += 2) {
-            __stcg(t.nbox32 + 6 * node + q, fminf(bl[q], br[q]));
-            __stcg(t.nbox32 + 6 * node + q + 1, fmaxf(bl[q + 1], br[q + 1]));
-            __stcg(t.nbox64 + 6 * node + q, fmin(dl[q], dr[q]));
-            __stcg(t.nbox64 + 6 * node + q + 1, fmax(dl[q + 1], dr[q + 1]));
+            b[q] = first ? w.mb[j][q] : fminf(b[q], w.mb[j][q]);
+            b[q + 1] = first ? w.mb[j][q + 1] : fmaxf(b[q + 1], w.mb[j][q + 1]);
+            d[q] = first ? w.mb64[j][q] : fmin(d[q], w.mb64[j][q]);
+            d[q + 1] = first ? w.mb64[j][q + 1] : fmax(d[q + 1], w.mb64[j][q + 1]);
         }
-        __stcg(t.count + node, ref_count(t, l) + ref_count(t, r));
-        __stcg(t.cost + node, w.c[order_set[k]] - 0.f);
-        __threadfence();
+        cnt += w.mcount[j];
+        first = false;
     }
+    for (int q = 0; q < 6; q++) {
+        __stcg(t.nbox32 + 6 * node + q, b[q]);
+        __stcg(t.nbox64 + 6 * node + q, d[q]);
+    }
+    __stcg(t.count + node, cnt);
+    __stcg(t.cost + node, w.c[s]);
+    __threadfence();
 }
 
 constexpr int kTreeletThreads = 128;
@@ -255,7 +277,9 @@ __global__ void __launch_bounds__(kTreeletThreads) k_treelets(int n, TreeArrays 
             __syncwarp();
             if (w.m >= 3) {
                 treelet_dp(w, lane);
-                if (lane == owner) rebuild_treelet(t, x, w);
+                if (lane == owner) rebuild_plan(t, x, w);
+                __syncwarp();
+                rebuild_write(t, w, lane);
             }
             __syncwarp();
         }
