@@ -14,6 +14,8 @@ computed with the FP32 traversal + FP64 fix-up kernel. Synthetic, seeded inputs 
   into pinned host memory, per call, as the reference's sample_sdf_bvh does per call;
 * ``roofline``: the query kernel against the measured FP32 FMA peak of this GPU (the path is
   FP32-pipe bound; its HBM traffic is the output stream), flops counted by an instrumented launch;
+  ``roofline.traffic`` and ``roofline.issue`` (the share of issue slots the kernel keeps busy, the
+  limit it actually meets) come from the committed ncu summary ``profiles/traffic.json``;
 * ``cpu_baseline``: the reference's own OpenMP ``edf_celllist<double>`` (compiled from its sources
   into oracle/_ref) on a seeded sample of the same grid nodes, all host threads;
 * ``error``: the fix-up result against the plain FP64 one at every node (distance bits and closest
@@ -816,13 +818,16 @@ def _hbm_peak():
 
 
 def _attach_traffic(line):
-    """DRAM bytes per launch of the query kernel from the committed ncu summary, if present."""
+    """DRAM bytes per launch of the query kernel, and the share of issue slots it keeps busy, from the
+    committed ncu summary, if present."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(path) as f:
             t = json.load(f)
         line["roofline"]["traffic"] = t["dram_bytes_per_launch"]
         line["roofline"]["traffic_source"] = t.get("source")
+        if "issue" in t:  # the bound that binds: instruction issue (flops counted per test undercount it)
+            line["roofline"]["issue"] = t["issue"]
     except Exception:
         pass
 

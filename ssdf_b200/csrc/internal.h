@@ -1,6 +1,8 @@
 // internal.h -- shared declarations of the library's host runtime and kernels.
 #pragma once
 
+#include <cmath>
+
 #include <cuda_runtime.h>
 #include <stddef.h>
 #include <stdint.h>
@@ -310,15 +312,19 @@ inline int grid_blocks(long long n, int threads) { return int((n + threads - 1) 
 // for the repeated work (the 256-mesh batch: 257 -> 275 ms).
 constexpr int kWarpBudget = 2048;
 constexpr long long kBudgetMaxQueries = 1ll << 21;
-// QueryArgs::warp_budget for a launch of n queries when it was left to the default (< 0): an eighth of
-// the mesh's triangles, within [256, kWarpBudget] -- a packet that has tested that share of a mesh is
-// in a near-equidistant region. Measured on B200, 64^3 grid on a 5,120-triangle sphere: budget 2048
-// 1.17 ms, 1024 0.73, 640 (its eighth) 0.60, 256 0.67.
+// QueryArgs::warp_budget for a launch of n queries when it was left to the default (< 0): 5.6 sqrt(T)
+// records for a mesh of T triangles, within [128, kWarpBudget] -- a packet that has tested that many
+// is in a near-equidistant region. Measured on B200 (sphere grids, the best budget of each sweep in
+// brackets): 1,280 triangles 48^3 [200]: 0.20 ms against 0.28 ms at 400; 5,120 triangles 64^3 [400]:
+// 0.49 ms against 0.58 at 640 and 0.53 at 480; 20,480 triangles 96^3 [600 .. 1,280]: 1.64 ms against
+// 1.89 at 2048; the serving leg's 110^3 grid on 81,920 triangles [1,536 .. 2,048]: 8.2 ms against 8.7
+// at 1024 and 10.1 at 512.
+constexpr int kWarpBudgetMin = 128;
 inline int resolve_warp_budget(int b, long long n, int ntri) {
     if (b >= 0) return b;
     if (n > kBudgetMaxQueries) return 0;
-    const int eighth = ntri / 8;
-    return eighth < 256 ? 256 : (eighth > kWarpBudget ? kWarpBudget : eighth);
+    const int v = int(5.6 * std::sqrt(double(ntri > 0 ? ntri : 0)));
+    return v < kWarpBudgetMin ? kWarpBudgetMin : (v > kWarpBudget ? kWarpBudget : v);
 }
 // Point lists of at least this many queries are visited in Morton order (SSDF_B200_SORT_POINTS=0
 // keeps input order).
