@@ -1211,8 +1211,14 @@ __global__ void __launch_bounds__(kThreads, PREC == SSDF_PREC_F64 ? kF64MinBlock
 // order. The boxes and the float test are the first stage's, on the binary tree: the double winner
 // lies inside the window by the margin tau, so its boxes pass under either arity.
 constexpr int kWinStack = 1024;  // node slots of a warp's shared stack
+// Blocks per SM of the second stage's grid. Its kernel keeps its registers (116: capping them at 64 or
+// 40 spilled the double evaluation and lost 10-100 %), so 4 blocks are resident per SM; a grid of 12
+// per SM queues the rest behind them, so a warp takes one query where 4 per SM had each take two or
+// three, and blocks that finish early make room. Measured: 64^3 icosphere step 0.487 -> 0.447 ms,
+// 20,480-triangle sphere 96^3 1.58 -> 1.44 ms, the serving leg's heaviest grid 8.22 -> 8.03 ms, the
+// torus knot unchanged.
 #ifndef SSDF_B200_WINDOW_BLOCKS_PER_SM
-#define SSDF_B200_WINDOW_BLOCKS_PER_SM 4
+#define SSDF_B200_WINDOW_BLOCKS_PER_SM 12
 #endif
 constexpr int kWindowBlocksPerSm = SSDF_B200_WINDOW_BLOCKS_PER_SM;
 
@@ -1605,8 +1611,8 @@ int morton_point_order(long long n, const void *x, const void *y, const void *z,
     return st;
 }
 
-// Blocks of the second fix-up stage (kWindowBlocksPerSm per SM, four warps each). The warps stride
-// over the overflow count, which is only known on the device.
+// Blocks of the second fix-up stage (kWindowBlocksPerSm per SM, four warps each; more than fit at
+// once). The warps stride over the overflow count, which is only known on the device.
 unsigned window_grid() {
     static int cached[64] = {0};
     int dev = 0;
