@@ -1200,9 +1200,11 @@ __global__ void __launch_bounds__(kThreads, PREC == SSDF_PREC_F64 ? kF64MinBlock
 
 // ---- second fix-up stage: one warp per overflowed query --------------------------------------------
 //
-// A query whose window overflowed its slots is walked again with the window fixed at its final
-// extent: every triangle whose float distance is inside it is re-evaluated in double. With the
-// window fixed the visiting order is free, so the warp walks the tree breadth-parallel: each step
+// A query whose window overflowed its slots is walked again from its final window, and a query whose
+// packet ran out of budget from the window it had then: every triangle whose float distance is
+// inside the window is re-evaluated in double. The window only shrinks (after each step, to what the
+// warp's smallest non-proxy key allows, by the first stage's rule), so the visiting order is free,
+// and the warp walks the tree breadth-parallel: each step
 // the 32 lanes take up to 32 nodes from the warp's shared stack, test their children, run the
 // wanted leaves, and push the wanted internal children (ballot-compacted). A lane keeps the
 // lexicographic (d^2, index) minimum of the triangles it evaluated (the incoming bound ranks -1, so
@@ -1231,12 +1233,16 @@ struct WindowBest {
 // float filter's range, whose keys may have overflowed, is answered this way: exactly, in double).
 __device__ __forceinline__ bool in_window(float key, float thr) { return key < thr || thr == finf(); }
 
+// kbest: the smallest key of a non-proxy triangle the lane has met (the window may shrink to it, as in
+// the first stage: any such key bounds the window from below, so the double winner stays inside).
 __device__ __forceinline__ void window_leaf(const DeviceMesh &m, int ref, float px, float py, float pz, float thr,
                                             double qx, double qy, double qz, WindowBest &b, Counters &cnt,
-                                            bool count) {
+                                            bool count, float &kbest) {
     const int first = leaf_first(ref), n = leaf_count(ref);
     for (int k = 0; k < n; k++) {
-        const float f = tri_dist_sq_filter(px, py, pz, load_filt(m.filt32, first + k));  // the first stage's key
+        const FiltRec r = load_filt(m.filt32, first + k);
+        const float f = tri_dist_sq_filter(px, py, pz, r);  // the first stage's key
+        if (r.pen == 0.f && f < kbest) kbest = f;
         if (count) cnt.tri++;
         if (in_window(f, thr)) {
             const Tri64 u = load_tri64(m.tris64, first + k);
@@ -1253,7 +1259,7 @@ __device__ __forceinline__ void window_leaf(const DeviceMesh &m, int ref, float 
 // children holds at most depth + 1 entries.
 __device__ __noinline__ void window_subtree(const DeviceMesh &m, int root, float px, float py, float pz, float thr,
                                             double qx, double qy, double qz, WindowBest &b, Counters &cnt,
-                                            bool count) {
+                                            bool count, float &kbest) {
     int st[kStackSize];
     int sp = 0;
     st[sp++] = root;
@@ -1267,7 +1273,7 @@ __device__ __noinline__ void window_subtree(const DeviceMesh &m, int root, float
             const int c = h ? n.r1 : n.r0;
             if (c == kEmptyRef || !in_window(h ? d1 : d0, thr)) continue;
             if (c < 0)
-                window_leaf(m, c, px, py, pz, thr, qx, qy, qz, b, cnt, count);
+                window_leaf(m, c, px, py, pz, thr, qx, qy, qz, b, cnt, count, kbest);
             else if (sp < kStackSize)
                 st[sp++] = c;
         }
@@ -1285,7 +1291,9 @@ __device__ void window_warp(const QueryArgs &a, int idx, int *__restrict__ stack
     double qx, qy, qz;
     query_point(a, q, i, j, k, qx, qy, qz);
     const float px = float(qx), py = float(qy), pz = float(qz);
-    const float thr = a.fallback_thr[idx];
+    float thr = a.fallback_thr[idx];
+    const bool shrink = thr < finf();  // an infinite window (a point beyond the float range) stays
+    float kbest = finf();
     const DeviceMesh &m = a.m;
     WindowBest b{initial_bound(a, q), -1, -1};
     if (lane == 0) stack[0] = 0;
@@ -1307,13 +1315,17 @@ __device__ void window_warp(const QueryArgs &a, int idx, int *__restrict__ stack
             w0 = c0 != kEmptyRef && in_window(d0, thr);
             w1 = c1 != kEmptyRef && in_window(d1, thr);
             if (w0 && c0 < 0) {
-                window_leaf(m, c0, px, py, pz, thr, qx, qy, qz, b, cnt, COUNT);
+                window_leaf(m, c0, px, py, pz, thr, qx, qy, qz, b, cnt, COUNT, kbest);
                 w0 = false;
             }
             if (w1 && c1 < 0) {
-                window_leaf(m, c1, px, py, pz, thr, qx, qy, qz, b, cnt, COUNT);
+                window_leaf(m, c1, px, py, pz, thr, qx, qy, qz, b, cnt, COUNT, kbest);
                 w1 = false;
             }
+        }
+        if (shrink) {  // the window the warp's smallest key allows, as the first stage computes it
+            const float wb = __uint_as_float(__reduce_min_sync(kAll, __float_as_uint(kbest)));
+            thr = fminf(thr, window_thr(wb, a.tau_rel, m.coord_scale));
         }
         const unsigned m0 = __ballot_sync(kAll, w0), m1 = __ballot_sync(kAll, w1);
         const int n0 = __popc(m0), total = n0 + __popc(m1);
@@ -1323,8 +1335,8 @@ __device__ void window_warp(const QueryArgs &a, int idx, int *__restrict__ stack
             if (w1) stack[sp + n0 + __popc(m1 & below)] = c1;
             sp += total;
         } else {
-            if (w0) window_subtree(m, c0, px, py, pz, thr, qx, qy, qz, b, cnt, COUNT);
-            if (w1) window_subtree(m, c1, px, py, pz, thr, qx, qy, qz, b, cnt, COUNT);
+            if (w0) window_subtree(m, c0, px, py, pz, thr, qx, qy, qz, b, cnt, COUNT, kbest);
+            if (w1) window_subtree(m, c1, px, py, pz, thr, qx, qy, qz, b, cnt, COUNT, kbest);
         }
         __syncwarp();
     }
