@@ -204,18 +204,6 @@ __device__ __forceinline__ void boxes4_exact<double>(const DeviceMesh &m, int no
     r[0] = int(unsigned(a)), r[1] = int(unsigned(a >> 32)), r[2] = int(unsigned(b)), r[3] = int(unsigned(b >> 32));
 }
 
-__device__ __forceinline__ void boxes4_fast(const DeviceMesh &m, int node, float px, float py, float pz,
-                                            float (&d)[4], int (&r)[4]) {
-    const float4 *p = m.nodes4_32 + 8 * node;
-    const float4 lx = __ldg(p), hx = __ldg(p + 1), ly = __ldg(p + 2), hy = __ldg(p + 3), lz = __ldg(p + 4),
-                 hz = __ldg(p + 5), rr = __ldg(p + 6);
-    d[0] = box_dist_sq_fast(px, py, pz, lx.x, hx.x, ly.x, hy.x, lz.x, hz.x);
-    d[1] = box_dist_sq_fast(px, py, pz, lx.y, hx.y, ly.y, hy.y, lz.y, hz.y);
-    d[2] = box_dist_sq_fast(px, py, pz, lx.z, hx.z, ly.z, hy.z, lz.z, hz.z);
-    d[3] = box_dist_sq_fast(px, py, pz, lx.w, hx.w, ly.w, hy.w, lz.w, hz.w);
-    r[0] = __float_as_int(rr.x), r[1] = __float_as_int(rr.y), r[2] = __float_as_int(rr.z), r[3] = __float_as_int(rr.w);
-}
-
 // box_dist_sq_fast of both children of a node at once, bit for bit: the clamps per child, the
 // differences and the squared norms as packed FP32 pairs (child 0, child 1) of sm_100's
 // two-wide FP32 instructions (__fadd2_rn, __fmul2_rn and __ffma2_rn round each half as the scalar
@@ -230,7 +218,8 @@ __device__ __forceinline__ float2 box_dist_sq_pair(const float px, const float p
     return __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
 }
 
-// boxes4_fast's distances, bit for bit, with children (0, 1) and (2, 3) as packed FP32 pairs.
+// The 4-wide node's child-box distances (box_dist_sq_fast's, bit for bit), children (0, 1) and (2, 3)
+// as packed FP32 pairs.
 __device__ __forceinline__ void boxes4_pair(const DeviceMesh &m, int node, float px, float py, float pz,
                                             float (&d)[4], int (&r)[4]) {
     const float4 *p = m.nodes4_32 + 8 * node;
