@@ -389,7 +389,7 @@ typedef struct {
     int leaf_size;    /* triangles per BVH leaf, 1..16 (0: 4)                                 */
     int keep_fp64;    /* 1: also keep double triangles and nodes (F64 and fix-up queries)      */
     int normals;      /* 1: build pseudo-normals (signed queries)                             */
-    int treelet_opt;  /* rounds of SAH treelet refinement of the LBVH (0: plain LBVH; <= 8); 1 by default */
+    int treelet_opt;  /* rounds of SAH treelet refinement of the LBVH (0: plain LBVH; <= 8); 3 when opts is null */
 } ssdf_build_opts;
 
 typedef struct {

@@ -619,14 +619,19 @@ def points_aabb_signed_distance_device(x, y, z, box, out, absolute=False, stream
                                                 _stream_handle(stream)), "ssdf_points_aabb_signed_distance")
 
 
+RESIDENT_TREELET_ROUNDS = 3  # treelet rounds of a resident mesh's BVH (the library's default)
+
+
 class DeviceMesh:
-    """A mesh, its BVH and (optionally) pseudo-normals, resident on the current GPU."""
+    """A mesh, its BVH and (optionally) pseudo-normals, resident on the current GPU. ``treelet``: rounds
+    of SAH treelet refinement (True: the resident default, 3; False: none)."""
 
     def __init__(self, mesh, coord_dtype=np.float64, leaf_size=0, keep_fp64=True, normals=True, treelet=True,
                  stream=None):
         hm = _HostMesh(mesh, coord_dtype)
         self._h = C.c_void_p()
-        opts = BuildOpts(int(leaf_size), int(keep_fp64), int(normals), int(treelet))
+        rounds = RESIDENT_TREELET_ROUNDS if treelet is True else int(treelet)
+        opts = BuildOpts(int(leaf_size), int(keep_fp64), int(normals), rounds)
         ct = F64 if np.dtype(coord_dtype) == np.float64 else F32
         _check(lib.ssdf_mesh_create(C.byref(self._h), *hm.args(), ct, 0, C.byref(opts), _stream_handle(stream)),
                "ssdf_mesh_create")

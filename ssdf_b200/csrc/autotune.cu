@@ -108,7 +108,7 @@ int ssdf_autotune_grid(ptrdiff_t nselements, const int *s0, const int *s1, const
         bo.leaf_size = leaves[li];
         bo.keep_fp64 = 1;
         bo.normals = 1;
-        bo.treelet_opt = 1;
+        bo.treelet_opt = kResidentTreeletRounds;
         ssdf_mesh *m = nullptr;
         st = ssdf_mesh_create(&m, nselements, s0, s1, s2, nspoints, sx, sy, sz, SSDF_F64, 0, &bo, stream);
         if (st != SSDF_OK) break;

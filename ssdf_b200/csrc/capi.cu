@@ -624,7 +624,7 @@ int ssdf_mesh_create(ssdf_mesh **mesh, ptrdiff_t nselements, const int *s0, cons
     if (opts) {
         o = *opts;
     } else {
-        o.leaf_size = 0, o.keep_fp64 = 1, o.normals = 1, o.treelet_opt = 1;
+        o.leaf_size = 0, o.keep_fp64 = 1, o.normals = 1, o.treelet_opt = kResidentTreeletRounds;
     }
     if (!device_ptrs) SSDF_CHECK(check_mesh_host(nselements, s0, s1, s2, nspoints, sx, sy, sz));
     cudaStream_t s = (cudaStream_t)stream;

@@ -301,6 +301,14 @@ template <typename G, typename T>
 int round_device(const GridDesc &gd, const T *d_f, T radius, T band, bool open, bool close, long long stride, T *d_out,
                  T *d_f0, cudaStream_t stream);
 
+// Treelet refinement rounds of a resident mesh's BVH (built once, queried many times). Measured on the
+// current kernels, queries against 1 round: beam lattice (8e6 points + 512^3 grid, float) 335.6 ->
+// 313.1 / 308.7 / 304.8 ms for 2 / 3 / 4 rounds; torus knot 256^3 16.70 -> 16.63 ms (3); 64^3
+// icosphere 0.470 -> 0.465 ms; the serving leg's heaviest grid 3.74 -> 3.67 ms. Each round adds about
+// 1.5 ms to the torus knot's build, which calls that build per query do not repay
+// (call_treelet_rounds).
+constexpr int kResidentTreeletRounds = 3;
+
 // ---- small helpers -------------------------------------------------------------------------------
 inline int grid_blocks(long long n, int threads) { return int((n + threads - 1) / threads); }
 // Default of QueryArgs::warp_budget, for launches (single, or a whole batch) of at most

@@ -159,7 +159,7 @@ int build_resident(ssdf_server *s, int id, Resident *r) {
     bo.leaf_size = s->opts.leaf_size;
     bo.keep_fp64 = 1;
     bo.normals = 1;
-    bo.treelet_opt = 1;
+    bo.treelet_opt = kResidentTreeletRounds;
     ssdf_mesh *m = nullptr;
     SSDF_CHECK(ssdf_mesh_create(&m, ptrdiff_t(h.s0.size()), h.s0.data(), h.s1.data(), h.s2.data(),
                                 ptrdiff_t(h.sx.size()), h.sx.data(), h.sy.data(), h.sz.data(), SSDF_F64, 0, &bo,

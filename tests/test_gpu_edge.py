@@ -121,7 +121,7 @@ def test_treelet_refinement(leaf):
         with env(SSDF_B200_LEAF=leaf, SSDF_B200_TREELET=1, SSDF_B200_ARITY=arity):
             got, gtri = S.sample_sdf_bvh(mesh, g, with_index=True)
         assert np.array_equal(got, want) and np.array_equal(gtri, wtri)
-    plain = S.DeviceMesh(mesh, leaf_size=leaf).stats()
+    plain = S.DeviceMesh(mesh, leaf_size=leaf, treelet=False).stats()
     tuned = S.DeviceMesh(mesh, leaf_size=leaf, treelet=True).stats()
     assert tuned["leaves"] > 0 and tuned["depth"] < 64 and plain["leaves"] > 0
 
