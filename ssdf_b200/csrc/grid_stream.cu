@@ -131,6 +131,26 @@ ChunkPlan plan_chunks(const QueryArgs &a) {
 
 }  // namespace
 
+// A host copy of at least 8 MB split across up to 8 threads: one thread's memcpy bandwidth would
+// otherwise cap the served query rate (staging of large requests, tens of MB per batch at high load)
+// and lengthen the streamed download's last copy after the query has ended.
+void par_memcpy(void *dst, const void *src, size_t bytes) {
+    constexpr size_t kChunk = size_t(4) << 20;
+    if (bytes < 2 * kChunk) {
+        memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t parts = std::min<size_t>(8, bytes / kChunk);
+    const size_t step = (bytes + parts - 1) / parts;
+    std::vector<std::thread> th;
+    for (size_t k = 1; k < parts; k++) {
+        const size_t off = k * step, len = std::min(step, bytes - off);
+        th.emplace_back([=] { memcpy(static_cast<char *>(dst) + off, static_cast<const char *>(src) + off, len); });
+    }
+    memcpy(dst, src, std::min(step, bytes));
+    for (auto &t : th) t.join();
+}
+
 bool streamed_download_applies(long long n, const void *host_out, const int *host_tri) {
     (void)host_out;
     (void)host_tri;
@@ -236,8 +256,8 @@ int launch_query_streamed(const QueryArgs &args, int precision, void *host_out, 
             const long long lo = plan.lo(c);
             const size_t cnt = size_t(plan.hi(c) - lo);
             const char *stage = r->stage + size_t(i) * slot_bytes;
-            if (!out_direct) memcpy((char *)host_out + lo * esz, stage, cnt * esz);
-            if (!tri_direct) memcpy(host_tri + lo, stage + out_part, sizeof(int) * cnt);
+            if (!out_direct) par_memcpy((char *)host_out + lo * esz, stage, cnt * esz);
+            if (!tri_direct) par_memcpy(host_tri + lo, stage + out_part, sizeof(int) * cnt);
             slot_chunk[i] = -1;
             delivered++;
             progress = true;

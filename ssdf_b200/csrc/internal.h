@@ -203,6 +203,8 @@ int launch_query_keep(const QueryArgs &args, int precision, cudaStream_t stream,
 // query. Returns when the host arrays hold the results (the same bits as launch_query followed by a
 // copy).
 int launch_query_streamed(const QueryArgs &args, int precision, void *host_out, int *host_tri, cudaStream_t stream);
+// Host copy split across up to 8 threads (copies of at least 8 MB).
+void par_memcpy(void *dst, const void *src, size_t bytes);
 // Whether the streamed grid download applies: n queries (at least 2^22) and the switch on.
 bool streamed_download_applies(long long n, const void *host_out, const int *host_tri);
 int launch_query_noalloc(const QueryArgs &args, cudaStream_t stream);

@@ -134,25 +134,6 @@ struct ssdf_server {
 
 namespace {
 
-// Host staging copies of large requests (tens of MB per batch at high load) split across threads:
-// one thread's memcpy bandwidth would otherwise cap the served query rate.
-void par_memcpy(void *dst, const void *src, size_t bytes) {
-    constexpr size_t kChunk = size_t(4) << 20;
-    if (bytes < 2 * kChunk) {
-        memcpy(dst, src, bytes);
-        return;
-    }
-    const size_t parts = std::min<size_t>(8, bytes / kChunk);
-    const size_t step = (bytes + parts - 1) / parts;
-    std::vector<std::thread> th;
-    for (size_t k = 1; k < parts; k++) {
-        const size_t off = k * step, len = std::min(step, bytes - off);
-        th.emplace_back([=] { memcpy(static_cast<char *>(dst) + off, static_cast<const char *>(src) + off, len); });
-    }
-    memcpy(dst, src, std::min(step, bytes));
-    for (auto &t : th) t.join();
-}
-
 int build_resident(ssdf_server *s, int id, Resident *r) {
     const HostMeshCopy &h = s->meshes[id];
     ssdf_build_opts bo;
