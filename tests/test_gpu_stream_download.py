@@ -150,9 +150,10 @@ def test_streamed_flat_and_tall_grids(mesh, shape):
     assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
 
 
-def test_streamed_calls_from_two_threads(mesh, grid):
-    """Each calling thread polls its own chunk flags: two threads streaming at once both get their
-    own grid's bits."""
+@pytest.mark.parametrize("page_locked", [True, False])
+def test_streamed_calls_from_two_threads(mesh, grid, page_locked):
+    """Each calling thread polls its own chunk flags and copies through its own staging slots: two
+    threads streaming at once both get their own grid's bits, into page-locked or ordinary arrays."""
     import threading
 
     import torch
@@ -164,7 +165,7 @@ def test_streamed_calls_from_two_threads(mesh, grid):
         w = np.zeros(g.size)
         plain_call("ssdf_b200_sample_sdf_bvh_dd", mesh, g, w, np.float64)
         wants.append(w)
-    outs = [pinned(g.size, torch.float64) for g in grids]
+    outs = [pinned(g.size, torch.float64) if page_locked else np.empty(g.size) for g in grids]
     errors = []
 
     def work(i):
