@@ -80,6 +80,7 @@ struct TreeletWork {
     float old_cost;
     float c[kSubsets];
     unsigned char split[kSubsets];
+    unsigned char subs[40];  // a round's subsets, in increasing order (at most C(7, 3) = 35)
     // the rebuilt arrangement: internal node onode[k] now covers the members of subset oset[k]
     int onode[kTreeletLeaves - 1], oset[kTreeletLeaves - 1];
     int norder;
@@ -137,32 +138,63 @@ __device__ void form_treelet(const TreeArrays &t, int x, TreeletWork &w) {
 }
 
 // The whole warp: the best binary tree over the members, by dynamic programming over the member
-// subsets in rounds of growing size (a round reads only smaller subsets), the lanes sharing each
-// round's subsets. Each subset's split search is the sequential one (same order, same ties).
+// subsets in rounds of growing size (a round reads only smaller subsets). A round's subsets are listed
+// in increasing order and dealt to groups of g lanes (g as large as the count allows: one lane per
+// subset in the crowded rounds, 4 per subset for the 7 subsets of 6 members, all 32 for the full set);
+// the lanes of a group search every g-th split of their subset in the sequential order, and the group
+// keeps the cheapest split, the first in that order among equals -- the sequential search's choice.
 __device__ void treelet_dp(TreeletWork &w, int lane) {
+    constexpr unsigned kAll = 0xffffffffu;
     const int m = w.m, full = (1 << m) - 1;
     for (int s = 1 + lane; s <= full; s += 32)
         if ((s & (s - 1)) == 0) w.c[s] = w.mcost[__ffs(s) - 1], w.split[s] = 0;
     __syncwarp();
     for (int size = 2; size <= m; size++) {
-        for (int s = 1 + lane; s <= full; s += 32) {
-            if (__popc(s) != size) continue;
-            float b[6] = {FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX};
-            for (int k = 0; k < m; k++) {
-                if (!((s >> k) & 1)) continue;
-                for (int q = 0; q < 6; q += 2) b[q] = fminf(b[q], w.mb[k][q]), b[q + 1] = fmaxf(b[q + 1], w.mb[k][q + 1]);
-            }
+        int nsub = 0;
+        for (int base = 1; base <= full; base += 32) {
+            const int s = base + lane;
+            const bool in = s <= full && __popc(s) == size;
+            const unsigned bal = __ballot_sync(kAll, in);
+            if (in) w.subs[nsub + __popc(bal & ((1u << lane) - 1u))] = (unsigned char)s;
+            nsub += __popc(bal);
+        }
+        __syncwarp();
+        int g = 1;
+        while (g * 2 * nsub <= 32) g *= 2;
+        const int r = lane & (g - 1);
+        for (int first = 0; first < nsub; first += 32 / g) {
+            const int j = first + lane / g;
+            const int s = j < nsub ? int(w.subs[j]) : 0;
             float best = FLT_MAX;
-            int bp = 0;
-            // partitions (p, s \ p) with p holding the lowest member of s: each split once
-            const int low = s & -s;
-            for (int p = (s - 1) & s; p > 0; p = (p - 1) & s) {
-                if (!(p & low)) continue;
-                const float v = w.c[p] + w.c[s ^ p];
-                if (v < best) best = v, bp = p;
+            int bp = 0, bk = 0x7fffffff;
+            if (s) {
+                // partitions (p, s \ p) with p holding the lowest member of s: each split once
+                const int low = s & -s;
+                int k = 0;
+                for (int p = (s - 1) & s; p > 0; p = (p - 1) & s) {
+                    if (!(p & low)) continue;
+                    if ((k & (g - 1)) == r) {
+                        const float v = w.c[p] + w.c[s ^ p];
+                        if (v < best) best = v, bp = p, bk = k;
+                    }
+                    k++;
+                }
             }
-            w.c[s] = area6(b) + best;
-            w.split[s] = (unsigned char)bp;
+            for (int o = 1; o < g; o <<= 1) {
+                const float ob = __shfl_xor_sync(kAll, best, o);
+                const int obp = __shfl_xor_sync(kAll, bp, o), obk = __shfl_xor_sync(kAll, bk, o);
+                if (ob < best || (ob == best && obk < bk)) best = ob, bp = obp, bk = obk;
+            }
+            if (s && r == 0) {
+                float b[6] = {FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX, FLT_MAX, -FLT_MAX};
+                for (int k = 0; k < m; k++) {
+                    if (!((s >> k) & 1)) continue;
+                    for (int q = 0; q < 6; q += 2)
+                        b[q] = fminf(b[q], w.mb[k][q]), b[q + 1] = fmaxf(b[q + 1], w.mb[k][q + 1]);
+                }
+                w.c[s] = area6(b) + best;
+                w.split[s] = (unsigned char)bp;
+            }
         }
         __syncwarp();
     }
