@@ -520,15 +520,15 @@ __device__ bool filter_record(double ax, double ay, double az, double bx, double
 }
 
 // The fix-up window's bound term of one filter record (the triangle the float corners describe, or its
-// proxy): the FP32 filter's error at a query p is at most u (8 R + 7.7 alpha L) + min(D, 2 D^2 / d) with
-// D = 90 u alpha R (device_geom.cuh, tri_dist_sq_filter, states the terms it bounds: input rounding,
-// each fmaf, the quotient and reciprocal, the region decisions), u = 2^-24, L the record's longest
-// edge, alpha = L^2 / |ab x ac| and R the largest distance from p to a corner. That is at most u (17 d + (16 + 188 alpha) L) at any distance d (near the record R <= 2L; far
-// from it the D^2 term is below u d); with the input rounding of p and of the corners it stays below
-// u (18.1 d + 2 sqrt(3) M) + u (20 + 188 alpha) L, M the largest coordinate magnitude. This returns the
-// record's term (20 + 188 alpha) L, and false when the record is not safe
-// for the float filter: an edge shorter than 2^-23 (its products underflow), a record that rounding
-// to float made degenerate or needle-like (alpha > 16), or a non-finite value.
+// proxy): the FP32 filter's error at a query p is at most u (8 R + 7.7 alpha L) + min(D, 2 D^2 / d) with D
+// = 90 u alpha R (device_geom.cuh, tri_dist_sq_filter, states the terms it bounds: input rounding, each
+// fmaf, the quotient and reciprocal, the region decisions), u = 2^-24, L the record's longest edge, alpha =
+// L^2 / |ab x ac| and R the largest distance from p to a corner. That is at most u (17 d + (16 + 188 alpha)
+// L) at any distance d (near the record R <= 2L; far from it the D^2 term is below u d); with the input
+// rounding of p and of the corners it stays below u (18.1 d + 2 sqrt(3) M) + u (20 + 188 alpha) L, M the
+// largest coordinate magnitude. This returns the record's term (20 + 188 alpha) L, and false when the
+// record is not safe for the float filter: an edge shorter than 2^-23 (its products underflow), a record
+// that rounding to float made degenerate or needle-like (alpha > 16), or a non-finite value.
 __device__ bool filter_bound(const float4 *__restrict__ rec, float *term) {
     const double e1[3] = {rec[1].x, rec[1].y, rec[1].z}, e2[3] = {rec[2].x, rec[2].y, rec[2].z};
     const double e3[3] = {e2[0] - e1[0], e2[1] - e1[1], e2[2] - e1[2]};
